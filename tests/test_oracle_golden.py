@@ -1,0 +1,223 @@
+"""Pin the CPU oracle against fixtures produced by the reference's own kernels.
+
+The fixtures in tests/golden/ come from running lizhuoh9/MPM-LBM's unmodified
+Taichi kernel bodies under tests/golden/taichi_shim.py (sequential, f32
+storage); see tests/golden/make_fixtures.py.  Tolerances: f32 populations to
+rtol 2e-5 / atol 2e-7 (summation-order rounding only); integer masks and
+link counts bit-exact.
+"""
+
+import json
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as orc
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def load(name):
+    path = os.path.join(GOLD, name + ".npz")
+    if not os.path.exists(path):
+        pytest.skip(f"fixture {name} missing")
+    return np.load(path, allow_pickle=False)
+
+
+def lbm_from(d, nx, ny, nz, dtype=np.float32, **kw):
+    lbm = orc.OracleLBM(nx, ny, nz, dtype=dtype, **kw)
+    return lbm
+
+
+def test_step115_accumulator_known_answer():
+    # tests/test_step115_lbm_open_boundary_and_force_accumulation_contract.py:25-45
+    lbm = orc.OracleLBM(4, 4, 4)
+    lbm.clear_moving_boundary_force_accumulator()
+    lbm.hydro_force[1, 1, 1] = (1.0, 0.0, 0.0)
+    lbm.accumulate_moving_boundary_force_sample()
+    lbm.hydro_force[1, 1, 1] = (3.0, 0.0, 0.0)
+    lbm.accumulate_moving_boundary_force_sample()
+    lbm.finalize_moving_boundary_force_accumulator()
+    st = lbm.get_moving_boundary_accumulation_stats()
+    assert np.allclose(lbm.hydro_force[1, 1, 1], [2.0, 0.0, 0.0], rtol=0.0, atol=1e-6)
+    assert st["mb_subcycle_force_sample_count"] == 2
+    assert abs(st["mb_subcycle_force_accum_norm_max"] - 4.0) <= 1e-6
+    assert abs(st["mb_subcycle_force_mean_norm_max"] - 2.0) <= 1e-6
+
+
+def test_step115_regularized_smoke_bounded():
+    # tests/test_step115_...:99-126
+    lbm = orc.OracleLBM(6, 4, 4, open_boundary_semantics="regularized_velocity_pressure", bc=(2, 1, 0, 0, 0, 0),
+                        vel_bc=((0.02, 0, 0), (0, 0, 0), (0, 0, 0), (0, 0, 0), (0, 0, 0), (0, 0, 0)))
+    lbm.init_simulation()
+    for _ in range(3):
+        lbm.step()
+    st = lbm.get_stats()
+    assert 0.8 < st["rho_min"] < 1.2 and 0.8 < st["rho_max"] < 1.2
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_lbm_kernels_match_reference(dtype):
+    d = load("lbm_kernels")
+    nx, ny, nz = d["F"].shape[:3]
+    lbm = orc.OracleLBM(nx, ny, nz, niu=float(d["niu"]), relaxation_semantics="standard_lattice_kinematic_viscosity",
+                        force=tuple(d["force"]), dtype=dtype)
+    lbm.init_simulation()
+    tol = dict(rtol=2e-5, atol=2e-7) if dtype == np.float32 else dict(rtol=1e-5, atol=1e-7)
+    lbm.F[...] = d["F"]
+    lbm.rho[...] = d["rho"]
+    lbm.v[...] = d["v"]
+    lbm.cell_force[...] = d["cell_force"]
+    lbm.solid[...] = d["solid"]
+    lbm.solid_vel[...] = d["solid_vel"]
+    lbm.f[...] = 0
+    lbm.colission()
+    fluid = d["solid"] == 0
+    np.testing.assert_allclose(lbm.f[fluid], d["collide_f"][fluid], **tol)
+    f_post = lbm.f.copy()
+    lbm.F[...] = d["F"]
+    lbm.streaming1()
+    np.testing.assert_allclose(lbm.F, d["stream_static_F"], **tol)
+    lbm.F[...] = d["F"]
+    lbm.f[...] = f_post
+    lbm.streaming_moving_bounceback()
+    np.testing.assert_allclose(lbm.F, d["stream_moving_F"], **tol)
+    np.testing.assert_allclose(lbm.hydro_force, d["stream_moving_hydro"], rtol=1e-4, atol=1e-6)
+    st = lbm.get_moving_boundary_stats()
+    assert st["bb_link_count"] == int(d["bb_link_count"])
+    dst = lbm.get_moving_boundary_directional_stats()
+    np.testing.assert_array_equal(dst["link_count_by_dir"], d["dir_link_count_by_dir"])
+    np.testing.assert_allclose(dst["solid_force_by_dir"], d["dir_solid_force_by_dir"], rtol=1e-4, atol=1e-6)
+    np.testing.assert_allclose(dst["correction_abs_max_by_dir"], d["dir_correction_abs_max_by_dir"], rtol=1e-5,
+                               atol=1e-9)
+    lbm.streaming3()
+    np.testing.assert_allclose(lbm.rho, d["macros_rho"], **tol)
+    np.testing.assert_allclose(lbm.v, d["macros_v"], rtol=1e-4, atol=1e-7)
+    # dynamic mask + reinit: bit-exact masks
+    lbm.solid[...] = d["solid"]
+    lbm.static_solid[...] = d["mask_static"]
+    lbm.solid_phi[...] = d["mask_phi"]
+    lbm.update_dynamic_solid(0.5)
+    np.testing.assert_array_equal(lbm.solid, d["mask_solid"])
+    np.testing.assert_array_equal(lbm.old_solid, d["mask_old"])
+    np.testing.assert_array_equal(lbm.reinit_flag, d["mask_reinit"])
+    lbm.reinitialize_new_fluid_cells()
+    np.testing.assert_allclose(lbm.F, d["reinit_F"], **tol)
+    np.testing.assert_allclose(lbm.rho, d["reinit_rho"], **tol)
+    np.testing.assert_allclose(lbm.v, d["reinit_v"], **tol)
+
+
+def test_boundaries_match_reference():
+    d = load("lbm_boundaries")
+    nx, ny, nz = d["F"].shape[:3]
+    for name, sem, bl, br, lim in json.loads(str(d["cases"])):
+        lbm = orc.OracleLBM(nx, ny, nz, open_boundary_semantics=sem, bc=(bl, br, 0, 0, 0, 0),
+                            rho_bc=(1.01, 0.99, 1, 1, 1, 1),
+                            vel_bc=((0.04, 0.003, -0.002), (0.03, 0.0, 0.001), (0, 0, 0), (0, 0, 0), (0, 0, 0),
+                                    (0, 0, 0)),
+                            limiter_enabled=lim, ob_u_max=0.035, ob_noneq_cap=0.004, ob_rho_min=0.995,
+                            ob_rho_max=1.005, ob_floor=0.0 if lim else None)
+        lbm.F[...] = d["F"]
+        lbm.rho[...] = d["rho"]
+        lbm.v[...] = d["v"]
+        lbm.solid[...] = d["solid"]
+        lbm.Boundary_condition()
+        np.testing.assert_allclose(lbm.F, d[name + "_F"], rtol=2e-6, atol=1e-8, err_msg=name)
+        if lim:
+            s = lbm.get_open_boundary_limiter_stats()
+            got = [s["rho_clip_count_step"], s["velocity_clip_count_step"], s["noneq_clip_count_step"],
+                   s["population_floor_count_step"], s["reconstructed_population_count_step"]]
+            np.testing.assert_array_equal(got, d[name + "_counts"], err_msg=name)
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_mpm_kernels_match_reference(dtype):
+    d = load("mpm_kernels")
+    n = d["x"].shape[0]
+    ng = int(d["n_grid"])
+    s = orc.OracleMPM(ng, 1.0 / ng, float(d["dt"]), n, gravity=tuple(d["gravity"]), young_modulus=float(d["E"]),
+                      poisson_ratio=float(d["nu"]), p_rho=1.2, dtype=dtype)
+    s.x[...] = d["x"]
+    s.v[...] = d["v"]
+    s.F[...] = d["F"]
+    s.C[...] = d["C"]
+    s.vol0[...] = d["vol0"]
+    s.mass[...] = d["mass"]
+    s.fixed_mask[...] = d["fixed"]
+    s.fixed_x[...] = d["fixed_x"]
+    s.clear_grid()
+    s.p2g()
+    np.testing.assert_allclose(s.grid_m, d["p2g_grid_m"], rtol=1e-5, atol=1e-12)
+    np.testing.assert_allclose(s.grid_v, d["p2g_grid_v"], rtol=2e-4, atol=2e-9)
+    np.testing.assert_allclose(s.Jp, d["p2g_Jp"], rtol=1e-5, atol=1e-6)
+    s.grid_f_ext[...] = d["grid_f_ext"]
+    s.grid_update()
+    np.testing.assert_allclose(s.grid_v, d["update_grid_v"], rtol=2e-4, atol=2e-6)
+    s.g2p()
+    np.testing.assert_allclose(s.x, d["g2p_x"], rtol=1e-6, atol=1e-7)
+    np.testing.assert_allclose(s.v, d["g2p_v"], rtol=2e-4, atol=2e-6)
+    np.testing.assert_allclose(s.C, d["g2p_C"], rtol=2e-3, atol=2e-4)
+    np.testing.assert_allclose(s.F, d["g2p_F"], rtol=1e-5, atol=1e-6)
+    np.testing.assert_allclose(s.Jp, d["g2p_Jp"], rtol=1e-5, atol=1e-6)
+
+
+def test_coupling_kernels_match_reference():
+    d = load("coupling_kernels")
+    ng = int(d["n_grid"])
+    lbm = orc.OracleLBM(ng, ng, ng)
+    n = d["x"].shape[0]
+    s = orc.OracleMPM(ng, float(d["dx_norm"]), 4e-4, n)
+    s.x[...] = d["x"]
+    s.v[...] = d["v"]
+    s.Jp[...] = d["Jp"]
+    s.vol0[...] = d["vol0"]
+    s.mass[...] = d["mass"]
+    cpl = orc.OracleCoupling(ng, float(d["dx_norm"]), float(d["lbm_dt_phys"]), beta_lbm=0.05,
+                             penalty_force_cap=2.0e-4, mb_force_cap_norm=2.0e-5)
+    cpl.project(s, lbm)
+    np.testing.assert_allclose(lbm.solid_phi, d["proj_phi"], rtol=1e-5, atol=1e-7)
+    np.testing.assert_allclose(lbm.solid_mass, d["proj_mass"], rtol=1e-5, atol=1e-12)
+    np.testing.assert_allclose(lbm.solid_vel, d["proj_vel"], rtol=1e-4, atol=1e-9)
+    ps = d["proj_stats"]
+    st = cpl.stats
+    assert st.active_cell_count == int(ps[4])
+    assert abs(st.projected_mass - ps[0]) <= 1e-5 * abs(ps[0])
+    lbm.rho[...] = d["pen_rho"]
+    lbm.v[...] = d["pen_v"]
+    lbm.solid[...] = d["pen_solid"]
+    cpl.build_penalty_force(lbm)
+    np.testing.assert_allclose(lbm.cell_force, d["pen_cell_force"], rtol=1e-5, atol=1e-12)
+    np.testing.assert_allclose(lbm.hydro_force, d["pen_hydro"], rtol=1e-5, atol=1e-12)
+    assert cpl.stats.active_force_cell_count == int(d["pen_stats"][0])
+    lbm.hydro_force[...] = d["react_hydro"]
+    s.clear_grid()
+    cpl.reaction(0, s, lbm)
+    np.testing.assert_allclose(s.grid_f_ext, d["react_pen_gfe"], rtol=1e-4, atol=1e-10)
+    s.clear_grid()
+    cpl.reaction(1, s, lbm)
+    np.testing.assert_allclose(s.grid_f_ext, d["react_mb_gfe"], rtol=1e-4, atol=1e-10)
+    assert cpl.stats.active_reaction_particle_count == int(d["react_mb_stats"][0])
+
+
+def test_polar_rotation_properties():
+    rng = np.random.default_rng(7)
+    import ctypes
+
+    L = orc.lib()
+    for trial in range(200):
+        F = np.eye(3) + 0.4 * rng.standard_normal((3, 3))
+        if trial == 0:
+            F = np.diag([1.1, -0.9, 1.0])
+        R = np.zeros(9)
+        L.orc_polar_rotation(F.ctypes.data_as(ctypes.c_void_p), R.ctypes.data_as(ctypes.c_void_p))
+        R = R.reshape(3, 3)
+        np.testing.assert_allclose(R @ R.T, np.eye(3), atol=1e-12)
+        assert abs(np.linalg.det(R) - 1.0) < 1e-12
+        u, sv, vt = np.linalg.svd(F)
+        v = vt.T
+        if np.linalg.det(u) < 0:
+            u[:, 2] *= -1
+        if np.linalg.det(v) < 0:
+            v[:, 2] *= -1
+        np.testing.assert_allclose(R, u @ v.T, atol=1e-9)
