@@ -1,0 +1,254 @@
+/*
+ * fsi_b200.h -- C ABI of the B200 coupled MPM-LBM FSI step.
+ *
+ * The reference (lizhuoh9/MPM-LBM) has no native boundary: its hot path is a
+ * set of Taichi kernels called from Python (src/mpm_lbm/sim/drivers/
+ * fsi_driver.py:425-575).  Each entry point below replaces one or more of those
+ * kernel calls; the Python package mpm_lbm_b200 binds them with ctypes behind
+ * the reference's FSIDriver3D / LBMFluid3D / MPMSolid3D / coupler API.
+ *
+ * Conventions
+ *  - Every pointer inside the structs is a DEVICE pointer owned by the caller
+ *    (torch tensors); no entry point allocates or frees memory.
+ *  - Calls are asynchronous and ordered on the given cudaStream_t (passed as
+ *    void*, NULL = legacy default stream).  Return 0 on success or a negative
+ *    FSI_E_* code; fsi_last_error() returns the message of the last failure
+ *    on the calling thread.
+ *  - Cell fields use the lattice layout: cell = (k * ny + j) * nx + i (x
+ *    fastest); vector fields are planar: comp c of cell at [c * pitch + cell].
+ *  - Populations use the in-place AA pattern: the layout of `pop` alternates
+ *    with FsiStepCtl.parity (0: every cell holds its own populations; 1: each
+ *    fluid-fluid link's pair of slots is swapped).  fsi_lbm_readout decodes it.
+ */
+#ifndef FSI_B200_H
+#define FSI_B200_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FSI_ABI_VERSION 1
+
+enum {
+  FSI_OK = 0,
+  FSI_E_INVALID = -1,   /* bad argument or unsupported configuration */
+  FSI_E_CUDA = -2,      /* a CUDA launch or runtime call failed */
+  FSI_E_DEVICE = -3,    /* the device reported an error status */
+};
+
+/* cell flag bits */
+enum {
+  FSI_CELL_SOLID = 1,     /* solid (static or dynamic) */
+  FSI_CELL_NEAR = 2,      /* fluid cell with a solid neighbour; FsiLbmState.nbr valid */
+  FSI_CELL_LINK = 4,      /* solid cell with a fluid neighbour (receives link forces) */
+  FSI_CELL_OVERRIDE = 8,  /* collide with the stored rho/vel instead of recomputing them */
+  FSI_CELL_CF = 16,       /* cell_force / hydro hold a non-zero penalty force */
+};
+
+/* open-boundary semantics (src/mpm_lbm/sim/lbm/fluid.py:16-19) */
+enum {
+  FSI_OB_EQUILIBRIUM_RESET = 0,
+  FSI_OB_REGULARIZED = 1,
+  FSI_OB_REGULARIZED_LIMITED = 2,
+  FSI_OB_CONVECTIVE = 3,
+};
+
+/* step mode bits */
+enum {
+  FSI_MODE_MOVING_BB = 1,  /* streaming_moving_bounceback (fluid.py:488) instead of streaming1 (431) */
+  FSI_MODE_SUBCYCLED = 2,  /* link forces feed the subcycle accumulator (fluid.py:460-486) */
+  FSI_MODE_DIRSTATS = 4,   /* produce the per-direction bounce-back reductions this step */
+  FSI_MODE_PENALTY = 8,    /* build the penalty force in the step (coupling/penalty.py:59-88) */
+};
+
+/* device-resident reductions; zeroed by the caller where noted */
+typedef struct FsiLbmDiag {
+  int32_t link_count[19];            /* bb_link_count_by_dir */
+  float corr_abs_sum[19];            /* bb_correction_abs_sum_by_dir */
+  float corr_abs_max[19];            /* bb_correction_abs_max_by_dir (non-negative, max via int bits) */
+  float fluid_impulse[19][3];        /* bb_fluid_impulse_by_dir (solid force = -this) */
+  float accum_norm_max;              /* mb_subcycle_force_accum_norm_max */
+  float mean_norm_max;               /* mb_subcycle_force_mean_norm_max */
+  int32_t ob_step[5];                /* rho, velocity, noneq, floor, reconstructed counts of the last BC */
+  int32_t ob_run[5];                 /* cumulative */
+  int32_t penalty_active;            /* active_force_cell_count */
+  float penalty_max_norm;            /* max_cell_force_norm == max_hydro_force_norm */
+  float penalty_net[3];              /* net_cell_force (net hydro = -this) */
+  int32_t change_count;              /* cells whose solid bit flipped in the last mask rebuild */
+  int32_t status;                    /* non-zero: device-side error code */
+  int32_t pad[2];
+} FsiLbmDiag;
+
+typedef struct FsiLbmState {
+  int32_t nx, ny, nz;
+  int32_t store_fp16;       /* 0: float populations; 1: half (f/w - rho0) */
+  int64_t pitch;            /* >= nx*ny*nz, multiple of 32 */
+  void* pop;                /* [19][pitch] float or __half */
+  uint8_t* flags;           /* [pitch] FSI_CELL_* */
+  uint32_t* nbr;            /* [pitch] bit s: cell + e_s is solid (valid with FSI_CELL_NEAR) */
+  float* rho;               /* [pitch] stored density (override cells, readout) */
+  float* vel;               /* [3][pitch] stored velocity */
+  uint8_t* static_solid;    /* [pitch] */
+  uint8_t* old_solid;       /* [pitch] */
+  uint8_t* reinit_flag;     /* [pitch] */
+  float* phi;               /* [pitch] solid_phi */
+  float* smass;             /* [pitch] solid_mass */
+  float* svel;              /* [3][pitch] solid_vel (lattice units) */
+  float* cell_force;        /* [3][pitch] */
+  float* hydro;             /* [3][pitch] hydro_force (penalty / subcycled mean) */
+  float* hpp;               /* [2][3][pitch] per-step link forces, ping-pong */
+  float* accum;             /* [3][pitch] hydro_force_accum */
+  float* plane;             /* [4][4][ny*nz] rho,ux,uy,uz of x = 0, 1, nx-2, nx-1 of the last step */
+  int32_t* change_list;     /* [pitch] scratch for the mask rebuild */
+  FsiLbmDiag* diag;         /* device */
+} FsiLbmState;
+
+typedef struct FsiLbmParams {
+  float rho0;
+  float force[3];           /* set_force (fluid.py:2025) */
+  float s_v, s_o;           /* MRT rates (fluid.py:301-302); s_o == s_v gives the BGK form */
+  int32_t bc_left, bc_right;   /* 0 periodic, 1 pressure, 2 velocity (x faces) */
+  int32_t ob_semantics;     /* FSI_OB_* */
+  int32_t limiter, floor_enabled;
+  float rho_bc_left, rho_bc_right;
+  float vel_bc_left[3], vel_bc_right[3];
+  float ob_rho_min, ob_rho_max, ob_u_max, ob_noneq_cap, ob_floor;
+  float penalty_beta, penalty_phi_min, penalty_cap;
+  int32_t pad;
+} FsiLbmParams;
+
+typedef struct FsiStepCtl {
+  int32_t parity;       /* AA layout parity of the input state */
+  int32_t bc_pending;   /* 1: the open-boundary step of the previous step is still to be applied */
+  int32_t pp;           /* ping-pong slot of hpp written by this step */
+  int32_t mode;         /* FSI_MODE_* */
+} FsiStepCtl;
+
+/* ---- LBM (replaces LBMFluid3D kernels) ---------------------------------- */
+
+/* init (fluid.py:328-344): populations feq(rho0, 0), rho = rho0, vel = 0,
+ * flags = solid bits of static_solid | OVERRIDE, old_solid = static_solid,
+ * neighbour masks rebuilt.  Layout parity 0. */
+int fsi_lbm_init_equilibrium(const FsiLbmState* s, const FsiLbmParams* p, void* stream);
+
+/* Rebuild neighbour masks and NEAR/LINK flags from the solid bits (init_geo,
+ * fluid.py:347-353 + copy_solid_to_static 1841). Requires parity 0. */
+int fsi_lbm_set_solid(const FsiLbmState* s, const uint8_t* solid, void* stream);
+
+/* Convert a parity-1 state to parity 0 (pure data movement). */
+int fsi_lbm_to_natural(const FsiLbmState* s, void* stream);
+
+/* One fused LBM step: pending open boundary of the previous step
+ * (Boundary_condition, fluid.py:538-569) -> macroscopic update (streaming3,
+ * 1794-1814) -> optional penalty force (coupling/penalty.py:59-88) -> MRT
+ * collision (398-413) -> AA streaming with static or moving half-way
+ * bounce-back and momentum-exchange link forces (431-440 / 488-536). */
+int fsi_lbm_substep(const FsiLbmState* s, const FsiLbmParams* p, const FsiStepCtl* ctl, void* stream);
+
+/* Apply a pending open-boundary step into the state (so that a mask rebuild
+ * sees the same populations as the reference). */
+int fsi_lbm_flush_bc(const FsiLbmState* s, const FsiLbmParams* p, const FsiStepCtl* ctl, void* stream);
+
+/* update_dynamic_solid + reinitialize_new_fluid_cells (fluid.py:1847-1877),
+ * including the AA re-pairing of links whose fluid/solid status changed. */
+int fsi_mask_rebuild(const FsiLbmState* s, const FsiLbmParams* p, const FsiStepCtl* ctl, float threshold,
+                     void* stream);
+
+/* finalize_moving_boundary_force_accumulator (fluid.py:475-486): folds the
+ * last substep, hydro = accum / sample_count. */
+int fsi_force_accum_finalize(const FsiLbmState* s, const FsiStepCtl* ctl, int32_t sample_count, void* stream);
+
+/* Decode the public fields: F (== f) [19][pitch], rho [pitch], vel [3][pitch]
+ * with any pending open boundary applied (read-only on the state). */
+int fsi_lbm_readout(const FsiLbmState* s, const FsiLbmParams* p, const FsiStepCtl* ctl, float* out_pop,
+                    float* out_rho, float* out_vel, void* stream);
+
+/* ---- particles, projection, reaction transfer, MPM ---------------------- */
+
+typedef struct FsiParticles {
+  int32_t n;
+  int32_t pad;
+  float* x;          /* [3][n] */
+  float* v;          /* [3][n] */
+  float* C;          /* [9][n] row-major components */
+  float* F;          /* [9][n] */
+  float* Jp;         /* [n] */
+  float* mass;       /* [n] */
+  float* vol0;       /* [n] */
+  uint8_t* fixed;    /* [n] */
+  float* fixed_x;    /* [3][n] */
+} FsiParticles;
+
+typedef struct FsiGrid {
+  int32_t n;         /* MPM grid edge (n^3 nodes, node = (k * n + j) * n + i) */
+  int32_t pad;
+  float* v;          /* [3][n^3] grid_v (momentum during P2G) */
+  float* m;          /* [n^3] */
+  float* f_ext;      /* [3][n^3] */
+} FsiGrid;
+
+typedef struct FsiMpmParams {
+  float dx, inv_dx, dt, mu, la;
+  float gravity[3];
+  float damping;     /* >0 enables particle_velocity_post_g2p damping */
+  int32_t bound;
+  int32_t lock_z;
+  int32_t pad;
+} FsiMpmParams;
+
+typedef struct FsiCouplingParams {
+  float inv_dx_norm, cell_volume_norm, vel_scale, eps_mass;
+  float phi_min, force_cap, reaction_scale, force_density_scale;
+  int32_t kind;           /* 0 penalty, 1 engineering, 2 link-area */
+  int32_t area_policy;    /* link-area: 0 uniform, 1 inverse_length, 2 length */
+  float area_scale_min, area_scale_max;
+} FsiCouplingParams;
+
+/* f64 reductions of the coupling step */
+typedef struct FsiCouplingStats {
+  double projected_mass, projected_volume_raw, projected_volume_clamped;
+  float max_phi_raw;
+  int32_t active_cell_count;
+  int32_t active_reaction_particle_count;
+  float max_particle_reaction_norm;
+  float max_grid_reaction_norm;
+  float area_scale, raw_area_scale;
+  int32_t pad;
+  double net_particle_reaction[3];
+  double net_grid_reaction[3];
+} FsiCouplingStats;
+
+/* MPMToLBMProjector3D.project (coupling/projection.py:21-97): clear, P2G of
+ * phi/mass/momentum onto the lattice, normalise + clamp.  stats: device. */
+int fsi_project(const FsiLbmState* s, const FsiParticles* pt, const FsiCouplingParams* cp, FsiCouplingStats* stats,
+                void* stream);
+
+/* Reaction transfer LBM -> MPM grid: penalty (coupling/penalty.py:90-129),
+ * engineering (moving_boundary.py:58-110) or link-area (link_area.py:84-193,
+ * area scale computed on the device from the last directional reductions).
+ * hydro: the hydro-force field to sample ([3][pitch]). */
+int fsi_reaction_to_grid(const FsiLbmState* s, const float* hydro, const FsiParticles* pt, const FsiGrid* g,
+                         const FsiCouplingParams* cp, FsiCouplingStats* stats, void* stream);
+
+/* MPMSolid3D.p2g (mpm/solid.py:219-249): fixed-corotated stress with the
+ * polar rotation computed in FP64; grid must be cleared by the caller. */
+int fsi_mpm_p2g(const FsiParticles* pt, const FsiGrid* g, const FsiMpmParams* mp, void* stream);
+
+/* MPMSolid3D.grid_update (mpm/solid.py:251-259, boundary 97-111). */
+int fsi_mpm_grid_update(const FsiGrid* g, const FsiMpmParams* mp, void* stream);
+
+/* MPMSolid3D.g2p (mpm/solid.py:261-315): APIC gather, advection, clamp,
+ * F update, damping / z-lock controls, fixed-base reset. */
+int fsi_mpm_g2p(const FsiParticles* pt, const FsiGrid* g, const FsiMpmParams* mp, void* stream);
+
+/* ---- misc --------------------------------------------------------------- */
+int fsi_abi_version(void);
+int fsi_last_error(char* buf, size_t len);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FSI_B200_H */

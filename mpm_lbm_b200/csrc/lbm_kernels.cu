@@ -1,0 +1,1050 @@
+// LBM kernels of the coupled FSI step (D3Q19 MRT, AA-pattern, SoA).
+//
+// Reference semantics (src/mpm_lbm/sim/lbm/fluid.py):
+//   step_moving_bounceback 2105-2111 = clear diag 443 -> colission 398 ->
+//   streaming_moving_bounceback 488 -> finalize diag 521 -> Boundary_condition
+//   538 -> streaming3 1794.
+// One launch of k_lbm_step performs, per cell, the previous step's open
+// boundary (pending) and macroscopic update, then this step's collision and
+// streaming, so a step costs one read and one write of the 19 populations.
+//
+// Thread layout: blockDim = (32, 8); a warp covers 32 consecutive x cells of
+// one (j, k) row, so the x-face open boundaries (which read the populations of
+// x = 1, nx-2, nx-3 of the same row) resolve with warp shuffles.
+
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <cmath>
+
+#include "common.cuh"
+#include "d3q19.cuh"
+
+namespace fsi {
+
+constexpr uint8_t kSolid = FSI_CELL_SOLID, kNear = FSI_CELL_NEAR, kLink = FSI_CELL_LINK,
+                  kOverride = FSI_CELL_OVERRIDE, kCF = FSI_CELL_CF;
+
+// unknown populations of the x faces (fluid.py:26-27): {1,7,9,11,13} / {2,8,10,12,14}
+__host__ __device__ constexpr int kUnknownL(int q) { return q == 0 ? 1 : 2 * q + 5; }
+__host__ __device__ constexpr int kUnknownR(int q) { return kUnknownL(q) + 1; }
+
+struct Case {
+  FsiLbmState s;
+  FsiLbmParams p;
+  FsiStepCtl c;
+  MrtK K;
+};
+
+// ------------------------------------------------------------ storage ----
+template <bool H>
+struct Pop;
+
+template <>
+struct Pop<false> {
+  static __device__ __forceinline__ float ld(const Case& c, int s, int64_t cell) {
+    return __ldg(static_cast<const float*>(c.s.pop) + (int64_t)s * c.s.pitch + cell);
+  }
+  static __device__ __forceinline__ float ld_rw(const Case& c, int s, int64_t cell) {
+    return static_cast<const float*>(c.s.pop)[(int64_t)s * c.s.pitch + cell];
+  }
+  static __device__ __forceinline__ void st(const Case& c, int s, int64_t cell, float v) {
+    static_cast<float*>(c.s.pop)[(int64_t)s * c.s.pitch + cell] = v;
+  }
+};
+
+// half storage of the scaled deviation from rest equilibrium: h = f / w - rho0
+template <>
+struct Pop<true> {
+  static __device__ __forceinline__ float ld(const Case& c, int s, int64_t cell) {
+    const __half h = static_cast<const __half*>(c.s.pop)[(int64_t)s * c.s.pitch + cell];
+    return lattice_w(s) * (c.p.rho0 + __half2float(h));
+  }
+  static __device__ __forceinline__ float ld_rw(const Case& c, int s, int64_t cell) { return ld(c, s, cell); }
+  static __device__ __forceinline__ void st(const Case& c, int s, int64_t cell, float v) {
+    const float inv_w = s == 0 ? 3.0f : (s <= 6 ? 18.0f : 36.0f);
+    static_cast<__half*>(c.s.pop)[(int64_t)s * c.s.pitch + cell] = __float2half_rn(v * inv_w - c.p.rho0);
+  }
+};
+
+struct Coord {
+  int x, j, k;
+};
+
+__device__ __forceinline__ int wrapi(int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); }
+
+__device__ __forceinline__ int64_t cell_of(const Case& c, int x, int j, int k) {
+  return ((int64_t)k * c.s.ny + j) * c.s.nx + x;
+}
+
+__device__ __forceinline__ int64_t nb_cell(const Case& c, const Coord& q, int dx, int dy, int dz) {
+  return cell_of(c, wrapi(q.x + dx, c.s.nx), wrapi(q.j + dy, c.s.ny), wrapi(q.k + dz, c.s.nz));
+}
+
+// Location of population s of fluid cell q in the current AA layout.
+__device__ __forceinline__ void pop_slot(const Case& c, const Coord& q, int64_t cell, uint8_t fl, uint32_t nb, int s,
+                                         int& slot_s, int64_t& slot_cell) {
+  if (c.c.parity == 0 || s == 0 || (fl & kSolid)) {
+    slot_s = s;
+    slot_cell = cell;
+    return;
+  }
+  const bool src_solid = (fl & kNear) && ((nb >> kOpp(s)) & 1u);
+  if (src_solid) {
+    slot_s = s;
+    slot_cell = cell;
+  } else {
+    slot_s = kOpp(s);
+    slot_cell = nb_cell(c, q, -kEx(s), -kEy(s), -kEz(s));
+  }
+}
+
+template <bool H>
+__device__ __forceinline__ float decode_pop(const Case& c, const Coord& q, int s) {
+  const int64_t cell = cell_of(c, q.x, q.j, q.k);
+  const uint8_t fl = c.s.flags[cell];
+  const uint32_t nb = (fl & kNear) ? c.s.nbr[cell] : 0u;
+  int ss;
+  int64_t sc;
+  pop_slot(c, q, cell, fl, nb, s, ss, sc);
+  return Pop<H>::ld_rw(c, ss, sc);
+}
+
+// ------------------------------------------------------- open boundary ----
+struct FaceIn {
+  float Fni[5];      // populations of ni in the unknown directions
+  float Fn2[5];      // populations of n2i (convective outlet)
+  bool n1_solid;     // solid[1] (left face) / solid[nx-2] (right face)
+  bool n2_fluid;     // solid[n2i] == 0
+  float mac_n[4];    // rho, ux, uy, uz of ni from the previous macroscopic update
+  float mac_leg[4];  // legacy pressure face: v[1] or v[0] (left), v[nx-2] (right)
+};
+
+// fluid.py:1059-1096 (limited) and 1026-1029 (plain) for one unknown population
+__device__ __forceinline__ float regularized_pop(const FsiLbmParams& p, bool limited, int s, float trho, float tu0,
+                                                 float tu1, float tu2, float Fn, const float* mac, int* cnt) {
+  float rl = trho, u0 = tu0, u1 = tu1, u2 = tu2;
+  if (limited && p.limiter) {
+    cnt[4] += 1;
+    if (rl < p.ob_rho_min) {
+      rl = p.ob_rho_min;
+      cnt[0] += 1;
+    }
+    if (rl > p.ob_rho_max) {
+      rl = p.ob_rho_max;
+      cnt[0] += 1;
+    }
+    const float nrm = sqrtf(u0 * u0 + u1 * u1 + u2 * u2);
+    if (nrm > p.ob_u_max) {
+      const float sc = p.ob_u_max / nrm;
+      u0 *= sc;
+      u1 *= sc;
+      u2 *= sc;
+      cnt[1] += 1;
+    }
+  }
+  float noneq = Fn - feq(s, mac[0], mac[1], mac[2], mac[3]);
+  if (limited && p.limiter) {
+    if (noneq > p.ob_noneq_cap) {
+      noneq = p.ob_noneq_cap;
+      cnt[2] += 1;
+    }
+    if (noneq < -p.ob_noneq_cap) {
+      noneq = -p.ob_noneq_cap;
+      cnt[2] += 1;
+    }
+  }
+  float out = feq(s, rl, u0, u1, u2) + noneq;
+  if (limited && p.limiter && p.floor_enabled && out < p.ob_floor) {
+    out = p.ob_floor;
+    cnt[3] += 1;
+  }
+  return out;
+}
+
+// Boundary_condition for one fluid face cell (fluid.py:926-1024, 1348-1493).
+__device__ void apply_face_bc(const FsiLbmParams& p, int side, const FaceIn& in, float* F, int* cnt) {
+  const int bc = side == 0 ? p.bc_left : p.bc_right;
+  
+  if (p.ob_semantics == FSI_OB_EQUILIBRIUM_RESET) {
+    if (bc == 2) {
+      const float* vb = side == 0 ? p.vel_bc_left : p.vel_bc_right;
+#pragma unroll
+      for (int s = 0; s < 19; ++s) F[s] = feq(s, 1.0f, vb[0], vb[1], vb[2]);
+    } else if (bc == 1) {
+      const float rb = side == 0 ? p.rho_bc_left : p.rho_bc_right;
+#pragma unroll
+      for (int s = 0; s < 19; ++s) F[s] = feq(s, rb, in.mac_leg[1], in.mac_leg[2], in.mac_leg[3]);
+    }
+    return;
+  }
+  if (p.ob_semantics == FSI_OB_CONVECTIVE && side == 1 && bc == 1) {
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+      float ex = in.Fni[q];
+      if (in.n2_fluid) ex = 2.0f * in.Fni[q] - in.Fn2[q];
+      if (p.limiter && p.floor_enabled && ex < p.ob_floor) ex = p.ob_floor;
+      F[(side == 0 ? kUnknownL(q) : kUnknownR(q))] = ex;
+    }
+    return;
+  }
+  const bool limited = p.ob_semantics == FSI_OB_REGULARIZED_LIMITED;
+  float trho, t0, t1, t2;
+  if (bc == 1) {
+    trho = side == 0 ? p.rho_bc_left : p.rho_bc_right;
+    t0 = in.mac_n[1];
+    t1 = in.mac_n[2];
+    t2 = in.mac_n[3];
+  } else {
+    trho = in.mac_n[0];
+    if (trho <= 1.0e-6f) trho = p.rho0;
+    const float* vb = side == 0 ? p.vel_bc_left : p.vel_bc_right;
+    t0 = vb[0];
+    t1 = vb[1];
+    t2 = vb[2];
+  }
+#pragma unroll
+  for (int q = 0; q < 5; ++q) F[(side == 0 ? kUnknownL(q) : kUnknownR(q))] = regularized_pop(p, limited, (side == 0 ? kUnknownL(q) : kUnknownR(q)), trho, t0, t1, t2, in.Fni[q], in.mac_n, cnt);
+}
+
+__device__ __forceinline__ const float* plane_ptr(const Case& c, int plane) {
+  return c.s.plane + (int64_t)plane * 4 * c.s.ny * c.s.nz;
+}
+
+__device__ __forceinline__ void load_plane(const Case& c, int plane, int row, float* m) {
+  const float* pp = plane_ptr(c, plane);
+  const int64_t n = (int64_t)c.s.ny * c.s.nz;
+#pragma unroll
+  for (int a = 0; a < 4; ++a) m[a] = pp[a * n + row];
+}
+
+__device__ __forceinline__ void flush_counts(const Case& c, const int* cnt) {
+#pragma unroll
+  for (int a = 0; a < 5; ++a) {
+    int v = cnt[a];
+    v += __shfl_xor_sync(0xffffffffu, v, 16);
+    v += __shfl_xor_sync(0xffffffffu, v, 8);
+    v += __shfl_xor_sync(0xffffffffu, v, 4);
+    v += __shfl_xor_sync(0xffffffffu, v, 2);
+    v += __shfl_xor_sync(0xffffffffu, v, 1);
+    if ((threadIdx.x & 31) == 0 && v) {
+      atomicAdd(&c.s.diag->ob_step[a], v);
+      atomicAdd(&c.s.diag->ob_run[a], v);
+    }
+  }
+}
+
+// --------------------------------------------------------- step kernel ----
+struct DirAcc {
+  int cnt[19];
+  float csum[19];
+  float cmax[19];
+  float imp[19][3];
+  int any;
+};
+
+template <bool ODD, bool H>
+__global__ void __launch_bounds__(256) k_lbm_step(const Case c) {
+  __shared__ DirAcc acc;
+  const int lane = threadIdx.x;
+  const int tid = threadIdx.y * 32 + lane;
+  const int nx = c.s.nx, ny = c.s.ny, nz = c.s.nz;
+  const int x = blockIdx.x * 32 + lane;
+  const int row = blockIdx.y * blockDim.y + threadIdx.y;
+  const bool inrow = row < ny * nz;
+  const bool valid = inrow && x < nx;
+  const Coord q{x, inrow ? row % ny : 0, inrow ? row / ny : 0};
+  const int64_t cell = (int64_t)row * nx + x;
+  const int mode = c.c.mode;
+  const bool moving = mode & FSI_MODE_MOVING_BB;
+  const bool dirstats = (mode & FSI_MODE_DIRSTATS) && moving;
+  if (dirstats) {
+    for (int i = tid; i < 19; i += 256) {
+      acc.cnt[i] = 0;
+      acc.csum[i] = 0.f;
+      acc.cmax[i] = 0.f;
+      acc.imp[i][0] = acc.imp[i][1] = acc.imp[i][2] = 0.f;
+    }
+    if (tid == 0) acc.any = 0;
+    __syncthreads();
+  }
+
+  uint8_t fl = valid ? c.s.flags[cell] : kSolid;
+  const bool fluid = !(fl & kSolid);
+  const uint32_t nb = (fluid && (fl & kNear)) ? c.s.nbr[cell] : 0u;
+
+  // ---- load the post-streaming populations of this cell
+  float F[19];
+  if (fluid) {
+#pragma unroll
+    for (int s = 0; s < 19; ++s) {
+      if (!ODD || s == 0) {
+        F[s] = Pop<H>::ld(c, s, cell);
+      } else {
+        const bool src_solid = (nb >> kOpp(s)) & 1u;
+        F[s] = src_solid ? Pop<H>::ld(c, s, cell)
+                         : Pop<H>::ld(c, kOpp(s), nb_cell(c, q, -kEx(s), -kEy(s), -kEz(s)));
+      }
+    }
+  } else {
+#pragma unroll
+    for (int s = 0; s < 19; ++s) F[s] = 0.f;
+  }
+
+  // ---- pending open boundary of the previous step (warp-uniform branches)
+  const bool open_bc = c.p.bc_left != 0 || c.p.bc_right != 0;
+  const int right_block = (nx - 1) >> 5;
+  if (c.c.bc_pending && inrow) {
+    int cnt[5] = {0, 0, 0, 0, 0};
+    const bool warp_left = c.p.bc_left != 0 && blockIdx.x == 0;
+    const bool warp_right = c.p.bc_right != 0 && (int)blockIdx.x == right_block;
+    if (warp_left) {
+      const bool n1_solid = __shfl_sync(0xffffffffu, (int)(fl & kSolid), 1) != 0;
+      const int src = n1_solid ? 0 : 1;
+      FaceIn in;
+#pragma unroll
+      for (int t = 0; t < 5; ++t) in.Fni[t] = __shfl_sync(0xffffffffu, F[kUnknownL(t)], src);
+      if (lane == 0 && fluid) {
+        in.n1_solid = n1_solid;
+        in.n2_fluid = false;
+        load_plane(c, n1_solid ? 0 : 1, row, in.mac_n);
+        load_plane(c, n1_solid ? 1 : 0, row, in.mac_leg);
+        apply_face_bc(c.p, 0, in, F, cnt);
+      }
+    }
+    if (warp_right) {
+      const int l1 = (nx - 2) & 31, l2 = (nx - 3) & 31, lf = (nx - 1) & 31;
+      const bool n1_solid = __shfl_sync(0xffffffffu, (int)(fl & kSolid), l1) != 0;
+      const bool n2s = __shfl_sync(0xffffffffu, (int)(fl & kSolid), l2) != 0;
+      const int src1 = n1_solid ? lf : l1;
+      const int src2 = n1_solid ? lf : l2;
+      FaceIn in;
+#pragma unroll
+      for (int t = 0; t < 5; ++t) {
+        in.Fni[t] = __shfl_sync(0xffffffffu, F[kUnknownR(t)], src1);
+        in.Fn2[t] = __shfl_sync(0xffffffffu, F[kUnknownR(t)], src2);
+      }
+      if (lane == lf && x == nx - 1 && fluid) {
+        in.n1_solid = n1_solid;
+        in.n2_fluid = n1_solid ? true : !n2s;
+        load_plane(c, n1_solid ? 3 : 2, row, in.mac_n);
+        load_plane(c, 2, row, in.mac_leg);
+        apply_face_bc(c.p, 1, in, F, cnt);
+      }
+    }
+    if (c.p.limiter && (warp_left || warp_right)) flush_counts(c, cnt);
+  }
+
+  // ---- macroscopic state the collision uses (streaming3 of the previous step)
+  float rho = c.p.rho0, ux = 0.f, uy = 0.f, uz = 0.f;
+  float cfp[3] = {0.f, 0.f, 0.f};
+  if (fluid) {
+    if (fl & kCF) {
+#pragma unroll
+      for (int a = 0; a < 3; ++a) cfp[a] = c.s.cell_force[(int64_t)a * c.s.pitch + cell];
+    }
+    if (fl & kOverride) {
+      rho = c.s.rho[cell];
+      ux = c.s.vel[cell];
+      uy = c.s.vel[c.s.pitch + cell];
+      uz = c.s.vel[2 * c.s.pitch + cell];
+    } else {
+      float jx, jy, jz;
+      moments0(F, rho, jx, jy, jz);
+      const float inv = 1.0f / rho;
+      ux = jx * inv + (0.5f * (c.p.force[0] + cfp[0])) * inv;
+      uy = jy * inv + (0.5f * (c.p.force[1] + cfp[1])) * inv;
+      uz = jz * inv + (0.5f * (c.p.force[2] + cfp[2])) * inv;
+    }
+  }
+  // store the macroscopic state of the planes the next open boundary reads
+  if (open_bc) {
+    __syncwarp();
+    int plane = -1;
+    if (x == 0) plane = 0;
+    else if (x == 1) plane = 1;
+    else if (x == nx - 2) plane = 2;
+    else if (x == nx - 1) plane = 3;
+    if (valid && plane >= 0) {
+      float* pp = c.s.plane + (int64_t)plane * 4 * ny * nz;
+      const int64_t n = (int64_t)ny * nz;
+      pp[row] = rho;
+      pp[n + row] = ux;
+      pp[2 * n + row] = uy;
+      pp[3 * n + row] = uz;
+    }
+  }
+
+  // ---- penalty force (coupling/penalty.py:59-88), built from this state
+  float Ax = c.p.force[0], Ay = c.p.force[1], Az = c.p.force[2];
+  uint8_t nfl = fl & (uint8_t)~kOverride;
+  if (mode & FSI_MODE_PENALTY) {
+    float f0 = 0.f, f1 = 0.f, f2 = 0.f;
+    bool active = false;
+    if (fluid) {
+      const float phi = c.s.phi[cell];
+      if (phi > c.p.penalty_phi_min) {
+        const float sc = c.p.penalty_beta * phi * rho;
+        f0 = sc * (c.s.svel[cell] - ux);
+        f1 = sc * (c.s.svel[c.s.pitch + cell] - uy);
+        f2 = sc * (c.s.svel[2 * c.s.pitch + cell] - uz);
+        const float nrm = sqrtf(f0 * f0 + f1 * f1 + f2 * f2);
+        if (nrm > c.p.penalty_cap) {
+          const float r = c.p.penalty_cap / nrm;
+          f0 *= r;
+          f1 *= r;
+          f2 *= r;
+        }
+        active = true;
+      }
+    }
+    if (active || (valid && (fl & kCF))) {
+      const int64_t P = c.s.pitch;
+      c.s.cell_force[cell] = f0;
+      c.s.cell_force[P + cell] = f1;
+      c.s.cell_force[2 * P + cell] = f2;
+      c.s.hydro[cell] = -f0;
+      c.s.hydro[P + cell] = -f1;
+      c.s.hydro[2 * P + cell] = -f2;
+    }
+    nfl = active ? (nfl | kCF) : (nfl & (uint8_t)~kCF);
+    Ax += f0;
+    Ay += f1;
+    Az += f2;
+    if (__any_sync(0xffffffffu, active)) {
+      const int na = __popc(__ballot_sync(0xffffffffu, active));
+      const float mx = warp_max(sqrtf(f0 * f0 + f1 * f1 + f2 * f2));
+      const float s0 = warp_sum(f0), s1 = warp_sum(f1), s2 = warp_sum(f2);
+      if (lane == 0) {
+        atomicAdd(&c.s.diag->penalty_active, na);
+        atomic_max_nonneg(&c.s.diag->penalty_max_norm, mx);
+        atomicAdd(&c.s.diag->penalty_net[0], s0);
+        atomicAdd(&c.s.diag->penalty_net[1], s1);
+        atomicAdd(&c.s.diag->penalty_net[2], s2);
+      }
+    }
+  } else if (fluid && (fl & kCF)) {
+    // a cell force left by an earlier penalty step keeps acting (fluid.py:393-396)
+    Ax += cfp[0];
+    Ay += cfp[1];
+    Az += cfp[2];
+    nfl = fl & (uint8_t)~kOverride;
+  }
+  if (valid && nfl != fl) c.s.flags[cell] = nfl;
+
+  // ---- collision and streaming
+  float* hpp = c.s.hpp + (int64_t)c.c.pp * 3 * c.s.pitch;
+  if (fluid) {
+    float out[19];
+    mrt_collide(F, rho, ux, uy, uz, Ax, Ay, Az, c.K, out);
+#pragma unroll
+    for (int s = 0; s < 19; ++s) {
+      float val = out[s];
+      const bool bb = (nb >> s) & 1u;  // cell + e_s is solid
+      if (bb && moving) {
+        const int64_t ip = nb_cell(c, q, kEx(s), kEy(s), kEz(s));
+        const int64_t P = c.s.pitch;
+        const float ew = (float)kEx(s) * c.s.svel[ip] + (float)kEy(s) * c.s.svel[P + ip] + (float)kEz(s) * c.s.svel[2 * P + ip];
+        const float corr = -6.0f * lattice_w(s) * rho * ew;
+        const float f0 = val;
+        val = f0 + corr;
+        const float tot = val + f0;  // solid force = e_s (bounced + f)
+        if (kEx(s)) atomicAdd(hpp + ip, (float)kEx(s) * tot);
+        if (kEy(s)) atomicAdd(hpp + P + ip, (float)kEy(s) * tot);
+        if (kEz(s)) atomicAdd(hpp + 2 * P + ip, (float)kEz(s) * tot);
+        if (dirstats) {
+          const float ac = fabsf(corr);
+          atomicAdd(&acc.cnt[s], 1);
+          atomicAdd(&acc.csum[s], ac);
+          atomic_max_nonneg(&acc.cmax[s], ac);
+          if (kEx(s)) atomicAdd(&acc.imp[s][0], -(float)kEx(s) * tot);
+          if (kEy(s)) atomicAdd(&acc.imp[s][1], -(float)kEy(s) * tot);
+          if (kEz(s)) atomicAdd(&acc.imp[s][2], -(float)kEz(s) * tot);
+          acc.any = 1;
+        }
+      }
+      if (!ODD) {
+        Pop<H>::st(c, kOpp(s), cell, val);
+      } else if (s == 0 || bb) {
+        Pop<H>::st(c, kOpp(s), cell, val);
+      } else {
+        Pop<H>::st(c, s, nb_cell(c, q, kEx(s), kEy(s), kEz(s)), val);
+      }
+    }
+  } else if (valid && (fl & kLink) && moving) {
+    // solid cell receiving link forces: recycle last step's ping-pong slot
+    const int64_t P = c.s.pitch;
+    float* prev = c.s.hpp + (int64_t)(c.c.pp ^ 1) * 3 * P;
+    if (mode & FSI_MODE_SUBCYCLED) {
+      float a[3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        a[d] = c.s.accum[d * P + cell] + prev[d * P + cell];
+        c.s.accum[d * P + cell] = a[d];
+        prev[d * P + cell] = 0.f;
+      }
+      atomic_max_nonneg(&c.s.diag->accum_norm_max, sqrtf(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]));
+    } else {
+#pragma unroll
+      for (int d = 0; d < 3; ++d) prev[d * P + cell] = 0.f;
+    }
+  }
+
+  if (dirstats) {
+    __syncthreads();
+    if (acc.any) {
+      for (int i = tid; i < 19; i += 256) {
+        if (acc.cnt[i]) {
+          atomicAdd(&c.s.diag->link_count[i], acc.cnt[i]);
+          atomicAdd(&c.s.diag->corr_abs_sum[i], acc.csum[i]);
+          atomic_max_nonneg(&c.s.diag->corr_abs_max[i], acc.cmax[i]);
+          atomicAdd(&c.s.diag->fluid_impulse[i][0], acc.imp[i][0]);
+          atomicAdd(&c.s.diag->fluid_impulse[i][1], acc.imp[i][1]);
+          atomicAdd(&c.s.diag->fluid_impulse[i][2], acc.imp[i][2]);
+        }
+      }
+    }
+  }
+}
+
+// ------------------------------------------------- init / neighbours ----
+__global__ void k_init(const Case c) {
+  const int64_t n = (int64_t)c.s.nx * c.s.ny * c.s.nz;
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint8_t st = c.s.static_solid[i] ? kSolid : 0;
+  c.s.flags[i] = st | kOverride;
+  c.s.old_solid[i] = st ? 1 : 0;
+  c.s.reinit_flag[i] = 0;
+  c.s.rho[i] = c.p.rho0;
+  for (int a = 0; a < 3; ++a) c.s.vel[(int64_t)a * c.s.pitch + i] = 0.f;
+  for (int s = 0; s < 19; ++s) {
+    const float fe = feq(s, c.p.rho0, 0.f, 0.f, 0.f);
+    if (c.s.store_fp16)
+      Pop<true>::st(c, s, i, fe);
+    else
+      Pop<false>::st(c, s, i, fe);
+  }
+}
+
+__device__ __forceinline__ void neighbour_data(const Case& c, const Coord& q, uint32_t& mask, bool& any_fluid) {
+  mask = 0u;
+  any_fluid = false;
+#pragma unroll
+  for (int s = 1; s < 19; ++s) {
+    const int64_t m = nb_cell(c, q, kEx(s), kEy(s), kEz(s));
+    if (c.s.flags[m] & kSolid)
+      mask |= 1u << s;
+    else
+      any_fluid = true;
+  }
+}
+
+__global__ void k_neighbours_all(const Case c) {
+  const int64_t n = (int64_t)c.s.nx * c.s.ny * c.s.nz;
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const Coord q{(int)(i % c.s.nx), (int)((i / c.s.nx) % c.s.ny), (int)(i / ((int64_t)c.s.nx * c.s.ny))};
+  uint32_t mask;
+  bool anyf;
+  neighbour_data(c, q, mask, anyf);
+  const uint8_t fl = c.s.flags[i];
+  const bool solid = fl & kSolid;
+  uint8_t nfl = fl & (uint8_t)~(kNear | kLink);
+  if (!solid && mask) nfl |= kNear;
+  if (solid && anyf) nfl |= kLink;
+  c.s.flags[i] = nfl;
+  c.s.nbr[i] = mask;
+}
+
+__global__ void k_set_solid(const Case c, const uint8_t* solid) {
+  const int64_t n = (int64_t)c.s.nx * c.s.ny * c.s.nz;
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint8_t s = solid[i] ? 1 : 0;
+  c.s.flags[i] = (c.s.flags[i] & (uint8_t)~kSolid) | (s ? kSolid : 0);
+  c.s.static_solid[i] = s;
+  c.s.old_solid[i] = s;
+}
+
+// parity 1 -> parity 0: swap the two slots of every fluid-fluid link
+template <bool H>
+__global__ void k_to_natural(const Case c) {
+  const int64_t n = (int64_t)c.s.nx * c.s.ny * c.s.nz;
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (c.s.flags[i] & kSolid) return;
+  const Coord q{(int)(i % c.s.nx), (int)((i / c.s.nx) % c.s.ny), (int)(i / ((int64_t)c.s.nx * c.s.ny))};
+#pragma unroll
+  for (int s = 1; s < 19; s += 2) {
+    const int64_t z = nb_cell(c, q, kEx(s), kEy(s), kEz(s));
+    if (c.s.flags[z] & kSolid) continue;
+    const float a = Pop<H>::ld_rw(c, s, z);
+    const float b = Pop<H>::ld_rw(c, kOpp(s), i);
+    Pop<H>::st(c, s, z, b);
+    Pop<H>::st(c, kOpp(s), i, a);
+  }
+}
+
+// ------------------------------------------------------- mask rebuild ----
+// update_dynamic_solid (fluid.py:1847-1861)
+__global__ void k_mask_update(const Case c, float thr) {
+  const int64_t n = (int64_t)c.s.nx * c.s.ny * c.s.nz;
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint8_t fl = c.s.flags[i];
+  const uint8_t prev = (fl & kSolid) ? 1 : 0;
+  c.s.old_solid[i] = prev;
+  const bool dyn = c.s.phi[i] >= thr;
+  const uint8_t nw = (c.s.static_solid[i] != 0 || dyn) ? 1 : 0;
+  c.s.reinit_flag[i] = (prev && !nw) ? 1 : 0;
+  if (nw != prev) {
+    c.s.flags[i] = (fl & (uint8_t)~kSolid) | (nw ? kSolid : 0);
+    const int slot = atomicAdd(&c.s.diag->change_count, 1);
+    c.s.change_list[slot] = (int32_t)i;
+  }
+}
+
+__device__ __forceinline__ void flag_bits(uint8_t* flags, int64_t i, uint8_t set, uint8_t clear) {
+  uintptr_t addr = reinterpret_cast<uintptr_t>(flags + i);
+  unsigned int* word = reinterpret_cast<unsigned int*>(addr & ~(uintptr_t)3);
+  const int sh = (int)(addr & 3) * 8;
+  if (clear) atomicAnd(word, ~((unsigned int)clear << sh));
+  if (set) atomicOr(word, (unsigned int)set << sh);
+}
+
+__device__ __forceinline__ Coord coord_of(const Case& c, int64_t i) {
+  return Coord{(int)(i % c.s.nx), (int)((i / c.s.nx) % c.s.ny), (int)(i / ((int64_t)c.s.nx * c.s.ny))};
+}
+
+__device__ __forceinline__ void reset_velocity(const Case& c, int64_t i, float* u) {
+  // reinitialize_new_fluid_cells (fluid.py:1867-1869)
+  const int64_t P = c.s.pitch;
+  const float a = c.s.svel[i], b = c.s.svel[P + i], d = c.s.svel[2 * P + i];
+  if (sqrtf(a * a + b * b + d * d) > 0.f) {
+    u[0] = a;
+    u[1] = b;
+    u[2] = d;
+  } else {
+    u[0] = u[1] = u[2] = 0.f;
+  }
+}
+
+__device__ __forceinline__ bool is_changed(const Case& c, int64_t i) {
+  return ((c.s.flags[i] & kSolid) ? 1 : 0) != c.s.old_solid[i];
+}
+
+// reinitialize_new_fluid_cells (fluid.py:1863-1877) and AA re-pairing.
+template <bool H>
+__global__ void k_relink(const Case c) {
+  const int count = c.s.diag->change_count;
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < count; idx += gridDim.x * blockDim.x) {
+    const int64_t ci = c.s.change_list[idx];
+    const Coord q = coord_of(c, ci);
+    // neighbour-derived data of ci and its 18 neighbours
+    for (int t = 0; t < 19; ++t) {
+      const int64_t m = t == 0 ? ci : nb_cell(c, q, kEx(t), kEy(t), kEz(t));
+      const Coord qm = coord_of(c, m);
+      uint32_t mask;
+      bool anyf;
+      neighbour_data(c, qm, mask, anyf);
+      const uint8_t fl = c.s.flags[m];
+      const bool solid = fl & kSolid;
+      const uint8_t want = (uint8_t)((!solid && mask) ? kNear : 0) | (uint8_t)((solid && anyf) ? kLink : 0);
+      c.s.nbr[m] = mask;
+      const bool link_now = want & kLink;
+      if (!link_now || !(fl & kLink)) {
+        const int64_t P = c.s.pitch;
+        for (int a = 0; a < 6; ++a) c.s.hpp[(int64_t)a * P + m] = 0.f;
+      }
+      flag_bits(c.s.flags, m, want, (uint8_t)((kNear | kLink) & ~want));
+    }
+    const bool reinit_c = c.s.reinit_flag[ci] != 0;
+    if (c.c.parity == 0 && !reinit_c) continue;
+    for (int s = 1; s < 19; ++s) {
+      const int64_t z = nb_cell(c, q, kEx(s), kEy(s), kEz(s));
+      if (z != ci && is_changed(c, z) && z < ci) continue;  // handled by the other endpoint
+      // canonical orientation: link (y, zz = y + e_sd) with sd odd
+      int64_t y, zz;
+      int sd;
+      if (s & 1) {
+        y = ci;
+        zz = z;
+        sd = s;
+      } else {
+        y = z;
+        zz = ci;
+        sd = kOpp(s);
+      }
+      const bool yf = !(c.s.flags[y] & kSolid), zf = !(c.s.flags[zz] & kSolid);
+      if (c.c.parity == 1) {
+        const bool old_ff = !c.s.old_solid[y] && !c.s.old_solid[zz];
+        const bool new_ff = yf && zf;
+        if (old_ff != new_ff) {
+          const float a = Pop<H>::ld_rw(c, sd, zz);
+          const float b = Pop<H>::ld_rw(c, kOpp(sd), y);
+          Pop<H>::st(c, sd, zz, b);
+          Pop<H>::st(c, kOpp(sd), y, a);
+        }
+      }
+      if (c.s.reinit_flag[zz]) {
+        float u[3];
+        reset_velocity(c, zz, u);
+        const float v = feq(sd, c.p.rho0, u[0], u[1], u[2]);
+        if (c.c.parity == 1 && yf)
+          Pop<H>::st(c, kOpp(sd), y, v);
+        else
+          Pop<H>::st(c, sd, zz, v);
+      }
+      if (c.s.reinit_flag[y]) {
+        float u[3];
+        reset_velocity(c, y, u);
+        const float v = feq(kOpp(sd), c.p.rho0, u[0], u[1], u[2]);
+        if (c.c.parity == 1 && zf)
+          Pop<H>::st(c, sd, zz, v);
+        else
+          Pop<H>::st(c, kOpp(sd), y, v);
+      }
+    }
+    if (reinit_c) {
+      float u[3];
+      reset_velocity(c, ci, u);
+      Pop<H>::st(c, 0, ci, feq(0, c.p.rho0, u[0], u[1], u[2]));
+      c.s.rho[ci] = c.p.rho0;
+      c.s.vel[ci] = u[0];
+      c.s.vel[c.s.pitch + ci] = u[1];
+      c.s.vel[2 * c.s.pitch + ci] = u[2];
+      flag_bits(c.s.flags, ci, kOverride, 0);
+    }
+  }
+}
+
+// reinit flags are consumed only after every link of every changed cell is done
+__global__ void k_clear_reinit(const Case c) {
+  const int count = c.s.diag->change_count;
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < count; idx += gridDim.x * blockDim.x)
+    c.s.reinit_flag[c.s.change_list[idx]] = 0;
+}
+
+// ------------------------------------------------ BC flush and readout ----
+template <bool H>
+__device__ void face_inputs(const Case& c, int side, int j, int k, FaceIn& in, int& face_x) {
+  const int nx = c.s.nx;
+  const int row = k * c.s.ny + j;
+  
+  face_x = side == 0 ? 0 : nx - 1;
+  const int x1 = side == 0 ? 1 : nx - 2;
+  in.n1_solid = c.s.flags[cell_of(c, x1, j, k)] & kSolid;
+  const int ni = in.n1_solid ? face_x : x1;
+  const int n2i = in.n1_solid ? face_x : nx - 3;
+  in.n2_fluid = !(c.s.flags[cell_of(c, n2i, j, k)] & kSolid);
+#pragma unroll
+  for (int t = 0; t < 5; ++t) {
+    in.Fni[t] = decode_pop<H>(c, Coord{ni, j, k}, (side == 0 ? kUnknownL(t) : kUnknownR(t)));
+    in.Fn2[t] = side == 1 ? decode_pop<H>(c, Coord{n2i, j, k}, (side == 0 ? kUnknownL(t) : kUnknownR(t))) : 0.f;
+  }
+  if (side == 0) {
+    load_plane(c, in.n1_solid ? 0 : 1, row, in.mac_n);
+    load_plane(c, in.n1_solid ? 1 : 0, row, in.mac_leg);
+  } else {
+    load_plane(c, in.n1_solid ? 3 : 2, row, in.mac_n);
+    load_plane(c, 2, row, in.mac_leg);
+  }
+}
+
+// applies a pending open-boundary step into the state
+template <bool H>
+__global__ void k_flush_bc(const Case c) {
+  const int nrow = c.s.ny * c.s.nz;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  int cnt[5] = {0, 0, 0, 0, 0};
+  if (t < 2 * nrow) {
+    const int side = t / nrow, row = t % nrow;
+    const int bc = side == 0 ? c.p.bc_left : c.p.bc_right;
+    const int j = row % c.s.ny, k = row / c.s.ny;
+    const int fx = side == 0 ? 0 : c.s.nx - 1;
+    const int64_t cell = cell_of(c, fx, j, k);
+    const uint8_t fl = c.s.flags[cell];
+    if (bc != 0 && !(fl & kSolid)) {
+      FaceIn in;
+      int face_x;
+      face_inputs<H>(c, side, j, k, in, face_x);
+      const Coord q{fx, j, k};
+      const uint32_t nb = (fl & kNear) ? c.s.nbr[cell] : 0u;
+      float F[19];
+      int ss[19];
+      int64_t sc[19];
+#pragma unroll
+      for (int s = 0; s < 19; ++s) {
+        pop_slot(c, q, cell, fl, nb, s, ss[s], sc[s]);
+        F[s] = Pop<H>::ld_rw(c, ss[s], sc[s]);
+      }
+      apply_face_bc(c.p, side, in, F, cnt);
+#pragma unroll
+      for (int s = 0; s < 19; ++s) Pop<H>::st(c, ss[s], sc[s], F[s]);
+    }
+  }
+  if (c.p.limiter) flush_counts(c, cnt);
+}
+
+template <bool H>
+__global__ void k_readout(const Case c, float* out_pop, float* out_rho, float* out_vel) {
+  const int64_t n = (int64_t)c.s.nx * c.s.ny * c.s.nz;
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const Coord q = coord_of(c, i);
+  const uint8_t fl = c.s.flags[i];
+  const uint32_t nb = (fl & kNear) ? c.s.nbr[i] : 0u;
+  float F[19];
+#pragma unroll
+  for (int s = 0; s < 19; ++s) {
+    int ss;
+    int64_t sc;
+    pop_slot(c, q, i, fl, nb, s, ss, sc);
+    F[s] = Pop<H>::ld_rw(c, ss, sc);
+  }
+  const bool fluid = !(fl & kSolid);
+  if (fluid && c.c.bc_pending) {
+    int cnt[5];
+    for (int side = 0; side < 2; ++side) {
+      const int bc = side == 0 ? c.p.bc_left : c.p.bc_right;
+      const int fx = side == 0 ? 0 : c.s.nx - 1;
+      if (bc == 0 || q.x != fx) continue;
+      FaceIn in;
+      int face_x;
+      face_inputs<H>(c, side, q.j, q.k, in, face_x);
+      apply_face_bc(c.p, side, in, F, cnt);
+    }
+  }
+  const int64_t P = c.s.pitch;
+  for (int s = 0; s < 19; ++s) out_pop[(int64_t)s * P + i] = F[s];
+  float rho = c.p.rho0, u[3] = {0.f, 0.f, 0.f};
+  if (fluid) {
+    if (fl & kOverride) {
+      rho = c.s.rho[i];
+      for (int a = 0; a < 3; ++a) u[a] = c.s.vel[a * P + i];
+    } else {
+      float j[3];
+      moments0(F, rho, j[0], j[1], j[2]);
+      const float inv = 1.0f / rho;
+      for (int a = 0; a < 3; ++a) {
+        const float cf = (fl & kCF) ? c.s.cell_force[a * P + i] : 0.f;
+        u[a] = j[a] * inv + (0.5f * (c.p.force[a] + cf)) * inv;
+      }
+    }
+  }
+  out_rho[i] = rho;
+  for (int a = 0; a < 3; ++a) out_vel[a * P + i] = u[a];
+}
+
+// finalize_moving_boundary_force_accumulator (fluid.py:475-486)
+__global__ void k_accum_finalize(const Case c, int32_t sample_count) {
+  const int64_t n = (int64_t)c.s.nx * c.s.ny * c.s.nz;
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  float mean_n = 0.f;
+  if (i < n) {
+    const int64_t P = c.s.pitch;
+    float a[3];
+    for (int d = 0; d < 3; ++d) a[d] = c.s.accum[d * P + i];
+    if ((c.c.mode & FSI_MODE_SUBCYCLED) && (c.s.flags[i] & kLink)) {
+      float* last = c.s.hpp + (int64_t)c.c.pp * 3 * P;
+      for (int d = 0; d < 3; ++d) {
+        a[d] += last[d * P + i];
+        last[d * P + i] = 0.f;
+        c.s.accum[d * P + i] = a[d];
+      }
+      atomic_max_nonneg(&c.s.diag->accum_norm_max, sqrtf(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]));
+    }
+    if (sample_count > 0) {
+      const float inv = 1.0f / (float)sample_count;
+      float m[3];
+      for (int d = 0; d < 3; ++d) {
+        m[d] = a[d] * inv;
+        c.s.hydro[d * P + i] = m[d];
+      }
+      mean_n = sqrtf(m[0] * m[0] + m[1] * m[1] + m[2] * m[2]);
+    }
+  }
+  const float mx = warp_max(mean_n);
+  if ((threadIdx.x & 31) == 0 && mx > 0.f) atomic_max_nonneg(&c.s.diag->mean_norm_max, mx);
+}
+
+// ------------------------------------------------------------- host ABI ----
+static int check_state(const FsiLbmState* s, const FsiLbmParams* p) {
+  if (!s || !p) return invalid("null state or params");
+  if (s->nx < 3 || s->ny < 1 || s->nz < 1) return invalid("lattice must have nx >= 3, ny >= 1, nz >= 1");
+  if (s->pitch < (int64_t)s->nx * s->ny * s->nz || (s->pitch % 32) != 0)
+    return invalid("pitch must cover nx*ny*nz and be a multiple of 32");
+  if ((p->bc_left || p->bc_right) && (s->nx < 4 || (s->nx % 32 == 1) || (s->nx % 32 == 2)))
+    return invalid("x open boundaries need nx >= 4 and nx % 32 not in {1, 2}");
+  if (!s->pop || !s->flags || !s->nbr || !s->diag) return invalid("null device pointer in FsiLbmState");
+  return FSI_OK;
+}
+
+static Case make_case(const FsiLbmState* s, const FsiLbmParams* p, const FsiStepCtl* ctl) {
+  Case c;
+  c.s = *s;
+  c.p = *p;
+  if (ctl)
+    c.c = *ctl;
+  else
+    c.c = FsiStepCtl{0, 0, 0, 0};
+  c.K = make_mrt_k(p->s_v, p->s_o);
+  return c;
+}
+
+static inline unsigned blocks_for(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
+
+}  // namespace fsi
+
+using namespace fsi;
+
+extern "C" int fsi_lbm_init_equilibrium(const FsiLbmState* s, const FsiLbmParams* p, void* stream) {
+  int rc = check_state(s, p);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  const Case c = make_case(s, p, nullptr);
+  const int64_t n = (int64_t)s->nx * s->ny * s->nz;
+  k_init<<<blocks_for(n, 256), 256, 0, st>>>(c);
+  if ((rc = launch_check("k_init"))) return rc;
+  k_neighbours_all<<<blocks_for(n, 256), 256, 0, st>>>(c);
+  return launch_check("k_neighbours_all");
+}
+
+extern "C" int fsi_lbm_set_solid(const FsiLbmState* s, const uint8_t* solid, void* stream) {
+  if (!s || !solid) return invalid("null argument");
+  cudaStream_t st = (cudaStream_t)stream;
+  FsiLbmParams p{};
+  p.rho0 = 1.f;
+  p.s_v = p.s_o = 1.f;
+  const Case c = make_case(s, &p, nullptr);
+  const int64_t n = (int64_t)s->nx * s->ny * s->nz;
+  k_set_solid<<<blocks_for(n, 256), 256, 0, st>>>(c, solid);
+  int rc = launch_check("k_set_solid");
+  if (rc) return rc;
+  k_neighbours_all<<<blocks_for(n, 256), 256, 0, st>>>(c);
+  return launch_check("k_neighbours_all");
+}
+
+extern "C" int fsi_lbm_to_natural(const FsiLbmState* s, void* stream) {
+  if (!s) return invalid("null state");
+  FsiLbmParams p{};
+  p.rho0 = 1.f;
+  p.s_v = p.s_o = 1.f;
+  const Case c = make_case(s, &p, nullptr);
+  const int64_t n = (int64_t)s->nx * s->ny * s->nz;
+  if (s->store_fp16)
+    k_to_natural<true><<<blocks_for(n, 256), 256, 0, (cudaStream_t)stream>>>(c);
+  else
+    k_to_natural<false><<<blocks_for(n, 256), 256, 0, (cudaStream_t)stream>>>(c);
+  return launch_check("k_to_natural");
+}
+
+extern "C" int fsi_lbm_substep(const FsiLbmState* s, const FsiLbmParams* p, const FsiStepCtl* ctl, void* stream) {
+  int rc = check_state(s, p);
+  if (rc) return rc;
+  if (!ctl) return invalid("null step control");
+  cudaStream_t st = (cudaStream_t)stream;
+  if (ctl->bc_pending && p->limiter) {
+    rc = cuda_check(cudaMemsetAsync(s->diag->ob_step, 0, sizeof(s->diag->ob_step), st), "memset ob_step");
+    if (rc) return rc;
+  }
+  if ((ctl->mode & FSI_MODE_DIRSTATS) && (ctl->mode & FSI_MODE_MOVING_BB)) {
+    rc = cuda_check(cudaMemsetAsync(s->diag, 0, offsetof(FsiLbmDiag, accum_norm_max), st), "memset dirstats");
+    if (rc) return rc;
+  }
+  if (ctl->mode & FSI_MODE_PENALTY) {
+    rc = cuda_check(cudaMemsetAsync(&s->diag->penalty_active, 0,
+                                    offsetof(FsiLbmDiag, change_count) - offsetof(FsiLbmDiag, penalty_active), st),
+                    "memset penalty stats");
+    if (rc) return rc;
+  }
+  const Case c = make_case(s, p, ctl);
+  dim3 block(32, 8);
+  dim3 grid((unsigned)((s->nx + 31) / 32), (unsigned)((s->ny * s->nz + 7) / 8));
+  const bool odd = ctl->parity != 0;
+  if (s->store_fp16) {
+    if (odd)
+      k_lbm_step<true, true><<<grid, block, 0, st>>>(c);
+    else
+      k_lbm_step<false, true><<<grid, block, 0, st>>>(c);
+  } else {
+    if (odd)
+      k_lbm_step<true, false><<<grid, block, 0, st>>>(c);
+    else
+      k_lbm_step<false, false><<<grid, block, 0, st>>>(c);
+  }
+  return launch_check("k_lbm_step");
+}
+
+extern "C" int fsi_lbm_flush_bc(const FsiLbmState* s, const FsiLbmParams* p, const FsiStepCtl* ctl, void* stream) {
+  int rc = check_state(s, p);
+  if (rc) return rc;
+  if (!ctl) return invalid("null step control");
+  if (!ctl->bc_pending || (!p->bc_left && !p->bc_right)) return FSI_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (p->limiter) {
+    rc = cuda_check(cudaMemsetAsync(s->diag->ob_step, 0, sizeof(s->diag->ob_step), st), "memset ob_step");
+    if (rc) return rc;
+  }
+  const Case c = make_case(s, p, ctl);
+  const int64_t n = 2LL * s->ny * s->nz;
+  if (s->store_fp16)
+    k_flush_bc<true><<<blocks_for(n, 128), 128, 0, st>>>(c);
+  else
+    k_flush_bc<false><<<blocks_for(n, 128), 128, 0, st>>>(c);
+  return launch_check("k_flush_bc");
+}
+
+extern "C" int fsi_mask_rebuild(const FsiLbmState* s, const FsiLbmParams* p, const FsiStepCtl* ctl, float threshold,
+                                void* stream) {
+  int rc = check_state(s, p);
+  if (rc) return rc;
+  if (!ctl) return invalid("null step control");
+  if (!s->change_list || !s->phi || !s->static_solid || !s->old_solid || !s->reinit_flag)
+    return invalid("mask rebuild needs phi, static_solid, old_solid, reinit_flag and change_list");
+  cudaStream_t st = (cudaStream_t)stream;
+  rc = cuda_check(cudaMemsetAsync(&s->diag->change_count, 0, sizeof(int32_t), st), "memset change_count");
+  if (rc) return rc;
+  const Case c = make_case(s, p, ctl);
+  const int64_t n = (int64_t)s->nx * s->ny * s->nz;
+  k_mask_update<<<blocks_for(n, 256), 256, 0, st>>>(c, threshold);
+  if ((rc = launch_check("k_mask_update"))) return rc;
+  const unsigned g = 148 * 4;
+  if (s->store_fp16)
+    k_relink<true><<<g, 128, 0, st>>>(c);
+  else
+    k_relink<false><<<g, 128, 0, st>>>(c);
+  if ((rc = launch_check("k_relink"))) return rc;
+  k_clear_reinit<<<g, 128, 0, st>>>(c);
+  return launch_check("k_clear_reinit");
+}
+
+extern "C" int fsi_force_accum_finalize(const FsiLbmState* s, const FsiStepCtl* ctl, int32_t sample_count,
+                                        void* stream) {
+  if (!s || !ctl) return invalid("null argument");
+  cudaStream_t st = (cudaStream_t)stream;
+  int rc = cuda_check(cudaMemsetAsync(&s->diag->mean_norm_max, 0, sizeof(float), st), "memset mean_norm_max");
+  if (rc) return rc;
+  FsiLbmParams p{};
+  p.rho0 = 1.f;
+  p.s_v = p.s_o = 1.f;
+  const Case c = make_case(s, &p, ctl);
+  const int64_t n = (int64_t)s->nx * s->ny * s->nz;
+  k_accum_finalize<<<blocks_for(n, 256), 256, 0, st>>>(c, sample_count);
+  return launch_check("k_accum_finalize");
+}
+
+extern "C" int fsi_lbm_readout(const FsiLbmState* s, const FsiLbmParams* p, const FsiStepCtl* ctl, float* out_pop,
+                               float* out_rho, float* out_vel, void* stream) {
+  int rc = check_state(s, p);
+  if (rc) return rc;
+  if (!ctl || !out_pop || !out_rho || !out_vel) return invalid("null argument");
+  const Case c = make_case(s, p, ctl);
+  const int64_t n = (int64_t)s->nx * s->ny * s->nz;
+  if (s->store_fp16)
+    k_readout<true><<<blocks_for(n, 256), 256, 0, (cudaStream_t)stream>>>(c, out_pop, out_rho, out_vel);
+  else
+    k_readout<false><<<blocks_for(n, 256), 256, 0, (cudaStream_t)stream>>>(c, out_pop, out_rho, out_vel);
+  return launch_check("k_readout");
+}

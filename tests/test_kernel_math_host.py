@@ -1,0 +1,90 @@
+"""The device arithmetic of the LBM collision (mpm_lbm_b200/csrc/d3q19.cuh)
+and of the FP64 polar rotation (csrc/polar3.cuh), compiled as host C++,
+against the CPU oracle (dense-matrix restatement of fluid.py:398-413)."""
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from oracle import oracle as orc
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+CSRC = os.path.join(ROOT, "mpm_lbm_b200", "csrc")
+
+SRC = r"""
+#include "d3q19.cuh"
+#include "polar3.cuh"
+extern "C" void host_collide(const float* F, float rho, const float* u, const float* A, float s_v, float s_o, float* out) {
+  const fsi::MrtK K = fsi::make_mrt_k(s_v, s_o);
+  fsi::mrt_collide(F, rho, u[0], u[1], u[2], A[0], A[1], A[2], K, out);
+}
+extern "C" void host_moments(const float* F, float* m) { fsi::moments0(F, m[0], m[1], m[2], m[3]); }
+extern "C" void host_polar(const double* F, double* R) { fsi::polar_rotation_d(F, R); }
+"""
+
+
+@pytest.fixture(scope="module")
+def hostlib(tmp_path_factory):
+    d = tmp_path_factory.mktemp("hostmath")
+    src = d / "m.cpp"
+    src.write_text(SRC)
+    so = d / "libm.so"
+    subprocess.run(["g++", "-O2", "-std=c++17", "-shared", "-fPIC", "-I", CSRC, str(src), "-o", str(so)], check=True)
+    return ctypes.CDLL(str(so))
+
+
+def P(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+@pytest.mark.parametrize("collision", ["mrt", "bgk"])
+def test_fast_collision_equals_dense_reference(hostlib, collision):
+    rng = np.random.default_rng(1)
+    n = 64
+    lbm = orc.OracleLBM(n, 1, 1, niu=1.0 / 30.0, relaxation_semantics="standard_lattice_kinematic_viscosity",
+                        force=(1e-5, -3e-6, 2e-6), collision=collision, dtype=np.float64)
+    lbm.init_simulation()
+    w = orc.W
+    F = (w[None, :] * (1 + 0.05 * rng.standard_normal((n, 19)))).reshape(n, 1, 1, 19)
+    lbm.F[...] = F
+    lbm.rho[...] = 1 + 0.01 * rng.standard_normal((n, 1, 1))
+    lbm.v[...] = 0.03 * rng.standard_normal((n, 1, 1, 3))
+    lbm.cell_force[...] = 1e-4 * rng.standard_normal((n, 1, 1, 3))
+    lbm.colission()
+    s = np.array(lbm.p.S[:])
+    s_v, s_o = s[1], s[4]
+    out = np.zeros(19, np.float32)
+    for c in range(n):
+        Fc = lbm.F[c, 0, 0].astype(np.float32)
+        u = lbm.v[c, 0, 0].astype(np.float32)
+        A = (np.array(lbm.p.force[:]) + lbm.cell_force[c, 0, 0]).astype(np.float32)
+        hostlib.host_collide(P(Fc), ctypes.c_float(lbm.rho[c, 0, 0]), P(u), P(A), ctypes.c_float(s_v),
+                             ctypes.c_float(s_o), P(out))
+        np.testing.assert_allclose(out, lbm.f[c, 0, 0], rtol=2e-6, atol=3e-8)
+
+
+def test_moments(hostlib):
+    rng = np.random.default_rng(2)
+    F = rng.random(19).astype(np.float32)
+    m = np.zeros(4, np.float32)
+    hostlib.host_moments(P(F), P(m))
+    np.testing.assert_allclose(m[0], F.sum(), rtol=1e-6)
+    np.testing.assert_allclose(m[1:], F @ orc.E.astype(np.float32), rtol=1e-5, atol=1e-6)
+
+
+def test_polar_rotation_matches_oracle(hostlib):
+    rng = np.random.default_rng(3)
+    L = orc.lib()
+    for t in range(300):
+        F = np.eye(3) + 0.5 * rng.standard_normal((3, 3))
+        if t == 0:
+            F = np.diag([1.2, -0.8, 1.0])
+        if t == 1:
+            F = np.eye(3)
+        R1, R2 = np.zeros(9), np.zeros(9)
+        hostlib.host_polar(P(F.reshape(-1).copy()), P(R1))
+        L.orc_polar_rotation(P(F.reshape(-1).copy()), P(R2))
+        np.testing.assert_allclose(R1, R2, atol=1e-10)
