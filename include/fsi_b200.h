@@ -104,6 +104,8 @@ typedef struct FsiLbmState {
   float* plane;             /* [4][4][ny*nz] rho,ux,uy,uz of x = 0, 1, nx-2, nx-1 of the last step */
   int32_t* change_list;     /* [pitch] scratch for the mask rebuild */
   FsiLbmDiag* diag;         /* device */
+  const float* vel_left_dyn;  /* optional [3]: x-min inlet velocity read on the device each step
+                                 (bc_vel_x_left_dynamic, fluid.py:287-288, 1979); NULL = vel_bc_left */
 } FsiLbmState;
 
 typedef struct FsiLbmParams {

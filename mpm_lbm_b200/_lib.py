@@ -34,7 +34,7 @@ class FsiLbmState(ctypes.Structure):
         ("pop", c_p), ("flags", c_p), ("nbr", c_p), ("rho", c_p), ("vel", c_p), ("static_solid", c_p),
         ("old_solid", c_p), ("reinit_flag", c_p), ("phi", c_p), ("smass", c_p), ("svel", c_p),
         ("cell_force", c_p), ("hydro", c_p), ("hpp", c_p), ("accum", c_p), ("plane", c_p),
-        ("change_list", c_p), ("diag", c_p),
+        ("change_list", c_p), ("diag", c_p), ("vel_left_dyn", c_p),
     ]
 
 

@@ -163,12 +163,13 @@ __device__ __forceinline__ float regularized_pop(const FsiLbmParams& p, bool lim
 }
 
 // Boundary_condition for one fluid face cell (fluid.py:926-1024, 1348-1493).
-__device__ void apply_face_bc(const FsiLbmParams& p, int side, const FaceIn& in, float* F, int* cnt) {
+__device__ void apply_face_bc(const FsiLbmParams& p, const float* vdyn, int side, const FaceIn& in, float* F,
+                              int* cnt) {
   const int bc = side == 0 ? p.bc_left : p.bc_right;
   
   if (p.ob_semantics == FSI_OB_EQUILIBRIUM_RESET) {
     if (bc == 2) {
-      const float* vb = side == 0 ? p.vel_bc_left : p.vel_bc_right;
+      const float* vb = side == 0 ? (vdyn ? vdyn : p.vel_bc_left) : p.vel_bc_right;
 #pragma unroll
       for (int s = 0; s < 19; ++s) F[s] = feq(s, 1.0f, vb[0], vb[1], vb[2]);
     } else if (bc == 1) {
@@ -198,7 +199,7 @@ __device__ void apply_face_bc(const FsiLbmParams& p, int side, const FaceIn& in,
   } else {
     trho = in.mac_n[0];
     if (trho <= 1.0e-6f) trho = p.rho0;
-    const float* vb = side == 0 ? p.vel_bc_left : p.vel_bc_right;
+    const float* vb = side == 0 ? (vdyn ? vdyn : p.vel_bc_left) : p.vel_bc_right;
     t0 = vb[0];
     t1 = vb[1];
     t2 = vb[2];
@@ -218,18 +219,112 @@ __device__ __forceinline__ void load_plane(const Case& c, int plane, int row, fl
   for (int a = 0; a < 4; ++a) m[a] = pp[a * n + row];
 }
 
+constexpr unsigned kFull = 0xffffffffu;
+
+// Limiter counters of one warp (rho, velocity, noneq, floor, reconstructed).
 __device__ __forceinline__ void flush_counts(const Case& c, const int* cnt) {
 #pragma unroll
   for (int a = 0; a < 5; ++a) {
-    int v = cnt[a];
-    v += __shfl_xor_sync(0xffffffffu, v, 16);
-    v += __shfl_xor_sync(0xffffffffu, v, 8);
-    v += __shfl_xor_sync(0xffffffffu, v, 4);
-    v += __shfl_xor_sync(0xffffffffu, v, 2);
-    v += __shfl_xor_sync(0xffffffffu, v, 1);
+    const int v = (int)__reduce_add_sync(kFull, (unsigned)cnt[a]);
     if ((threadIdx.x & 31) == 0 && v) {
       atomicAdd(&c.s.diag->ob_step[a], v);
       atomicAdd(&c.s.diag->ob_run[a], v);
+    }
+  }
+}
+
+// One population of a face cell, evaluated by lane `lane` (population index
+// lane for the equilibrium reset, unknown population number lane otherwise).
+struct FaceVal {
+  float val;
+  int packed;  // five 6-bit limiter counters
+};
+
+__device__ __forceinline__ FaceVal face_population(const FsiLbmParams& p, const float* vdyn, int side, int lane,
+                                                   float Fn, float Fn2, bool n2_fluid, const float* mac_n,
+                                                   const float* mac_l) {
+  FaceVal r{0.f, 0};
+  const int bc = side == 0 ? p.bc_left : p.bc_right;
+  const float* vb = side == 0 ? (vdyn ? vdyn : p.vel_bc_left) : p.vel_bc_right;
+  if (p.ob_semantics == FSI_OB_EQUILIBRIUM_RESET) {  // fluid.py:926-1024
+    if (lane < 19) {
+      if (bc == 2) r.val = feq(lane, 1.0f, vb[0], vb[1], vb[2]);
+      else r.val = feq(lane, side == 0 ? p.rho_bc_left : p.rho_bc_right, mac_l[1], mac_l[2], mac_l[3]);
+    }
+    return r;
+  }
+  if (lane >= 5) return r;
+  const int s = side == 0 ? kUnknownL(lane) : kUnknownR(lane);
+  if (p.ob_semantics == FSI_OB_CONVECTIVE && side == 1 && bc == 1) {  // fluid.py:1098-1103
+    float ex = n2_fluid ? 2.0f * Fn - Fn2 : Fn;
+    if (p.limiter && p.floor_enabled && ex < p.ob_floor) ex = p.ob_floor;
+    r.val = ex;
+    return r;
+  }
+  float trho, t0, t1, t2;
+  if (bc == 1) {
+    trho = side == 0 ? p.rho_bc_left : p.rho_bc_right;
+    t0 = mac_n[1];
+    t1 = mac_n[2];
+    t2 = mac_n[3];
+  } else {
+    trho = mac_n[0];
+    if (trho <= 1.0e-6f) trho = p.rho0;
+    t0 = vb[0];
+    t1 = vb[1];
+    t2 = vb[2];
+  }
+  int cnt[5] = {0, 0, 0, 0, 0};
+  r.val = regularized_pop(p, p.ob_semantics == FSI_OB_REGULARIZED_LIMITED, s, trho, t0, t1, t2, Fn, mac_n, cnt);
+  r.packed = cnt[0] | (cnt[1] << 6) | (cnt[2] << 12) | (cnt[3] << 18) | (cnt[4] << 24);
+  return r;
+}
+
+// Open boundary of one x face for the warp holding that face cell: the five
+// (or nineteen) face populations are computed by different lanes and gathered
+// into the face lane with shuffles.
+template <int SIDE>
+__device__ __forceinline__ void bc_face_warp(const Case& c, int lane, int row, uint8_t fl, float* F) {
+  const int nx = c.s.nx;
+  const int lf = SIDE == 0 ? 0 : ((nx - 1) & 31);
+  const int l1 = SIDE == 0 ? 1 : ((nx - 2) & 31);
+  const int l2 = SIDE == 0 ? 1 : ((nx - 3) & 31);
+  const unsigned solid_bits = __ballot_sync(kFull, (fl & kSolid) != 0);
+  if ((solid_bits >> lf) & 1u) return;
+  const bool n1_solid = (solid_bits >> l1) & 1u;
+  const bool n2_fluid = n1_solid ? true : !((solid_bits >> l2) & 1u);
+  const int src1 = n1_solid ? lf : l1, src2 = n1_solid ? lf : l2;
+  float Fn = 0.f, Fn2 = 0.f;
+#pragma unroll
+  for (int q = 0; q < 5; ++q) {
+    const int s = SIDE == 0 ? kUnknownL(q) : kUnknownR(q);
+    const float a = __shfl_sync(kFull, F[s], src1);
+    const float b = __shfl_sync(kFull, F[s], src2);
+    if (lane == q) {
+      Fn = a;
+      Fn2 = b;
+    }
+  }
+  float mac_n[4], mac_l[4];
+  load_plane(c, SIDE == 0 ? (n1_solid ? 0 : 1) : (n1_solid ? 3 : 2), row, mac_n);
+  load_plane(c, SIDE == 0 ? (n1_solid ? 1 : 0) : 2, row, mac_l);
+  const FaceVal r = face_population(c.p, c.s.vel_left_dyn, SIDE, lane, Fn, Fn2, n2_fluid, mac_n, mac_l);
+  if (c.p.ob_semantics == FSI_OB_EQUILIBRIUM_RESET) {
+#pragma unroll
+    for (int s = 0; s < 19; ++s) {
+      const float v = __shfl_sync(kFull, r.val, s);
+      if (lane == lf) F[s] = v;
+    }
+  } else {
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+      const float v = __shfl_sync(kFull, r.val, q);
+      if (lane == lf) F[SIDE == 0 ? kUnknownL(q) : kUnknownR(q)] = v;
+    }
+    if (c.p.limiter) {
+      const int cnt[5] = {r.packed & 63, (r.packed >> 6) & 63, (r.packed >> 12) & 63, (r.packed >> 18) & 63,
+                          (r.packed >> 24) & 63};
+      flush_counts(c, cnt);
     }
   }
 }
@@ -243,22 +338,92 @@ struct DirAcc {
   int any;
 };
 
-template <bool ODD, bool H>
+// wrapped neighbourhood of a cell: row bases for dy, dz in {-1, 0, 1} and x +- 1
+struct Nbh {
+  int rb[3][3];
+  int xm, xp, x;
+  __device__ __forceinline__ int at(int dx, int dy, int dz) const {
+    return rb[dz + 1][dy + 1] + (dx < 0 ? xm : (dx > 0 ? xp : x));
+  }
+};
+
+__device__ __forceinline__ void make_nbh(const Case& c, int x, int j, int k, Nbh& n) {
+  const int nx = c.s.nx, ny = c.s.ny, nz = c.s.nz;
+  const int jj[3] = {j == 0 ? ny - 1 : j - 1, j, j == ny - 1 ? 0 : j + 1};
+  const int kk[3] = {k == 0 ? nz - 1 : k - 1, k, k == nz - 1 ? 0 : k + 1};
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = 0; b < 3; ++b) n.rb[a][b] = (kk[a] * ny + jj[b]) * nx;
+  n.xm = x == 0 ? nx - 1 : x - 1;
+  n.xp = x == nx - 1 ? 0 : x + 1;
+  n.x = x;
+}
+
+template <bool H>
+__device__ __forceinline__ float ldp(const Case& c, int s, int idx) {
+  return Pop<H>::ld(c, s, (int64_t)idx);
+}
+
+template <bool H>
+__device__ __forceinline__ void stp(const Case& c, int s, int idx, float v) {
+  Pop<H>::st(c, s, (int64_t)idx, v);
+}
+
+// Streaming of a cell next to a solid: half-way bounce-back, with the
+// moving-wall correction and momentum-exchange link force when MOVING
+// (fluid.py:431-440, 488-519).
+template <bool ODD, bool H, bool MOVING>
+__device__ __forceinline__ void store_near_solid(const Case& c, const Nbh& n, int cell, uint32_t nb, float rho,
+                                              const float* out, bool dirstats, DirAcc* acc) {
+  float* hpp = c.s.hpp + (int64_t)c.c.pp * 3 * c.s.pitch;
+  const int64_t P = c.s.pitch;
+#pragma unroll
+  for (int s = 0; s < 19; ++s) {
+    float val = out[s];
+    const bool bb = (nb >> s) & 1u;
+    if (MOVING && bb) {
+      const int ip = n.at(kEx(s), kEy(s), kEz(s));
+      const float ew = (float)kEx(s) * c.s.svel[ip] + (float)kEy(s) * c.s.svel[P + ip] + (float)kEz(s) * c.s.svel[2 * P + ip];
+      const float corr = -6.0f * lattice_w(s) * rho * ew;
+      const float f0 = val;
+      val = f0 + corr;
+      const float tot = val + f0;  // solid force = e_s (bounced + f)
+      if (kEx(s)) atomicAdd(hpp + ip, (float)kEx(s) * tot);
+      if (kEy(s)) atomicAdd(hpp + P + ip, (float)kEy(s) * tot);
+      if (kEz(s)) atomicAdd(hpp + 2 * P + ip, (float)kEz(s) * tot);
+      if (dirstats) {
+        const float ac = fabsf(corr);
+        atomicAdd(&acc->cnt[s], 1);
+        atomicAdd(&acc->csum[s], ac);
+        atomic_max_nonneg(&acc->cmax[s], ac);
+        if (kEx(s)) atomicAdd(&acc->imp[s][0], -(float)kEx(s) * tot);
+        if (kEy(s)) atomicAdd(&acc->imp[s][1], -(float)kEy(s) * tot);
+        if (kEz(s)) atomicAdd(&acc->imp[s][2], -(float)kEz(s) * tot);
+        acc->any = 1;
+      }
+    }
+    if (!ODD || s == 0 || bb)
+      stp<H>(c, kOpp(s), cell, val);
+    else
+      stp<H>(c, s, n.at(kEx(s), kEy(s), kEz(s)), val);
+  }
+}
+
+template <bool ODD, bool H, bool MOVING, bool BCW, bool PEN>
 __global__ void __launch_bounds__(256) k_lbm_step(const Case c) {
   __shared__ DirAcc acc;
   const int lane = threadIdx.x;
-  const int tid = threadIdx.y * 32 + lane;
   const int nx = c.s.nx, ny = c.s.ny, nz = c.s.nz;
   const int x = blockIdx.x * 32 + lane;
   const int row = blockIdx.y * blockDim.y + threadIdx.y;
   const bool inrow = row < ny * nz;
   const bool valid = inrow && x < nx;
-  const Coord q{x, inrow ? row % ny : 0, inrow ? row / ny : 0};
-  const int64_t cell = (int64_t)row * nx + x;
-  const int mode = c.c.mode;
-  const bool moving = mode & FSI_MODE_MOVING_BB;
-  const bool dirstats = (mode & FSI_MODE_DIRSTATS) && moving;
+  const int j = inrow ? row % ny : 0, k = inrow ? row / ny : 0;
+  const int cell = row * nx + x;
+  const bool dirstats = MOVING && (c.c.mode & FSI_MODE_DIRSTATS);
   if (dirstats) {
+    const int tid = threadIdx.y * 32 + lane;
     for (int i = tid; i < 19; i += 256) {
       acc.cnt[i] = 0;
       acc.csum[i] = 0.f;
@@ -269,21 +434,28 @@ __global__ void __launch_bounds__(256) k_lbm_step(const Case c) {
     __syncthreads();
   }
 
-  uint8_t fl = valid ? c.s.flags[cell] : kSolid;
+  const uint8_t fl = valid ? c.s.flags[cell] : kSolid;
   const bool fluid = !(fl & kSolid);
   const uint32_t nb = (fluid && (fl & kNear)) ? c.s.nbr[cell] : 0u;
+  Nbh n;
+  if (ODD || nb) make_nbh(c, x < nx ? x : 0, j, k, n);
 
-  // ---- load the post-streaming populations of this cell
+  // ---- post-streaming populations of this cell (AA layout, fluid.py:431-440)
   float F[19];
   if (fluid) {
+    if (!ODD) {
 #pragma unroll
-    for (int s = 0; s < 19; ++s) {
-      if (!ODD || s == 0) {
-        F[s] = Pop<H>::ld(c, s, cell);
-      } else {
+      for (int s = 0; s < 19; ++s) F[s] = ldp<H>(c, s, cell);
+    } else if (nb == 0) {
+      F[0] = ldp<H>(c, 0, cell);
+#pragma unroll
+      for (int s = 1; s < 19; ++s) F[s] = ldp<H>(c, kOpp(s), n.at(-kEx(s), -kEy(s), -kEz(s)));
+    } else {
+      F[0] = ldp<H>(c, 0, cell);
+#pragma unroll
+      for (int s = 1; s < 19; ++s) {
         const bool src_solid = (nb >> kOpp(s)) & 1u;
-        F[s] = src_solid ? Pop<H>::ld(c, s, cell)
-                         : Pop<H>::ld(c, kOpp(s), nb_cell(c, q, -kEx(s), -kEy(s), -kEz(s)));
+        F[s] = src_solid ? ldp<H>(c, s, cell) : ldp<H>(c, kOpp(s), n.at(-kEx(s), -kEy(s), -kEz(s)));
       }
     }
   } else {
@@ -291,94 +463,51 @@ __global__ void __launch_bounds__(256) k_lbm_step(const Case c) {
     for (int s = 0; s < 19; ++s) F[s] = 0.f;
   }
 
-  // ---- pending open boundary of the previous step (warp-uniform branches)
-  const bool open_bc = c.p.bc_left != 0 || c.p.bc_right != 0;
-  const int right_block = (nx - 1) >> 5;
-  if (c.c.bc_pending && inrow) {
-    int cnt[5] = {0, 0, 0, 0, 0};
-    const bool warp_left = c.p.bc_left != 0 && blockIdx.x == 0;
-    const bool warp_right = c.p.bc_right != 0 && (int)blockIdx.x == right_block;
-    if (warp_left) {
-      const bool n1_solid = __shfl_sync(0xffffffffu, (int)(fl & kSolid), 1) != 0;
-      const int src = n1_solid ? 0 : 1;
-      FaceIn in;
-#pragma unroll
-      for (int t = 0; t < 5; ++t) in.Fni[t] = __shfl_sync(0xffffffffu, F[kUnknownL(t)], src);
-      if (lane == 0 && fluid) {
-        in.n1_solid = n1_solid;
-        in.n2_fluid = false;
-        load_plane(c, n1_solid ? 0 : 1, row, in.mac_n);
-        load_plane(c, n1_solid ? 1 : 0, row, in.mac_leg);
-        apply_face_bc(c.p, 0, in, F, cnt);
-      }
-    }
-    if (warp_right) {
-      const int l1 = (nx - 2) & 31, l2 = (nx - 3) & 31, lf = (nx - 1) & 31;
-      const bool n1_solid = __shfl_sync(0xffffffffu, (int)(fl & kSolid), l1) != 0;
-      const bool n2s = __shfl_sync(0xffffffffu, (int)(fl & kSolid), l2) != 0;
-      const int src1 = n1_solid ? lf : l1;
-      const int src2 = n1_solid ? lf : l2;
-      FaceIn in;
-#pragma unroll
-      for (int t = 0; t < 5; ++t) {
-        in.Fni[t] = __shfl_sync(0xffffffffu, F[kUnknownR(t)], src1);
-        in.Fn2[t] = __shfl_sync(0xffffffffu, F[kUnknownR(t)], src2);
-      }
-      if (lane == lf && x == nx - 1 && fluid) {
-        in.n1_solid = n1_solid;
-        in.n2_fluid = n1_solid ? true : !n2s;
-        load_plane(c, n1_solid ? 3 : 2, row, in.mac_n);
-        load_plane(c, 2, row, in.mac_leg);
-        apply_face_bc(c.p, 1, in, F, cnt);
-      }
-    }
-    if (c.p.limiter && (warp_left || warp_right)) flush_counts(c, cnt);
+  // ---- pending open boundary of the previous step (fluid.py:538-569)
+  if (BCW && c.c.bc_pending && inrow) {
+    if (c.p.bc_left != 0 && blockIdx.x == 0) bc_face_warp<0>(c, lane, row, fl, F);
+    if (c.p.bc_right != 0 && (int)blockIdx.x == ((nx - 1) >> 5)) bc_face_warp<1>(c, lane, row, fl, F);
   }
 
-  // ---- macroscopic state the collision uses (streaming3 of the previous step)
+  // ---- macroscopic state the collision uses (streaming3 of the previous step, fluid.py:1794-1814)
   float rho = c.p.rho0, ux = 0.f, uy = 0.f, uz = 0.f;
-  float cfp[3] = {0.f, 0.f, 0.f};
-  if (fluid) {
-    if (fl & kCF) {
-#pragma unroll
-      for (int a = 0; a < 3; ++a) cfp[a] = c.s.cell_force[(int64_t)a * c.s.pitch + cell];
-    }
-    if (fl & kOverride) {
-      rho = c.s.rho[cell];
-      ux = c.s.vel[cell];
-      uy = c.s.vel[c.s.pitch + cell];
-      uz = c.s.vel[2 * c.s.pitch + cell];
-    } else {
-      float jx, jy, jz;
-      moments0(F, rho, jx, jy, jz);
-      const float inv = 1.0f / rho;
-      ux = jx * inv + (0.5f * (c.p.force[0] + cfp[0])) * inv;
-      uy = jy * inv + (0.5f * (c.p.force[1] + cfp[1])) * inv;
-      uz = jz * inv + (0.5f * (c.p.force[2] + cfp[2])) * inv;
-    }
+  float cf0 = 0.f, cf1 = 0.f, cf2 = 0.f;
+  const int64_t P = c.s.pitch;
+  if (fluid && (fl & kCF)) {
+    cf0 = c.s.cell_force[cell];
+    cf1 = c.s.cell_force[P + cell];
+    cf2 = c.s.cell_force[2 * P + cell];
   }
-  // store the macroscopic state of the planes the next open boundary reads
-  if (open_bc) {
+  if (valid && (fl & kOverride)) {
+    rho = c.s.rho[cell];
+    ux = c.s.vel[cell];
+    uy = c.s.vel[P + cell];
+    uz = c.s.vel[2 * P + cell];
+  } else if (fluid) {
+    float jx, jy, jz;
+    moments0(F, rho, jx, jy, jz);
+    const float inv = __frcp_rn(rho);
+    ux = (jx + 0.5f * (c.p.force[0] + cf0)) * inv;
+    uy = (jy + 0.5f * (c.p.force[1] + cf1)) * inv;
+    uz = (jz + 0.5f * (c.p.force[2] + cf2)) * inv;
+  }
+  if (BCW) {
     __syncwarp();
-    int plane = -1;
-    if (x == 0) plane = 0;
-    else if (x == 1) plane = 1;
-    else if (x == nx - 2) plane = 2;
-    else if (x == nx - 1) plane = 3;
+    const int plane = x == 0 ? 0 : (x == 1 ? 1 : (x == nx - 2 ? 2 : (x == nx - 1 ? 3 : -1)));
     if (valid && plane >= 0) {
       float* pp = c.s.plane + (int64_t)plane * 4 * ny * nz;
-      const int64_t n = (int64_t)ny * nz;
+      const int64_t m = (int64_t)ny * nz;
       pp[row] = rho;
-      pp[n + row] = ux;
-      pp[2 * n + row] = uy;
-      pp[3 * n + row] = uz;
+      pp[m + row] = ux;
+      pp[2 * m + row] = uy;
+      pp[3 * m + row] = uz;
     }
   }
 
-  // ---- penalty force (coupling/penalty.py:59-88), built from this state
-  float Ax = c.p.force[0], Ay = c.p.force[1], Az = c.p.force[2];
+  // ---- penalty force built from this state (coupling/penalty.py:59-88)
+  float Ax = c.p.force[0] + cf0, Ay = c.p.force[1] + cf1, Az = c.p.force[2] + cf2;
   uint8_t nfl = fl & (uint8_t)~kOverride;
-  if (mode & FSI_MODE_PENALTY) {
+  if (PEN) {
     float f0 = 0.f, f1 = 0.f, f2 = 0.f;
     bool active = false;
     if (fluid) {
@@ -386,8 +515,8 @@ __global__ void __launch_bounds__(256) k_lbm_step(const Case c) {
       if (phi > c.p.penalty_phi_min) {
         const float sc = c.p.penalty_beta * phi * rho;
         f0 = sc * (c.s.svel[cell] - ux);
-        f1 = sc * (c.s.svel[c.s.pitch + cell] - uy);
-        f2 = sc * (c.s.svel[2 * c.s.pitch + cell] - uz);
+        f1 = sc * (c.s.svel[P + cell] - uy);
+        f2 = sc * (c.s.svel[2 * P + cell] - uz);
         const float nrm = sqrtf(f0 * f0 + f1 * f1 + f2 * f2);
         if (nrm > c.p.penalty_cap) {
           const float r = c.p.penalty_cap / nrm;
@@ -399,7 +528,6 @@ __global__ void __launch_bounds__(256) k_lbm_step(const Case c) {
       }
     }
     if (active || (valid && (fl & kCF))) {
-      const int64_t P = c.s.pitch;
       c.s.cell_force[cell] = f0;
       c.s.cell_force[P + cell] = f1;
       c.s.cell_force[2 * P + cell] = f2;
@@ -408,11 +536,11 @@ __global__ void __launch_bounds__(256) k_lbm_step(const Case c) {
       c.s.hydro[2 * P + cell] = -f2;
     }
     nfl = active ? (nfl | kCF) : (nfl & (uint8_t)~kCF);
-    Ax += f0;
-    Ay += f1;
-    Az += f2;
-    if (__any_sync(0xffffffffu, active)) {
-      const int na = __popc(__ballot_sync(0xffffffffu, active));
+    Ax = c.p.force[0] + f0;
+    Ay = c.p.force[1] + f1;
+    Az = c.p.force[2] + f2;
+    if (__any_sync(kFull, active)) {
+      const int na = __popc(__ballot_sync(kFull, active));
       const float mx = warp_max(sqrtf(f0 * f0 + f1 * f1 + f2 * f2));
       const float s0 = warp_sum(f0), s1 = warp_sum(f1), s2 = warp_sum(f2);
       if (lane == 0) {
@@ -423,59 +551,28 @@ __global__ void __launch_bounds__(256) k_lbm_step(const Case c) {
         atomicAdd(&c.s.diag->penalty_net[2], s2);
       }
     }
-  } else if (fluid && (fl & kCF)) {
-    // a cell force left by an earlier penalty step keeps acting (fluid.py:393-396)
-    Ax += cfp[0];
-    Ay += cfp[1];
-    Az += cfp[2];
-    nfl = fl & (uint8_t)~kOverride;
   }
   if (valid && nfl != fl) c.s.flags[cell] = nfl;
 
-  // ---- collision and streaming
-  float* hpp = c.s.hpp + (int64_t)c.c.pp * 3 * c.s.pitch;
+  // ---- collision (fluid.py:398-413) and AA streaming
   if (fluid) {
-    float out[19];
-    mrt_collide(F, rho, ux, uy, uz, Ax, Ay, Az, c.K, out);
-#pragma unroll
-    for (int s = 0; s < 19; ++s) {
-      float val = out[s];
-      const bool bb = (nb >> s) & 1u;  // cell + e_s is solid
-      if (bb && moving) {
-        const int64_t ip = nb_cell(c, q, kEx(s), kEy(s), kEz(s));
-        const int64_t P = c.s.pitch;
-        const float ew = (float)kEx(s) * c.s.svel[ip] + (float)kEy(s) * c.s.svel[P + ip] + (float)kEz(s) * c.s.svel[2 * P + ip];
-        const float corr = -6.0f * lattice_w(s) * rho * ew;
-        const float f0 = val;
-        val = f0 + corr;
-        const float tot = val + f0;  // solid force = e_s (bounced + f)
-        if (kEx(s)) atomicAdd(hpp + ip, (float)kEx(s) * tot);
-        if (kEy(s)) atomicAdd(hpp + P + ip, (float)kEy(s) * tot);
-        if (kEz(s)) atomicAdd(hpp + 2 * P + ip, (float)kEz(s) * tot);
-        if (dirstats) {
-          const float ac = fabsf(corr);
-          atomicAdd(&acc.cnt[s], 1);
-          atomicAdd(&acc.csum[s], ac);
-          atomic_max_nonneg(&acc.cmax[s], ac);
-          if (kEx(s)) atomicAdd(&acc.imp[s][0], -(float)kEx(s) * tot);
-          if (kEy(s)) atomicAdd(&acc.imp[s][1], -(float)kEy(s) * tot);
-          if (kEz(s)) atomicAdd(&acc.imp[s][2], -(float)kEz(s) * tot);
-          acc.any = 1;
-        }
-      }
+    mrt_collide(F, rho, ux, uy, uz, Ax, Ay, Az, c.K, F);
+    if (nb == 0) {
       if (!ODD) {
-        Pop<H>::st(c, kOpp(s), cell, val);
-      } else if (s == 0 || bb) {
-        Pop<H>::st(c, kOpp(s), cell, val);
+#pragma unroll
+        for (int s = 0; s < 19; ++s) stp<H>(c, kOpp(s), cell, F[s]);
       } else {
-        Pop<H>::st(c, s, nb_cell(c, q, kEx(s), kEy(s), kEz(s)), val);
+        stp<H>(c, 0, cell, F[0]);
+#pragma unroll
+        for (int s = 1; s < 19; ++s) stp<H>(c, s, n.at(kEx(s), kEy(s), kEz(s)), F[s]);
       }
+    } else {
+      store_near_solid<ODD, H, MOVING>(c, n, cell, nb, rho, F, dirstats, &acc);
     }
-  } else if (valid && (fl & kLink) && moving) {
+  } else if (MOVING && valid && (fl & kLink)) {
     // solid cell receiving link forces: recycle last step's ping-pong slot
-    const int64_t P = c.s.pitch;
     float* prev = c.s.hpp + (int64_t)(c.c.pp ^ 1) * 3 * P;
-    if (mode & FSI_MODE_SUBCYCLED) {
+    if (c.c.mode & FSI_MODE_SUBCYCLED) {
       float a[3];
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
@@ -493,6 +590,7 @@ __global__ void __launch_bounds__(256) k_lbm_step(const Case c) {
   if (dirstats) {
     __syncthreads();
     if (acc.any) {
+      const int tid = threadIdx.y * 32 + lane;
       for (int i = tid; i < 19; i += 256) {
         if (acc.cnt[i]) {
           atomicAdd(&c.s.diag->link_count[i], acc.cnt[i]);
@@ -779,7 +877,7 @@ __global__ void k_flush_bc(const Case c) {
         pop_slot(c, q, cell, fl, nb, s, ss[s], sc[s]);
         F[s] = Pop<H>::ld_rw(c, ss[s], sc[s]);
       }
-      apply_face_bc(c.p, side, in, F, cnt);
+      apply_face_bc(c.p, c.s.vel_left_dyn, side, in, F, cnt);
 #pragma unroll
       for (int s = 0; s < 19; ++s) Pop<H>::st(c, ss[s], sc[s], F[s]);
     }
@@ -805,7 +903,7 @@ __global__ void k_readout(const Case c, float* out_pop, float* out_rho, float* o
   }
   const bool fluid = !(fl & kSolid);
   if (fluid && c.c.bc_pending) {
-    int cnt[5];
+    int cnt[5] = {0, 0, 0, 0, 0};
     for (int side = 0; side < 2; ++side) {
       const int bc = side == 0 ? c.p.bc_left : c.p.bc_right;
       const int fx = side == 0 ? 0 : c.s.nx - 1;
@@ -813,12 +911,16 @@ __global__ void k_readout(const Case c, float* out_pop, float* out_rho, float* o
       FaceIn in;
       int face_x;
       face_inputs<H>(c, side, q.j, q.k, in, face_x);
-      apply_face_bc(c.p, side, in, F, cnt);
+      apply_face_bc(c.p, c.s.vel_left_dyn, side, in, F, cnt);
     }
   }
   const int64_t P = c.s.pitch;
   for (int s = 0; s < 19; ++s) out_pop[(int64_t)s * P + i] = F[s];
   float rho = c.p.rho0, u[3] = {0.f, 0.f, 0.f};
+  if (!fluid && (fl & kOverride)) {
+    rho = c.s.rho[i];
+    for (int a = 0; a < 3; ++a) u[a] = c.s.vel[a * P + i];
+  }
   if (fluid) {
     if (fl & kOverride) {
       rho = c.s.rho[i];
@@ -962,18 +1064,25 @@ extern "C" int fsi_lbm_substep(const FsiLbmState* s, const FsiLbmParams* p, cons
   const Case c = make_case(s, p, ctl);
   dim3 block(32, 8);
   dim3 grid((unsigned)((s->nx + 31) / 32), (unsigned)((s->ny * s->nz + 7) / 8));
-  const bool odd = ctl->parity != 0;
-  if (s->store_fp16) {
-    if (odd)
-      k_lbm_step<true, true><<<grid, block, 0, st>>>(c);
-    else
-      k_lbm_step<false, true><<<grid, block, 0, st>>>(c);
+  const bool odd = ctl->parity != 0, h = s->store_fp16 != 0;
+  const bool moving = ctl->mode & FSI_MODE_MOVING_BB, pen = ctl->mode & FSI_MODE_PENALTY;
+  const bool bcw = p->bc_left != 0 || p->bc_right != 0;
+  if (moving && pen) return invalid("penalty steps use static bounce-back (fluid.py:2099-2103)");
+#define FSI_LAUNCH(O, HH, M, B, PN) k_lbm_step<O, HH, M, B, PN><<<grid, block, 0, st>>>(c)
+#define FSI_BY_H(O, M, B, PN) \
+  if (h) FSI_LAUNCH(O, true, M, B, PN); else FSI_LAUNCH(O, false, M, B, PN)
+#define FSI_BY_O(M, B, PN) \
+  if (odd) { FSI_BY_H(true, M, B, PN); } else { FSI_BY_H(false, M, B, PN); }
+  if (moving) {
+    if (bcw) { FSI_BY_O(true, true, false) } else { FSI_BY_O(true, false, false) }
+  } else if (pen) {
+    if (bcw) { FSI_BY_O(false, true, true) } else { FSI_BY_O(false, false, true) }
   } else {
-    if (odd)
-      k_lbm_step<true, false><<<grid, block, 0, st>>>(c);
-    else
-      k_lbm_step<false, false><<<grid, block, 0, st>>>(c);
+    if (bcw) { FSI_BY_O(false, true, false) } else { FSI_BY_O(false, false, false) }
   }
+#undef FSI_BY_O
+#undef FSI_BY_H
+#undef FSI_LAUNCH
   return launch_check("k_lbm_step");
 }
 

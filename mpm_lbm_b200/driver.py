@@ -42,7 +42,8 @@ DIAGNOSTIC_TEXT_FIELDS = {"coupling_mode", "mb_subcycle_force_accumulation_mode"
 
 class FSIDriver3D:
     def __init__(self, config: FSIDriverConfig, out_dir: str, *, population_storage="fp32", collision="mrt",
-                 lattice_shape=None, material=None, device=None):
+                 lattice_shape=None, material=None, static_solid=None, initial_particles=None, use_cuda_graph=False,
+                 device=None):
         self.config = config
         self.out_dir = out_dir
         self.sim = config.make_unified_sim_config()
@@ -71,6 +72,11 @@ class FSIDriver3D:
         self.duct_static_geometry_report = None
         self.sampling_stats = None
         self.timed_sync = False  # synchronise around phases so the timing dict holds device time
+        self.static_solid = None if static_solid is None else np.asarray(static_solid, np.int8)
+        self.initial_particles = initial_particles
+        self.use_cuda_graph = bool(use_cuda_graph)
+        self._graph = None
+        self._graph_steps = 0
 
     # ------------------------------------------------------------ init
     def _geometry_config(self):
@@ -103,7 +109,11 @@ class FSIDriver3D:
             json.dump(self.config.to_dict(), f, indent=2)
         gcfg = self._geometry_config()
         nx, ny, nz = self.lattice_shape
-        if self.config.lbm_boundary_condition_mode == "duct_velocity_inlet_pressure_outlet":
+        if self.static_solid is not None:
+            if self.static_solid.shape != (nx, ny, nz):
+                raise ValueError(f"static_solid shape {self.static_solid.shape} != lattice {(nx, ny, nz)}")
+            solid = self.static_solid
+        elif self.config.lbm_boundary_condition_mode == "duct_velocity_inlet_pressure_outlet":
             if gcfg is None or gcfg.geometry_type != "duct_flap_proxy":
                 raise ValueError("duct_velocity_inlet_pressure_outlet requires duct_flap_proxy geometry_config")
             if self.lattice_shape != (self.config.n_grid,) * 3:
@@ -124,7 +134,13 @@ class FSIDriver3D:
         mpm_over.update(self.material)
         self.solid = MPMSolid3D(self.sim.make_mpm_config(**mpm_over), n_particles=self.config.n_particles,
                                 device=self.device)
-        if self.config.geometry_type == "box" and self.config.geometry_config_path is None:
+        if self.initial_particles is not None:
+            ip = self.initial_particles
+            self.solid.init_from_numpy(ip["x"], ip["vol0"], ip["mass"], fixed_mask_np=ip.get("fixed"))
+            self.initial_particle_positions = np.asarray(ip["x"], np.float32).copy()
+            tip = ip.get("free_tip")
+            self.free_tip_proxy_mask = None if tip is None else np.asarray(tip, bool)
+        elif self.config.geometry_type == "box" and self.config.geometry_config_path is None:
             self.solid.init_box()
         else:
             cloud = sample_particles(gcfg)
@@ -176,9 +192,56 @@ class FSIDriver3D:
             torch.cuda.synchronize()
         self.timing[key] += time.perf_counter() - t0
 
+    def _graph_period(self):
+        # the captured sequence must return the AA layout parity and the ping-pong slot to their start values
+        S = self.config.lbm_substeps_per_fsi_step if self.config.fsi_exchange_mode == "lbm_subcycled_per_fsi_step" else 1
+        return 1 if S % 2 == 0 else 2
+
     def step_once(self):
         if not self.initialized:
             self.initialize()
+        if self.use_cuda_graph:
+            self._step_graph()
+            return
+        self._step_eager()
+
+    def _step_graph(self):
+        """Replay a CUDA graph of whole FSI steps (captured after one eager step)."""
+        if self._graph is None and self.current_lbm_step == 0:
+            self._step_eager()  # warm-up: allocates lazily created buffers, leaves bc_pending set
+            return
+        period = self._graph_period()
+        if self._graph is None:
+            if self.current_lbm_step % period:
+                self._step_eager()
+                return
+            torch.cuda.synchronize()
+            snap = self._counters()
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g):
+                for _ in range(period):
+                    self._step_eager()
+            self._graph_delta = tuple(b - a for a, b in zip(snap, self._counters()))
+            self._restore_counters(snap)
+            self._graph = g
+            self._graph_steps = 0
+        if self._graph_steps == 0:
+            self._graph.replay()
+            self.lbm._version += 1  # device state advanced outside Python: invalidate readout caches
+            self._graph_steps = period
+        self._graph_steps -= 1
+        d = self._graph_delta
+        self.current_lbm_step += 1
+        self.total_lbm_substeps += d[1] // period
+        self.total_mpm_substeps += d[2] // period
+
+    def _counters(self):
+        return (self.current_lbm_step, self.total_lbm_substeps, self.total_mpm_substeps)
+
+    def _restore_counters(self, snap):
+        self.current_lbm_step, self.total_lbm_substeps, self.total_mpm_substeps = snap
+
+    def _step_eager(self):
         if self.config.fsi_exchange_mode == "lbm_subcycled_per_fsi_step":
             if self.config.coupling_mode != "moving_boundary":
                 raise ValueError("subcycled FSI exchange currently supports only moving_boundary coupling")

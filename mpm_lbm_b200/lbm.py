@@ -87,13 +87,15 @@ class LBMFluid3D:
         self.t_change = torch.zeros(P, dtype=torch.int32, device=dev)
         self.t_diag = torch.zeros((ctypes.sizeof(FsiLbmDiag) + 255) // 256 * 256, dtype=torch.uint8, device=dev)
         self.t_out_pop = None
+        # inlet velocity read on the device every step (bc_vel_x_left_dynamic, fluid.py:287-288)
+        self.t_vin = torch.tensor([self.vx_bcxl, self.vy_bcxl, self.vz_bcxl], dtype=torch.float32, device=dev)
         self.state = FsiLbmState(
             nx=self.nx, ny=self.ny, nz=self.nz, store_fp16=int(self.fp16), pitch=P, pop=ptr(self.t_pop),
             flags=ptr(self.t_flags), nbr=ptr(self.t_nbr), rho=ptr(self.t_rho), vel=ptr(self.t_vel),
             static_solid=ptr(self.t_static), old_solid=ptr(self.t_old), reinit_flag=ptr(self.t_reinit),
             phi=ptr(self.t_phi), smass=ptr(self.t_smass), svel=ptr(self.t_svel), cell_force=ptr(self.t_cf),
             hydro=ptr(self.t_hydro), hpp=ptr(self.t_hpp), accum=ptr(self.t_accum), plane=ptr(self.t_plane),
-            change_list=ptr(self.t_change), diag=ptr(self.t_diag))
+            change_list=ptr(self.t_change), diag=ptr(self.t_diag), vel_left_dyn=ptr(self.t_vin))
         self.params = FsiLbmParams()
         self._penalty = None
         self.parity = 0
@@ -304,7 +306,13 @@ class LBMFluid3D:
     def set_bc_vel_x0(self, vel):
         self.bc_x_left = 2
         self.vx_bcxl, self.vy_bcxl, self.vz_bcxl = (float(v) for v in vel)
+        self.t_vin.copy_(torch.tensor([self.vx_bcxl, self.vy_bcxl, self.vz_bcxl], dtype=torch.float32))
         self._sync_params()
+
+    def set_inlet_velocity_async(self, vel_host):
+        """Stream-ordered update of the x-min inlet velocity from a (pinned) host
+        tensor of 3 floats; steps captured in a CUDA graph read the new value."""
+        self.t_vin.copy_(vel_host, non_blocking=True)
 
     def set_bc_vel_x1(self, vel):
         self.bc_x_right = 2

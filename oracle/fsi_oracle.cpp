@@ -257,8 +257,16 @@ inline int wrap(int i, int n) { return i < 0 ? n - 1 : (i > n - 1 ? 0 : i); }  /
 // fluid.py:431-440 (streaming1, moving=0) and 488-519 (streaming_moving_bounceback, moving=1),
 // including clear_moving_boundary_diagnostics 443-458 and finalize 521-536 when moving.
 template <typename R>
+void lbm_stream_mt(const OrcLbmParams& p, int moving, const R* f, R* F, const int8_t* solid, const R* rho,
+                   const R* solid_vel, R* hydro_force, OrcLbmDiag* d, int threads);
+
+template <typename R>
 void lbm_stream(const OrcLbmParams& p, int moving, const R* f, R* F, const int8_t* solid, const R* rho,
-                const R* solid_vel, R* hydro_force, OrcLbmDiag* d) {
+                const R* solid_vel, R* hydro_force, OrcLbmDiag* d, int threads = 1) {
+  if (threads > 1) {
+    lbm_stream_mt<R>(p, moving, f, F, solid, rho, solid_vel, hydro_force, d, threads);
+    return;
+  }
   Grid<R> g{p.nx, p.ny, p.nz};
   R link_fluid[19][3], link_solid[19][3], corr_sum[19], corr_max[19], max_corr = 0;
   R net_fluid[3] = {0, 0, 0}, net_solid[3] = {0, 0, 0};
@@ -344,6 +352,82 @@ void lbm_stream(const OrcLbmParams& p, int moving, const R* f, R* F, const int8_
       d->bb_fluid_impulse_by_dir[s][a] = (double)link_fluid[s][a];
       d->bb_solid_force_by_dir[s][a] = (double)link_solid[s][a];
     }
+  }
+}
+
+// Same as lbm_stream, parallel over x-slices for the timed CPU baseline; the
+// diagnostic sums use per-thread partials and hydro_force uses atomics, so
+// their summation order differs from the single-thread restatement.
+template <typename R>
+void lbm_stream_mt(const OrcLbmParams& p, int moving, const R* f, R* F, const int8_t* solid, const R* rho,
+                   const R* solid_vel, R* hydro_force, OrcLbmDiag* d, int threads) {
+  Grid<R> g{p.nx, p.ny, p.nz};
+  if (moving) std::memset(hydro_force, 0, sizeof(R) * 3 * g.n());
+  int count[19] = {0};
+  R csum[19] = {0}, cmax[19] = {0}, imp[19][3] = {{0}};
+#pragma omp parallel num_threads(threads)
+  {
+    int lcount[19] = {0};
+    R lsum[19] = {0}, lmax[19] = {0}, limp[19][3] = {{0}};
+#pragma omp for schedule(static)
+    for (int i = 0; i < p.nx; ++i)
+      for (int j = 0; j < p.ny; ++j)
+        for (int k = 0; k < p.nz; ++k) {
+          const int64_t c = g.id(i, j, k);
+          if (solid[c] != 0) continue;
+          for (int s = 0; s < 19; ++s) {
+            const int64_t ip = g.id(wrap(i + E[s][0], p.nx), wrap(j + E[s][1], p.ny), wrap(k + E[s][2], p.nz));
+            if (solid[ip] == 0) {
+              F[ip * 19 + s] = f[c * 19 + s];
+            } else if (!moving) {
+              F[c * 19 + LR[s]] = f[c * 19 + s];
+            } else {
+              const R* uw = solid_vel + ip * 3;
+              const R eu = (R)E[s][0] * uw[0] + (R)E[s][1] * uw[1] + (R)E[s][2] * uw[2];
+              const R corr = (R)-6.0 * (R)W[s] * rho[c] * eu;
+              const R b = f[c * 19 + s] + corr;
+              F[c * 19 + LR[s]] = b;
+              const R ac = std::fabs(corr);
+              lcount[s] += 1;
+              lsum[s] += ac;
+              lmax[s] = std::max(lmax[s], ac);
+              for (int a = 0; a < 3; ++a) {
+                const R fi = (R)E[LR[s]][a] * b - (R)E[s][a] * f[c * 19 + s];
+                limp[s][a] += fi;
+#pragma omp atomic
+                hydro_force[ip * 3 + a] += -fi;
+              }
+            }
+          }
+        }
+#pragma omp critical
+    for (int s = 0; s < 19; ++s) {
+      count[s] += lcount[s];
+      csum[s] += lsum[s];
+      cmax[s] = std::max(cmax[s], lmax[s]);
+      for (int a = 0; a < 3; ++a) imp[s][a] += limp[s][a];
+    }
+  }
+  if (!moving) return;
+  int lc = 0;
+  R fsum[3] = {0, 0, 0}, mc = 0;
+  for (int s = 0; s < 19; ++s) {
+    lc += count[s];
+    mc = std::max(mc, cmax[s]);
+    d->bb_link_count_by_dir[s] = count[s];
+    d->bb_correction_abs_sum_by_dir[s] = (double)csum[s];
+    d->bb_correction_abs_max_by_dir[s] = (double)cmax[s];
+    for (int a = 0; a < 3; ++a) {
+      fsum[a] += imp[s][a];
+      d->bb_fluid_impulse_by_dir[s][a] = (double)imp[s][a];
+      d->bb_solid_force_by_dir[s][a] = -(double)imp[s][a];
+    }
+  }
+  d->bb_link_count = lc;
+  d->bb_max_correction = (double)mc;
+  for (int a = 0; a < 3; ++a) {
+    d->bb_net_fluid_impulse[a] = (double)fsum[a];
+    d->bb_net_solid_force[a] = -(double)fsum[a];
   }
 }
 
@@ -1178,8 +1262,8 @@ void couple_reaction(int kind, const OrcCouplingParams& cp, const OrcLbmParams& 
     lbm_collide<R>(*p, F, rho, v, cf, solid, f, threads);                                                          \
   }                                                                                                                \
   extern "C" void orc##SUF##_lbm_stream(const OrcLbmParams* p, int moving, const R* f, R* F, const int8_t* solid,  \
-                                        const R* rho, const R* sv, R* hydro, OrcLbmDiag* d) {                     \
-    lbm_stream<R>(*p, moving, f, F, solid, rho, sv, hydro, d);                                                     \
+                                        const R* rho, const R* sv, R* hydro, OrcLbmDiag* d, int threads) {        \
+    lbm_stream<R>(*p, moving, f, F, solid, rho, sv, hydro, d, threads);                                            \
   }                                                                                                                \
   extern "C" void orc##SUF##_lbm_boundary(const OrcLbmParams* p, R* F, const R* rho, const R* v,                   \
                                           const int8_t* solid, OrcLbmDiag* d) {                                   \

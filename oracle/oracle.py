@@ -259,12 +259,12 @@ class OracleLBM:
     def streaming1(self):
         _fn(self.pfx, "lbm_stream")(ctypes.byref(self.p), 0, _ptr(self.f), _ptr(self.F), _ptr(self.solid),
                                     _ptr(self.rho), _ptr(self.solid_vel), _ptr(self.hydro_force),
-                                    ctypes.byref(self.diag))
+                                    ctypes.byref(self.diag), self.threads)
 
     def streaming_moving_bounceback(self):
         _fn(self.pfx, "lbm_stream")(ctypes.byref(self.p), 1, _ptr(self.f), _ptr(self.F), _ptr(self.solid),
                                     _ptr(self.rho), _ptr(self.solid_vel), _ptr(self.hydro_force),
-                                    ctypes.byref(self.diag))
+                                    ctypes.byref(self.diag), self.threads)
 
     def Boundary_condition(self):
         _fn(self.pfx, "lbm_boundary")(ctypes.byref(self.p), _ptr(self.F), _ptr(self.rho), _ptr(self.v),

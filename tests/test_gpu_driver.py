@@ -6,7 +6,8 @@ modes none / penalty / moving_boundary (engineering and link-area) /
 subcycled / duct with the limited regularized open boundary.  The CUDA driver
 runs the same config; tolerances (FP32 after a few coupled steps): fields
 rtol 1e-3 on rho/v-scale quantities, particle positions atol 1e-6 (normalised
-units), diagnostics rows rtol 2e-3; masks and link counts exact.
+units), diagnostics rows rtol 2e-3 / atol 2e-7 (the reference's f32 rest state
+carries ~4e-9 round-off velocities); masks and link counts exact.
 """
 
 import json
@@ -69,4 +70,4 @@ def test_driver_matches_reference(name, tmp_path):
                        "total_mpm_substeps"):
                 assert int(got[k]) == int(v), (k, got[k], v)
             else:
-                assert np.isclose(got[k], v, rtol=2e-3, atol=1e-9), (k, got[k], v)
+                assert np.isclose(got[k], v, rtol=2e-3, atol=2e-7), (k, got[k], v)

@@ -1,6 +1,9 @@
 """GPU parity of the LBM step (CUDA path through the C ABI) against the CPU
 oracle on seeded inputs.  Tolerances (FP32): populations rtol 2e-5 /
-atol 1e-7 after N steps; masks and link counts bit-exact."""
+atol 1e-7 after N steps; link forces rtol 1e-4 / atol 1e-7 (a solid cell sums
+up to 18 partly cancelling link terms whose order differs between the
+oracle's sequential loop and device atomics); masks and link counts
+bit-exact."""
 
 import numpy as np
 import pytest
@@ -102,7 +105,7 @@ def test_moving_bounceback_matches_oracle():
         ora.step_moving_bounceback()
         gpu.step_moving_bounceback()
         compare(ora, gpu)
-        np.testing.assert_allclose(gpu.hydro_force.to_numpy(), ora.hydro_force, rtol=1e-4, atol=1e-8)
+        np.testing.assert_allclose(gpu.hydro_force.to_numpy(), ora.hydro_force, rtol=1e-4, atol=1e-7)
         go, oo = gpu.get_moving_boundary_directional_stats(), ora.get_moving_boundary_directional_stats()
         np.testing.assert_array_equal(go["link_count_by_dir"], oo["link_count_by_dir"])
         np.testing.assert_allclose(go["solid_force_by_dir"], oo["solid_force_by_dir"], rtol=1e-4, atol=1e-7)
@@ -172,7 +175,7 @@ def test_dynamic_mask_reinit_matches_oracle(steps_before):
             ora.step_moving_bounceback()
             gpu.step_moving_bounceback()
         compare(ora, gpu)
-        np.testing.assert_allclose(gpu.hydro_force.to_numpy(), ora.hydro_force, rtol=1e-4, atol=1e-8)
+        np.testing.assert_allclose(gpu.hydro_force.to_numpy(), ora.hydro_force, rtol=1e-4, atol=1e-7)
 
 
 def test_subcycled_accumulator_matches_oracle():
@@ -187,8 +190,8 @@ def test_subcycled_accumulator_matches_oracle():
             o.accumulate_moving_boundary_force_sample()
     for o in (ora, gpu):
         o.finalize_moving_boundary_force_accumulator()
-    np.testing.assert_allclose(gpu.hydro_force.to_numpy(), ora.hydro_force, rtol=1e-4, atol=1e-8)
-    np.testing.assert_allclose(gpu.hydro_force_accum.to_numpy(), ora.hydro_force_accum, rtol=1e-4, atol=1e-8)
+    np.testing.assert_allclose(gpu.hydro_force.to_numpy(), ora.hydro_force, rtol=1e-4, atol=1e-7)
+    np.testing.assert_allclose(gpu.hydro_force_accum.to_numpy(), ora.hydro_force_accum, rtol=1e-4, atol=1e-7)
     a, b = gpu.get_moving_boundary_accumulation_stats(), ora.get_moving_boundary_accumulation_stats()
     assert a["mb_subcycle_force_sample_count"] == b["mb_subcycle_force_sample_count"] == 3
     np.testing.assert_allclose(a["mb_subcycle_force_accum_norm_max"], b["mb_subcycle_force_accum_norm_max"], rtol=1e-4)
@@ -232,5 +235,5 @@ def test_penalty_step_matches_oracle():
         ora.step()
         gpu.step()
         compare(ora, gpu)
-        np.testing.assert_allclose(gpu.cell_force.to_numpy(), ora.cell_force, rtol=1e-4, atol=1e-10)
-        np.testing.assert_allclose(gpu.hydro_force.to_numpy(), ora.hydro_force, rtol=1e-4, atol=1e-10)
+        np.testing.assert_allclose(gpu.cell_force.to_numpy(), ora.cell_force, rtol=1e-4, atol=2e-9)
+        np.testing.assert_allclose(gpu.hydro_force.to_numpy(), ora.hydro_force, rtol=1e-4, atol=2e-9)
