@@ -246,6 +246,57 @@ int fsi_mpm_grid_update(const FsiGrid* g, const FsiMpmParams* mp, void* stream);
  * F update, damping / z-lock controls, fixed-base reset. */
 int fsi_mpm_g2p(const FsiParticles* pt, const FsiGrid* g, const FsiMpmParams* mp, void* stream);
 
+/* ---- binned MPM substep --------------------------------------------------
+ * The same substep as clear -> p2g -> reaction -> grid_update -> g2p above
+ * (one call of MPMSolid3D.substep plus the coupler's reaction transfer, as
+ * driven by fsi_driver.py's MPM loops), organised around particle bins:
+ *   - fsi_mpm_bin sorts particle ids by 4x4x4-cell block of their B-spline
+ *     base cell and cuts every bin into chunks of at most FSI_BIN_CHUNK
+ *     particles (bins may go stale between calls: that costs speed only);
+ *   - fsi_mpm_substep_binned scatters each chunk into a shared-memory tile
+ *     covering the chunk's stencil box and flushes the tile with one atomic
+ *     per touched node value, then gathers with the grid update evaluated per
+ *     node while staging.  It alternates between two grid buffers: a substep
+ *     with buffer b leaves momentum (not velocity), mass and f_ext in grid[b]
+ *     and zeroes the boxes recorded by the previous substep in grid[1 - b],
+ *     so no dense pass over the grid is made. */
+#define FSI_BIN_CHUNK 128
+#define FSI_BIN_EDGE 4
+
+/* count, start and chunk must be 16-byte aligned */
+typedef struct FsiMpmBins {
+  int32_t n_bins;       /* ceil(n_grid / FSI_BIN_EDGE)^3 */
+  int32_t max_chunks;   /* capacity of chunk[] and of each half of box[] */
+  int32_t* key;         /* [n_particles] bin of each particle */
+  int32_t* count;       /* [n_bins] zero before the first fsi_mpm_bin; kept zero after each call */
+  int32_t* start;       /* [n_bins] end offset of each bin in perm after fsi_mpm_bin */
+  int32_t* perm;        /* [n_particles] particle ids ordered by bin */
+  int32_t* chunk;       /* [max_chunks][2] (first slot in perm, particle count) */
+  int32_t* box;         /* [2][max_chunks][6] node box (lo xyz, hi xyz) touched per chunk and buffer */
+  int32_t* meta;        /* [4] chunk count, records in box[0], records in box[1], overflowed chunks;
+                           zero before the first call */
+} FsiMpmBins;
+
+/* n_bins and max_chunks for a particle count and grid edge */
+int fsi_mpm_bins_layout(int32_t n_particles, int32_t n_grid, int32_t* n_bins, int32_t* max_chunks);
+
+/* (re)bin the particles at their current positions */
+int fsi_mpm_bin(const FsiParticles* pt, const FsiGrid* g, const FsiMpmParams* mp, const FsiMpmBins* bins,
+                void* stream);
+
+/* One MPM substep into grid[buffer] (buffer 0 or 1; grid[buffer] must be zero
+ * apart from the boxes recorded for it, which the previous substep with the
+ * other buffer cleared).  With cp != NULL the reaction transfer of kind
+ * cp->kind is added (s, hydro as for fsi_reaction_to_grid) and its reductions
+ * go to stats[buffer]; the reaction part of stats[1 - buffer] is zeroed. */
+int fsi_mpm_substep_binned(const FsiParticles* pt, const FsiGrid grid[2], const FsiMpmBins* bins,
+                           const FsiMpmParams* mp, int32_t buffer, const FsiLbmState* s, const float* hydro,
+                           const FsiCouplingParams* cp, FsiCouplingStats stats[2], void* stream);
+
+/* grid velocity after a binned substep (the grid_v of the reference after
+ * grid_update) from grid's momentum, mass and f_ext, into out [3][n^3] */
+int fsi_mpm_grid_velocity(const FsiGrid* g, const FsiMpmParams* mp, float* out, void* stream);
+
 /* ---- misc --------------------------------------------------------------- */
 int fsi_abi_version(void);
 int fsi_last_error(char* buf, size_t len);

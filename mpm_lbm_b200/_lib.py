@@ -62,6 +62,11 @@ class FsiGrid(ctypes.Structure):
     _fields_ = [("n", c_i32), ("pad", c_i32), ("v", c_p), ("m", c_p), ("f_ext", c_p)]
 
 
+class FsiMpmBins(ctypes.Structure):
+    _fields_ = [("n_bins", c_i32), ("max_chunks", c_i32), ("key", c_p), ("count", c_p), ("start", c_p),
+                ("perm", c_p), ("chunk", c_p), ("box", c_p), ("meta", c_p)]
+
+
 class FsiMpmParams(ctypes.Structure):
     _fields_ = [("dx", c_f32), ("inv_dx", c_f32), ("dt", c_f32), ("mu", c_f32), ("la", c_f32),
                 ("gravity", c_f32 * 3), ("damping", c_f32), ("bound", c_i32), ("lock_z", c_i32), ("pad", c_i32)]
@@ -85,7 +90,7 @@ class FsiCouplingStats(ctypes.Structure):
 STRUCTS = {
     "FsiLbmDiag": FsiLbmDiag, "FsiLbmState": FsiLbmState, "FsiLbmParams": FsiLbmParams, "FsiStepCtl": FsiStepCtl,
     "FsiParticles": FsiParticles, "FsiGrid": FsiGrid, "FsiMpmParams": FsiMpmParams,
-    "FsiCouplingParams": FsiCouplingParams, "FsiCouplingStats": FsiCouplingStats,
+    "FsiCouplingParams": FsiCouplingParams, "FsiCouplingStats": FsiCouplingStats, "FsiMpmBins": FsiMpmBins,
 }
 
 # entry point -> argtypes (all return int)
@@ -104,6 +109,11 @@ SIGNATURES = {
     "fsi_mpm_p2g": [_P(FsiParticles), _P(FsiGrid), _P(FsiMpmParams), c_p],
     "fsi_mpm_grid_update": [_P(FsiGrid), _P(FsiMpmParams), c_p],
     "fsi_mpm_g2p": [_P(FsiParticles), _P(FsiGrid), _P(FsiMpmParams), c_p],
+    "fsi_mpm_bins_layout": [c_i32, c_i32, _P(c_i32), _P(c_i32)],
+    "fsi_mpm_bin": [_P(FsiParticles), _P(FsiGrid), _P(FsiMpmParams), _P(FsiMpmBins), c_p],
+    "fsi_mpm_substep_binned": [_P(FsiParticles), _P(FsiGrid), _P(FsiMpmBins), _P(FsiMpmParams), c_i32,
+                               _P(FsiLbmState), c_p, _P(FsiCouplingParams), c_p, c_p],
+    "fsi_mpm_grid_velocity": [_P(FsiGrid), _P(FsiMpmParams), c_p, c_p],
     "fsi_abi_version": [],
     "fsi_last_error": [ctypes.c_char_p, ctypes.c_size_t],
 }

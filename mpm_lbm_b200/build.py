@@ -19,8 +19,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(BUILD, "libfsi_b200.so")
-SOURCES = ["fsi_abi.cu", "lbm_kernels.cu", "mpm_kernels.cu"]
-HEADERS = ["common.cuh", "d3q19.cuh", "polar3.cuh"]
+SOURCES = ["fsi_abi.cu", "lbm_kernels.cu", "mpm_kernels.cu", "mpm_binned.cu"]
+HEADERS = ["common.cuh", "d3q19.cuh", "polar3.cuh", "mpm_common.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I" + os.path.join(ROOT, "include")]
 

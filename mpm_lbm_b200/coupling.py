@@ -15,14 +15,36 @@ AREA_POLICIES = ("uniform", "inverse_length", "length")
 
 
 class _StatsBuffer:
-    def __init__(self, device):
-        self.t = torch.zeros((ctypes.sizeof(FsiCouplingStats) + 255) // 256 * 256, dtype=torch.uint8, device=device)
+    """count consecutive FsiCouplingStats records on the device."""
 
-    def read(self) -> FsiCouplingStats:
-        return FsiCouplingStats.from_buffer_copy(self.t[: ctypes.sizeof(FsiCouplingStats)].cpu().numpy().tobytes())
+    def __init__(self, device, count=1):
+        size = ctypes.sizeof(FsiCouplingStats)
+        self.t = torch.zeros((size * count + 255) // 256 * 256, dtype=torch.uint8, device=device)
+
+    def read(self, i=0) -> FsiCouplingStats:
+        size = ctypes.sizeof(FsiCouplingStats)
+        return FsiCouplingStats.from_buffer_copy(self.t[i * size: (i + 1) * size].cpu().numpy().tobytes())
 
     def ptr(self):
         return ptr(self.t)
+
+
+class _BinnedReaction:
+    """Reaction transfer fused into MPMSolid3D.substep_binned: the kernel
+    writes the reductions of a substep with grid buffer b to record b."""
+
+    def _init_binned(self, device):
+        self.binned_stats = _StatsBuffer(device, count=2)
+        self._binned_slot = None
+
+    def _binned_args(self, lbm):
+        self._lbm = lbm
+        return lbm.state, lbm._hydro_tensor(), self.params, self.binned_stats.ptr()
+
+    def _reaction_stats(self) -> FsiCouplingStats:
+        if self._binned_slot is not None:
+            return self.binned_stats.read(self._binned_slot)
+        return self.stats.read()
 
 
 def _base_params(sim_config):
@@ -66,7 +88,7 @@ class MPMToLBMProjector3D:
                 "cell_volume_norm": float(self.cell_volume_norm)}
 
 
-class PenaltyFSICoupler3D:
+class PenaltyFSICoupler3D(_BinnedReaction):
     """penalty.py:5-152.  The penalty force is built inside the next LBM step
     from the same macroscopic state the reference uses (the step's fused
     prologue), so build_penalty_force() only arms it."""
@@ -92,6 +114,7 @@ class PenaltyFSICoupler3D:
         self.params.kind = 0
         self.params.reaction_scale = self.reaction_scale
         self.stats = _StatsBuffer(device if device is not None else "cuda")
+        self._init_binned(device if device is not None else "cuda")
         self._lbm = None
 
     def clear_force_fields(self, lbm):
@@ -103,11 +126,12 @@ class PenaltyFSICoupler3D:
         self._lbm = lbm
 
     def add_lbm_reaction_to_mpm_grid(self, solid, lbm):
+        self._binned_slot = None
         call("fsi_reaction_to_grid", ctypes.byref(lbm.state), ptr(lbm._hydro_tensor()), ctypes.byref(solid.particles),
              ctypes.byref(solid.grid), ctypes.byref(self.params), self.stats.ptr(), stream_handle())
 
     def get_stats(self):
-        s = self.stats.read()
+        s = self._reaction_stats()
         out = {"n_grid": self.n_grid, "dx_norm": self.dx_norm, "inv_dx_norm": self.inv_dx_norm,
                "lbm_dt_phys": self.lbm_dt_phys, "beta_lbm": self.beta_lbm, "phi_min": self.phi_min,
                "force_cap_lbm": self.force_cap_lbm, "reaction_scale": self.reaction_scale,
@@ -124,7 +148,7 @@ class PenaltyFSICoupler3D:
         return out
 
 
-class MovingBoundaryFSICoupler3D:
+class MovingBoundaryFSICoupler3D(_BinnedReaction):
     """moving_boundary.py:5-130 (engineering reaction transfer)."""
 
     kind = 1
@@ -148,12 +172,14 @@ class MovingBoundaryFSICoupler3D:
         self.params.force_cap = self.force_cap_norm
         self.params.phi_min = self.phi_min
         self.stats = _StatsBuffer(device if device is not None else "cuda")
+        self._init_binned(device if device is not None else "cuda")
 
     def clear_reaction_diagnostics(self):
         """The reaction entry point clears its reductions itself."""
         return None
 
     def _react(self, solid, lbm):
+        self._binned_slot = None
         call("fsi_reaction_to_grid", ctypes.byref(lbm.state), ptr(lbm._hydro_tensor()), ctypes.byref(solid.particles),
              ctypes.byref(solid.grid), ctypes.byref(self.params), self.stats.ptr(), stream_handle())
 
@@ -161,7 +187,7 @@ class MovingBoundaryFSICoupler3D:
         self._react(solid, lbm)
 
     def _common_stats(self):
-        s = self.stats.read()
+        s = self._reaction_stats()
         return s, {"n_grid": self.n_grid, "dx_norm": self.dx_norm, "inv_dx_norm": self.inv_dx_norm,
                    "lbm_dt_phys": self.lbm_dt_phys, "reaction_scale": self.reaction_scale,
                    "force_cap_norm": self.force_cap_norm, "phi_min": self.phi_min,

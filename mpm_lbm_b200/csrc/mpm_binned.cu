@@ -1,0 +1,686 @@
+// Binned MPM substep: particles sorted by 4x4x4-cell block, P2G (+ reaction
+// transfer) staged in a shared-memory tile per chunk of a bin, G2P with the
+// grid update evaluated while staging the chunk's node box, and two grid
+// buffers so that only the boxes touched one substep earlier are zeroed.
+//
+// The per-particle and per-node arithmetic is the one of the one-phase
+// kernels (mpm_common.cuh): solid.py:212-315 and the reaction transfers of
+// penalty.py:90-129, moving_boundary.py:58-110, link_area.py:84-193.  Only
+// the summation order of the grid sums differs (shared-memory atomics, then
+// one global atomic per chunk and touched node value).
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <climits>
+
+#include "common.cuh"
+#include "mpm_common.cuh"
+
+namespace fsi {
+namespace {
+
+constexpr int kChunk = FSI_BIN_CHUNK;  // particles per chunk = threads per CTA
+constexpr int kEdge = FSI_BIN_EDGE;
+// nodes staged per CTA: a chunk of one bin spans (4 + 2)^3 nodes; the rest
+// absorbs drift since the last binning.  7 floats per node in P2G = 35 KB.
+constexpr int kTileCap = 1280;
+
+__device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+// bin of a particle: the cell block of its B-spline base cell (solid.py:222-223)
+__device__ __forceinline__ int particle_bin(const float X[3], float inv_dx, int G, int nb) {
+  int c[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const float Xp = __fmul_rn(X[a], inv_dx);
+    c[a] = clampi((int)(Xp - 0.5f), 0, G - 1) / kEdge;
+  }
+  return (c[2] * nb + c[1]) * nb + c[0];
+}
+
+__global__ void k_bin_count(FsiParticles pt, float inv_dx, int G, int nb, int32_t* __restrict__ key,
+                            int32_t* __restrict__ count) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= pt.n) return;
+  const int n = pt.n;
+  const float X[3] = {pt.x[p], pt.x[n + p], pt.x[2 * n + p]};
+  const int k = particle_bin(X, inv_dx, G, nb);
+  key[p] = k;
+  atomicAdd(count + k, 1);
+}
+
+// One CTA: exclusive scan of the bin counts and of the chunks per bin, the
+// chunk table, and the counts reset to zero for the next binning.  Each
+// thread owns a contiguous, 4-aligned range of bins and reads it with 16-byte
+// loads, so the pass costs a few memory latencies rather than one per bin.
+__device__ __forceinline__ int4 ld_bins4(const int32_t* p, int b, int b1) {
+  if (b + 4 <= b1) return *reinterpret_cast<const int4*>(p + b);
+  int4 v = make_int4(0, 0, 0, 0);
+  if (b < b1) v.x = p[b];
+  if (b + 1 < b1) v.y = p[b + 1];
+  if (b + 2 < b1) v.z = p[b + 2];
+  return v;
+}
+
+__global__ __launch_bounds__(1024) void k_bin_scan(int nbins, int32_t* __restrict__ count,
+                                                   int32_t* __restrict__ start, int2* __restrict__ chunk,
+                                                   int32_t* __restrict__ meta) {
+  __shared__ int s_p[32], s_c[32];
+  const int T = blockDim.x, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int per = ((nbins + T - 1) / T + 3) & ~3;
+  const int b0 = min(tid * per, nbins), b1 = min(b0 + per, nbins);
+  int ps = 0, cs = 0;
+  for (int b = b0; b < b1; b += 4) {
+    const int4 c = ld_bins4(count, b, b1);
+    ps += c.x + c.y + c.z + c.w;
+    cs += (c.x + kChunk - 1) / kChunk + (c.y + kChunk - 1) / kChunk + (c.z + kChunk - 1) / kChunk +
+          (c.w + kChunk - 1) / kChunk;
+  }
+  int pi = ps, ci = cs;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int a = __shfl_up_sync(0xffffffffu, pi, o), c = __shfl_up_sync(0xffffffffu, ci, o);
+    if (lane >= o) {
+      pi += a;
+      ci += c;
+    }
+  }
+  if (lane == 31) {
+    s_p[wid] = pi;
+    s_c[wid] = ci;
+  }
+  __syncthreads();
+  if (wid == 0) {
+    const int nw = T >> 5;
+    const int a0 = lane < nw ? s_p[lane] : 0, c0 = lane < nw ? s_c[lane] : 0;
+    int a = a0, c = c0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int x = __shfl_up_sync(0xffffffffu, a, o), y = __shfl_up_sync(0xffffffffu, c, o);
+      if (lane >= o) {
+        a += x;
+        c += y;
+      }
+    }
+    if (lane < nw) {
+      s_p[lane] = a - a0;
+      s_c[lane] = c - c0;
+    }
+  }
+  __syncthreads();
+  int po = s_p[wid] + pi - ps, co = s_c[wid] + ci - cs;
+  for (int b = b0; b < b1; b += 4) {
+    const int4 c4 = ld_bins4(count, b, b1);
+    const int cv[4] = {c4.x, c4.y, c4.z, c4.w};
+    int st[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      st[q] = po;
+      for (int j = 0; j < cv[q]; j += kChunk) chunk[co++] = make_int2(po + j, min(kChunk, cv[q] - j));
+      po += cv[q];
+    }
+    if (b + 4 <= b1) {
+      *reinterpret_cast<int4*>(start + b) = make_int4(st[0], st[1], st[2], st[3]);
+      *reinterpret_cast<int4*>(count + b) = make_int4(0, 0, 0, 0);
+    } else {
+      for (int q = 0; q < 4 && b + q < b1; ++q) {
+        start[b + q] = st[q];
+        count[b + q] = 0;
+      }
+    }
+  }
+  if (tid == T - 1) meta[0] = co;
+}
+
+__global__ void k_bin_scatter(int n, const int32_t* __restrict__ key, int32_t* __restrict__ cursor,
+                              int32_t* __restrict__ perm) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  perm[atomicAdd(cursor + key[p], 1)] = p;
+}
+
+struct Box {
+  int lo[3], ext[3];
+  int vol;
+};
+
+__device__ __forceinline__ Box load_box(const int32_t* r) {
+  Box b;
+  long long v = 1;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    b.lo[a] = r[a];
+    b.ext[a] = max(r[3 + a] - r[a] + 1, 0);
+    v *= b.ext[a];
+  }
+  b.vol = v > INT_MAX ? INT_MAX : (int)v;
+  return b;
+}
+
+__device__ __forceinline__ int64_t box_node(const Box& b, int li, int G) {
+  const int i = b.lo[0] + li % b.ext[0];
+  const int j = b.lo[1] + (li / b.ext[0]) % b.ext[1];
+  const int k = b.lo[2] + li / (b.ext[0] * b.ext[1]);
+  return ((int64_t)k * G + j) * G + i;
+}
+
+// quadratic B-spline weight of offset o for the fractional position f (the
+// expressions of bspline())
+__device__ __forceinline__ float bspline_w(float f, int o) {
+  return o == 0 ? 0.5f * (1.5f - f) * (1.5f - f) : (o == 1 ? 0.75f - (f - 1.0f) * (f - 1.0f) : 0.5f * (f - 0.5f) * (f - 0.5f));
+}
+
+// Fallbacks for chunks whose node box does not fit the shared-memory tile
+// (bins gone stale): rolled loops, so that the staged path stays compact.
+__device__ __forceinline__ void g2p_gather_global(const FsiGrid& g, const FsiMpmParams& mp, const BSpline& b,
+                                                  float nvl[3], float nC[9]) {
+  const int G = g.n;
+  const int64_t N = (int64_t)G * G * G;
+  const float s4 = 4.0f * mp.inv_dx * mp.inv_dx;
+#pragma unroll 1
+  for (int o = 0; o < 27; ++o) {
+    const int ox = o / 9, oy = (o / 3) % 3, oz = o % 3;
+    const int I = b.base[0] + ox, Jj = b.base[1] + oy, K = b.base[2] + oz;
+    if (I < 0 || I >= G || Jj < 0 || Jj >= G || K < 0 || K >= G) continue;
+    const int64_t node = ((int64_t)K * G + Jj) * G + I;
+    const float m = g.m[node];
+    const float P[3] = {g.v[node], g.v[N + node], g.v[2 * N + node]};
+    float gv[3] = {P[0], P[1], P[2]};
+    if (m > 0.0f) {
+      const float f[3] = {g.f_ext[node], g.f_ext[N + node], g.f_ext[2 * N + node]};
+      grid_node_velocity(P, m, f, I, Jj, K, G, mp, gv);
+    }
+    const float dpos[3] = {((float)ox - b.fx[0]) * mp.dx, ((float)oy - b.fx[1]) * mp.dx, ((float)oz - b.fx[2]) * mp.dx};
+    const float w = bspline_w(b.fx[0], ox) * bspline_w(b.fx[1], oy) * bspline_w(b.fx[2], oz);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      nvl[a] += w * gv[a];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) nC[a * 3 + c] += (w * gv[a]) * dpos[c] * s4;
+    }
+  }
+}
+
+__device__ __forceinline__ void reaction_global(const LatView& L, const float* hydro, const float* phi,
+                                                const FsiCouplingParams& cp, const BSpline& b, float Jp, float vol0,
+                                                float scale, ReactParticle& r) {
+  float hs[3] = {0.f, 0.f, 0.f}, ps = 0.f;
+#pragma unroll 1
+  for (int o = 0; o < 27; ++o) {
+    const int ox = o / 9, oy = (o / 3) % 3, oz = o % 3;
+    const int I = b.base[0] + ox, Jj = b.base[1] + oy, K = b.base[2] + oz;
+    if (I < 0 || I >= L.nx || Jj < 0 || Jj >= L.ny || K < 0 || K >= L.nz) continue;
+    const float w = bspline_w(b.fx[0], ox) * bspline_w(b.fx[1], oy) * bspline_w(b.fx[2], oz);
+    const int64_t c = lat_cell(L, I, Jj, K);
+    hs[0] += w * hydro[c];
+    hs[1] += w * hydro[L.pitch + c];
+    hs[2] += w * hydro[2 * L.pitch + c];
+    if (cp.kind != 0) ps += w * phi[c];
+  }
+  reaction_from_sums(cp, hs, ps, Jp, vol0, scale, r);
+}
+
+// per-particle values handed from phase 1 to phase 2 of the P2G kernel
+enum { kPfx = 0, kPbase = 3, kPmv = 6, kPaff = 9, kPmass = 18, kPpf = 19, kPn = 22 };
+
+// P2G (+ reaction) of the chunks of this CTA into grid buffer g.
+//  phase 0: the chunk's node box; for the reaction, the box's lattice hydro
+//           force and phi staged in shared memory;
+//  phase 1: one thread per particle: stress and affine momentum (FP64 polar
+//           rotation) and the reaction force gathered from the staged box;
+//  phase 2: the 27 x chunk (particle, node) pairs spread over the threads, so
+//           the lanes of one shared-memory atomic touch distinct nodes;
+//  phase 3: one global atomic per touched node value.
+template <bool REACT>
+__global__ __launch_bounds__(kChunk) void k_p2g_binned(FsiParticles pt, FsiGrid g, FsiMpmParams mp,
+                                                       const int32_t* __restrict__ perm,
+                                                       const int2* __restrict__ chunks, int32_t* meta, int32_t* box,
+                                                       int buf, LatView L, const float* __restrict__ hydro,
+                                                       const float* __restrict__ phi, FsiCouplingParams cp,
+                                                       FsiCouplingStats* st, const FsiLbmDiag* diag) {
+  __shared__ float tile[7 * kTileCap];
+  __shared__ float sp[kPn][kChunk];
+  __shared__ int s_lo[3], s_hi[3];
+  __shared__ float s_scale;
+  const int tid = threadIdx.x;
+  const int G = g.n;
+  const int64_t N = (int64_t)G * G * G;
+  const int nch = meta[0];
+  if (blockIdx.x == 0 && tid == 0) meta[1 + buf] = nch;
+  if (REACT && tid == 0) {
+    float raw = 1.f;
+    s_scale = cp.kind == 2 ? link_area_scale(diag, cp, &raw) : 1.0f;
+    if (blockIdx.x == 0 && cp.kind == 2) {
+      st->area_scale = s_scale;
+      st->raw_area_scale = raw;
+    }
+  }
+  float* const dst[7] = {g.v, g.v + N, g.v + 2 * N, g.m, g.f_ext, g.f_ext + N, g.f_ext + 2 * N};
+  int n_act = 0;
+  float pmax = 0.f, gmax = 0.f;
+  double pn[3] = {0.0, 0.0, 0.0}, gn[3] = {0.0, 0.0, 0.0};
+  for (int c = blockIdx.x; c < nch; c += gridDim.x) {
+    __syncthreads();  // the previous chunk's flush has read the tile
+    if (tid < 3) {
+      s_lo[tid] = INT_MAX;
+      s_hi[tid] = INT_MIN;
+    }
+    const int2 ch = chunks[c];
+    const bool live = tid < ch.y;
+    const int p = live ? perm[ch.x + tid] : 0;
+    float X[3] = {0.f, 0.f, 0.f};
+    if (live) {
+      X[0] = pt.x[p];
+      X[1] = pt.x[pt.n + p];
+      X[2] = pt.x[2 * pt.n + p];
+    }
+    BSpline b;
+    bspline(X, mp.inv_dx, b);
+    __syncthreads();
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const int lo = __reduce_min_sync(0xffffffffu, live ? b.base[a] : INT_MAX);
+      const int hi = __reduce_max_sync(0xffffffffu, live ? b.base[a] : INT_MIN);
+      if ((tid & 31) == 0) {
+        atomicMin(&s_lo[a], lo);
+        atomicMax(&s_hi[a], hi);
+      }
+    }
+    __syncthreads();
+    int32_t rec[6];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      rec[a] = max(s_lo[a], 0);
+      rec[3 + a] = s_hi[a] == INT_MIN ? -1 : min(min(s_hi[a], G) + 2, G - 1);
+    }
+    const Box bx = load_box(rec);
+    const bool staged = bx.vol <= kTileCap;
+    if (tid == 0) {
+#pragma unroll
+      for (int a = 0; a < 6; ++a) box[6 * c + a] = rec[a];
+      if (!staged) atomicAdd(meta + 3, 1);
+    }
+    const int nv = staged ? bx.vol : 0;
+    // ---- phase 0: lattice hydro / phi of the box (zero outside the lattice)
+    if (REACT && staged) {
+      for (int li = tid; li < nv; li += kChunk) {
+        const int i = bx.lo[0] + li % bx.ext[0];
+        const int j = bx.lo[1] + (li / bx.ext[0]) % bx.ext[1];
+        const int k = bx.lo[2] + li / (bx.ext[0] * bx.ext[1]);
+        float h0 = 0.f, h1 = 0.f, h2 = 0.f, ph = 0.f;
+        if (i < L.nx && j < L.ny && k < L.nz) {
+          const int64_t cell = lat_cell(L, i, j, k);
+          h0 = hydro[cell];
+          h1 = hydro[L.pitch + cell];
+          h2 = hydro[2 * L.pitch + cell];
+          if (cp.kind != 0) ph = phi[cell];
+        }
+        tile[li] = h0;
+        tile[nv + li] = h1;
+        tile[2 * nv + li] = h2;
+        tile[3 * nv + li] = ph;
+      }
+      __syncthreads();
+    }
+    // ---- phase 1: per particle
+    if (live) {
+      P2GParticle q;
+      p2g_particle(pt, p, mp, q);
+      pt.Jp[p] = q.J;
+      float pf[3] = {0.f, 0.f, 0.f};
+      if (REACT) {
+        ReactParticle r;
+        if (staged) {
+          // reaction_particle over the staged box: the same products, in the
+          // same order; cells outside the lattice hold zeros
+          float hs[3] = {0.f, 0.f, 0.f}, ps = 0.f;
+#pragma unroll
+          for (int ox = 0; ox < 3; ++ox)
+#pragma unroll
+            for (int oy = 0; oy < 3; ++oy)
+#pragma unroll
+              for (int oz = 0; oz < 3; ++oz) {
+                const int I = b.base[0] + ox, Jj = b.base[1] + oy, K = b.base[2] + oz;
+                if (I < 0 || I >= L.nx || Jj < 0 || Jj >= L.ny || K < 0 || K >= L.nz) continue;
+                const float w = b.w[0][ox] * b.w[1][oy] * b.w[2][oz];
+                const int li = ((K - bx.lo[2]) * bx.ext[1] + (Jj - bx.lo[1])) * bx.ext[0] + (I - bx.lo[0]);
+                hs[0] += w * tile[li];
+                hs[1] += w * tile[nv + li];
+                hs[2] += w * tile[2 * nv + li];
+                if (cp.kind != 0) ps += w * tile[3 * nv + li];
+              }
+          reaction_from_sums(cp, hs, ps, q.J, pt.vol0[p], s_scale, r);
+        } else {
+          reaction_global(L, hydro, phi, cp, b, q.J, pt.vol0[p], s_scale, r);
+        }
+        n_act += r.act ? 1 : 0;
+        pmax = fmaxf(pmax, r.pnorm);
+        if (r.gated)
+          for (int a = 0; a < 3; ++a) pn[a] += (double)r.pf[a];
+        if (r.scatter)
+          for (int a = 0; a < 3; ++a) pf[a] = r.pf[a];
+      }
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        sp[kPfx + a][tid] = b.fx[a];
+        sp[kPbase + a][tid] = __int_as_float(b.base[a]);
+        sp[kPmv + a][tid] = q.mv[a];
+        sp[kPpf + a][tid] = pf[a];
+      }
+#pragma unroll
+      for (int a = 0; a < 9; ++a) sp[kPaff + a][tid] = q.aff[a];
+      sp[kPmass][tid] = q.mass;
+    }
+    __syncthreads();
+    for (int i = tid; i < 7 * nv; i += kChunk) tile[i] = 0.f;
+    __syncthreads();
+    // ---- phase 2: (particle, node) pairs
+    const int npair = ch.y * 27;
+    for (int idx = tid; idx < npair; idx += kChunk) {
+      const int lp = idx / 27, o = idx - lp * 27;
+      const int ox = o / 9, oy = (o / 3) % 3, oz = o % 3;
+      const int I = __float_as_int(sp[kPbase][lp]) + ox, Jj = __float_as_int(sp[kPbase + 1][lp]) + oy,
+                K = __float_as_int(sp[kPbase + 2][lp]) + oz;
+      if (I < 0 || I >= G || Jj < 0 || Jj >= G || K < 0 || K >= G) continue;
+      const float fx[3] = {sp[kPfx][lp], sp[kPfx + 1][lp], sp[kPfx + 2][lp]};
+      // B-spline weights and offsets as in bspline() / p2g_node()
+      const float w = bspline_w(fx[0], ox) * bspline_w(fx[1], oy) * bspline_w(fx[2], oz);
+      const float dpos[3] = {((float)ox - fx[0]) * mp.dx, ((float)oy - fx[1]) * mp.dx, ((float)oz - fx[2]) * mp.dx};
+      float val[7];
+#pragma unroll
+      for (int a = 0; a < 3; ++a)
+        val[a] = w * (sp[kPmv + a][lp] + (sp[kPaff + 3 * a][lp] * dpos[0] + sp[kPaff + 3 * a + 1][lp] * dpos[1] +
+                                          sp[kPaff + 3 * a + 2][lp] * dpos[2]));
+      val[3] = w * sp[kPmass][lp];
+      int nq = 4;
+      if (REACT) {
+        const float f0 = sp[kPpf][lp], f1 = sp[kPpf + 1][lp], f2 = sp[kPpf + 2][lp];
+        if (f0 != 0.f || f1 != 0.f || f2 != 0.f) {
+          val[4] = w * f0;
+          val[5] = w * f1;
+          val[6] = w * f2;
+          nq = 7;
+          gn[0] += val[4];
+          gn[1] += val[5];
+          gn[2] += val[6];
+          gmax = fmaxf(gmax, sqrtf(val[4] * val[4] + val[5] * val[5] + val[6] * val[6]));
+        }
+      }
+      if (staged) {
+        const int li = ((K - bx.lo[2]) * bx.ext[1] + (Jj - bx.lo[1])) * bx.ext[0] + (I - bx.lo[0]);
+#pragma unroll
+        for (int q = 0; q < 7; ++q)
+          if (q < nq) atomicAdd(&tile[q * nv + li], val[q]);
+      } else {
+        const int64_t node = ((int64_t)K * G + Jj) * G + I;
+#pragma unroll
+        for (int q = 0; q < 7; ++q)
+          if (q < nq) atomicAdd(dst[q] + node, val[q]);
+      }
+    }
+    __syncthreads();
+    // ---- phase 3: one global atomic per touched node value of the chunk
+    for (int li = tid; li < nv; li += kChunk) {
+      const int64_t node = box_node(bx, li, G);
+#pragma unroll
+      for (int q = 0; q < 7; ++q) {
+        const float v = tile[q * nv + li];
+        if (v != 0.f) atomicAdd(dst[q] + node, v);
+      }
+    }
+  }
+  if (REACT) {
+    // diagnostics reductions (penalty.py:202-240, moving_boundary.py:312-374)
+    const int na = __reduce_add_sync(0xffffffffu, (unsigned)n_act);
+    const float pm = warp_max(pmax), gm = warp_max(gmax);
+    double sp3[3], sg[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      sp3[a] = warp_sum_d(pn[a]);
+      sg[a] = warp_sum_d(gn[a]);
+    }
+    if ((tid & 31) == 0) {
+      if (na) atomicAdd(&st->active_reaction_particle_count, na);
+      if (pm > 0.f) atomic_max_nonneg(&st->max_particle_reaction_norm, pm);
+      if (gm > 0.f) atomic_max_nonneg(&st->max_grid_reaction_norm, gm);
+      for (int a = 0; a < 3; ++a) {
+        if (sp3[a] != 0.0) atomicAdd(&st->net_particle_reaction[a], sp3[a]);
+        if (sg[a] != 0.0) atomicAdd(&st->net_grid_reaction[a], sg[a]);
+      }
+    }
+  }
+}
+
+// G2P of the chunks of this CTA from grid buffer g; zeroes the boxes the
+// previous substep recorded in the other buffer go.
+__global__ __launch_bounds__(kChunk) void k_g2p_binned(FsiParticles pt, FsiGrid g, FsiGrid go, FsiMpmParams mp,
+                                                       const int32_t* __restrict__ perm,
+                                                       const int2* __restrict__ chunks, const int32_t* meta,
+                                                       const int32_t* __restrict__ box_b,
+                                                       const int32_t* __restrict__ box_o, int buf,
+                                                       FsiCouplingStats* st_other) {
+  __shared__ float vt[3 * kTileCap];
+  const int tid = threadIdx.x;
+  const int G = g.n;
+  const int64_t N = (int64_t)G * G * G;
+  const int nrec = meta[1 + (1 - buf)];
+  for (int r = blockIdx.x; r < nrec; r += gridDim.x) {
+    const Box bx = load_box(box_o + 6 * r);
+    for (int li = tid; li < bx.vol; li += kChunk) {
+      const int64_t node = box_node(bx, li, G);
+      go.v[node] = 0.f;
+      go.v[N + node] = 0.f;
+      go.v[2 * N + node] = 0.f;
+      go.m[node] = 0.f;
+      go.f_ext[node] = 0.f;
+      go.f_ext[N + node] = 0.f;
+      go.f_ext[2 * N + node] = 0.f;
+    }
+  }
+  if (st_other && blockIdx.x == 0 && tid == 0) {
+    st_other->active_reaction_particle_count = 0;
+    st_other->max_particle_reaction_norm = 0.f;
+    st_other->max_grid_reaction_norm = 0.f;
+    st_other->area_scale = 0.f;
+    st_other->raw_area_scale = 0.f;
+    for (int a = 0; a < 3; ++a) {
+      st_other->net_particle_reaction[a] = 0.0;
+      st_other->net_grid_reaction[a] = 0.0;
+    }
+  }
+  const int nch = meta[0];
+  const float s4 = 4.0f * mp.inv_dx * mp.inv_dx;
+  for (int c = blockIdx.x; c < nch; c += gridDim.x) {
+    __syncthreads();  // the previous chunk's gathers are done
+    const Box bx = load_box(box_b + 6 * c);
+    const bool staged = bx.vol <= kTileCap;
+    const int nv = staged ? bx.vol : 0;
+    for (int li = tid; li < nv; li += kChunk) {
+      const int64_t node = box_node(bx, li, G);
+      const float m = g.m[node];
+      const float P[3] = {g.v[node], g.v[N + node], g.v[2 * N + node]};
+      float v[3] = {P[0], P[1], P[2]};
+      if (m > 0.0f) {
+        const float f[3] = {g.f_ext[node], g.f_ext[N + node], g.f_ext[2 * N + node]};
+        const int i = (int)(node % G), j = (int)((node / G) % G), k = (int)(node / ((int64_t)G * G));
+        grid_node_velocity(P, m, f, i, j, k, G, mp, v);
+      }
+      vt[li] = v[0];
+      vt[nv + li] = v[1];
+      vt[2 * nv + li] = v[2];
+    }
+    __syncthreads();
+    const int2 ch = chunks[c];
+    if (tid < ch.y) {
+      const int p = perm[ch.x + tid];
+      const int n = pt.n;
+      float X[3] = {pt.x[p], pt.x[n + p], pt.x[2 * n + p]};
+      BSpline b;
+      bspline(X, mp.inv_dx, b);
+      float nvl[3] = {0.f, 0.f, 0.f}, nC[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+      if (!staged) {
+        g2p_gather_global(g, mp, b, nvl, nC);
+      } else {
+#pragma unroll
+      for (int ox = 0; ox < 3; ++ox)
+#pragma unroll
+        for (int oy = 0; oy < 3; ++oy)
+#pragma unroll
+          for (int oz = 0; oz < 3; ++oz) {
+            const int I = b.base[0] + ox, Jj = b.base[1] + oy, K = b.base[2] + oz;
+            if (I < 0 || I >= G || Jj < 0 || Jj >= G || K < 0 || K >= G) continue;
+            const int li = ((K - bx.lo[2]) * bx.ext[1] + (Jj - bx.lo[1])) * bx.ext[0] + (I - bx.lo[0]);
+            const float gv[3] = {vt[li], vt[nv + li], vt[2 * nv + li]};
+            g2p_node(b, ox, oy, oz, mp.dx, s4, gv, nvl, nC);
+          }
+      }
+      g2p_finish(pt, p, mp, X, nvl, nC);
+    }
+  }
+}
+
+__global__ void k_grid_velocity(FsiGrid g, FsiMpmParams mp, float* __restrict__ out) {
+  const int G = g.n;
+  const int64_t N = (int64_t)G * G * G;
+  const int64_t node = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (node >= N) return;
+  const float m = g.m[node];
+  const float P[3] = {g.v[node], g.v[N + node], g.v[2 * N + node]};
+  float v[3] = {P[0], P[1], P[2]};
+  if (m > 0.0f) {
+    const float f[3] = {g.f_ext[node], g.f_ext[N + node], g.f_ext[2 * N + node]};
+    grid_node_velocity(P, m, f, (int)(node % G), (int)((node / G) % G), (int)(node / ((int64_t)G * G)), G, mp, v);
+  }
+  out[node] = v[0];
+  out[N + node] = v[1];
+  out[2 * N + node] = v[2];
+}
+
+int layout(int32_t n_particles, int32_t n_grid, int32_t* n_bins, int32_t* max_chunks) {
+  if (n_particles <= 0 || n_grid <= 0) return invalid("n_particles and n_grid must be positive");
+  const int64_t nb = (n_grid + kEdge - 1) / kEdge;
+  const int64_t bins = nb * nb * nb;
+  const int64_t mc = ((int64_t)n_particles + kChunk - 1) / kChunk + std::min<int64_t>(n_particles, bins);
+  if (bins > INT_MAX || mc > INT_MAX / 12) return invalid("grid or particle count too large for binning");
+  *n_bins = (int32_t)bins;
+  *max_chunks = (int32_t)mc;
+  return FSI_OK;
+}
+
+int check_bins(const FsiMpmBins* bins, int32_t n_particles, int32_t n_grid) {
+  if (!bins) return invalid("null bins");
+  if (!bins->key || !bins->count || !bins->start || !bins->perm || !bins->chunk || !bins->box || !bins->meta)
+    return invalid("null bins array");
+  int32_t nb = 0, mc = 0;
+  const int rc = layout(n_particles, n_grid, &nb, &mc);
+  if (rc) return rc;
+  if (bins->n_bins != nb) return invalid("bins->n_bins does not match the grid (see fsi_mpm_bins_layout)");
+  if (bins->max_chunks < mc) return invalid("bins->max_chunks below fsi_mpm_bins_layout's capacity");
+  if (((uintptr_t)bins->count | (uintptr_t)bins->start | (uintptr_t)bins->chunk) & 15)
+    return invalid("bins->count, start and chunk must be 16-byte aligned");
+  return FSI_OK;
+}
+
+int check_particles(const FsiParticles* pt) {
+  if (!pt) return invalid("null particles");
+  if (pt->n <= 0) return invalid("n_particles must be positive");
+  if (!pt->x || !pt->v || !pt->C || !pt->F || !pt->Jp || !pt->mass || !pt->vol0 || !pt->fixed || !pt->fixed_x)
+    return invalid("null particle field");
+  return FSI_OK;
+}
+
+int check_grid(const FsiGrid* g) {
+  if (!g || g->n <= 0 || !g->v || !g->m || !g->f_ext) return invalid("bad grid");
+  return FSI_OK;
+}
+
+int sm_count() {
+  static int cached[64] = {0};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+  if (!cached[dev]) {
+    int n = 0;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+    cached[dev] = n;
+  }
+  return cached[dev];
+}
+
+inline unsigned nblk(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
+
+}  // namespace
+}  // namespace fsi
+
+using namespace fsi;
+
+extern "C" int fsi_mpm_bins_layout(int32_t n_particles, int32_t n_grid, int32_t* n_bins, int32_t* max_chunks) {
+  if (!n_bins || !max_chunks) return invalid("null output");
+  return layout(n_particles, n_grid, n_bins, max_chunks);
+}
+
+extern "C" int fsi_mpm_bin(const FsiParticles* pt, const FsiGrid* g, const FsiMpmParams* mp, const FsiMpmBins* bins,
+                           void* stream) {
+  int rc = check_particles(pt);
+  if (rc) return rc;
+  if (!g || g->n <= 0 || !mp) return invalid("bad grid or params");
+  if ((rc = check_bins(bins, pt->n, g->n))) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int nb = (g->n + kEdge - 1) / kEdge;
+  k_bin_count<<<nblk(pt->n, 256), 256, 0, st>>>(*pt, mp->inv_dx, g->n, nb, bins->key, bins->count);
+  if ((rc = launch_check("k_bin_count"))) return rc;
+  k_bin_scan<<<1, 1024, 0, st>>>(bins->n_bins, bins->count, bins->start, reinterpret_cast<int2*>(bins->chunk),
+                                 bins->meta);
+  if ((rc = launch_check("k_bin_scan"))) return rc;
+  k_bin_scatter<<<nblk(pt->n, 256), 256, 0, st>>>(pt->n, bins->key, bins->start, bins->perm);
+  return launch_check("k_bin_scatter");
+}
+
+extern "C" int fsi_mpm_substep_binned(const FsiParticles* pt, const FsiGrid grid[2], const FsiMpmBins* bins,
+                                      const FsiMpmParams* mp, int32_t buffer, const FsiLbmState* s,
+                                      const float* hydro, const FsiCouplingParams* cp, FsiCouplingStats stats[2],
+                                      void* stream) {
+  int rc = check_particles(pt);
+  if (rc) return rc;
+  if (!grid || !mp) return invalid("null grid or params");
+  if ((rc = check_grid(&grid[0])) || (rc = check_grid(&grid[1]))) return rc;
+  if (grid[0].n != grid[1].n) return invalid("the two grid buffers differ in size");
+  if (buffer != 0 && buffer != 1) return invalid("buffer must be 0 or 1");
+  if ((rc = check_bins(bins, pt->n, grid[0].n))) return rc;
+  if (cp) {
+    if (!s || !hydro || !stats) return invalid("reaction transfer needs the lattice state, hydro and stats");
+    if (cp->kind < 0 || cp->kind > 2) return invalid("reaction kind must be 0 (penalty), 1 (engineering), 2 (link-area)");
+    if (cp->kind != 0 && !s->phi) return invalid("moving-boundary reaction needs phi");
+    if (cp->kind == 2 && !s->diag) return invalid("link-area reaction needs the directional reductions");
+    if (cp->inv_dx_norm != mp->inv_dx)
+      return invalid("binned substep needs the coupling and MPM grids to share dx (inv_dx_norm == inv_dx)");
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  const int grid_ctas = (int)std::min<int64_t>(bins->max_chunks, (int64_t)sm_count() * 4);
+  int32_t* box_b = bins->box + (int64_t)6 * bins->max_chunks * buffer;
+  int32_t* box_o = bins->box + (int64_t)6 * bins->max_chunks * (1 - buffer);
+  const int2* chunks = reinterpret_cast<const int2*>(bins->chunk);
+  const FsiGrid g = grid[buffer], go = grid[1 - buffer];
+  if (cp) {
+    const LatView L{s->nx, s->ny, s->nz, s->pitch};
+    k_p2g_binned<true><<<grid_ctas, kChunk, 0, st>>>(*pt, g, *mp, bins->perm, chunks, bins->meta, box_b, buffer, L,
+                                                     hydro, s->phi, *cp, &stats[buffer], s->diag);
+  } else {
+    const LatView L{0, 0, 0, 0};
+    k_p2g_binned<false><<<grid_ctas, kChunk, 0, st>>>(*pt, g, *mp, bins->perm, chunks, bins->meta, box_b, buffer, L,
+                                                      nullptr, nullptr, FsiCouplingParams{}, nullptr, nullptr);
+  }
+  if ((rc = launch_check("k_p2g_binned"))) return rc;
+  k_g2p_binned<<<grid_ctas, kChunk, 0, st>>>(*pt, g, go, *mp, bins->perm, chunks, bins->meta, box_b, box_o, buffer,
+                                             cp ? &stats[1 - buffer] : nullptr);
+  return launch_check("k_g2p_binned");
+}
+
+extern "C" int fsi_mpm_grid_velocity(const FsiGrid* g, const FsiMpmParams* mp, float* out, void* stream) {
+  int rc = check_grid(g);
+  if (rc) return rc;
+  if (!mp || !out) return invalid("null params or output");
+  const int64_t N = (int64_t)g->n * g->n * g->n;
+  k_grid_velocity<<<nblk(N, 256), 256, 0, (cudaStream_t)stream>>>(*g, *mp, out);
+  return launch_check("k_grid_velocity");
+}

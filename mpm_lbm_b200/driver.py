@@ -43,7 +43,10 @@ DIAGNOSTIC_TEXT_FIELDS = {"coupling_mode", "mb_subcycle_force_accumulation_mode"
 class FSIDriver3D:
     def __init__(self, config: FSIDriverConfig, out_dir: str, *, population_storage="fp32", collision="mrt",
                  lattice_shape=None, material=None, static_solid=None, initial_particles=None, use_cuda_graph=False,
-                 device=None):
+                 mpm_path="binned", device=None):
+        if mpm_path not in ("binned", "one_phase"):
+            raise ValueError("mpm_path must be 'binned' (fsi_mpm_substep_binned) or 'one_phase' (one kernel per phase)")
+        self.mpm_path = mpm_path
         self.config = config
         self.out_dir = out_dir
         self.sim = config.make_unified_sim_config()
@@ -193,9 +196,11 @@ class FSIDriver3D:
         self.timing[key] += time.perf_counter() - t0
 
     def _graph_period(self):
-        # the captured sequence must return the AA layout parity and the ping-pong slot to their start values
+        # the captured sequence must return the AA layout parity, the ping-pong slot and the binned
+        # substep's grid buffer to their start values
         S = self.config.lbm_substeps_per_fsi_step if self.config.fsi_exchange_mode == "lbm_subcycled_per_fsi_step" else 1
-        return 1 if S % 2 == 0 else 2
+        M = self.config.mpm_substeps_per_lbm_step if self.mpm_path == "binned" else 0
+        return 2 if S % 2 or M % 2 else 1
 
     def step_once(self):
         if not self.initialized:
@@ -265,16 +270,33 @@ class FSIDriver3D:
         self.projector.project(self.solid, self.lbm)
         self._t("projection_time", t0)
 
+    def _mpm_loop(self, coupler=None, one_phase_reaction=None):
+        """The FSI step's MPM substeps, each with the coupler's reaction
+        transfer when given (fsi_driver.py's MPM loops)."""
+        t0 = time.perf_counter()
+        M = self.config.mpm_substeps_per_lbm_step
+        if self.mpm_path == "binned":
+            self.solid.rebin()
+            for _ in range(M):
+                self.solid.substep_binned(coupler, self.lbm if coupler is not None else None)
+                self.total_mpm_substeps += 1
+        else:
+            for _ in range(M):
+                self.solid.clear_grid()
+                self.solid.p2g()
+                if one_phase_reaction is not None:
+                    one_phase_reaction()
+                self.solid.grid_update()
+                self.solid.g2p()
+                self.total_mpm_substeps += 1
+        self._t("mpm_substep_time", t0)
+
     def _step_none(self):
         self._project()
         t0 = time.perf_counter()
         self.lbm.step()
         self._t("lbm_step_time", t0)
-        t0 = time.perf_counter()
-        for _ in range(self.config.mpm_substeps_per_lbm_step):
-            self.solid.substep()
-            self.total_mpm_substeps += 1
-        self._t("mpm_substep_time", t0)
+        self._mpm_loop()
 
     def _step_penalty(self):
         self._project()
@@ -285,15 +307,8 @@ class FSIDriver3D:
         t0 = time.perf_counter()
         self.lbm.step()
         self._t("lbm_step_time", t0)
-        t0 = time.perf_counter()
-        for _ in range(self.config.mpm_substeps_per_lbm_step):
-            self.solid.clear_grid()
-            self.solid.p2g()
-            self.penalty_coupler.add_lbm_reaction_to_mpm_grid(self.solid, self.lbm)
-            self.solid.grid_update()
-            self.solid.g2p()
-            self.total_mpm_substeps += 1
-        self._t("mpm_substep_time", t0)
+        pc = self.penalty_coupler
+        self._mpm_loop(pc, lambda: pc.add_lbm_reaction_to_mpm_grid(self.solid, self.lbm))
 
     def _step_moving_boundary(self):
         self._project()
@@ -331,19 +346,15 @@ class FSIDriver3D:
         self._advance_mpm_with_moving_boundary_reaction()
 
     def _advance_mpm_with_moving_boundary_reaction(self):
-        t0 = time.perf_counter()
         coupler = self.mb_coupler if self.config.reaction_transfer_mode == "engineering" else self.link_area_coupler
         if coupler is None:
             raise ValueError(f"unsupported reaction_transfer_mode: {self.config.reaction_transfer_mode}")
-        for _ in range(self.config.mpm_substeps_per_lbm_step):
-            self.solid.clear_grid()
-            self.solid.p2g()
+
+        def react():
             coupler.clear_reaction_diagnostics()
             coupler._react(self.solid, self.lbm)
-            self.solid.grid_update()
-            self.solid.g2p()
-            self.total_mpm_substeps += 1
-        self._t("mpm_substep_time", t0)
+
+        self._mpm_loop(coupler, react)
 
     def run(self):
         total = time.perf_counter()

@@ -14,16 +14,20 @@ import os
 import numpy as np
 import torch
 
-from ._lib import FsiGrid, FsiMpmParams, FsiParticles, call, ptr, stream_handle
+from ._lib import FsiCouplingStats, FsiGrid, FsiMpmBins, FsiMpmParams, FsiParticles, call, ptr, stream_handle
 from .config import MPMConfig
 from .fields import ParticleField
 
 
 class _GridField:
-    """grid_v / grid_m / grid_f_ext in the reference shape (n, n, n[, 3])."""
+    """grid_v / grid_m / grid_f_ext in the reference shape (n, n, n[, 3]).
 
-    def __init__(self, get, n, comps):
+    get() returns the tensor holding the reference's values; for_write()
+    returns the tensor a write must go to (the one-phase grid)."""
+
+    def __init__(self, get, n, comps, for_write=None):
         self._get, self.ng, self.comps = get, n, comps
+        self._for_write = for_write if for_write is not None else get
 
     @property
     def shape(self):
@@ -37,7 +41,7 @@ class _GridField:
         return t.reshape(g, g, g).permute(2, 1, 0).contiguous().cpu().numpy()
 
     def from_numpy(self, arr):
-        t = self._get()
+        t = self._for_write()
         a = torch.as_tensor(np.ascontiguousarray(arr), device=t.device)
         if self.comps:
             t.copy_(a.permute(3, 2, 1, 0).reshape(t.shape).to(t.dtype))
@@ -112,9 +116,16 @@ class MPMSolid3D:
         self.vol0 = ParticleField(lambda: self.t_vol0, (), np.float32, name="vol0")
         self.fixed_mask = ParticleField(lambda: self.t_fixed, (), np.int8, name="fixed_mask")
         self.fixed_x = ParticleField(lambda: self.t_fixed_x, (3,), np.float32, name="fixed_x")
-        self.grid_v = _GridField(lambda: self.t_gv, self.n_grid, 3)
-        self.grid_m = _GridField(lambda: self.t_gm, self.n_grid, 0)
-        self.grid_f_ext = _GridField(lambda: self.t_gf, self.n_grid, 3)
+        self.grid_v = _GridField(self._grid_velocity, self.n_grid, 3, lambda: self._one_phase_grid()[0])
+        self.grid_m = _GridField(lambda: self._last_grid()[1], self.n_grid, 0, lambda: self._one_phase_grid()[1])
+        self.grid_f_ext = _GridField(lambda: self._last_grid()[2], self.n_grid, 3, lambda: self._one_phase_grid()[2])
+        # binned substep (fsi_mpm_substep_binned): second grid buffer and bins, made on first use
+        self._bins = None
+        self._buf = 0             # buffer the next binned substep scatters into
+        self._binned_last = None  # buffer of the last binned substep while the grid holds its result
+        self._binned_clean = True  # both buffers zero outside the recorded boxes
+        self._since_bin = 0
+        self.rebin_interval = 64  # binned substeps between automatic re-binnings
 
     def _stream(self):
         return stream_handle()
@@ -199,18 +210,22 @@ class MPMSolid3D:
         self.t_v[:, self.t_fixed != 0] = 0.0
 
     def clear_grid(self):
+        self._one_phase_grid()
         self.t_gv.zero_()
         self.t_gm.zero_()
         self.t_gf.zero_()
 
     def p2g(self):
+        self._one_phase_grid()
         call("fsi_mpm_p2g", ctypes.byref(self.particles), ctypes.byref(self.grid), ctypes.byref(self.params),
              self._stream())
 
     def grid_update(self):
+        self._one_phase_grid()
         call("fsi_mpm_grid_update", ctypes.byref(self.grid), ctypes.byref(self.params), self._stream())
 
     def g2p(self):
+        self._one_phase_grid()
         call("fsi_mpm_g2p", ctypes.byref(self.particles), ctypes.byref(self.grid), ctypes.byref(self.params),
              self._stream())
 
@@ -219,6 +234,89 @@ class MPMSolid3D:
         self.p2g()
         self.grid_update()
         self.g2p()
+
+    # ---- binned substep -------------------------------------------------
+    def _ensure_binned(self):
+        if self._bins is not None:
+            return
+        nb, mc = ctypes.c_int32(), ctypes.c_int32()
+        call("fsi_mpm_bins_layout", self.n_particles, self.n_grid, ctypes.byref(nb), ctypes.byref(mc))
+        dev, n, G = self.device, self.n_particles, self.n_grid ** 3
+        i32 = lambda *s: torch.zeros(*s, dtype=torch.int32, device=dev)  # noqa: E731
+        f32 = lambda *s: torch.zeros(*s, dtype=torch.float32, device=dev)  # noqa: E731
+        t = {"key": i32(n), "count": i32(nb.value), "start": i32(nb.value), "perm": i32(n),
+             "chunk": i32(mc.value, 2), "box": i32(2, mc.value, 6), "meta": i32(4)}
+        self.t_gv1, self.t_gm1, self.t_gf1 = f32(3, G), f32(G), f32(3, G)
+        grids = (FsiGrid * 2)()
+        grids[0] = self.grid
+        grids[1] = FsiGrid(n=self.n_grid, v=ptr(self.t_gv1), m=ptr(self.t_gm1), f_ext=ptr(self.t_gf1))
+        bins = FsiMpmBins(n_bins=nb.value, max_chunks=mc.value, **{k: ptr(v) for k, v in t.items()})
+        self._bins = {"t": t, "grids": grids, "struct": bins}
+        self._binned_clean = True
+        self._buf = 0
+        self._since_bin = None
+
+    def _buffers(self, b):
+        return (self.t_gv, self.t_gm, self.t_gf) if b == 0 else (self.t_gv1, self.t_gm1, self.t_gf1)
+
+    def _last_grid(self):
+        """(momentum or velocity, mass, f_ext) tensors of the last grid state."""
+        return self._buffers(self._binned_last) if self._binned_last is not None else (self.t_gv, self.t_gm, self.t_gf)
+
+    def _grid_velocity(self):
+        if self._binned_last is None:
+            return self.t_gv
+        b = self._binned_last
+        out = torch.empty_like(self.t_gv)
+        call("fsi_mpm_grid_velocity", ctypes.byref(self._bins["grids"][b]), ctypes.byref(self.params), ptr(out),
+             self._stream())
+        return out
+
+    def _one_phase_grid(self):
+        """Switch the grid to the one-phase layout (buffer 0 holds grid_v as
+        velocity), materialising the last binned substep's grid first."""
+        if self._binned_last is not None:
+            v = self._grid_velocity()
+            m, f = self._last_grid()[1:]
+            self.t_gv.copy_(v)
+            if self._binned_last != 0:
+                self.t_gm.copy_(m)
+                self.t_gf.copy_(f)
+            self._binned_last = None
+        self._binned_clean = False
+        return self.t_gv, self.t_gm, self.t_gf
+
+    def rebin(self):
+        """Sort particle ids by 4x4x4-cell block (fsi_mpm_bin)."""
+        self._ensure_binned()
+        call("fsi_mpm_bin", ctypes.byref(self.particles), ctypes.byref(self.grid), ctypes.byref(self.params),
+             ctypes.byref(self._bins["struct"]), self._stream())
+        self._since_bin = 0
+
+    def substep_binned(self, coupler=None, lbm=None):
+        """One substep through fsi_mpm_substep_binned: the same update as
+        substep() (plus the coupler's reaction transfer when given, as the
+        driver's MPM loops call it), with binned, shared-memory-staged P2G."""
+        self._ensure_binned()
+        if not self._binned_clean:
+            for t in self._buffers(0) + self._buffers(1):
+                t.zero_()
+            self._bins["t"]["meta"][1:3].zero_()  # no recorded boxes; the chunk table stays valid
+            self._buf, self._binned_last, self._binned_clean = 0, None, True
+        if self._since_bin is None or self._since_bin >= self.rebin_interval:
+            self.rebin()
+        if coupler is not None:
+            state, hydro, cp, stats = coupler._binned_args(lbm)
+            args = (ctypes.byref(state), ptr(hydro), ctypes.byref(cp), stats)
+        else:
+            args = (None, None, None, None)
+        call("fsi_mpm_substep_binned", ctypes.byref(self.particles), self._bins["grids"],
+             ctypes.byref(self._bins["struct"]), ctypes.byref(self.params), self._buf, *args, self._stream())
+        if coupler is not None:
+            coupler._binned_slot = self._buf
+        self._binned_last = self._buf
+        self._buf ^= 1
+        self._since_bin += 1
 
     def inside_grid(self, I):
         return all(0 <= int(i) < self.n_grid for i in I)

@@ -29,8 +29,9 @@ def _load(name):
     return np.load(p, allow_pickle=False)
 
 
+@pytest.mark.parametrize("mpm_path", ["binned", "one_phase"])
 @pytest.mark.parametrize("name", CASES)
-def test_driver_matches_reference(name, tmp_path):
+def test_driver_matches_reference(name, mpm_path, tmp_path):
     from mpm_lbm_b200.config import FSIDriverConfig
     from mpm_lbm_b200.driver import FSIDriver3D
 
@@ -42,7 +43,7 @@ def test_driver_matches_reference(name, tmp_path):
         gp = str(tmp_path / "duct_geo.json")
         _duct_geometry_json(gp, cfg["n_particles"])
         cfg["geometry_config_path"] = gp
-    drv = FSIDriver3D(FSIDriverConfig(**cfg), str(tmp_path / "out"))
+    drv = FSIDriver3D(FSIDriverConfig(**cfg), str(tmp_path / "out"), mpm_path=mpm_path)
     drv.initialize()
     np.testing.assert_array_equal(drv.lbm.solid.to_numpy(), d["init_solid"])
     np.testing.assert_allclose(drv.solid.x.to_numpy(), d["init_x"], rtol=0, atol=1e-7)

@@ -23,6 +23,8 @@ extern "C" void host_collide(const float* F, float rho, const float* u, const fl
 }
 extern "C" void host_moments(const float* F, float* m) { fsi::moments0(F, m[0], m[1], m[2], m[3]); }
 extern "C" void host_polar(const double* F, double* R) { fsi::polar_rotation_d(F, R); }
+extern "C" void host_polar_jacobi(const double* F, double* R) { fsi::polar_rotation_jacobi_d(F, R); }
+extern "C" int host_polar_newton(const double* F, double* R) { return fsi::polar_rotation_newton_d(F, R) ? 1 : 0; }
 """
 
 
@@ -88,3 +90,37 @@ def test_polar_rotation_matches_oracle(hostlib):
         hostlib.host_polar(P(F.reshape(-1).copy()), P(R1))
         L.orc_polar_rotation(P(F.reshape(-1).copy()), P(R2))
         np.testing.assert_allclose(R1, R2, atol=1e-10)
+
+
+def test_polar_newton_agrees_with_jacobi(hostlib):
+    """The Newton fast path and the Jacobi/QR path give the same proper rotation
+    wherever Newton applies (det F > 0), including strongly stretched and nearly
+    singular gradients; inverted gradients are left to the Jacobi path."""
+    hostlib.host_polar_newton.restype = ctypes.c_int
+    rng = np.random.default_rng(11)
+    used = 0
+    for t in range(2000):
+        A = rng.standard_normal((3, 3))
+        Q, _ = np.linalg.qr(A)
+        Q *= np.sign(np.linalg.det(Q))
+        s = np.exp(rng.uniform(-6 if t % 4 == 0 else -1, 1, 3))
+        V, _ = np.linalg.qr(rng.standard_normal((3, 3)))
+        F = Q @ np.diag(s) @ V.T
+        if t % 7 == 0:
+            F = F @ np.diag([1, 1, -1])  # inverted
+        R1, R2 = np.zeros(9), np.zeros(9)
+        ok = hostlib.host_polar_newton(P(F.reshape(-1).copy()), P(R1))
+        hostlib.host_polar_jacobi(P(F.reshape(-1).copy()), P(R2))
+        if np.linalg.det(F) <= 0:
+            assert ok == 0
+            continue
+        assert ok == 1, F
+        used += 1
+        np.testing.assert_allclose(R1, R2, atol=1e-9)
+        R = R1.reshape(3, 3)
+        np.testing.assert_allclose(R @ R.T, np.eye(3), atol=1e-12)
+        # the polar factor itself: R = F (F^T F)^-1/2
+        w, U = np.linalg.eigh(F.T @ F)
+        Rref = F @ U @ np.diag(w ** -0.5) @ U.T
+        np.testing.assert_allclose(R, Rref, atol=1e-6)
+    assert used > 1500
