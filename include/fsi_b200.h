@@ -159,6 +159,18 @@ int fsi_lbm_flush_bc(const FsiLbmState* s, const FsiLbmParams* p, const FsiStepC
 int fsi_mask_rebuild(const FsiLbmState* s, const FsiLbmParams* p, const FsiStepCtl* ctl, float threshold,
                      void* stream);
 
+/* fsi_mask_rebuild without the change_list scratch: the list of flipped
+ * cells lives in a file-scope device array of the library, so the caller
+ * passes no scratch (s->change_list is ignored) and nothing is allocated.
+ * No counterpart in the reference.  For callers that own the lattice state
+ * but cannot provide one more device buffer (e.g. a host binding without a
+ * device allocator).  Limits: nx*ny*nz <= 1048576 cells, else FSI_E_INVALID;
+ * all calls on one device share the array, so calls must not overlap in
+ * time (order them on one stream); the first call on each device looks the
+ * array up (cudaGetSymbolAddress) and should be made outside stream capture. */
+int fsi_mask_rebuild_static_scratch(const FsiLbmState* s, const FsiLbmParams* p, const FsiStepCtl* ctl,
+                                    float threshold, void* stream);
+
 /* finalize_moving_boundary_force_accumulator (fluid.py:475-486): folds the
  * last substep, hydro = accum / sample_count. */
 int fsi_force_accum_finalize(const FsiLbmState* s, const FsiStepCtl* ctl, int32_t sample_count, void* stream);

@@ -102,6 +102,7 @@ SIGNATURES = {
     "fsi_lbm_substep": [_P(FsiLbmState), _P(FsiLbmParams), _P(FsiStepCtl), c_p],
     "fsi_lbm_flush_bc": [_P(FsiLbmState), _P(FsiLbmParams), _P(FsiStepCtl), c_p],
     "fsi_mask_rebuild": [_P(FsiLbmState), _P(FsiLbmParams), _P(FsiStepCtl), c_f32, c_p],
+    "fsi_mask_rebuild_static_scratch": [_P(FsiLbmState), _P(FsiLbmParams), _P(FsiStepCtl), c_f32, c_p],
     "fsi_force_accum_finalize": [_P(FsiLbmState), _P(FsiStepCtl), c_i32, c_p],
     "fsi_lbm_readout": [_P(FsiLbmState), _P(FsiLbmParams), _P(FsiStepCtl), c_p, c_p, c_p, c_p],
     "fsi_project": [_P(FsiLbmState), _P(FsiParticles), _P(FsiCouplingParams), c_p, c_p],

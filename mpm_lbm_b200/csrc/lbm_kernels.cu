@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <mutex>
 
 #include "common.cuh"
 #include "d3q19.cuh"
@@ -1156,4 +1157,54 @@ extern "C" int fsi_lbm_readout(const FsiLbmState* s, const FsiLbmParams* p, cons
   else
     k_readout<false><<<blocks_for(n, 256), 256, 0, (cudaStream_t)stream>>>(c, out_pop, out_rho, out_vel);
   return launch_check("k_readout");
+}
+
+// ---- mask rebuild with a built-in change list ----------------------------
+// fsi_mask_rebuild needs a pitch-sized int32 scratch (FsiLbmState.change_list)
+// to list the cells whose solid bit flipped.  Some callers hold the lattice
+// state but have no way to hand over another device buffer: a foreign-language
+// host that received the state's buffers from elsewhere and owns no device
+// allocator, or code running where allocating is not allowed.  For them the
+// list lives in this file-scope array, sized for lattices of up to
+// kStaticChangeCap cells (4 MiB of device memory per device that loads the
+// library).  Its contents need no initial value: the count of listed cells is
+// diag->change_count, which every call zeroes before use.
+namespace fsi {
+constexpr int64_t kStaticChangeCap = int64_t(1) << 20;
+constexpr int kStaticScratchDevices = 64;
+static __device__ __align__(256) int32_t g_change_scratch[kStaticChangeCap];
+
+// address of g_change_scratch on the current device, looked up once per device
+static int static_change_scratch(int32_t** out) {
+  static std::mutex mu;
+  static int32_t* addr[kStaticScratchDevices] = {};
+  int dev = 0;
+  int rc = cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+  if (rc) return rc;
+  if (dev < 0 || dev >= kStaticScratchDevices) return invalid("device ordinal out of range for the built-in scratch");
+  std::lock_guard<std::mutex> lock(mu);
+  if (!addr[dev]) {
+    void* p = nullptr;
+    rc = cuda_check(cudaGetSymbolAddress(&p, g_change_scratch), "cudaGetSymbolAddress(change-list scratch)");
+    if (rc) return rc;
+    addr[dev] = static_cast<int32_t*>(p);
+  }
+  *out = addr[dev];
+  return FSI_OK;
+}
+}  // namespace fsi
+
+extern "C" int fsi_mask_rebuild_static_scratch(const FsiLbmState* s, const FsiLbmParams* p, const FsiStepCtl* ctl,
+                                               float threshold, void* stream) {
+  if (!s) return invalid("null state");
+  const int64_t n = (int64_t)s->nx * s->ny * s->nz;
+  if (n > kStaticChangeCap)
+    return invalid("lattice of " + std::to_string(n) + " cells exceeds the built-in change list of " +
+                   std::to_string(kStaticChangeCap) + " cells; use fsi_mask_rebuild with a caller-provided change_list");
+  int32_t* scratch = nullptr;
+  const int rc = static_change_scratch(&scratch);
+  if (rc) return rc;
+  FsiLbmState local = *s;
+  local.change_list = scratch;
+  return fsi_mask_rebuild(&local, p, ctl, threshold, stream);
 }
