@@ -9,7 +9,7 @@ moving_boundary coupling subcycled with 120 LBM substeps per FSI step and
 40 MPM substeps per FSI step (the explicit MPM limit for this plate).
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-                       [--storage fp32|fp16]
+                       [--storage fp32|fp16] [--workload NAME]
 Prints one JSON line (rank 0).  Multi-GPU runs are independent replicas
 (weak scaling): every rank advances its own case, no data-path collective.
 """
@@ -31,64 +31,91 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-NX, NY, NZ = 128, 64, 64
+# Workloads: the duct with a cantilevered plate of the benchmark configurations.
+#   duct_plate_128x64x64: 128 x 64 x 64 lattice, tau 0.55, inlet u_x 0.05, plate
+#     2 x 32 x 48 cells (24,576 particles); the metric's configuration (default).
+#   duct_plate_256x128x128: 256 x 128 x 128 lattice, tau 0.52, inlet u_x 0.04,
+#     plate 4 x 64 x 96 cells (196,608 particles); the precision form's
+#     configuration, and a lattice larger than L2 for DRAM profiles.
+# Both: walls at j in {0, ny-1} and k in {0, nz-1}, E = 0.02 and nu = 0.3 in
+# lattice units, density 1.2, moving_boundary coupling subcycled with 120 LBM
+# substeps per FSI step and 40 MPM substeps per FSI step (the explicit MPM
+# limit for E = 0.02: c dt / dx ~ 0.45 at 3 lattice steps per MPM substep).
+WORKLOADS = {
+    "duct_plate_128x64x64": dict(lattice=(128, 64, 64), tau=0.55, u_in=0.05, plate=(2, 32, 48)),
+    "duct_plate_256x128x128": dict(lattice=(256, 128, 128), tau=0.52, u_in=0.04, plate=(4, 64, 96)),
+}
+DEFAULT_WORKLOAD = "duct_plate_128x64x64"
 S_SUB = 120
-TAU = 0.55
-U_IN = 0.05
 DT_LBM = 1.0e-3            # physical seconds per LBM step (sets the unit bridge)
 E_LU, NU_POISSON, RHO_S = 0.02, 0.3, 1.2
 M_SUB = 40                 # MPM substeps per FSI step (M = 1 with E = 0.02 lu is CFL-unstable: c dt/dx ~ 15)
-PLATE = (2, 32, 48)
 # The reference's default inlet/outlet (equilibrium reset).  Its regularized
 # variants diverge after ~450 substeps in this duct with the reference's own
 # operator (the CPU oracle and the CUDA path agree), so they are exercised by
 # the parity tests, not by the benchmark run.
 OPEN_BOUNDARY = "equilibrium_all_population_reset"
-# reaction-force cap per particle (normalised units); the reference default
-# (1e-4) lets a particle of this plate accelerate at ~1.4e3 and the plate folds
-REACTION_CAP = 1.0e-8
+# reaction-force cap per particle (normalised units) at 128 cells along x,
+# scaled with the particle volume; the reference default (1e-4) lets a
+# particle of this plate accelerate at ~1.4e3 and the plate folds
+REACTION_CAP_128 = 1.0e-8
 FALLBACK_HBM_GBS = 6650.0
 
 
-def case_config():
+class Workload:
+    def __init__(self, name):
+        if name not in WORKLOADS:
+            raise SystemExit(f"unknown workload {name!r}; choose from {sorted(WORKLOADS)}")
+        w = WORKLOADS[name]
+        self.name = name
+        self.nx, self.ny, self.nz = w["lattice"]
+        self.tau, self.u_in, self.plate = w["tau"], w["u_in"], w["plate"]
+        self.reaction_cap = REACTION_CAP_128 * (128.0 / self.nx) ** 3
+        self.cells = self.nx * self.ny * self.nz
+
+    def tag(self):
+        return f"{self.name}_S{S_SUB}_M{M_SUB}"
+
+
+def case_config(wl):
     from mpm_lbm_b200.config import FSIDriverConfig
 
-    dx_phys = 1.0 / NX
-    nu_phys = (TAU - 0.5) / 3.0 * dx_phys ** 2 / DT_LBM
-    n_part = PLATE[0] * PLATE[1] * PLATE[2] * 8
+    dx_phys = 1.0 / wl.nx
+    nu_phys = (wl.tau - 0.5) / 3.0 * dx_phys ** 2 / DT_LBM
+    n_part = wl.plate[0] * wl.plate[1] * wl.plate[2] * 8
     return FSIDriverConfig(
-        coupling_mode="moving_boundary", n_grid=NX, n_particles=n_part, n_lbm_steps=10 ** 6,
-        mpm_substeps_per_lbm_step=M_SUB, mpm_dt=S_SUB * DT_LBM / M_SUB, target_u_lbm=(U_IN, 0.0, 0.0),
+        coupling_mode="moving_boundary", n_grid=wl.nx, n_particles=n_part, n_lbm_steps=10 ** 6,
+        mpm_substeps_per_lbm_step=M_SUB, mpm_dt=S_SUB * DT_LBM / M_SUB, target_u_lbm=(wl.u_in, 0.0, 0.0),
         lbm_boundary_condition_mode="duct_velocity_inlet_pressure_outlet",
-        lbm_open_boundary_semantics=OPEN_BOUNDARY, mb_force_cap_norm=REACTION_CAP,
+        lbm_open_boundary_semantics=OPEN_BOUNDARY, mb_force_cap_norm=wl.reaction_cap,
         fsi_exchange_mode="lbm_subcycled_per_fsi_step", lbm_substeps_per_fsi_step=S_SUB,
-        lbm_dt_phys_override_s=DT_LBM, official_fsi_dt_s=S_SUB * DT_LBM, target_u_lbm_for_dimensional_mapping=U_IN,
-        physical_duct_length_m=1.0, target_inlet_velocity_mps=U_IN * dx_phys / DT_LBM,
+        lbm_dt_phys_override_s=DT_LBM, official_fsi_dt_s=S_SUB * DT_LBM, target_u_lbm_for_dimensional_mapping=wl.u_in,
+        physical_duct_length_m=1.0, target_inlet_velocity_mps=wl.u_in * dx_phys / DT_LBM,
         lbm_viscosity_semantics="physical_nu_mapping", fluid_kinematic_viscosity_m2_s=nu_phys, output_interval=10)
 
 
-def case_geometry(seed=0):
+def case_geometry(wl, seed=0):
     from mpm_lbm_b200.geometry import duct_plate_case
 
-    solid, x, fixed, tip = duct_plate_case(NX, NY, NZ, plate_cells=PLATE, seed=seed)
-    dx = 1.0 / NX
+    solid, x, fixed, tip = duct_plate_case(wl.nx, wl.ny, wl.nz, plate_cells=wl.plate, seed=seed)
+    dx = 1.0 / wl.nx
     vol0 = np.full(len(x), dx ** 3 / 8.0, np.float32)
     mass = (vol0 * np.float32(RHO_S)).astype(np.float32)
     return solid, {"x": x, "vol0": vol0, "mass": mass, "fixed": fixed, "free_tip": tip}
 
 
-def material():
-    e_norm = E_LU * ((1.0 / NX) / DT_LBM) ** 2
+def material(wl):
+    e_norm = E_LU * ((1.0 / wl.nx) / DT_LBM) ** 2
     return {"young_modulus": e_norm, "poisson_ratio": NU_POISSON, "p_rho": RHO_S}
 
 
-def make_driver(storage="fp32", graph=True, device="cuda"):
+def make_driver(wl, storage="fp32", graph=True, device="cuda"):
     from mpm_lbm_b200.driver import FSIDriver3D
 
-    solid, parts = case_geometry()
-    drv = FSIDriver3D(case_config(), tempfile.mkdtemp(prefix="fsi_bench_"), population_storage=storage,
-                      lattice_shape=(NX, NY, NZ), material=material(), static_solid=solid, initial_particles=parts,
-                      use_cuda_graph=graph, device=device)
+    solid, parts = case_geometry(wl)
+    drv = FSIDriver3D(case_config(wl), tempfile.mkdtemp(prefix="fsi_bench_"), population_storage=storage,
+                      lattice_shape=(wl.nx, wl.ny, wl.nz), material=material(wl), static_solid=solid,
+                      initial_particles=parts, use_cuda_graph=graph, device=device)
     drv.initialize()
     return drv
 
@@ -104,12 +131,16 @@ def measured_peak():
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+    """nvidia-smi clocks / throttle reasons sampled during the timed region.
+
+    The sampler is started and its first sample awaited before the timed
+    region opens, so that the samples cover the region itself."""
 
     def __init__(self, gpu_index=0):
         self.proc = None
         self.lines = []
         self.gpu = gpu_index
+        self.marks = []
 
     def __enter__(self):
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
@@ -121,13 +152,22 @@ class ClockSampler:
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            t0 = time.time()
+            while not self.lines and time.time() - t0 < 5.0:
+                time.sleep(0.01)
         except Exception:
             self.proc = None
         return self
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.time(), line.strip()))
+
+    def open_region(self):
+        self.marks = [time.time()]
+
+    def close_region(self):
+        self.marks.append(time.time())
 
     def __exit__(self, *a):
         if self.proc is not None:
@@ -140,7 +180,10 @@ class ClockSampler:
     def summary(self):
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        lo, hi = (self.marks + [None, None])[:2] if self.marks else (None, None)
+        for ts, ln in self.lines:
+            if lo is not None and hi is not None and not (lo - 0.1 <= ts <= hi + 0.1):
+                continue
             p = [x.strip() for x in ln.split(",")]
             if len(p) < 9:
                 continue
@@ -157,38 +200,48 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_baseline(sample_substeps=S_SUB, sample_steps=1, mpm_substeps=M_SUB):
-    """The CPU oracle (C++ restatement, OpenMP, all host threads) on the same case."""
+def oracle_driver(wl, substeps, mpm_substeps):
+    """The CPU oracle (C++ restatement, OpenMP over cells on all host threads)
+    set up on the same case: FSI steps of `substeps` LBM substeps and
+    `mpm_substeps` MPM substeps."""
     from oracle import oracle as orc
 
-    cfg = case_config()
-    solid, parts = case_geometry()
+    cfg = case_config(wl)
+    solid, parts = case_geometry(wl)
     sim = cfg.make_unified_sim_config()
     threads = os.cpu_count() or 1
-    vel = ((U_IN, 0, 0), (0, 0, 0), (0, 0, 0), (0, 0, 0), (0, 0, 0), (0, 0, 0))
-    lbm = orc.OracleLBM(NX, NY, NZ, niu=sim.lbm_niu, relaxation_semantics=sim.lbm_relaxation_semantics,
+    vel = ((wl.u_in, 0, 0), (0, 0, 0), (0, 0, 0), (0, 0, 0), (0, 0, 0), (0, 0, 0))
+    lbm = orc.OracleLBM(wl.nx, wl.ny, wl.nz, niu=sim.lbm_niu, relaxation_semantics=sim.lbm_relaxation_semantics,
                         open_boundary_semantics=cfg.lbm_open_boundary_semantics, bc=(2, 1, 0, 0, 0, 0),
                         rho_bc=(1.0,) * 6, vel_bc=vel, limiter_enabled=cfg.open_boundary_limiter_enabled)
     lbm.threads = threads
     lbm.init_geo_array(solid)
     lbm.init_simulation()
-    mat = material()
+    mat = material(wl)
     mc = sim.make_mpm_config(gravity=cfg.gravity, **mat)
-    mpm = orc.OracleMPM(NX, mc.dx, mc.dt, len(parts["x"]), gravity=mc.gravity, young_modulus=mc.young_modulus,
+    mpm = orc.OracleMPM(wl.nx, mc.dx, mc.dt, len(parts["x"]), gravity=mc.gravity, young_modulus=mc.young_modulus,
                         poisson_ratio=mc.poisson_ratio, p_rho=mc.p_rho)
     mpm.init_from_numpy(parts["x"], parts["vol0"], parts["mass"], fixed_mask_np=parts["fixed"])
-    cpl = orc.OracleCoupling(NX, sim.dx_norm, sim.lbm_dt_phys, mb_force_cap_norm=cfg.mb_force_cap_norm)
+    cpl = orc.OracleCoupling(wl.nx, sim.dx_norm, sim.lbm_dt_phys, mb_force_cap_norm=cfg.mb_force_cap_norm)
     drv = orc.OracleFSIDriver(lbm, mpm, cpl, fsi_exchange_mode="lbm_subcycled_per_fsi_step",
-                              lbm_substeps_per_fsi_step=sample_substeps, mpm_substeps_per_lbm_step=mpm_substeps)
+                              lbm_substeps_per_fsi_step=substeps, mpm_substeps_per_lbm_step=mpm_substeps)
+    return drv, threads
+
+
+def cpu_sample_text(wl, steps, substeps, mpm_substeps):
+    return (f"{steps} FSI step(s) x ({substeps} LBM substeps + {mpm_substeps} MPM substeps) of the same "
+            f"{wl.nx}x{wl.ny}x{wl.nz} case, CPU oracle (C++ restatement, OpenMP over cells)")
+
+
+def cpu_baseline(wl, substeps=S_SUB, steps=1, mpm_substeps=M_SUB):
+    """MLUPS of the CPU oracle on a bounded sample of the workload."""
+    drv, threads = oracle_driver(wl, substeps, mpm_substeps)
     t0 = time.perf_counter()
-    for _ in range(sample_steps):
+    for _ in range(steps):
         drv.step_once()
     dt = time.perf_counter() - t0
-    mlups = sample_steps * sample_substeps * NX * NY * NZ / dt / 1e6
-    return {"value": mlups, "unit": "MLUPS", "cores": threads, "kind": "port",
-            "sample": f"{sample_steps} FSI step(s) x ({sample_substeps} LBM substeps + {mpm_substeps} MPM substeps) of "
-                      f"the same {NX}x{NY}x{NZ} case, CPU oracle (C++ restatement, OpenMP for the cell loops)",
-            "seconds": dt}
+    return {"value": steps * substeps * wl.cells / dt / 1e6, "unit": "MLUPS", "cores": threads, "kind": "port",
+            "sample": cpu_sample_text(wl, steps, substeps, mpm_substeps)}
 
 
 def dist_setup():
@@ -206,49 +259,92 @@ def dist_setup():
     return ws, rank, local
 
 
-def run_reference(args, ws, rank):
+def run_reference(args, wl, ws, rank):
+    """The reference arm: the reference's algorithm on the host CPU cores.  The
+    reference itself (Taichi) is not installed on this image, so its CPU
+    restatement (the oracle) runs; each step is a bounded sample of the
+    workload: one FSI step of --ref-substeps LBM substeps."""
     if rank != 0:
         return
-    steps = []
+    sub = args.ref_substeps
+    msub = max(1, sub // 3)
+    drv, threads = oracle_driver(wl, sub, msub)
     for _ in range(args.warmup):
-        cpu_baseline(sample_substeps=4, sample_steps=1, mpm_substeps=1)
+        drv.step_once()
+    t0 = time.perf_counter()
     for _ in range(args.steps):
-        steps.append(cpu_baseline())
-    secs = sum(s["seconds"] for s in steps)
-    cells = args.steps * S_SUB * NX * NY * NZ
-    value = cells / secs / 1e6
-    cb = dict(steps[-1])
-    cb["value"] = value
-    cb.pop("seconds", None)
+        drv.step_once()
+    secs = time.perf_counter() - t0
+    value = args.steps * sub * wl.cells / secs / 1e6
+    cb = {"value": value, "unit": "MLUPS", "cores": threads, "kind": "port",
+          "sample": cpu_sample_text(wl, args.steps, sub, msub)}
     print(json.dumps({"impl": "reference", "metric": "coupled-FSI MLUPS", "value": value, "unit": "MLUPS",
                       "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
                       "ms_per_step": 1e3 * secs / args.steps, "higher_is_better": True, "scaling": "weak",
                       "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                      "config": {"workload": f"duct_plate_{NX}x{NY}x{NZ}_S{S_SUB}_M{M_SUB}",
-                                 "reference_runtime": "CPU oracle port; taichi is not installed on this image"},
+                      "config": {"workload": wl.tag(), "reference_step": f"{sub} LBM + {msub} MPM substeps",
+                                 "reference_runtime": "CPU restatement of the reference (taichi is not installed "
+                                                      "on this image)"},
                       "cpu_baseline": cb,
                       "e2e": {"value": value, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}),
           flush=True)
 
 
+def time_lbm_kernel(drv, storage, n_k1=40, reps=5):
+    """Average duration of the fused LBM step kernel: a CUDA graph of n_k1
+    back-to-back moving-boundary substeps, replayed reps times between events on
+    the stream the kernels run on."""
+    import torch
+
+    lbm = drv.lbm
+    stream = torch.cuda.current_stream()
+    graph = torch.cuda.CUDAGraph()
+    lbm.dirstats_enabled = False
+    torch.cuda.synchronize()
+    with torch.cuda.graph(graph):
+        for _ in range(n_k1):
+            lbm.step_moving_bounceback()
+    torch.cuda.synchronize()
+    graph.replay()  # warm
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        graph.replay()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    k1_ms = e0.elapsed_time(e1) / (reps * n_k1)
+    del graph
+    return k1_ms
+
+
+# DRAM bytes (read + write) of one k_lbm_step launch from an ncu capture of the
+# same workload's kernel (the profiles/ summary named below), per launch
+NCU_LBM_TRAFFIC = {}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--storage", default="fp32", choices=["fp32", "fp16"])
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-substeps", type=int, default=30,
+                    help="LBM substeps per timed step of the reference arm (bounded CPU sample)")
     args = ap.parse_args()
+    wl = Workload(args.workload)
     ws, rank, local = dist_setup()
     if args.impl == "reference":
-        run_reference(args, ws, rank)
+        run_reference(args, wl, ws, rank)
         return
     import torch
 
     device = f"cuda:{local}"
     torch.cuda.set_device(local)
-    drv = make_driver(args.storage, graph=True, device=device)
+    drv = make_driver(wl, args.storage, graph=True, device=device)
     lbm = drv.lbm
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)  # > L2 (126 MB)
     stream = torch.cuda.current_stream()
@@ -260,12 +356,15 @@ def main():
     # ---- timed region: K FSI steps, each bracketed by events; L2 flushed in between
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        clk.open_region()
         for k in range(args.steps):
             flush.fill_(float(k))
             evs[k][0].record(stream)
             drv.step_once()
             evs[k][1].record(stream)
         torch.cuda.synchronize()
+        clk.close_region()
     step_ms = [a.elapsed_time(b) for a, b in evs]
     total_ms = float(sum(step_ms))
     if ws > 1:
@@ -273,67 +372,51 @@ def main():
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         total_ms = float(t.item())
         torch.distributed.barrier()
-    cells = NX * NY * NZ
     fluid_cells = int(lbm.fluid_mask().sum().item())
-    value = ws * args.steps * S_SUB * cells / (total_ms * 1e-3) / 1e6
+    value = ws * args.steps * S_SUB * wl.cells / (total_ms * 1e-3) / 1e6
     ms_step = total_ms / args.steps
     rows_ok = bool(np.isfinite(drv.lbm.get_stats()["rho_max"]))
+    kernels_per_step = drv.graph_kernels_per_step
 
-    # ---- dominant kernel: the fused LBM step, graph of S_SUB-1 launches timed with events
-    k1_graph = torch.cuda.CUDAGraph()
-    lbm.dirstats_enabled = False
-    torch.cuda.synchronize()
-    n_k1 = 40
-    with torch.cuda.graph(k1_graph):
-        for _ in range(n_k1):
-            lbm.step_moving_bounceback()
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    k1_graph.replay()  # warm
-    torch.cuda.synchronize()
-    reps = 5
-    e0.record(stream)
-    for _ in range(reps):
-        k1_graph.replay()
-    e1.record(stream)
-    torch.cuda.synchronize()
-    k1_ms = e0.elapsed_time(e1) / (reps * n_k1)
+    # ---- dominant kernel: the fused LBM step
+    k1_ms = time_lbm_kernel(drv, args.storage)
     pop_bytes = 2 if args.storage == "fp16" else 4
-    alg_bytes = fluid_cells * 19 * 2 * pop_bytes + cells * 1
+    alg_bytes = fluid_cells * 19 * 2 * pop_bytes + wl.cells * 1
     peak, peak_kind = measured_peak()
     achieved = alg_bytes / (k1_ms * 1e-3) / 1e9
+    traffic = NCU_LBM_TRAFFIC.get((wl.name, args.storage))
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": None, "peak_source": peak_kind, "kernel": "k_lbm_step",
+                "traffic": traffic, "peak_source": f"{peak_kind} (hbm_gbs)", "kernel": "k_lbm_step",
                 "kernel_ms": k1_ms, "alg_bytes_per_launch": alg_bytes,
-                "alg_bytes_per_cell": f"2*19*{pop_bytes} per fluid cell + 1 per cell"}
+                "alg_bytes_per_cell": f"2*19*{pop_bytes} per fluid cell + 1 (flags) per cell"}
 
     # ---- end to end through the public API with host buffers
-    pinned_in = torch.tensor([U_IN, 0.0, 0.0], dtype=torch.float32).pin_memory()
+    pinned_in = torch.tensor([wl.u_in, 0.0, 0.0], dtype=torch.float32).pin_memory()
     n = drv.solid.n_particles
     pinned_out = torch.empty(3, n, dtype=torch.float32).pin_memory()
-    drv2 = drv
     torch.cuda.synchronize()
     e_steps = max(3, args.steps // 2)
     t0 = time.perf_counter()
     for k in range(e_steps):
-        pinned_in[0] = U_IN
-        drv2.lbm.set_inlet_velocity_async(pinned_in)
-        drv2.step_once()
-        pinned_out.copy_(drv2.solid.t_x, non_blocking=True)
+        pinned_in[0] = wl.u_in
+        drv.lbm.set_inlet_velocity_async(pinned_in)
+        drv.step_once()
+        pinned_out.copy_(drv.solid.t_x, non_blocking=True)
         torch.cuda.current_stream().synchronize()
     e2e_s = time.perf_counter() - t0
-    e2e_value = ws * e_steps * S_SUB * cells / e2e_s / 1e6
+    e2e_value = ws * e_steps * S_SUB * wl.cells / e2e_s / 1e6
 
     result = {
         "metric": "coupled-FSI MLUPS", "value": value, "unit": "MLUPS", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32" if args.storage == "fp32" else "f16-storage/f32-compute",
         "data": "synthetic",
-        "config": {"workload": f"duct_plate_{NX}x{NY}x{NZ}_S{S_SUB}_M{M_SUB}", "lattice": [NX, NY, NZ],
+        "config": {"workload": wl.tag(), "lattice": [wl.nx, wl.ny, wl.nz],
                    "lbm_substeps_per_fsi_step": S_SUB, "mpm_substeps_per_fsi_step": M_SUB,
-                   "particles": int(n), "fluid_cells": fluid_cells, "collision": "mrt", "tau": TAU,
+                   "particles": int(n), "fluid_cells": fluid_cells, "collision": "mrt", "tau": wl.tau,
                    "coupling": "moving_boundary/engineering/subcycled",
-                   "open_boundary": OPEN_BOUNDARY, "reaction_cap": REACTION_CAP, "population_storage": args.storage,
+                   "open_boundary": OPEN_BOUNDARY, "reaction_cap": wl.reaction_cap,
+                   "population_storage": args.storage,
                    "l2": "flushed (256 MB write) between timed FSI steps", "cuda_graph": True,
                    "parallelism": f"replicas x{ws}"},
         "particle_updates_per_s": ws * args.steps * M_SUB * n / (total_ms * 1e-3),
@@ -341,18 +424,18 @@ def main():
         "clocks": clk.summary(),
         "e2e": {"value": e2e_value, "unit": "MLUPS", "h2d_bytes_per_step": 12, "d2h_bytes_per_step": 12 * n,
                 "api": "FSIDriver3D.step_once + inlet velocity H2D from pinned host + particle positions D2H"},
-        "gpu_launches": args.steps * (2 + 1 + 3 + S_SUB + 1 + 4 * M_SUB),
+        "gpu_launches": None if kernels_per_step is None else int(round(args.steps * kernels_per_step)),
+        "gpu_launches_per_step": kernels_per_step,
         "finite": rows_ok,
     }
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         try:
-            result["cpu_baseline"] = {k: v for k, v in cpu_baseline().items() if k != "seconds"}
+            result["cpu_baseline"] = cpu_baseline(wl)
         except Exception as exc:  # reported, not fatal
             result["cpu_baseline"] = {"error": str(exc)}
     if rank == 0:
         print(json.dumps(result), flush=True)
     if ws > 1:
-        del k1_graph
         drv._graph = None
         torch.distributed.destroy_process_group()
 

@@ -311,6 +311,11 @@ int fsi_mpm_grid_velocity(const FsiGrid* g, const FsiMpmParams* mp, float* out, 
 
 /* ---- misc --------------------------------------------------------------- */
 int fsi_abi_version(void);
+/* Kernel launches issued by this library since it was loaded (all threads).
+ * During stream capture a launch becomes a graph node, so the difference
+ * across a capture is the number of this library's kernels in the graph.
+ * Instrumentation only: the reference has no counterpart. */
+uint64_t fsi_launch_count(void);
 int fsi_last_error(char* buf, size_t len);
 
 #ifdef __cplusplus

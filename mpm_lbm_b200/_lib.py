@@ -117,7 +117,10 @@ SIGNATURES = {
     "fsi_mpm_grid_velocity": [_P(FsiGrid), _P(FsiMpmParams), c_p, c_p],
     "fsi_abi_version": [],
     "fsi_last_error": [ctypes.c_char_p, ctypes.c_size_t],
+    "fsi_launch_count": [],
 }
+# entry points that do not return int
+RESTYPES = {"fsi_launch_count": ctypes.c_uint64}
 
 _lock = threading.Lock()
 _lib = None
@@ -139,7 +142,7 @@ def load():
         for name, args in SIGNATURES.items():
             fn = getattr(lib, name)
             fn.argtypes = args
-            fn.restype = ctypes.c_int
+            fn.restype = RESTYPES.get(name, ctypes.c_int)
         if lib.fsi_abi_version() != 1:
             raise FsiError("libfsi_b200.so ABI version mismatch")
         _lib = lib
@@ -157,6 +160,11 @@ def call(name, *args):
     if rc != 0:
         raise FsiError(f"{name} failed ({rc}): {last_error()}")
     return rc
+
+
+def launch_count() -> int:
+    """Kernel launches issued by libfsi_b200.so so far (graph nodes while capturing)."""
+    return int(load().fsi_launch_count())
 
 
 def ptr(t):

@@ -11,6 +11,8 @@
 namespace fsi {
 
 void set_error(const std::string& msg);
+// counts kernel launches issued through this library (see fsi_launch_count)
+void count_launch();
 
 inline int cuda_check(cudaError_t e, const char* what) {
   if (e == cudaSuccess) return FSI_OK;
@@ -18,7 +20,12 @@ inline int cuda_check(cudaError_t e, const char* what) {
   return FSI_E_CUDA;
 }
 
-inline int launch_check(const char* what) { return cuda_check(cudaGetLastError(), what); }
+// every kernel launch of the library is followed by exactly one launch_check
+inline int launch_check(const char* what) {
+  const int rc = cuda_check(cudaGetLastError(), what);
+  if (rc == FSI_OK) count_launch();
+  return rc;
+}
 
 inline int invalid(const std::string& msg) {
   set_error(msg);

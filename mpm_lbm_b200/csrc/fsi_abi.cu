@@ -1,5 +1,6 @@
 // ABI housekeeping: error strings and version.
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <string>
 
@@ -8,7 +9,11 @@
 namespace fsi {
 static thread_local std::string g_last_error;
 void set_error(const std::string& msg) { g_last_error = msg; }
+static std::atomic<uint64_t> g_launches{0};
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 }  // namespace fsi
+
+extern "C" uint64_t fsi_launch_count(void) { return fsi::g_launches.load(std::memory_order_relaxed); }
 
 extern "C" int fsi_abi_version(void) { return FSI_ABI_VERSION; }
 

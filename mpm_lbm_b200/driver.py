@@ -22,6 +22,7 @@ import time
 import numpy as np
 import torch
 
+from ._lib import launch_count
 from .config import FSIDriverConfig, GridUnitMapper
 from .coupling import (LinkAreaMovingBoundaryCoupler3D, MovingBoundaryFSICoupler3D, MPMToLBMProjector3D,
                        PenaltyFSICoupler3D)
@@ -80,6 +81,7 @@ class FSIDriver3D:
         self.use_cuda_graph = bool(use_cuda_graph)
         self._graph = None
         self._graph_steps = 0
+        self.graph_kernels_per_step = None
 
     # ------------------------------------------------------------ init
     def _geometry_config(self):
@@ -223,9 +225,12 @@ class FSIDriver3D:
             torch.cuda.synchronize()
             snap = self._counters()
             g = torch.cuda.CUDAGraph()
+            n0 = launch_count()
             with torch.cuda.graph(g):
                 for _ in range(period):
                     self._step_eager()
+            # this library's kernels per replayed FSI step (torch's own fills/copies not included)
+            self.graph_kernels_per_step = (launch_count() - n0) / period
             self._graph_delta = tuple(b - a for a, b in zip(snap, self._counters()))
             self._restore_counters(snap)
             self._graph = g

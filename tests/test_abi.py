@@ -17,7 +17,7 @@ HEADER = os.path.join(ROOT, "include", "fsi_b200.h")
 
 def declared_functions():
     text = open(HEADER, encoding="utf-8").read()
-    return sorted(set(re.findall(r"^int\s+(fsi_\w+)\s*\(", text, flags=re.M)))
+    return sorted(set(re.findall(r"^(?:int|uint64_t)\s+(fsi_\w+)\s*\(", text, flags=re.M)))
 
 
 @pytest.fixture(scope="module")
@@ -33,6 +33,8 @@ def test_every_declared_symbol_is_exported_and_bound(lib):
         assert hasattr(lib, name), name
         assert name in _lib.SIGNATURES, name
     assert lib.fsi_abi_version() == 1
+    # no kernel has run in this process without a GPU
+    assert _lib.launch_count() == 0
 
 
 def test_struct_layouts_match_c(tmp_path):
