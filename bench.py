@@ -31,93 +31,43 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-# Workloads: the duct with a cantilevered plate of the benchmark configurations.
+# Workloads: the duct with a cantilevered plate of the benchmark configurations
+# (mpm_lbm_b200.cases.DuctPlateCase).
 #   duct_plate_128x64x64: 128 x 64 x 64 lattice, tau 0.55, inlet u_x 0.05, plate
 #     2 x 32 x 48 cells (24,576 particles); the metric's configuration (default).
 #   duct_plate_256x128x128: 256 x 128 x 128 lattice, tau 0.52, inlet u_x 0.04,
 #     plate 4 x 64 x 96 cells (196,608 particles); the precision form's
 #     configuration, and a lattice larger than L2 for DRAM profiles.
-# Both: walls at j in {0, ny-1} and k in {0, nz-1}, E = 0.02 and nu = 0.3 in
-# lattice units, density 1.2, moving_boundary coupling subcycled with 120 LBM
-# substeps per FSI step and 40 MPM substeps per FSI step (the explicit MPM
-# limit for E = 0.02: c dt / dx ~ 0.45 at 3 lattice steps per MPM substep).
+# Both: E = 0.02 and nu = 0.3 in lattice units, density 1.2, moving_boundary
+# coupling subcycled with S = 120 LBM substeps per FSI step and M = 40 MPM
+# substeps per FSI step (the explicit MPM limit for E = 0.02: c dt / dx ~ 0.45
+# at 3 lattice steps per MPM substep; M = 1 would give c dt / dx ~ 15).  The
+# open boundaries are the reference's default (equilibrium reset): its
+# regularized variants diverge after ~450 substeps in this duct with the
+# reference's own operator (the CPU oracle and the CUDA path agree), so they
+# are exercised by the parity tests, not by the benchmark run.
 WORKLOADS = {
     "duct_plate_128x64x64": dict(lattice=(128, 64, 64), tau=0.55, u_in=0.05, plate=(2, 32, 48)),
     "duct_plate_256x128x128": dict(lattice=(256, 128, 128), tau=0.52, u_in=0.04, plate=(4, 64, 96)),
 }
 DEFAULT_WORKLOAD = "duct_plate_128x64x64"
-S_SUB = 120
-DT_LBM = 1.0e-3            # physical seconds per LBM step (sets the unit bridge)
-E_LU, NU_POISSON, RHO_S = 0.02, 0.3, 1.2
-M_SUB = 40                 # MPM substeps per FSI step (M = 1 with E = 0.02 lu is CFL-unstable: c dt/dx ~ 15)
-# The reference's default inlet/outlet (equilibrium reset).  Its regularized
-# variants diverge after ~450 substeps in this duct with the reference's own
-# operator (the CPU oracle and the CUDA path agree), so they are exercised by
-# the parity tests, not by the benchmark run.
-OPEN_BOUNDARY = "equilibrium_all_population_reset"
-# reaction-force cap per particle (normalised units) at 128 cells along x,
-# scaled with the particle volume; the reference default (1e-4) lets a
-# particle of this plate accelerate at ~1.4e3 and the plate folds
-REACTION_CAP_128 = 1.0e-8
 FALLBACK_HBM_GBS = 6650.0
 
 
 class Workload:
     def __init__(self, name):
+        from mpm_lbm_b200.cases import DuctPlateCase
+
         if name not in WORKLOADS:
             raise SystemExit(f"unknown workload {name!r}; choose from {sorted(WORKLOADS)}")
-        w = WORKLOADS[name]
         self.name = name
-        self.nx, self.ny, self.nz = w["lattice"]
-        self.tau, self.u_in, self.plate = w["tau"], w["u_in"], w["plate"]
-        self.reaction_cap = REACTION_CAP_128 * (128.0 / self.nx) ** 3
-        self.cells = self.nx * self.ny * self.nz
+        self.case = DuctPlateCase(**WORKLOADS[name])
+        self.nx, self.ny, self.nz = self.case.lattice
+        self.cells = self.case.cells
+        self.S, self.M = self.case.lbm_substeps, self.case.mpm_substeps
 
     def tag(self):
-        return f"{self.name}_S{S_SUB}_M{M_SUB}"
-
-
-def case_config(wl):
-    from mpm_lbm_b200.config import FSIDriverConfig
-
-    dx_phys = 1.0 / wl.nx
-    nu_phys = (wl.tau - 0.5) / 3.0 * dx_phys ** 2 / DT_LBM
-    n_part = wl.plate[0] * wl.plate[1] * wl.plate[2] * 8
-    return FSIDriverConfig(
-        coupling_mode="moving_boundary", n_grid=wl.nx, n_particles=n_part, n_lbm_steps=10 ** 6,
-        mpm_substeps_per_lbm_step=M_SUB, mpm_dt=S_SUB * DT_LBM / M_SUB, target_u_lbm=(wl.u_in, 0.0, 0.0),
-        lbm_boundary_condition_mode="duct_velocity_inlet_pressure_outlet",
-        lbm_open_boundary_semantics=OPEN_BOUNDARY, mb_force_cap_norm=wl.reaction_cap,
-        fsi_exchange_mode="lbm_subcycled_per_fsi_step", lbm_substeps_per_fsi_step=S_SUB,
-        lbm_dt_phys_override_s=DT_LBM, official_fsi_dt_s=S_SUB * DT_LBM, target_u_lbm_for_dimensional_mapping=wl.u_in,
-        physical_duct_length_m=1.0, target_inlet_velocity_mps=wl.u_in * dx_phys / DT_LBM,
-        lbm_viscosity_semantics="physical_nu_mapping", fluid_kinematic_viscosity_m2_s=nu_phys, output_interval=10)
-
-
-def case_geometry(wl, seed=0):
-    from mpm_lbm_b200.geometry import duct_plate_case
-
-    solid, x, fixed, tip = duct_plate_case(wl.nx, wl.ny, wl.nz, plate_cells=wl.plate, seed=seed)
-    dx = 1.0 / wl.nx
-    vol0 = np.full(len(x), dx ** 3 / 8.0, np.float32)
-    mass = (vol0 * np.float32(RHO_S)).astype(np.float32)
-    return solid, {"x": x, "vol0": vol0, "mass": mass, "fixed": fixed, "free_tip": tip}
-
-
-def material(wl):
-    e_norm = E_LU * ((1.0 / wl.nx) / DT_LBM) ** 2
-    return {"young_modulus": e_norm, "poisson_ratio": NU_POISSON, "p_rho": RHO_S}
-
-
-def make_driver(wl, storage="fp32", graph=True, device="cuda"):
-    from mpm_lbm_b200.driver import FSIDriver3D
-
-    solid, parts = case_geometry(wl)
-    drv = FSIDriver3D(case_config(wl), tempfile.mkdtemp(prefix="fsi_bench_"), population_storage=storage,
-                      lattice_shape=(wl.nx, wl.ny, wl.nz), material=material(wl), static_solid=solid,
-                      initial_particles=parts, use_cuda_graph=graph, device=device)
-    drv.initialize()
-    return drv
+        return f"{self.name}_S{self.S}_M{self.M}"
 
 
 def measured_peak():
@@ -202,30 +152,11 @@ class ClockSampler:
 
 def oracle_driver(wl, substeps, mpm_substeps):
     """The CPU oracle (C++ restatement, OpenMP over cells on all host threads)
-    set up on the same case: FSI steps of `substeps` LBM substeps and
-    `mpm_substeps` MPM substeps."""
+    on the same case: FSI steps of `substeps` LBM and `mpm_substeps` MPM substeps."""
     from oracle import oracle as orc
 
-    cfg = case_config(wl)
-    solid, parts = case_geometry(wl)
-    sim = cfg.make_unified_sim_config()
     threads = os.cpu_count() or 1
-    vel = ((wl.u_in, 0, 0), (0, 0, 0), (0, 0, 0), (0, 0, 0), (0, 0, 0), (0, 0, 0))
-    lbm = orc.OracleLBM(wl.nx, wl.ny, wl.nz, niu=sim.lbm_niu, relaxation_semantics=sim.lbm_relaxation_semantics,
-                        open_boundary_semantics=cfg.lbm_open_boundary_semantics, bc=(2, 1, 0, 0, 0, 0),
-                        rho_bc=(1.0,) * 6, vel_bc=vel, limiter_enabled=cfg.open_boundary_limiter_enabled)
-    lbm.threads = threads
-    lbm.init_geo_array(solid)
-    lbm.init_simulation()
-    mat = material(wl)
-    mc = sim.make_mpm_config(gravity=cfg.gravity, **mat)
-    mpm = orc.OracleMPM(wl.nx, mc.dx, mc.dt, len(parts["x"]), gravity=mc.gravity, young_modulus=mc.young_modulus,
-                        poisson_ratio=mc.poisson_ratio, p_rho=mc.p_rho)
-    mpm.init_from_numpy(parts["x"], parts["vol0"], parts["mass"], fixed_mask_np=parts["fixed"])
-    cpl = orc.OracleCoupling(wl.nx, sim.dx_norm, sim.lbm_dt_phys, mb_force_cap_norm=cfg.mb_force_cap_norm)
-    drv = orc.OracleFSIDriver(lbm, mpm, cpl, fsi_exchange_mode="lbm_subcycled_per_fsi_step",
-                              lbm_substeps_per_fsi_step=substeps, mpm_substeps_per_lbm_step=mpm_substeps)
-    return drv, threads
+    return orc.fsi_driver_for_case(wl.case, substeps=substeps, mpm_substeps=mpm_substeps, threads=threads), threads
 
 
 def cpu_sample_text(wl, steps, substeps, mpm_substeps):
@@ -233,8 +164,9 @@ def cpu_sample_text(wl, steps, substeps, mpm_substeps):
             f"{wl.nx}x{wl.ny}x{wl.nz} case, CPU oracle (C++ restatement, OpenMP over cells)")
 
 
-def cpu_baseline(wl, substeps=S_SUB, steps=1, mpm_substeps=M_SUB):
-    """MLUPS of the CPU oracle on a bounded sample of the workload."""
+def cpu_baseline(wl, steps=1):
+    """MLUPS of the CPU oracle on a bounded sample of the workload: one FSI step."""
+    substeps, mpm_substeps = wl.S, wl.M
     drv, threads = oracle_driver(wl, substeps, mpm_substeps)
     t0 = time.perf_counter()
     for _ in range(steps):
@@ -332,6 +264,7 @@ def main():
     ap.add_argument("--storage", default="fp32", choices=["fp32", "fp16"])
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="default launch variants")
     ap.add_argument("--ref-substeps", type=int, default=30,
                     help="LBM substeps per timed step of the reference arm (bounded CPU sample)")
     args = ap.parse_args()
@@ -344,13 +277,19 @@ def main():
 
     device = f"cuda:{local}"
     torch.cuda.set_device(local)
-    drv = make_driver(wl, args.storage, graph=True, device=device)
+    drv = wl.case.make_driver(storage=args.storage, graph=True, device=device)
     lbm = drv.lbm
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)  # > L2 (126 MB)
     stream = torch.cuda.current_stream()
     for _ in range(max(args.warmup, 3)):
         drv.step_once()
     torch.cuda.synchronize()
+    tuning = None
+    if not args.no_autotune:
+        tuning = drv.autotune()  # launch variants timed on this state; the step graph is recaptured
+        for _ in range(2):
+            drv.step_once()
+        torch.cuda.synchronize()
     if ws > 1:
         torch.distributed.barrier()
     # ---- timed region: K FSI steps, each bracketed by events; L2 flushed in between
@@ -373,7 +312,7 @@ def main():
         total_ms = float(t.item())
         torch.distributed.barrier()
     fluid_cells = int(lbm.fluid_mask().sum().item())
-    value = ws * args.steps * S_SUB * wl.cells / (total_ms * 1e-3) / 1e6
+    value = ws * args.steps * wl.S * wl.cells / (total_ms * 1e-3) / 1e6
     ms_step = total_ms / args.steps
     rows_ok = bool(np.isfinite(drv.lbm.get_stats()["rho_max"]))
     kernels_per_step = drv.graph_kernels_per_step
@@ -391,20 +330,20 @@ def main():
                 "alg_bytes_per_cell": f"2*19*{pop_bytes} per fluid cell + 1 (flags) per cell"}
 
     # ---- end to end through the public API with host buffers
-    pinned_in = torch.tensor([wl.u_in, 0.0, 0.0], dtype=torch.float32).pin_memory()
+    pinned_in = torch.tensor([wl.case.u_in, 0.0, 0.0], dtype=torch.float32).pin_memory()
     n = drv.solid.n_particles
     pinned_out = torch.empty(3, n, dtype=torch.float32).pin_memory()
     torch.cuda.synchronize()
     e_steps = max(3, args.steps // 2)
     t0 = time.perf_counter()
     for k in range(e_steps):
-        pinned_in[0] = wl.u_in
+        pinned_in[0] = wl.case.u_in
         drv.lbm.set_inlet_velocity_async(pinned_in)
         drv.step_once()
         pinned_out.copy_(drv.solid.t_x, non_blocking=True)
         torch.cuda.current_stream().synchronize()
     e2e_s = time.perf_counter() - t0
-    e2e_value = ws * e_steps * S_SUB * wl.cells / e2e_s / 1e6
+    e2e_value = ws * e_steps * wl.S * wl.cells / e2e_s / 1e6
 
     result = {
         "metric": "coupled-FSI MLUPS", "value": value, "unit": "MLUPS", "n_gpus": ws, "steps": args.steps,
@@ -412,14 +351,16 @@ def main():
         "vs_baseline": None, "dtype": "f32" if args.storage == "fp32" else "f16-storage/f32-compute",
         "data": "synthetic",
         "config": {"workload": wl.tag(), "lattice": [wl.nx, wl.ny, wl.nz],
-                   "lbm_substeps_per_fsi_step": S_SUB, "mpm_substeps_per_fsi_step": M_SUB,
-                   "particles": int(n), "fluid_cells": fluid_cells, "collision": "mrt", "tau": wl.tau,
+                   "lbm_substeps_per_fsi_step": wl.S, "mpm_substeps_per_fsi_step": wl.M,
+                   "particles": int(n), "fluid_cells": fluid_cells, "collision": "mrt", "tau": wl.case.tau,
                    "coupling": "moving_boundary/engineering/subcycled",
-                   "open_boundary": OPEN_BOUNDARY, "reaction_cap": wl.reaction_cap,
+                   "open_boundary": wl.case.open_boundary, "reaction_cap": wl.case.reaction_cap,
                    "population_storage": args.storage,
                    "l2": "flushed (256 MB write) between timed FSI steps", "cuda_graph": True,
+                   "launch_variants": None if tuning is None else
+                   {"lbm_tune": tuning["lbm"]["choice"], "mpm_tune": tuning.get("mpm", {}).get("choice")},
                    "parallelism": f"replicas x{ws}"},
-        "particle_updates_per_s": ws * args.steps * M_SUB * n / (total_ms * 1e-3),
+        "particle_updates_per_s": ws * args.steps * wl.M * n / (total_ms * 1e-3),
         "roofline": roofline,
         "clocks": clk.summary(),
         "e2e": {"value": e2e_value, "unit": "MLUPS", "h2d_bytes_per_step": 12, "d2h_bytes_per_step": 12 * n,

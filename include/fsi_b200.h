@@ -119,8 +119,14 @@ typedef struct FsiLbmParams {
   float vel_bc_left[3], vel_bc_right[3];
   float ob_rho_min, ob_rho_max, ob_u_max, ob_noneq_cap, ob_floor;
   float penalty_beta, penalty_phi_min, penalty_cap;
-  int32_t pad;
+  int32_t tune;             /* FSI_TUNE_LBM_*: launch variant of the step kernel (results are identical) */
 } FsiLbmParams;
+
+/* launch variants of fsi_lbm_substep (FsiLbmParams.tune) */
+enum {
+  FSI_TUNE_LBM_OCC3 = 0,  /* registers for 3 CTAs of 256 threads per SM (default) */
+  FSI_TUNE_LBM_OCC4 = 1,  /* registers for 4 CTAs per SM (64 per thread) */
+};
 
 typedef struct FsiStepCtl {
   int32_t parity;       /* AA layout parity of the input state */
@@ -210,8 +216,18 @@ typedef struct FsiMpmParams {
   float damping;     /* >0 enables particle_velocity_post_g2p damping */
   int32_t bound;
   int32_t lock_z;
-  int32_t pad;
+  int32_t tune;      /* FSI_TUNE_MPM_* of the scatter | FSI_TUNE_MPM_* of the gather << 2 */
 } FsiMpmParams;
+
+/* launch variants of fsi_mpm_substep_binned (FsiMpmParams.tune = scatter
+ * variant | gather variant << 2); the other MPM entry points ignore it.
+ * Scatter: threads per chunk CTA of the P2G scatter.  Gather: threads per
+ * chunk CTA of the G2P, with 1, 2 or 4 lanes per particle. */
+enum {
+  FSI_TUNE_MPM_T128 = 0,  /* 128 threads per chunk CTA (default) */
+  FSI_TUNE_MPM_T256 = 1,  /* 256 threads */
+  FSI_TUNE_MPM_T512 = 2,  /* 512 threads */
+};
 
 typedef struct FsiCouplingParams {
   float inv_dx_norm, cell_volume_norm, vel_scale, eps_mass;
@@ -274,6 +290,7 @@ int fsi_mpm_g2p(const FsiParticles* pt, const FsiGrid* g, const FsiMpmParams* mp
  *     so no dense pass over the grid is made. */
 #define FSI_BIN_CHUNK 128
 #define FSI_BIN_EDGE 4
+#define FSI_MPM_PAYLOAD_ROWS 32
 
 /* count, start and chunk must be 16-byte aligned */
 typedef struct FsiMpmBins {
@@ -287,6 +304,7 @@ typedef struct FsiMpmBins {
   int32_t* box;         /* [2][max_chunks][6] node box (lo xyz, hi xyz) touched per chunk and buffer */
   int32_t* meta;        /* [4] chunk count, records in box[0], records in box[1], overflowed chunks;
                            zero before the first call */
+  float* payload;       /* [FSI_MPM_PAYLOAD_ROWS][n_particles] scratch: per-particle P2G data in bin order */
 } FsiMpmBins;
 
 /* n_bins and max_chunks for a particle count and grid edge */
@@ -308,6 +326,75 @@ int fsi_mpm_substep_binned(const FsiParticles* pt, const FsiGrid grid[2], const 
 /* grid velocity after a binned substep (the grid_v of the reference after
  * grid_update) from grid's momentum, mass and f_ext, into out [3][n^3] */
 int fsi_mpm_grid_velocity(const FsiGrid* g, const FsiMpmParams* mp, float* out, void* stream);
+
+/* ---- batched cases -------------------------------------------------------
+ * Many independent FSI cases (each its own lattice, particles, MPM grid,
+ * parameters and coupling mode) advanced together: each fsi_batch_* call
+ * runs one phase of the FSI step for every active case in one launch per
+ * kernel (grid.y = case slot, grid.x strides over the case's work).  The
+ * reference advances one FSIDriver3D per process (fsi_driver.py:425-531);
+ * a batch of N cases performs, per case, exactly the phases of
+ * FSIDriver3D.step_once with one LBM step per FSI step:
+ *   penalty:          fsi_batch_project, fsi_batch_lbm_substep (penalty force
+ *                     built in the step), then M x fsi_batch_mpm_substep
+ *   moving_boundary:  fsi_batch_project, fsi_batch_mask_rebuild,
+ *                     fsi_batch_lbm_substep, then M x fsi_batch_mpm_substep
+ * with fsi_batch_mpm_bin before the MPM substeps.  Cases must have no open
+ * boundaries (bc_left = bc_right = 0) and equal population storage.
+ *
+ * `cases` is a DEVICE array of FsiBatchCase; the calls read the descriptors
+ * there and advance the per-case step state (ctl, buf) on the device, so a
+ * sequence of calls can be captured in a CUDA graph and replayed.  The host
+ * keeps `dims` current (maxima over the active cases). */
+enum {
+  FSI_BATCH_PENALTY = 0,
+  FSI_BATCH_MOVING = 1,
+};
+
+typedef struct FsiBatchCase {
+  FsiLbmState lbm;
+  FsiLbmParams lp;
+  FsiStepCtl ctl;                 /* parity, pp advanced by fsi_batch_lbm_substep */
+  FsiParticles pt;
+  FsiGrid grid[2];                /* MPM grid buffers of the binned substep */
+  FsiMpmBins bins;
+  FsiMpmParams mp;
+  FsiCouplingParams cp;           /* reaction kind 0 penalty, 1 engineering, 2 link-area */
+  FsiCouplingStats* proj_stats;   /* device [1] */
+  FsiCouplingStats* react_stats;  /* device [2], zero before the first substep */
+  float mask_threshold;           /* dynamic_solid_threshold */
+  int32_t mode;                   /* FSI_BATCH_* */
+  int32_t active;                 /* 0: empty slot, skipped */
+  int32_t buf;                    /* grid buffer of the next MPM substep, advanced on the device */
+} FsiBatchCase;
+
+typedef struct FsiBatchDims {
+  int32_t n_cases;                /* slots in `cases` (active or not) */
+  int32_t store_fp16;             /* population storage of every case */
+  int32_t max_lbm_tiles;          /* max over cases of ceil(nx / 32) * ceil(ny * nz / 8) */
+  int32_t max_particles;
+  int64_t max_cells;              /* max nx * ny * nz */
+  int32_t max_chunks;             /* max FsiMpmBins.max_chunks */
+  int32_t max_bins;               /* max FsiMpmBins.n_bins */
+  int32_t mpm_tune;               /* FsiMpmParams.tune of the batched MPM substep (all cases) */
+  int32_t pad;
+} FsiBatchDims;
+
+/* MPMToLBMProjector3D.project per case (coupling/projection.py:21-97). */
+int fsi_batch_project(FsiBatchCase* cases, const FsiBatchDims* dims, void* stream);
+/* update_dynamic_solid + reinitialize_new_fluid_cells per moving-boundary case
+ * (fluid.py:1847-1877); penalty cases are skipped. */
+int fsi_batch_mask_rebuild(FsiBatchCase* cases, const FsiBatchDims* dims, void* stream);
+/* One LBM step per case: step_moving_bounceback (fluid.py:2105) for moving
+ * cases, step (2099) with the penalty force (penalty.py:59-88) for penalty
+ * cases; then the case's parity and ping-pong slot advance. */
+int fsi_batch_lbm_substep(FsiBatchCase* cases, const FsiBatchDims* dims, void* stream);
+/* fsi_mpm_bin per case. */
+int fsi_batch_mpm_bin(FsiBatchCase* cases, const FsiBatchDims* dims, void* stream);
+/* One binned MPM substep per case with its reaction transfer (penalty.py:
+ * 90-129 / moving_boundary.py:58-110 / link_area.py:139-193) from the last
+ * LBM step's force field; then the case's grid buffer advances. */
+int fsi_batch_mpm_substep(FsiBatchCase* cases, const FsiBatchDims* dims, void* stream);
 
 /* ---- misc --------------------------------------------------------------- */
 int fsi_abi_version(void);

@@ -1,0 +1,84 @@
+"""Autotuner for the launch variants of the step kernels.
+
+The variants differ only in how a kernel maps onto the SMs: the register
+budget of the LBM step kernel (3 or 4 resident CTAs per SM; bit-identical
+results), and the threads per particle chunk of the binned MPM substep (the
+same arithmetic; the grid sums are float atomics whose order, and so whose
+last-bit rounding, varies from run to run with any variant).  The tuner times each variant with CUDA events
+on the caller's own state -- trial steps on a device snapshot that is
+restored afterwards -- and keeps the fastest.  It runs before a CUDA graph of
+the step is captured (a captured graph keeps the variant it was built with).
+"""
+
+from __future__ import annotations
+
+import torch
+
+from ._lib import FSI_TUNE_LBM_OCC3, FSI_TUNE_LBM_OCC4, FSI_TUNE_MPM_T128, FSI_TUNE_MPM_T256, FSI_TUNE_MPM_T512
+
+
+def _time_ms(fn, steps, reps):
+    stream = torch.cuda.current_stream()
+    best = float("inf")
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1) / steps)
+    return best
+
+
+def tune_lbm(lbm, step_fn, candidates=(FSI_TUNE_LBM_OCC3, FSI_TUNE_LBM_OCC4), steps=10, reps=3):
+    """Pick lbm.tune among candidates by timing `step_fn` (one LBM substep of
+    the caller's kind) on a snapshot of the state.  Returns
+    {"choice": tune, "ms_per_substep": {tune: ms}}."""
+    snap = lbm.snapshot()
+    times = {}
+    try:
+        for t in candidates:
+            lbm.tune = int(t)
+            for _ in range(2):  # warm-up (parity returns to its start value)
+                step_fn()
+            torch.cuda.synchronize()
+            times[int(t)] = _time_ms(step_fn, steps if steps % 2 == 0 else steps + 1, reps)
+            lbm.restore(snap)
+    finally:
+        lbm.restore(snap)
+    best = min(times, key=times.get)
+    lbm.tune = best
+    lbm._sync_params()
+    return {"choice": best, "ms_per_substep": times}
+
+
+def mpm_tune_value(scatter, gather):
+    """FsiMpmParams.tune for the given FSI_TUNE_MPM_* scatter and gather variants."""
+    return int(scatter) | (int(gather) << 2)
+
+
+def tune_mpm(solid, substep_fn, extra=(), candidates=None, steps=8, reps=3):
+    """Pick solid.params.tune (threads per chunk CTA of the binned P2G scatter
+    and G2P gather) by timing `substep_fn` (one binned substep as the caller
+    runs it) on a snapshot of the particle / grid / bin state.  extra: further
+    tensors the substep writes (coupler statistics), restored afterwards.
+    Returns {"choice": tune, "ms_per_substep": {tune: ms}}."""
+    if candidates is None:
+        candidates = [mpm_tune_value(s, g) for s in (FSI_TUNE_MPM_T128, FSI_TUNE_MPM_T256, FSI_TUNE_MPM_T512)
+                      for g in (FSI_TUNE_MPM_T128, FSI_TUNE_MPM_T256, FSI_TUNE_MPM_T512)]
+    solid._ensure_binned()
+    snap = solid.snapshot(extra)
+    times = {}
+    try:
+        for t in candidates:
+            solid.params.tune = int(t)
+            substep_fn()
+            torch.cuda.synchronize()
+            times[int(t)] = _time_ms(substep_fn, steps, reps)
+            solid.restore(snap)
+    finally:
+        solid.restore(snap)
+    best = min(times, key=times.get)
+    solid.params.tune = best
+    return {"choice": best, "ms_per_substep": times}

@@ -50,7 +50,7 @@ struct MrtK {
   float kf;                            // 16, 17, 18
 };
 
-inline MrtK make_mrt_k(float s_v, float s_o) {
+FSI_HD MrtK make_mrt_k(float s_v, float s_o) {
   // K = (M M^T)^-1 S on the non-zero blocks (see d3q19.cuh); Gram blocks of the
   // reference's M (fluid.py:257-275): {0,1,2}: [[19,11,1],[11,13,11],[1,11,37]],
   // {3,4}: [[10,4],[4,16]], {9,10}: [[36,12],[12,36]], {11,12}: [[12,4],[4,12]],

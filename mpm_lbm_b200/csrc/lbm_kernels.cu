@@ -15,6 +15,7 @@
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <mutex>
 
@@ -41,16 +42,23 @@ struct Case {
 template <bool H>
 struct Pop;
 
+// Element index of population s of a cell: 32-bit arithmetic (the host
+// checks 19 * pitch < 2^32), so that each access is one integer multiply-add
+// plus the address computation.
+__device__ __forceinline__ uint32_t pop_index(const Case& c, int s, int64_t cell) {
+  return (uint32_t)s * (uint32_t)c.s.pitch + (uint32_t)cell;
+}
+
 template <>
 struct Pop<false> {
   static __device__ __forceinline__ float ld(const Case& c, int s, int64_t cell) {
-    return __ldg(static_cast<const float*>(c.s.pop) + (int64_t)s * c.s.pitch + cell);
+    return __ldg(static_cast<const float*>(c.s.pop) + pop_index(c, s, cell));
   }
   static __device__ __forceinline__ float ld_rw(const Case& c, int s, int64_t cell) {
-    return static_cast<const float*>(c.s.pop)[(int64_t)s * c.s.pitch + cell];
+    return static_cast<const float*>(c.s.pop)[pop_index(c, s, cell)];
   }
   static __device__ __forceinline__ void st(const Case& c, int s, int64_t cell, float v) {
-    static_cast<float*>(c.s.pop)[(int64_t)s * c.s.pitch + cell] = v;
+    static_cast<float*>(c.s.pop)[pop_index(c, s, cell)] = v;
   }
 };
 
@@ -58,13 +66,13 @@ struct Pop<false> {
 template <>
 struct Pop<true> {
   static __device__ __forceinline__ float ld(const Case& c, int s, int64_t cell) {
-    const __half h = static_cast<const __half*>(c.s.pop)[(int64_t)s * c.s.pitch + cell];
+    const __half h = static_cast<const __half*>(c.s.pop)[pop_index(c, s, cell)];
     return lattice_w(s) * (c.p.rho0 + __half2float(h));
   }
   static __device__ __forceinline__ float ld_rw(const Case& c, int s, int64_t cell) { return ld(c, s, cell); }
   static __device__ __forceinline__ void st(const Case& c, int s, int64_t cell, float v) {
     const float inv_w = s == 0 ? 3.0f : (s <= 6 ? 18.0f : 36.0f);
-    static_cast<__half*>(c.s.pop)[(int64_t)s * c.s.pitch + cell] = __float2half_rn(v * inv_w - c.p.rho0);
+    static_cast<__half*>(c.s.pop)[pop_index(c, s, cell)] = __float2half_rn(v * inv_w - c.p.rho0);
   }
 };
 
@@ -411,13 +419,16 @@ __device__ __forceinline__ void store_near_solid(const Case& c, const Nbh& n, in
   }
 }
 
+// One tile of the fused step: the 32 x 8 cells (x, row = k * ny + j) of tile
+// (bx, by).  Called by the single-case kernel (c in the parameter bank) and by
+// the batched kernel (c staged in shared memory); acc: the CTA's shared
+// per-direction accumulator.
 template <bool ODD, bool H, bool MOVING, bool BCW, bool PEN>
-__global__ void __launch_bounds__(256) k_lbm_step(const Case c) {
-  __shared__ DirAcc acc;
+__device__ __forceinline__ void lbm_step_tile(const Case& c, int bx, int by, DirAcc& acc) {
   const int lane = threadIdx.x;
   const int nx = c.s.nx, ny = c.s.ny, nz = c.s.nz;
-  const int x = blockIdx.x * 32 + lane;
-  const int row = blockIdx.y * blockDim.y + threadIdx.y;
+  const int x = bx * 32 + lane;
+  const int row = by * 8 + threadIdx.y;
   const bool inrow = row < ny * nz;
   const bool valid = inrow && x < nx;
   const int j = inrow ? row % ny : 0, k = inrow ? row / ny : 0;
@@ -466,8 +477,8 @@ __global__ void __launch_bounds__(256) k_lbm_step(const Case c) {
 
   // ---- pending open boundary of the previous step (fluid.py:538-569)
   if (BCW && c.c.bc_pending && inrow) {
-    if (c.p.bc_left != 0 && blockIdx.x == 0) bc_face_warp<0>(c, lane, row, fl, F);
-    if (c.p.bc_right != 0 && (int)blockIdx.x == ((nx - 1) >> 5)) bc_face_warp<1>(c, lane, row, fl, F);
+    if (c.p.bc_left != 0 && bx == 0) bc_face_warp<0>(c, lane, row, fl, F);
+    if (c.p.bc_right != 0 && bx == ((nx - 1) >> 5)) bc_face_warp<1>(c, lane, row, fl, F);
   }
 
   // ---- macroscopic state the collision uses (streaming3 of the previous step, fluid.py:1794-1814)
@@ -606,6 +617,15 @@ __global__ void __launch_bounds__(256) k_lbm_step(const Case c) {
   }
 }
 
+// MINB: resident CTAs per SM the register allocation must allow (3: no
+// spills; 4: 64 registers with a few spilled words).  The host picks it from
+// FsiLbmParams.tune (chosen by the autotuner of the Python layer).
+template <bool ODD, bool H, bool MOVING, bool BCW, bool PEN, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_lbm_step(const Case c) {
+  __shared__ DirAcc acc;
+  lbm_step_tile<ODD, H, MOVING, BCW, PEN>(c, blockIdx.x, blockIdx.y, acc);
+}
+
 // ------------------------------------------------- init / neighbours ----
 __global__ void k_init(const Case c) {
   const int64_t n = (int64_t)c.s.nx * c.s.ny * c.s.nz;
@@ -686,11 +706,8 @@ __global__ void k_to_natural(const Case c) {
 }
 
 // ------------------------------------------------------- mask rebuild ----
-// update_dynamic_solid (fluid.py:1847-1861)
-__global__ void k_mask_update(const Case c, float thr) {
-  const int64_t n = (int64_t)c.s.nx * c.s.ny * c.s.nz;
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+// update_dynamic_solid (fluid.py:1847-1861) for cell i
+__device__ __forceinline__ void mask_update_cell(const Case& c, float thr, int64_t i) {
   const uint8_t fl = c.s.flags[i];
   const uint8_t prev = (fl & kSolid) ? 1 : 0;
   c.s.old_solid[i] = prev;
@@ -702,6 +719,12 @@ __global__ void k_mask_update(const Case c, float thr) {
     const int slot = atomicAdd(&c.s.diag->change_count, 1);
     c.s.change_list[slot] = (int32_t)i;
   }
+}
+
+__global__ void k_mask_update(const Case c, float thr) {
+  const int64_t n = (int64_t)c.s.nx * c.s.ny * c.s.nz;
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) mask_update_cell(c, thr, i);
 }
 
 __device__ __forceinline__ void flag_bits(uint8_t* flags, int64_t i, uint8_t set, uint8_t clear) {
@@ -733,11 +756,12 @@ __device__ __forceinline__ bool is_changed(const Case& c, int64_t i) {
   return ((c.s.flags[i] & kSolid) ? 1 : 0) != c.s.old_solid[i];
 }
 
-// reinitialize_new_fluid_cells (fluid.py:1863-1877) and AA re-pairing.
+// reinitialize_new_fluid_cells (fluid.py:1863-1877) and AA re-pairing of the
+// changed cells idx0, idx0 + stride, ... of the change list.
 template <bool H>
-__global__ void k_relink(const Case c) {
+__device__ __forceinline__ void relink_cells(const Case& c, int idx0, int stride) {
   const int count = c.s.diag->change_count;
-  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < count; idx += gridDim.x * blockDim.x) {
+  for (int idx = idx0; idx < count; idx += stride) {
     const int64_t ci = c.s.change_list[idx];
     const Coord q = coord_of(c, ci);
     // neighbour-derived data of ci and its 18 neighbours
@@ -818,11 +842,19 @@ __global__ void k_relink(const Case c) {
   }
 }
 
+template <bool H>
+__global__ void k_relink(const Case c) {
+  relink_cells<H>(c, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+}
+
 // reinit flags are consumed only after every link of every changed cell is done
-__global__ void k_clear_reinit(const Case c) {
+__device__ __forceinline__ void clear_reinit_cells(const Case& c, int idx0, int stride) {
   const int count = c.s.diag->change_count;
-  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < count; idx += gridDim.x * blockDim.x)
-    c.s.reinit_flag[c.s.change_list[idx]] = 0;
+  for (int idx = idx0; idx < count; idx += stride) c.s.reinit_flag[c.s.change_list[idx]] = 0;
+}
+
+__global__ void k_clear_reinit(const Case c) {
+  clear_reinit_cells(c, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
 }
 
 // ------------------------------------------------ BC flush and readout ----
@@ -978,6 +1010,8 @@ static int check_state(const FsiLbmState* s, const FsiLbmParams* p) {
   if (s->nx < 3 || s->ny < 1 || s->nz < 1) return invalid("lattice must have nx >= 3, ny >= 1, nz >= 1");
   if (s->pitch < (int64_t)s->nx * s->ny * s->nz || (s->pitch % 32) != 0)
     return invalid("pitch must cover nx*ny*nz and be a multiple of 32");
+  if (19 * s->pitch > (int64_t)UINT32_MAX) return invalid("lattice too large: 19 * pitch must be below 2^32");
+  if (p->tune != FSI_TUNE_LBM_OCC3 && p->tune != FSI_TUNE_LBM_OCC4) return invalid("unknown FsiLbmParams.tune");
   if ((p->bc_left || p->bc_right) && (s->nx < 4 || (s->nx % 32 == 1) || (s->nx % 32 == 2)))
     return invalid("x open boundaries need nx >= 4 and nx % 32 not in {1, 2}");
   if (!s->pop || !s->flags || !s->nbr || !s->diag) return invalid("null device pointer in FsiLbmState");
@@ -1031,6 +1065,7 @@ extern "C" int fsi_lbm_set_solid(const FsiLbmState* s, const uint8_t* solid, voi
 
 extern "C" int fsi_lbm_to_natural(const FsiLbmState* s, void* stream) {
   if (!s) return invalid("null state");
+  if (19 * s->pitch > (int64_t)UINT32_MAX) return invalid("lattice too large: 19 * pitch must be below 2^32");
   FsiLbmParams p{};
   p.rho0 = 1.f;
   p.s_v = p.s_o = 1.f;
@@ -1069,9 +1104,13 @@ extern "C" int fsi_lbm_substep(const FsiLbmState* s, const FsiLbmParams* p, cons
   const bool moving = ctl->mode & FSI_MODE_MOVING_BB, pen = ctl->mode & FSI_MODE_PENALTY;
   const bool bcw = p->bc_left != 0 || p->bc_right != 0;
   if (moving && pen) return invalid("penalty steps use static bounce-back (fluid.py:2099-2103)");
-#define FSI_LAUNCH(O, HH, M, B, PN) k_lbm_step<O, HH, M, B, PN><<<grid, block, 0, st>>>(c)
+#define FSI_LAUNCH(O, HH, M, B, PN)                                        \
+  if (p->tune == FSI_TUNE_LBM_OCC4)                                        \
+    k_lbm_step<O, HH, M, B, PN, 4><<<grid, block, 0, st>>>(c);             \
+  else                                                                     \
+    k_lbm_step<O, HH, M, B, PN, 3><<<grid, block, 0, st>>>(c)
 #define FSI_BY_H(O, M, B, PN) \
-  if (h) FSI_LAUNCH(O, true, M, B, PN); else FSI_LAUNCH(O, false, M, B, PN)
+  if (h) { FSI_LAUNCH(O, true, M, B, PN); } else { FSI_LAUNCH(O, false, M, B, PN); }
 #define FSI_BY_O(M, B, PN) \
   if (odd) { FSI_BY_H(true, M, B, PN); } else { FSI_BY_H(false, M, B, PN); }
   if (moving) {
@@ -1207,4 +1246,156 @@ extern "C" int fsi_mask_rebuild_static_scratch(const FsiLbmState* s, const FsiLb
   FsiLbmState local = *s;
   local.change_list = scratch;
   return fsi_mask_rebuild(&local, p, ctl, threshold, stream);
+}
+
+// ---- batched cases ---------------------------------------------------------
+// grid.y = case slot; grid.x strides over the case's work.  Each CTA stages
+// its case's lattice descriptors in shared memory once.
+namespace fsi {
+
+__device__ __forceinline__ void copy_words(void* dst, const void* src, int bytes, int tid, int nt) {
+  const int* s = static_cast<const int*>(src);
+  int* d = static_cast<int*>(dst);
+  for (int i = tid; i < bytes / 4; i += nt) d[i] = s[i];
+}
+
+// stage the lattice part of a batch case (state, params, step control, and the
+// MRT rates when with_k) in shared memory; returns false for an inactive slot
+__device__ __forceinline__ bool stage_case(const FsiBatchCase& bc, Case& sc, bool with_k) {
+  const int tid = threadIdx.x + threadIdx.y * blockDim.x, nt = blockDim.x * blockDim.y;
+  if (!bc.active) return false;  // same value for every thread of the CTA
+  copy_words(&sc.s, &bc.lbm, (int)sizeof(FsiLbmState), tid, nt);
+  copy_words(&sc.p, &bc.lp, (int)sizeof(FsiLbmParams), tid, nt);
+  copy_words(&sc.c, &bc.ctl, (int)sizeof(FsiStepCtl), tid, nt);
+  if (with_k && tid == 0) sc.K = make_mrt_k(bc.lp.s_v, bc.lp.s_o);
+  __syncthreads();
+  return true;
+}
+
+template <bool H>
+__global__ void __launch_bounds__(256, 3) k_batch_lbm_step(const FsiBatchCase* __restrict__ cases) {
+  __shared__ Case sc;
+  __shared__ DirAcc acc;
+  const FsiBatchCase& bc = cases[blockIdx.y];
+  const int gx = (bc.lbm.nx + 31) / 32, nt = gx * ((bc.lbm.ny * bc.lbm.nz + 7) / 8);
+  if ((int)blockIdx.x >= nt || !stage_case(bc, sc, true)) return;
+  const bool moving = sc.c.mode & FSI_MODE_MOVING_BB;
+  const bool odd = sc.c.parity != 0;
+  for (int t = blockIdx.x; t < nt; t += gridDim.x) {
+    const int bx = t % gx, by = t / gx;
+    if (moving) {
+      if (odd)
+        lbm_step_tile<true, H, true, false, false>(sc, bx, by, acc);
+      else
+        lbm_step_tile<false, H, true, false, false>(sc, bx, by, acc);
+    } else {
+      if (odd)
+        lbm_step_tile<true, H, false, false, true>(sc, bx, by, acc);
+      else
+        lbm_step_tile<false, H, false, false, true>(sc, bx, by, acc);
+    }
+    __syncthreads();  // acc is reused by the next tile
+  }
+}
+
+__global__ void k_batch_mask_update(const FsiBatchCase* __restrict__ cases) {
+  __shared__ Case sc;
+  const FsiBatchCase& bc = cases[blockIdx.y];
+  if (bc.mode != FSI_BATCH_MOVING) return;
+  const int64_t n = (int64_t)bc.lbm.nx * bc.lbm.ny * bc.lbm.nz;
+  if ((int64_t)blockIdx.x * blockDim.x >= n || !stage_case(bc, sc, false)) return;
+  const float thr = bc.mask_threshold;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    mask_update_cell(sc, thr, i);
+}
+
+template <bool H>
+__global__ void k_batch_relink(const FsiBatchCase* __restrict__ cases) {
+  __shared__ Case sc;
+  const FsiBatchCase& bc = cases[blockIdx.y];
+  if (bc.mode != FSI_BATCH_MOVING || !stage_case(bc, sc, false)) return;
+  relink_cells<H>(sc, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+}
+
+__global__ void k_batch_clear_reinit(const FsiBatchCase* __restrict__ cases) {
+  __shared__ Case sc;
+  const FsiBatchCase& bc = cases[blockIdx.y];
+  if (bc.mode != FSI_BATCH_MOVING || !stage_case(bc, sc, false)) return;
+  clear_reinit_cells(sc, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+}
+
+// per-case bookkeeping between phases (one CTA of 32 threads per case)
+enum { kBatchLbmPre = 1, kBatchLbmPost = 2, kBatchMaskPre = 3 };
+
+__global__ void k_batch_ctl(FsiBatchCase* cases, int op) {
+  FsiBatchCase& bc = cases[blockIdx.x];
+  if (!bc.active) return;
+  const int tid = threadIdx.x;
+  FsiLbmDiag* d = bc.lbm.diag;
+  if (op == kBatchLbmPre) {
+    // the reductions fsi_lbm_substep zeroes before a step of this mode
+    int* w = reinterpret_cast<int*>(d);
+    if (bc.ctl.mode & FSI_MODE_MOVING_BB) {
+      for (int i = tid; i < (int)(offsetof(FsiLbmDiag, accum_norm_max) / 4); i += blockDim.x) w[i] = 0;
+    } else if (bc.ctl.mode & FSI_MODE_PENALTY) {
+      const int a = (int)(offsetof(FsiLbmDiag, penalty_active) / 4), b = (int)(offsetof(FsiLbmDiag, change_count) / 4);
+      for (int i = a + tid; i < b; i += blockDim.x) w[i] = 0;
+    }
+  } else if (op == kBatchLbmPost && tid == 0) {
+    bc.ctl.parity ^= 1;
+    bc.ctl.pp ^= 1;
+  } else if (op == kBatchMaskPre && tid == 0) {
+    d->change_count = 0;
+  }
+}
+
+int check_batch(const FsiBatchCase* cases, const FsiBatchDims* d) {
+  if (!cases || !d) return invalid("null batch argument");
+  if (d->n_cases <= 0 || d->n_cases > 65535) return invalid("n_cases must be in 1..65535");
+  if (d->max_lbm_tiles <= 0 || d->max_cells <= 0) return invalid("batch dims must be positive");
+  return FSI_OK;
+}
+
+static inline unsigned batch_x(int64_t work, int threads, int cap) {
+  const int64_t b = (work + threads - 1) / threads;
+  return (unsigned)std::max<int64_t>(1, std::min<int64_t>(b, cap));
+}
+
+}  // namespace fsi
+
+extern "C" int fsi_batch_lbm_substep(FsiBatchCase* cases, const FsiBatchDims* d, void* stream) {
+  int rc = check_batch(cases, d);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  k_batch_ctl<<<d->n_cases, 32, 0, st>>>(cases, kBatchLbmPre);
+  if ((rc = launch_check("k_batch_ctl"))) return rc;
+  // tiles of all cases: one CTA per tile up to 3 resident CTAs per SM in total
+  const int cap = std::max(1, 148 * 3 * 4 / std::max(1, d->n_cases));
+  const dim3 grid(batch_x(d->max_lbm_tiles, 1, std::max(cap, 8)), d->n_cases);
+  if (d->store_fp16)
+    k_batch_lbm_step<true><<<grid, dim3(32, 8), 0, st>>>(cases);
+  else
+    k_batch_lbm_step<false><<<grid, dim3(32, 8), 0, st>>>(cases);
+  if ((rc = launch_check("k_batch_lbm_step"))) return rc;
+  k_batch_ctl<<<d->n_cases, 32, 0, st>>>(cases, kBatchLbmPost);
+  return launch_check("k_batch_ctl");
+}
+
+extern "C" int fsi_batch_mask_rebuild(FsiBatchCase* cases, const FsiBatchDims* d, void* stream) {
+  int rc = check_batch(cases, d);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  k_batch_ctl<<<d->n_cases, 32, 0, st>>>(cases, kBatchMaskPre);
+  if ((rc = launch_check("k_batch_ctl"))) return rc;
+  const int cap = std::max(8, 148 * 8 / std::max(1, d->n_cases));
+  k_batch_mask_update<<<dim3(batch_x(d->max_cells, 256, cap), d->n_cases), 256, 0, st>>>(cases);
+  if ((rc = launch_check("k_batch_mask_update"))) return rc;
+  const dim3 g2(std::max(1, 148 * 4 / std::max(1, d->n_cases)), d->n_cases);
+  if (d->store_fp16)
+    k_batch_relink<true><<<g2, 128, 0, st>>>(cases);
+  else
+    k_batch_relink<false><<<g2, 128, 0, st>>>(cases);
+  if ((rc = launch_check("k_batch_relink"))) return rc;
+  k_batch_clear_reinit<<<g2, 128, 0, st>>>(cases);
+  return launch_check("k_batch_clear_reinit");
 }

@@ -20,11 +20,12 @@
 namespace fsi {
 namespace {
 
-constexpr int kChunk = FSI_BIN_CHUNK;  // particles per chunk = threads per CTA
+constexpr int kChunk = FSI_BIN_CHUNK;  // particles per chunk
 constexpr int kEdge = FSI_BIN_EDGE;
-// nodes staged per CTA: a chunk of one bin spans (4 + 2)^3 nodes; the rest
-// absorbs drift since the last binning.  7 floats per node in P2G = 35 KB.
-constexpr int kTileCap = 1280;
+// nodes staged per CTA: a chunk of one bin spans (4 + 3)^3 = 343 nodes; the
+// rest absorbs drift since the last binning (a 10^3 box).  7 floats per node
+// in P2G = 28 KB.
+constexpr int kTileCap = 1000;
 
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
@@ -39,15 +40,20 @@ __device__ __forceinline__ int particle_bin(const float X[3], float inv_dx, int 
   return (c[2] * nb + c[1]) * nb + c[0];
 }
 
-__global__ void k_bin_count(FsiParticles pt, float inv_dx, int G, int nb, int32_t* __restrict__ key,
-                            int32_t* __restrict__ count) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void bin_count_body(const FsiParticles& pt, float inv_dx, int G, int nb,
+                                               int32_t* __restrict__ key, int32_t* __restrict__ count, int vb, int vg) {
+  const int p = vb * blockDim.x + threadIdx.x;
   if (p >= pt.n) return;
   const int n = pt.n;
   const float X[3] = {pt.x[p], pt.x[n + p], pt.x[2 * n + p]};
   const int k = particle_bin(X, inv_dx, G, nb);
   key[p] = k;
   atomicAdd(count + k, 1);
+}
+
+__global__ void k_bin_count(FsiParticles pt, float inv_dx, int G, int nb, int32_t* __restrict__ key,
+                            int32_t* __restrict__ count) {
+  bin_count_body(pt, inv_dx, G, nb, key, count, blockIdx.x, gridDim.x);
 }
 
 // One CTA: exclusive scan of the bin counts and of the chunks per bin, the
@@ -63,9 +69,8 @@ __device__ __forceinline__ int4 ld_bins4(const int32_t* p, int b, int b1) {
   return v;
 }
 
-__global__ __launch_bounds__(1024) void k_bin_scan(int nbins, int32_t* __restrict__ count,
-                                                   int32_t* __restrict__ start, int2* __restrict__ chunk,
-                                                   int32_t* __restrict__ meta) {
+__device__ __forceinline__ void bin_scan_body(int nbins, int32_t* __restrict__ count, int32_t* __restrict__ start,
+                                              int2* __restrict__ chunk, int32_t* __restrict__ meta) {
   __shared__ int s_p[32], s_c[32];
   const int T = blockDim.x, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const int per = ((nbins + T - 1) / T + 3) & ~3;
@@ -133,11 +138,23 @@ __global__ __launch_bounds__(1024) void k_bin_scan(int nbins, int32_t* __restric
   if (tid == T - 1) meta[0] = co;
 }
 
-__global__ void k_bin_scatter(int n, const int32_t* __restrict__ key, int32_t* __restrict__ cursor,
-                              int32_t* __restrict__ perm) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ __launch_bounds__(1024) void k_bin_scan(int nbins, int32_t* __restrict__ count,
+                                                   int32_t* __restrict__ start, int2* __restrict__ chunk,
+                                                   int32_t* __restrict__ meta) {
+  bin_scan_body(nbins, count, start, chunk, meta);
+}
+
+__device__ __forceinline__ void bin_scatter_body(int n, const int32_t* __restrict__ key,
+                                                 int32_t* __restrict__ cursor, int32_t* __restrict__ perm, int vb,
+                                                 int vg) {
+  const int p = vb * blockDim.x + threadIdx.x;
   if (p >= n) return;
   perm[atomicAdd(cursor + key[p], 1)] = p;
+}
+
+__global__ void k_bin_scatter(int n, const int32_t* __restrict__ key, int32_t* __restrict__ cursor,
+                              int32_t* __restrict__ perm) {
+  bin_scatter_body(n, key, cursor, perm, blockIdx.x, gridDim.x);
 }
 
 struct Box {
@@ -202,89 +219,146 @@ __device__ __forceinline__ void g2p_gather_global(const FsiGrid& g, const FsiMpm
   }
 }
 
-__device__ __forceinline__ void reaction_global(const LatView& L, const float* hydro, const float* phi,
-                                                const FsiCouplingParams& cp, const BSpline& b, float Jp, float vol0,
-                                                float scale, ReactParticle& r) {
-  float hs[3] = {0.f, 0.f, 0.f}, ps = 0.f;
-#pragma unroll 1
-  for (int o = 0; o < 27; ++o) {
-    const int ox = o / 9, oy = (o / 3) % 3, oz = o % 3;
-    const int I = b.base[0] + ox, Jj = b.base[1] + oy, K = b.base[2] + oz;
-    if (I < 0 || I >= L.nx || Jj < 0 || Jj >= L.ny || K < 0 || K >= L.nz) continue;
-    const float w = bspline_w(b.fx[0], ox) * bspline_w(b.fx[1], oy) * bspline_w(b.fx[2], oz);
-    const int64_t c = lat_cell(L, I, Jj, K);
-    hs[0] += w * hydro[c];
-    hs[1] += w * hydro[L.pitch + c];
-    hs[2] += w * hydro[2 * L.pitch + c];
-    if (cp.kind != 0) ps += w * phi[c];
+// Per-particle P2G payload, one row per quantity, one column per particle slot
+// (the particle's position in the bin order perm): fractional position, base
+// node, momentum, affine matrix, mass, reaction force, and the B-spline
+// weights [axis][offset].
+enum { kPfx = 0, kPbase = 3, kPmv = 6, kPaff = 9, kPmass = 18, kPpf = 19, kPw = 22, kPn = 31 };
+static_assert(kPn <= FSI_MPM_PAYLOAD_ROWS, "payload rows exceed the caller's buffer");
+
+// P2G, per particle (one thread per slot): fixed-corotated stress and affine
+// momentum with the FP64 polar rotation (solid.py:231-249), the reaction force
+// gathered from the lattice hydro force (penalty.py:90-129,
+// moving_boundary.py:58-110, link_area.py:139-193) and its reductions, and the
+// particle's B-spline data -- written to the payload for the scatter kernel.
+template <bool REACT>
+__device__ __forceinline__ void p2g_payload_body(const FsiParticles& pt, const FsiMpmParams& mp,
+                                                 const int32_t* __restrict__ perm, float* __restrict__ payload,
+                                                 const LatView& L, const float* __restrict__ hydro,
+                                                 const float* __restrict__ phi, const FsiCouplingParams& cp,
+                                                 FsiCouplingStats* st, const FsiLbmDiag* diag, int vb, int vg) {
+  __shared__ float s_scale;
+  const int n = pt.n;
+  const int slot = vb * blockDim.x + threadIdx.x;
+  if (REACT) {
+    if (threadIdx.x == 0) {
+      float raw = 1.f;
+      s_scale = cp.kind == 2 ? link_area_scale(diag, cp, &raw) : 1.0f;
+      if (vb == 0 && cp.kind == 2) {
+        st->area_scale = s_scale;
+        st->raw_area_scale = raw;
+      }
+    }
+    __syncthreads();
   }
-  reaction_from_sums(cp, hs, ps, Jp, vol0, scale, r);
+  int n_act = 0;
+  float pmax = 0.f;
+  double pn[3] = {0.0, 0.0, 0.0};
+  if (slot < n) {
+    const int p = perm[slot];
+    const float X[3] = {pt.x[p], pt.x[n + p], pt.x[2 * n + p]};
+    BSpline b;
+    bspline(X, mp.inv_dx, b);
+    P2GParticle q;
+    p2g_particle(pt, p, mp, q);
+    pt.Jp[p] = q.J;
+    float pf[3] = {0.f, 0.f, 0.f};
+    if (REACT) {
+      ReactParticle r;
+      reaction_particle(L, hydro, phi, cp, b, q.J, pt.vol0[p], s_scale, r);
+      n_act = r.act ? 1 : 0;
+      pmax = r.pnorm;
+      if (r.gated)
+        for (int a = 0; a < 3; ++a) pn[a] = (double)r.pf[a];
+      if (r.scatter)
+        for (int a = 0; a < 3; ++a) pf[a] = r.pf[a];
+    }
+    float* const col = payload + slot;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      col[(int64_t)(kPfx + a) * n] = b.fx[a];
+      col[(int64_t)(kPbase + a) * n] = __int_as_float(b.base[a]);
+      col[(int64_t)(kPmv + a) * n] = q.mv[a];
+      col[(int64_t)(kPpf + a) * n] = pf[a];
+#pragma unroll
+      for (int o = 0; o < 3; ++o) col[(int64_t)(kPw + 3 * a + o) * n] = b.w[a][o];
+    }
+#pragma unroll
+    for (int a = 0; a < 9; ++a) col[(int64_t)(kPaff + a) * n] = q.aff[a];
+    col[(int64_t)kPmass * n] = q.mass;
+  }
+  if (REACT) {
+    // diagnostics reductions (penalty.py:202-240, moving_boundary.py:312-374)
+    const int na = __reduce_add_sync(0xffffffffu, (unsigned)n_act);
+    const float pm = warp_max(pmax);
+    double sp3[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) sp3[a] = warp_sum_d(pn[a]);
+    if ((threadIdx.x & 31) == 0) {
+      if (na) atomicAdd(&st->active_reaction_particle_count, na);
+      if (pm > 0.f) atomic_max_nonneg(&st->max_particle_reaction_norm, pm);
+      for (int a = 0; a < 3; ++a)
+        if (sp3[a] != 0.0) atomicAdd(&st->net_particle_reaction[a], sp3[a]);
+    }
+  }
 }
 
-// per-particle values handed from phase 1 to phase 2 of the P2G kernel
-enum { kPfx = 0, kPbase = 3, kPmv = 6, kPaff = 9, kPmass = 18, kPpf = 19, kPn = 22 };
-
-// P2G (+ reaction) of the chunks of this CTA into grid buffer g.
-//  phase 0: the chunk's node box; for the reaction, the box's lattice hydro
-//           force and phi staged in shared memory;
-//  phase 1: one thread per particle: stress and affine momentum (FP64 polar
-//           rotation) and the reaction force gathered from the staged box;
-//  phase 2: the 27 x chunk (particle, node) pairs spread over the threads, so
-//           the lanes of one shared-memory atomic touch distinct nodes;
-//  phase 3: one global atomic per touched node value.
 template <bool REACT>
-__global__ __launch_bounds__(kChunk) void k_p2g_binned(FsiParticles pt, FsiGrid g, FsiMpmParams mp,
-                                                       const int32_t* __restrict__ perm,
-                                                       const int2* __restrict__ chunks, int32_t* meta, int32_t* box,
-                                                       int buf, LatView L, const float* __restrict__ hydro,
-                                                       const float* __restrict__ phi, FsiCouplingParams cp,
-                                                       FsiCouplingStats* st, const FsiLbmDiag* diag) {
+__global__ __launch_bounds__(128) void k_p2g_payload(FsiParticles pt, FsiMpmParams mp,
+                                                     const int32_t* __restrict__ perm, float* __restrict__ payload,
+                                                     LatView L, const float* __restrict__ hydro,
+                                                     const float* __restrict__ phi, FsiCouplingParams cp,
+                                                     FsiCouplingStats* st, const FsiLbmDiag* diag) {
+  p2g_payload_body<REACT>(pt, mp, perm, payload, L, hydro, phi, cp, st, diag, blockIdx.x, gridDim.x);
+}
+
+// P2G scatter of the chunks of this CTA into grid buffer g, from the payload:
+//  stage the chunk's payload columns and find its node box;
+//  the 27 x chunk (particle, node) pairs spread over the T threads, so that
+//  the lanes of one shared-memory atomic touch distinct nodes (pair order:
+//  particle-major, offsets ox, oy, oz as in p2g);
+//  one global atomic per touched node value.
+// Chunks whose box exceeds the tile (bins gone stale) scatter with global
+// atomics directly.
+template <bool REACT, int T>
+__device__ __forceinline__ void p2g_scatter_body(const FsiGrid& g, const FsiMpmParams& mp,
+                                                 const float* __restrict__ payload, int n,
+                                                 const int2* __restrict__ chunks, int32_t* meta, int32_t* box, int buf,
+                                                 FsiCouplingStats* st, int vb, int vg) {
   __shared__ float tile[7 * kTileCap];
   __shared__ float sp[kPn][kChunk];
   __shared__ int s_lo[3], s_hi[3];
-  __shared__ float s_scale;
   const int tid = threadIdx.x;
   const int G = g.n;
   const int64_t N = (int64_t)G * G * G;
   const int nch = meta[0];
-  if (blockIdx.x == 0 && tid == 0) meta[1 + buf] = nch;
-  if (REACT && tid == 0) {
-    float raw = 1.f;
-    s_scale = cp.kind == 2 ? link_area_scale(diag, cp, &raw) : 1.0f;
-    if (blockIdx.x == 0 && cp.kind == 2) {
-      st->area_scale = s_scale;
-      st->raw_area_scale = raw;
-    }
-  }
+  if (vb == 0 && tid == 0) meta[1 + buf] = nch;
   float* const dst[7] = {g.v, g.v + N, g.v + 2 * N, g.m, g.f_ext, g.f_ext + N, g.f_ext + 2 * N};
-  int n_act = 0;
-  float pmax = 0.f, gmax = 0.f;
-  double pn[3] = {0.0, 0.0, 0.0}, gn[3] = {0.0, 0.0, 0.0};
-  for (int c = blockIdx.x; c < nch; c += gridDim.x) {
-    __syncthreads();  // the previous chunk's flush has read the tile
+  float gmax = 0.f;
+  double gn[3] = {0.0, 0.0, 0.0};
+  for (int c = vb; c < nch; c += vg) {
+    __syncthreads();  // the previous chunk's flush has read the tile and sp
     if (tid < 3) {
       s_lo[tid] = INT_MAX;
       s_hi[tid] = INT_MIN;
     }
     const int2 ch = chunks[c];
-    const bool live = tid < ch.y;
-    const int p = live ? perm[ch.x + tid] : 0;
-    float X[3] = {0.f, 0.f, 0.f};
-    if (live) {
-      X[0] = pt.x[p];
-      X[1] = pt.x[pt.n + p];
-      X[2] = pt.x[2 * pt.n + p];
+    for (int i = tid; i < kPn * ch.y; i += T) {
+      const int r = i / ch.y, k = i - r * ch.y;
+      sp[r][k] = payload[(int64_t)r * n + ch.x + k];
     }
-    BSpline b;
-    bspline(X, mp.inv_dx, b);
     __syncthreads();
+    if (tid < 32 * ((ch.y + 31) / 32)) {
+      const bool live = tid < ch.y;
 #pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      const int lo = __reduce_min_sync(0xffffffffu, live ? b.base[a] : INT_MAX);
-      const int hi = __reduce_max_sync(0xffffffffu, live ? b.base[a] : INT_MIN);
-      if ((tid & 31) == 0) {
-        atomicMin(&s_lo[a], lo);
-        atomicMax(&s_hi[a], hi);
+      for (int a = 0; a < 3; ++a) {
+        const int bs = live ? __float_as_int(sp[kPbase + a][tid]) : 0;
+        const int lo = __reduce_min_sync(0xffffffffu, live ? bs : INT_MAX);
+        const int hi = __reduce_max_sync(0xffffffffu, live ? bs : INT_MIN);
+        if ((tid & 31) == 0) {
+          atomicMin(&s_lo[a], lo);
+          atomicMax(&s_hi[a], hi);
+        }
       }
     }
     __syncthreads();
@@ -302,90 +376,18 @@ __global__ __launch_bounds__(kChunk) void k_p2g_binned(FsiParticles pt, FsiGrid 
       if (!staged) atomicAdd(meta + 3, 1);
     }
     const int nv = staged ? bx.vol : 0;
-    // ---- phase 0: lattice hydro / phi of the box (zero outside the lattice)
-    if (REACT && staged) {
-      for (int li = tid; li < nv; li += kChunk) {
-        const int i = bx.lo[0] + li % bx.ext[0];
-        const int j = bx.lo[1] + (li / bx.ext[0]) % bx.ext[1];
-        const int k = bx.lo[2] + li / (bx.ext[0] * bx.ext[1]);
-        float h0 = 0.f, h1 = 0.f, h2 = 0.f, ph = 0.f;
-        if (i < L.nx && j < L.ny && k < L.nz) {
-          const int64_t cell = lat_cell(L, i, j, k);
-          h0 = hydro[cell];
-          h1 = hydro[L.pitch + cell];
-          h2 = hydro[2 * L.pitch + cell];
-          if (cp.kind != 0) ph = phi[cell];
-        }
-        tile[li] = h0;
-        tile[nv + li] = h1;
-        tile[2 * nv + li] = h2;
-        tile[3 * nv + li] = ph;
-      }
-      __syncthreads();
-    }
-    // ---- phase 1: per particle
-    if (live) {
-      P2GParticle q;
-      p2g_particle(pt, p, mp, q);
-      pt.Jp[p] = q.J;
-      float pf[3] = {0.f, 0.f, 0.f};
-      if (REACT) {
-        ReactParticle r;
-        if (staged) {
-          // reaction_particle over the staged box: the same products, in the
-          // same order; cells outside the lattice hold zeros
-          float hs[3] = {0.f, 0.f, 0.f}, ps = 0.f;
-#pragma unroll
-          for (int ox = 0; ox < 3; ++ox)
-#pragma unroll
-            for (int oy = 0; oy < 3; ++oy)
-#pragma unroll
-              for (int oz = 0; oz < 3; ++oz) {
-                const int I = b.base[0] + ox, Jj = b.base[1] + oy, K = b.base[2] + oz;
-                if (I < 0 || I >= L.nx || Jj < 0 || Jj >= L.ny || K < 0 || K >= L.nz) continue;
-                const float w = b.w[0][ox] * b.w[1][oy] * b.w[2][oz];
-                const int li = ((K - bx.lo[2]) * bx.ext[1] + (Jj - bx.lo[1])) * bx.ext[0] + (I - bx.lo[0]);
-                hs[0] += w * tile[li];
-                hs[1] += w * tile[nv + li];
-                hs[2] += w * tile[2 * nv + li];
-                if (cp.kind != 0) ps += w * tile[3 * nv + li];
-              }
-          reaction_from_sums(cp, hs, ps, q.J, pt.vol0[p], s_scale, r);
-        } else {
-          reaction_global(L, hydro, phi, cp, b, q.J, pt.vol0[p], s_scale, r);
-        }
-        n_act += r.act ? 1 : 0;
-        pmax = fmaxf(pmax, r.pnorm);
-        if (r.gated)
-          for (int a = 0; a < 3; ++a) pn[a] += (double)r.pf[a];
-        if (r.scatter)
-          for (int a = 0; a < 3; ++a) pf[a] = r.pf[a];
-      }
-#pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        sp[kPfx + a][tid] = b.fx[a];
-        sp[kPbase + a][tid] = __int_as_float(b.base[a]);
-        sp[kPmv + a][tid] = q.mv[a];
-        sp[kPpf + a][tid] = pf[a];
-      }
-#pragma unroll
-      for (int a = 0; a < 9; ++a) sp[kPaff + a][tid] = q.aff[a];
-      sp[kPmass][tid] = q.mass;
-    }
+    for (int i = tid; i < 7 * nv; i += T) tile[i] = 0.f;
     __syncthreads();
-    for (int i = tid; i < 7 * nv; i += kChunk) tile[i] = 0.f;
-    __syncthreads();
-    // ---- phase 2: (particle, node) pairs
     const int npair = ch.y * 27;
-    for (int idx = tid; idx < npair; idx += kChunk) {
+    for (int idx = tid; idx < npair; idx += T) {
       const int lp = idx / 27, o = idx - lp * 27;
       const int ox = o / 9, oy = (o / 3) % 3, oz = o % 3;
       const int I = __float_as_int(sp[kPbase][lp]) + ox, Jj = __float_as_int(sp[kPbase + 1][lp]) + oy,
                 K = __float_as_int(sp[kPbase + 2][lp]) + oz;
       if (I < 0 || I >= G || Jj < 0 || Jj >= G || K < 0 || K >= G) continue;
       const float fx[3] = {sp[kPfx][lp], sp[kPfx + 1][lp], sp[kPfx + 2][lp]};
-      // B-spline weights and offsets as in bspline() / p2g_node()
-      const float w = bspline_w(fx[0], ox) * bspline_w(fx[1], oy) * bspline_w(fx[2], oz);
+      // weights of bspline() and offsets as in p2g_node()
+      const float w = sp[kPw + ox][lp] * sp[kPw + 3 + oy][lp] * sp[kPw + 6 + oz][lp];
       const float dpos[3] = {((float)ox - fx[0]) * mp.dx, ((float)oy - fx[1]) * mp.dx, ((float)oz - fx[2]) * mp.dx};
       float val[7];
 #pragma unroll
@@ -420,8 +422,7 @@ __global__ __launch_bounds__(kChunk) void k_p2g_binned(FsiParticles pt, FsiGrid 
       }
     }
     __syncthreads();
-    // ---- phase 3: one global atomic per touched node value of the chunk
-    for (int li = tid; li < nv; li += kChunk) {
+    for (int li = tid; li < nv; li += T) {
       const int64_t node = box_node(bx, li, G);
 #pragma unroll
       for (int q = 0; q < 7; ++q) {
@@ -431,43 +432,46 @@ __global__ __launch_bounds__(kChunk) void k_p2g_binned(FsiParticles pt, FsiGrid 
     }
   }
   if (REACT) {
-    // diagnostics reductions (penalty.py:202-240, moving_boundary.py:312-374)
-    const int na = __reduce_add_sync(0xffffffffu, (unsigned)n_act);
-    const float pm = warp_max(pmax), gm = warp_max(gmax);
-    double sp3[3], sg[3];
+    const float gm = warp_max(gmax);
+    double sg[3];
 #pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      sp3[a] = warp_sum_d(pn[a]);
-      sg[a] = warp_sum_d(gn[a]);
-    }
+    for (int a = 0; a < 3; ++a) sg[a] = warp_sum_d(gn[a]);
     if ((tid & 31) == 0) {
-      if (na) atomicAdd(&st->active_reaction_particle_count, na);
-      if (pm > 0.f) atomic_max_nonneg(&st->max_particle_reaction_norm, pm);
       if (gm > 0.f) atomic_max_nonneg(&st->max_grid_reaction_norm, gm);
-      for (int a = 0; a < 3; ++a) {
-        if (sp3[a] != 0.0) atomicAdd(&st->net_particle_reaction[a], sp3[a]);
+      for (int a = 0; a < 3; ++a)
         if (sg[a] != 0.0) atomicAdd(&st->net_grid_reaction[a], sg[a]);
-      }
     }
   }
 }
 
+template <bool REACT, int T>
+__global__ __launch_bounds__(T) void k_p2g_scatter(FsiGrid g, FsiMpmParams mp, const float* __restrict__ payload,
+                                                   int n, const int2* __restrict__ chunks, int32_t* meta,
+                                                   int32_t* box, int buf, FsiCouplingStats* st) {
+  p2g_scatter_body<REACT, T>(g, mp, payload, n, chunks, meta, box, buf, st, blockIdx.x, gridDim.x);
+}
+
 // G2P of the chunks of this CTA from grid buffer g; zeroes the boxes the
-// previous substep recorded in the other buffer go.
-__global__ __launch_bounds__(kChunk) void k_g2p_binned(FsiParticles pt, FsiGrid g, FsiGrid go, FsiMpmParams mp,
-                                                       const int32_t* __restrict__ perm,
-                                                       const int2* __restrict__ chunks, const int32_t* meta,
-                                                       const int32_t* __restrict__ box_b,
-                                                       const int32_t* __restrict__ box_o, int buf,
-                                                       FsiCouplingStats* st_other) {
+// previous substep recorded in the other buffer go.  T threads per CTA: each
+// particle's 27 nodes are split over T / kChunk adjacent lanes (offsets o =
+// sub, sub + T/kChunk, ...), whose partial sums are combined with shuffles
+// before the first of them finishes the particle.
+template <int T>
+__device__ __forceinline__ void g2p_binned_body(const FsiParticles& pt, const FsiGrid& g, const FsiGrid& go,
+                                                const FsiMpmParams& mp, const int32_t* __restrict__ perm,
+                                                const int2* __restrict__ chunks, const int32_t* meta,
+                                                const int32_t* __restrict__ box_b, const int32_t* __restrict__ box_o,
+                                                int buf, FsiCouplingStats* st_other, int vb, int vg) {
+  constexpr int GP = T / kChunk;  // lanes per particle: 1, 2 or 4
+  static_assert(GP == 1 || GP == 2 || GP == 4, "T must be 128, 256 or 512");
   __shared__ float vt[3 * kTileCap];
   const int tid = threadIdx.x;
   const int G = g.n;
   const int64_t N = (int64_t)G * G * G;
   const int nrec = meta[1 + (1 - buf)];
-  for (int r = blockIdx.x; r < nrec; r += gridDim.x) {
+  for (int r = vb; r < nrec; r += vg) {
     const Box bx = load_box(box_o + 6 * r);
-    for (int li = tid; li < bx.vol; li += kChunk) {
+    for (int li = tid; li < bx.vol; li += T) {
       const int64_t node = box_node(bx, li, G);
       go.v[node] = 0.f;
       go.v[N + node] = 0.f;
@@ -478,7 +482,7 @@ __global__ __launch_bounds__(kChunk) void k_g2p_binned(FsiParticles pt, FsiGrid 
       go.f_ext[2 * N + node] = 0.f;
     }
   }
-  if (st_other && blockIdx.x == 0 && tid == 0) {
+  if (st_other && vb == 0 && tid == 0) {
     st_other->active_reaction_particle_count = 0;
     st_other->max_particle_reaction_norm = 0.f;
     st_other->max_grid_reaction_norm = 0.f;
@@ -491,12 +495,13 @@ __global__ __launch_bounds__(kChunk) void k_g2p_binned(FsiParticles pt, FsiGrid 
   }
   const int nch = meta[0];
   const float s4 = 4.0f * mp.inv_dx * mp.inv_dx;
-  for (int c = blockIdx.x; c < nch; c += gridDim.x) {
+  const int lp = tid / GP, sub = tid % GP;
+  for (int c = vb; c < nch; c += vg) {
     __syncthreads();  // the previous chunk's gathers are done
     const Box bx = load_box(box_b + 6 * c);
     const bool staged = bx.vol <= kTileCap;
     const int nv = staged ? bx.vol : 0;
-    for (int li = tid; li < nv; li += kChunk) {
+    for (int li = tid; li < nv; li += T) {
       const int64_t node = box_node(bx, li, G);
       const float m = g.m[node];
       const float P[3] = {g.v[node], g.v[N + node], g.v[2 * N + node]};
@@ -512,32 +517,70 @@ __global__ __launch_bounds__(kChunk) void k_g2p_binned(FsiParticles pt, FsiGrid 
     }
     __syncthreads();
     const int2 ch = chunks[c];
-    if (tid < ch.y) {
-      const int p = perm[ch.x + tid];
+    // all GP lanes of a particle take the same branch (lp < ch.y is uniform
+    // over them), so the shuffles below see all their partners
+    if (lp < ch.y) {
+      const int p = perm[ch.x + lp];
       const int n = pt.n;
       float X[3] = {pt.x[p], pt.x[n + p], pt.x[2 * n + p]};
       BSpline b;
       bspline(X, mp.inv_dx, b);
       float nvl[3] = {0.f, 0.f, 0.f}, nC[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
       if (!staged) {
-        g2p_gather_global(g, mp, b, nvl, nC);
+        if (sub == 0) g2p_gather_global(g, mp, b, nvl, nC);
       } else {
 #pragma unroll
-      for (int ox = 0; ox < 3; ++ox)
-#pragma unroll
-        for (int oy = 0; oy < 3; ++oy)
-#pragma unroll
-          for (int oz = 0; oz < 3; ++oz) {
+        for (int o0 = 0; o0 < 27; o0 += GP) {
+          const int o = o0 + sub;
+          if (o < 27) {
+            const int ox = o / 9, oy = (o / 3) % 3, oz = o % 3;
             const int I = b.base[0] + ox, Jj = b.base[1] + oy, K = b.base[2] + oz;
-            if (I < 0 || I >= G || Jj < 0 || Jj >= G || K < 0 || K >= G) continue;
-            const int li = ((K - bx.lo[2]) * bx.ext[1] + (Jj - bx.lo[1])) * bx.ext[0] + (I - bx.lo[0]);
-            const float gv[3] = {vt[li], vt[nv + li], vt[2 * nv + li]};
-            g2p_node(b, ox, oy, oz, mp.dx, s4, gv, nvl, nC);
+            if (I >= 0 && I < G && Jj >= 0 && Jj < G && K >= 0 && K < G) {
+              const int li = ((K - bx.lo[2]) * bx.ext[1] + (Jj - bx.lo[1])) * bx.ext[0] + (I - bx.lo[0]);
+              const float gv[3] = {vt[li], vt[nv + li], vt[2 * nv + li]};
+              if (GP == 1) {
+                g2p_node(b, ox, oy, oz, mp.dx, s4, gv, nvl, nC);
+              } else {
+                // the offsets of this lane are not compile-time constants: weights by
+                // value instead of indexing b.w (g2p_node's arithmetic otherwise)
+                const float dpos[3] = {((float)ox - b.fx[0]) * mp.dx, ((float)oy - b.fx[1]) * mp.dx,
+                                       ((float)oz - b.fx[2]) * mp.dx};
+                const float w = bspline_w(b.fx[0], ox) * bspline_w(b.fx[1], oy) * bspline_w(b.fx[2], oz);
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                  nvl[a] += w * gv[a];
+#pragma unroll
+                  for (int cc = 0; cc < 3; ++cc) nC[a * 3 + cc] += (w * gv[a]) * dpos[cc] * s4;
+                }
+              }
+            }
           }
+        }
       }
-      g2p_finish(pt, p, mp, X, nvl, nC);
+      if (GP > 1) {
+        // partners of a particle are adjacent lanes, aligned to GP
+        const unsigned grp = ((1u << GP) - 1u) << ((tid & 31) & ~(GP - 1));
+#pragma unroll
+        for (int w = 1; w < GP; w <<= 1) {
+#pragma unroll
+          for (int a = 0; a < 3; ++a) nvl[a] += __shfl_xor_sync(grp, nvl[a], w, GP);
+#pragma unroll
+          for (int a = 0; a < 9; ++a) nC[a] += __shfl_xor_sync(grp, nC[a], w, GP);
+        }
+      }
+      if (sub == 0) g2p_finish(pt, p, mp, X, nvl, nC);
     }
   }
+}
+
+template <int T>
+__global__ __launch_bounds__(T) void k_g2p_binned(FsiParticles pt, FsiGrid g, FsiGrid go, FsiMpmParams mp,
+                                                  const int32_t* __restrict__ perm,
+                                                  const int2* __restrict__ chunks, const int32_t* meta,
+                                                  const int32_t* __restrict__ box_b,
+                                                  const int32_t* __restrict__ box_o, int buf,
+                                                  FsiCouplingStats* st_other) {
+  g2p_binned_body<T>(pt, g, go, mp, perm, chunks, meta, box_b, box_o, buf, st_other, blockIdx.x, gridDim.x);
 }
 
 __global__ void k_grid_velocity(FsiGrid g, FsiMpmParams mp, float* __restrict__ out) {
@@ -570,7 +613,8 @@ int layout(int32_t n_particles, int32_t n_grid, int32_t* n_bins, int32_t* max_ch
 
 int check_bins(const FsiMpmBins* bins, int32_t n_particles, int32_t n_grid) {
   if (!bins) return invalid("null bins");
-  if (!bins->key || !bins->count || !bins->start || !bins->perm || !bins->chunk || !bins->box || !bins->meta)
+  if (!bins->key || !bins->count || !bins->start || !bins->perm || !bins->chunk || !bins->box || !bins->meta ||
+      !bins->payload)
     return invalid("null bins array");
   int32_t nb = 0, mc = 0;
   const int rc = layout(n_particles, n_grid, &nb, &mc);
@@ -646,6 +690,8 @@ extern "C" int fsi_mpm_substep_binned(const FsiParticles* pt, const FsiGrid grid
   if ((rc = check_grid(&grid[0])) || (rc = check_grid(&grid[1]))) return rc;
   if (grid[0].n != grid[1].n) return invalid("the two grid buffers differ in size");
   if (buffer != 0 && buffer != 1) return invalid("buffer must be 0 or 1");
+  if (mp->tune < 0 || mp->tune > 15 || (mp->tune & 3) == 3 || ((mp->tune >> 2) & 3) == 3)
+    return invalid("unknown FsiMpmParams.tune");
   if ((rc = check_bins(bins, pt->n, grid[0].n))) return rc;
   if (cp) {
     if (!s || !hydro || !stats) return invalid("reaction transfer needs the lattice state, hydro and stats");
@@ -661,18 +707,38 @@ extern "C" int fsi_mpm_substep_binned(const FsiParticles* pt, const FsiGrid grid
   int32_t* box_o = bins->box + (int64_t)6 * bins->max_chunks * (1 - buffer);
   const int2* chunks = reinterpret_cast<const int2*>(bins->chunk);
   const FsiGrid g = grid[buffer], go = grid[1 - buffer];
+  const int tsc = mp->tune & 3, tg = (mp->tune >> 2) & 3;
+  const int T = tsc == FSI_TUNE_MPM_T512 ? 512 : (tsc == FSI_TUNE_MPM_T256 ? 256 : 128);
+  const int TG = tg == FSI_TUNE_MPM_T512 ? 512 : (tg == FSI_TUNE_MPM_T256 ? 256 : 128);
+  const LatView L = cp ? LatView{s->nx, s->ny, s->nz, s->pitch} : LatView{0, 0, 0, 0};
+  const float* hy = cp ? hydro : nullptr;
+  const float* ph = cp ? s->phi : nullptr;
+  const FsiCouplingParams cpv = cp ? *cp : FsiCouplingParams{};
+  FsiCouplingStats* stb = cp ? &stats[buffer] : nullptr;
+  const FsiLbmDiag* dg = cp ? s->diag : nullptr;
+  if (cp)
+    k_p2g_payload<true><<<nblk(pt->n, 128), 128, 0, st>>>(*pt, *mp, bins->perm, bins->payload, L, hy, ph, cpv, stb,
+                                                          dg);
+  else
+    k_p2g_payload<false><<<nblk(pt->n, 128), 128, 0, st>>>(*pt, *mp, bins->perm, bins->payload, L, hy, ph, cpv, stb,
+                                                           dg);
+  if ((rc = launch_check("k_p2g_payload"))) return rc;
+#define FSI_P2G(R, TT)                                                                                            \
+  k_p2g_scatter<R, TT><<<grid_ctas, TT, 0, st>>>(g, *mp, bins->payload, pt->n, chunks, bins->meta, box_b, buffer, \
+                                                 stb)
   if (cp) {
-    const LatView L{s->nx, s->ny, s->nz, s->pitch};
-    k_p2g_binned<true><<<grid_ctas, kChunk, 0, st>>>(*pt, g, *mp, bins->perm, chunks, bins->meta, box_b, buffer, L,
-                                                     hydro, s->phi, *cp, &stats[buffer], s->diag);
+    if (T == 512) FSI_P2G(true, 512); else if (T == 256) FSI_P2G(true, 256); else FSI_P2G(true, 128);
   } else {
-    const LatView L{0, 0, 0, 0};
-    k_p2g_binned<false><<<grid_ctas, kChunk, 0, st>>>(*pt, g, *mp, bins->perm, chunks, bins->meta, box_b, buffer, L,
-                                                      nullptr, nullptr, FsiCouplingParams{}, nullptr, nullptr);
+    if (T == 512) FSI_P2G(false, 512); else if (T == 256) FSI_P2G(false, 256); else FSI_P2G(false, 128);
   }
-  if ((rc = launch_check("k_p2g_binned"))) return rc;
-  k_g2p_binned<<<grid_ctas, kChunk, 0, st>>>(*pt, g, go, *mp, bins->perm, chunks, bins->meta, box_b, box_o, buffer,
-                                             cp ? &stats[1 - buffer] : nullptr);
+#undef FSI_P2G
+  if ((rc = launch_check("k_p2g_scatter"))) return rc;
+  FsiCouplingStats* sto = cp ? &stats[1 - buffer] : nullptr;
+#define FSI_G2P(TT)                                                                                                \
+  k_g2p_binned<TT><<<grid_ctas, TT, 0, st>>>(*pt, g, go, *mp, bins->perm, chunks, bins->meta, box_b, box_o, buffer, \
+                                             sto)
+  if (TG == 512) FSI_G2P(512); else if (TG == 256) FSI_G2P(256); else FSI_G2P(128);
+#undef FSI_G2P
   return launch_check("k_g2p_binned");
 }
 
@@ -683,4 +749,131 @@ extern "C" int fsi_mpm_grid_velocity(const FsiGrid* g, const FsiMpmParams* mp, f
   const int64_t N = (int64_t)g->n * g->n * g->n;
   k_grid_velocity<<<nblk(N, 256), 256, 0, (cudaStream_t)stream>>>(*g, *mp, out);
   return launch_check("k_grid_velocity");
+}
+
+// ---- batched cases: MPM (grid.y = case slot) --------------------------------
+namespace fsi {
+namespace {
+
+// the force field the reaction transfer samples: the last LBM step's link
+// forces (moving boundary, one LBM step per FSI step: the ping-pong slot the
+// step wrote, now pp ^ 1) or the penalty hydro force
+__device__ __forceinline__ const float* batch_hydro(const FsiBatchCase& bc) {
+  if (bc.mode == FSI_BATCH_MOVING) return bc.lbm.hpp + (int64_t)(bc.ctl.pp ^ 1) * 3 * bc.lbm.pitch;
+  return bc.lbm.hydro;
+}
+
+__global__ void k_batch_bin_count(const FsiBatchCase* __restrict__ cases) {
+  const FsiBatchCase& bc = cases[blockIdx.y];
+  if (!bc.active) return;
+  const int G = bc.grid[0].n, nb = (G + kEdge - 1) / kEdge;
+  const int nvb = (bc.pt.n + blockDim.x - 1) / blockDim.x;
+  for (int vb = blockIdx.x; vb < nvb; vb += gridDim.x)
+    bin_count_body(bc.pt, bc.mp.inv_dx, G, nb, bc.bins.key, bc.bins.count, vb, nvb);
+}
+
+__global__ __launch_bounds__(1024) void k_batch_bin_scan(const FsiBatchCase* __restrict__ cases) {
+  const FsiBatchCase& bc = cases[blockIdx.y];
+  if (!bc.active) return;
+  bin_scan_body(bc.bins.n_bins, bc.bins.count, bc.bins.start, reinterpret_cast<int2*>(bc.bins.chunk), bc.bins.meta);
+}
+
+__global__ void k_batch_bin_scatter(const FsiBatchCase* __restrict__ cases) {
+  const FsiBatchCase& bc = cases[blockIdx.y];
+  if (!bc.active) return;
+  const int nvb = (bc.pt.n + blockDim.x - 1) / blockDim.x;
+  for (int vb = blockIdx.x; vb < nvb; vb += gridDim.x)
+    bin_scatter_body(bc.pt.n, bc.bins.key, bc.bins.start, bc.bins.perm, vb, nvb);
+}
+
+__global__ __launch_bounds__(128) void k_batch_p2g_payload(const FsiBatchCase* __restrict__ cases) {
+  const FsiBatchCase& bc = cases[blockIdx.y];
+  if (!bc.active) return;
+  const LatView L{bc.lbm.nx, bc.lbm.ny, bc.lbm.nz, bc.lbm.pitch};
+  const int nvb = (bc.pt.n + blockDim.x - 1) / blockDim.x;
+  const float* hydro = batch_hydro(bc);
+  for (int vb = blockIdx.x; vb < nvb; vb += gridDim.x)
+    p2g_payload_body<true>(bc.pt, bc.mp, bc.bins.perm, bc.bins.payload, L, hydro, bc.lbm.phi, bc.cp,
+                           &bc.react_stats[bc.buf], bc.lbm.diag, vb, nvb);
+}
+
+template <int T>
+__global__ __launch_bounds__(T) void k_batch_p2g_scatter(const FsiBatchCase* __restrict__ cases) {
+  const FsiBatchCase& bc = cases[blockIdx.y];
+  if (!bc.active) return;
+  const int b = bc.buf;
+  int32_t* box_b = bc.bins.box + (int64_t)6 * bc.bins.max_chunks * b;
+  p2g_scatter_body<true, T>(bc.grid[b], bc.mp, bc.bins.payload, bc.pt.n, reinterpret_cast<const int2*>(bc.bins.chunk),
+                            bc.bins.meta, box_b, b, &bc.react_stats[b], blockIdx.x, gridDim.x);
+}
+
+template <int T>
+__global__ __launch_bounds__(T) void k_batch_g2p(const FsiBatchCase* __restrict__ cases) {
+  const FsiBatchCase& bc = cases[blockIdx.y];
+  if (!bc.active) return;
+  const int b = bc.buf;
+  const int32_t* box_b = bc.bins.box + (int64_t)6 * bc.bins.max_chunks * b;
+  const int32_t* box_o = bc.bins.box + (int64_t)6 * bc.bins.max_chunks * (1 - b);
+  g2p_binned_body<T>(bc.pt, bc.grid[b], bc.grid[1 - b], bc.mp, bc.bins.perm,
+                     reinterpret_cast<const int2*>(bc.bins.chunk), bc.bins.meta, box_b, box_o, b,
+                     &bc.react_stats[1 - b], blockIdx.x, gridDim.x);
+}
+
+__global__ void k_batch_mpm_post(FsiBatchCase* cases) {
+  FsiBatchCase& bc = cases[blockIdx.x];
+  if (bc.active && threadIdx.x == 0) bc.buf ^= 1;
+}
+
+int check_batch_mpm(const FsiBatchCase* cases, const FsiBatchDims* d) {
+  if (!cases || !d) return invalid("null batch argument");
+  if (d->n_cases <= 0 || d->n_cases > 65535) return invalid("n_cases must be in 1..65535");
+  if (d->max_particles <= 0 || d->max_chunks <= 0 || d->max_bins <= 0) return invalid("batch MPM dims must be positive");
+  if (d->mpm_tune < 0 || d->mpm_tune > 15 || (d->mpm_tune & 3) == 3 || ((d->mpm_tune >> 2) & 3) == 3)
+    return invalid("unknown FsiBatchDims.mpm_tune");
+  return FSI_OK;
+}
+
+}  // namespace
+}  // namespace fsi
+
+extern "C" int fsi_batch_mpm_bin(FsiBatchCase* cases, const FsiBatchDims* d, void* stream) {
+  int rc = check_batch_mpm(cases, d);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int cap = std::max(4, sm_count() * 8 / d->n_cases);
+  const dim3 g((unsigned)std::min<int64_t>(nblk(d->max_particles, 256), cap), d->n_cases);
+  k_batch_bin_count<<<g, 256, 0, st>>>(cases);
+  if ((rc = launch_check("k_batch_bin_count"))) return rc;
+  k_batch_bin_scan<<<dim3(1, d->n_cases), 1024, 0, st>>>(cases);
+  if ((rc = launch_check("k_batch_bin_scan"))) return rc;
+  k_batch_bin_scatter<<<g, 256, 0, st>>>(cases);
+  return launch_check("k_batch_bin_scatter");
+}
+
+extern "C" int fsi_batch_mpm_substep(FsiBatchCase* cases, const FsiBatchDims* d, void* stream) {
+  int rc = check_batch_mpm(cases, d);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int cap = std::max(4, sm_count() * 8 / d->n_cases);
+  const dim3 gp((unsigned)std::min<int64_t>(nblk(d->max_particles, 128), cap), d->n_cases);
+  k_batch_p2g_payload<<<gp, 128, 0, st>>>(cases);
+  if ((rc = launch_check("k_batch_p2g_payload"))) return rc;
+  const dim3 gc((unsigned)std::min<int64_t>(d->max_chunks, std::max(2, sm_count() * 4 / d->n_cases)), d->n_cases);
+  const int tsc = d->mpm_tune & 3, tg = (d->mpm_tune >> 2) & 3;
+  if (tsc == FSI_TUNE_MPM_T512)
+    k_batch_p2g_scatter<512><<<gc, 512, 0, st>>>(cases);
+  else if (tsc == FSI_TUNE_MPM_T256)
+    k_batch_p2g_scatter<256><<<gc, 256, 0, st>>>(cases);
+  else
+    k_batch_p2g_scatter<128><<<gc, 128, 0, st>>>(cases);
+  if ((rc = launch_check("k_batch_p2g_scatter"))) return rc;
+  if (tg == FSI_TUNE_MPM_T512)
+    k_batch_g2p<512><<<gc, 512, 0, st>>>(cases);
+  else if (tg == FSI_TUNE_MPM_T256)
+    k_batch_g2p<256><<<gc, 256, 0, st>>>(cases);
+  else
+    k_batch_g2p<128><<<gc, 128, 0, st>>>(cases);
+  if ((rc = launch_check("k_batch_g2p"))) return rc;
+  k_batch_mpm_post<<<d->n_cases, 32, 0, st>>>(cases);
+  return launch_check("k_batch_mpm_post");
 }

@@ -13,6 +13,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 
 #include "common.cuh"
@@ -21,10 +22,8 @@
 namespace fsi {
 
 // ---------------------------------------------------------- projection ----
-__global__ void k_project_scatter(LatView L, FsiParticles pt, FsiCouplingParams cp, float* phi, float* smass,
-                                  float* svel) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= pt.n) return;
+__device__ __forceinline__ void project_particle(const LatView& L, const FsiParticles& pt, const FsiCouplingParams& cp,
+                                                 float* phi, float* smass, float* svel, int p) {
   const int n = pt.n;
   const float X[3] = {pt.x[p], pt.x[n + p], pt.x[2 * n + p]};
   BSpline b;
@@ -52,10 +51,19 @@ __global__ void k_project_scatter(LatView L, FsiParticles pt, FsiCouplingParams 
       }
 }
 
-__global__ void k_project_normalize(LatView L, FsiCouplingParams cp, float* phi, float* smass, float* svel,
-                                    FsiCouplingStats* st) {
+__global__ void k_project_scatter(LatView L, FsiParticles pt, FsiCouplingParams cp, float* phi, float* smass,
+                                  float* svel) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < pt.n) project_particle(L, pt, cp, phi, smass, svel, p);
+}
+
+// cells base + lane of one warp (base warp-uniform: the reductions need the
+// whole warp)
+__device__ __forceinline__ void project_normalize_warp(const LatView& L, const FsiCouplingParams& cp, float* phi,
+                                                       float* smass, float* svel, FsiCouplingStats* st,
+                                                       int64_t base) {
   const int64_t n = (int64_t)L.nx * L.ny * L.nz;
-  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t c = base + (threadIdx.x & 31);
   double pm = 0.0, pvr = 0.0, pvc = 0.0;
   float mx = 0.f;
   int active = 0;
@@ -87,6 +95,12 @@ __global__ void k_project_normalize(LatView L, FsiCouplingParams cp, float* phi,
     if (mx > 0.f) atomic_max_nonneg(&st->max_phi_raw, mx);
     if (na) atomicAdd(&st->active_cell_count, na);
   }
+}
+
+__global__ void k_project_normalize(LatView L, FsiCouplingParams cp, float* phi, float* smass, float* svel,
+                                    FsiCouplingStats* st) {
+  project_normalize_warp(L, cp, phi, smass, svel, st,
+                         (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31));
 }
 
 // ------------------------------------------------------------ reaction ----
@@ -304,4 +318,74 @@ extern "C" int fsi_mpm_g2p(const FsiParticles* pt, const FsiGrid* g, const FsiMp
   if (!pt->fixed || !pt->fixed_x) return invalid("null fixed-particle fields");
   k_g2p<<<nblk(pt->n, 128), 128, 0, (cudaStream_t)stream>>>(*pt, *g, *mp);
   return launch_check("k_g2p");
+}
+
+// ---- batched cases: projection (grid.y = case slot) -------------------------
+namespace fsi {
+namespace {
+
+__device__ __forceinline__ LatView lat_of(const FsiBatchCase& bc) {
+  return LatView{bc.lbm.nx, bc.lbm.ny, bc.lbm.nz, bc.lbm.pitch};
+}
+
+// fsi_project's clears: solid_phi, solid_mass, solid_vel and the projection
+// reductions
+__global__ void k_batch_project_clear(FsiBatchCase* cases) {
+  const FsiBatchCase& bc = cases[blockIdx.y];
+  if (!bc.active) return;
+  const int64_t P = bc.lbm.pitch;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < P; i += stride) {
+    bc.lbm.phi[i] = 0.f;
+    bc.lbm.smass[i] = 0.f;
+    bc.lbm.svel[i] = 0.f;
+    bc.lbm.svel[P + i] = 0.f;
+    bc.lbm.svel[2 * P + i] = 0.f;
+  }
+  if (blockIdx.x == 0) {
+    int* w = reinterpret_cast<int*>(bc.proj_stats);
+    for (int i = threadIdx.x; i < (int)(offsetof(FsiCouplingStats, active_reaction_particle_count) / 4);
+         i += blockDim.x)
+      w[i] = 0;
+  }
+}
+
+__global__ void k_batch_project_scatter(const FsiBatchCase* __restrict__ cases) {
+  const FsiBatchCase& bc = cases[blockIdx.y];
+  if (!bc.active) return;
+  const LatView L = lat_of(bc);
+  const FsiParticles pt = bc.pt;
+  const FsiCouplingParams cp = bc.cp;
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < pt.n; p += gridDim.x * blockDim.x)
+    project_particle(L, pt, cp, bc.lbm.phi, bc.lbm.smass, bc.lbm.svel, p);
+}
+
+__global__ void k_batch_project_normalize(const FsiBatchCase* __restrict__ cases) {
+  const FsiBatchCase& bc = cases[blockIdx.y];
+  if (!bc.active) return;
+  const LatView L = lat_of(bc);
+  const FsiCouplingParams cp = bc.cp;
+  const int64_t n = (int64_t)L.nx * L.ny * L.nz;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t base = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += stride)
+    project_normalize_warp(L, cp, bc.lbm.phi, bc.lbm.smass, bc.lbm.svel, bc.proj_stats, base);
+}
+
+}  // namespace
+}  // namespace fsi
+
+extern "C" int fsi_batch_project(FsiBatchCase* cases, const FsiBatchDims* d, void* stream) {
+  if (!cases || !d || d->n_cases <= 0 || d->n_cases > 65535 || d->max_cells <= 0 || d->max_particles <= 0)
+    return invalid("bad batch arguments");
+  cudaStream_t st = (cudaStream_t)stream;
+  const int64_t cap = std::max(8, 148 * 8 / d->n_cases);
+  const unsigned gc = (unsigned)std::min<int64_t>((d->max_cells + 255) / 256, cap);
+  k_batch_project_clear<<<dim3(gc, d->n_cases), 256, 0, st>>>(cases);
+  int rc = launch_check("k_batch_project_clear");
+  if (rc) return rc;
+  const unsigned gp = (unsigned)std::min<int64_t>((d->max_particles + 127) / 128, cap);
+  k_batch_project_scatter<<<dim3(gp, d->n_cases), 128, 0, st>>>(cases);
+  if ((rc = launch_check("k_batch_project_scatter"))) return rc;
+  k_batch_project_normalize<<<dim3(gc, d->n_cases), 256, 0, st>>>(cases);
+  return launch_check("k_batch_project_normalize");
 }

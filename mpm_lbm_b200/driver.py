@@ -82,6 +82,7 @@ class FSIDriver3D:
         self._graph = None
         self._graph_steps = 0
         self.graph_kernels_per_step = None
+        self.tuning = None
 
     # ------------------------------------------------------------ init
     def _geometry_config(self):
@@ -190,6 +191,29 @@ class FSIDriver3D:
             self.initial_particle_positions = np.asarray(x, np.float32).copy()
             if free_tip_mask is not None:
                 self.free_tip_proxy_mask = np.asarray(free_tip_mask, bool)
+
+    # ------------------------------------------------------------ tuning
+    def autotune(self):
+        """Time the launch variants of the step kernels on this case's state and
+        keep the fastest (results are identical across variants).  Drops a
+        captured step graph so that the next step recaptures with the choice."""
+        from .autotune import tune_lbm, tune_mpm
+
+        if not self.initialized:
+            self.initialize()
+        self._graph = None
+        self._graph_steps = 0
+        step = self.lbm.step_moving_bounceback if self.config.coupling_mode == "moving_boundary" else self.lbm.step
+        self.tuning = {"lbm": tune_lbm(self.lbm, step)}
+        if self.mpm_path == "binned":
+            mode = self.config.coupling_mode
+            coupler = {"penalty": self.penalty_coupler, "none": None}.get(mode)
+            if mode == "moving_boundary":
+                coupler = self.mb_coupler if self.mb_coupler is not None else self.link_area_coupler
+            lbm = self.lbm if coupler is not None else None
+            extra = () if coupler is None else (coupler.binned_stats.t,)
+            self.tuning["mpm"] = tune_mpm(self.solid, lambda: self.solid.substep_binned(coupler, lbm), extra=extra)
+        return self.tuning
 
     # ------------------------------------------------------------ steps
     def _t(self, key, t0):

@@ -111,6 +111,7 @@ class LBMFluid3D:
         self._readout_version = -1
         self._old_equals_solid = False
         self.dirstats_enabled = True
+        self.tune = 0  # FSI_TUNE_LBM_* launch variant (mpm_lbm_b200.autotune picks it)
         self.tau_f = None
         self._sync_params()
         self._make_fields()
@@ -137,6 +138,7 @@ class LBMFluid3D:
         p.ob_floor = float(cfg.open_boundary_population_floor) if cfg.open_boundary_population_floor is not None else -1e30
         if self._penalty is not None:
             p.penalty_beta, p.penalty_phi_min, p.penalty_cap = self._penalty
+        p.tune = int(self.tune)
 
     def _ctl(self, mode=0, pp=None):
         return FsiStepCtl(parity=self.parity, bc_pending=int(self.bc_pending), pp=self.pp if pp is None else pp,
@@ -144,6 +146,26 @@ class LBMFluid3D:
 
     def _stream(self):
         return stream_handle()
+
+    # ------------------------------------------------- state snapshots
+    _SNAPSHOT = ("t_pop", "t_flags", "t_nbr", "t_rho", "t_vel", "t_old", "t_reinit", "t_cf", "t_hydro", "t_accum",
+                 "t_hpp", "t_plane", "t_diag")
+    _SNAPSHOT_ATTRS = ("parity", "bc_pending", "pp", "last_pp", "steps", "_accumulating", "_fused_accumulation",
+                       "_sample_count", "_hydro_src", "_old_equals_solid", "_penalty", "dirstats_enabled")
+
+    def snapshot(self):
+        """Device copies of the mutable state (for trial steps, e.g. autotuning)."""
+        return ({k: getattr(self, k).clone() for k in self._SNAPSHOT},
+                {k: getattr(self, k) for k in self._SNAPSHOT_ATTRS})
+
+    def restore(self, snap):
+        tensors, attrs = snap
+        for k, t in tensors.items():
+            getattr(self, k).copy_(t)
+        for k, v in attrs.items():
+            setattr(self, k, v)
+        self._sync_params()
+        self._version += 1
 
     # ------------------------------------------------------------ fields
     def _make_fields(self):

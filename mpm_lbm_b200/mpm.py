@@ -14,7 +14,8 @@ import os
 import numpy as np
 import torch
 
-from ._lib import FsiCouplingStats, FsiGrid, FsiMpmBins, FsiMpmParams, FsiParticles, call, ptr, stream_handle
+from ._lib import (FSI_MPM_PAYLOAD_ROWS, FsiCouplingStats, FsiGrid, FsiMpmBins, FsiMpmParams, FsiParticles, call,
+                   ptr, stream_handle)
 from .config import MPMConfig
 from .fields import ParticleField
 
@@ -245,7 +246,8 @@ class MPMSolid3D:
         i32 = lambda *s: torch.zeros(*s, dtype=torch.int32, device=dev)  # noqa: E731
         f32 = lambda *s: torch.zeros(*s, dtype=torch.float32, device=dev)  # noqa: E731
         t = {"key": i32(n), "count": i32(nb.value), "start": i32(nb.value), "perm": i32(n),
-             "chunk": i32(mc.value, 2), "box": i32(2, mc.value, 6), "meta": i32(4)}
+             "chunk": i32(mc.value, 2), "box": i32(2, mc.value, 6), "meta": i32(4),
+             "payload": f32(FSI_MPM_PAYLOAD_ROWS, n)}
         self.t_gv1, self.t_gm1, self.t_gf1 = f32(3, G), f32(G), f32(3, G)
         grids = (FsiGrid * 2)()
         grids[0] = self.grid
@@ -285,6 +287,31 @@ class MPMSolid3D:
             self._binned_last = None
         self._binned_clean = False
         return self.t_gv, self.t_gm, self.t_gf
+
+    # ---- state snapshots (trial substeps, e.g. autotuning) ----------------
+    _SNAPSHOT = ("t_x", "t_v", "t_C", "t_F", "t_Jp", "t_gv", "t_gm", "t_gf")
+    _SNAPSHOT_ATTRS = ("_buf", "_binned_last", "_binned_clean", "_since_bin")
+
+    def snapshot(self, extra=()):
+        """Device copies of the mutable particle, grid and bin state (plus the
+        given extra tensors)."""
+        names = list(self._SNAPSHOT)
+        if self._bins is not None:
+            names += ["t_gv1", "t_gm1", "t_gf1"]
+        tensors = {k: getattr(self, k).clone() for k in names}
+        bins = {} if self._bins is None else {k: v.clone() for k, v in self._bins["t"].items()}
+        return (tensors, bins, [(t, t.clone()) for t in extra], {k: getattr(self, k) for k in self._SNAPSHOT_ATTRS})
+
+    def restore(self, snap):
+        tensors, bins, extra, attrs = snap
+        for k, t in tensors.items():
+            getattr(self, k).copy_(t)
+        for k, t in bins.items():
+            self._bins["t"][k].copy_(t)
+        for t, c in extra:
+            t.copy_(c)
+        for k, v in attrs.items():
+            setattr(self, k, v)
 
     def rebin(self):
         """Sort particle ids by 4x4x4-cell block (fsi_mpm_bin)."""

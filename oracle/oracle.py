@@ -602,3 +602,30 @@ class OracleFSIDriver:
             solid.grid_update()
             solid.g2p()
             self.total_mpm_substeps += 1
+
+
+def fsi_driver_for_case(case, dtype=np.float32, substeps=None, mpm_substeps=None, threads=1):
+    """The oracle set up on a duct/plate case of ``mpm_lbm_b200.cases``: the
+    same geometry, particles, material, unit mapping and open boundaries as
+    ``case.make_driver()``, moving_boundary subcycled, engineering transfer.
+    substeps / mpm_substeps override the case's S and M per FSI step."""
+    cfg = case.config()
+    solid, parts = case.geometry()
+    sim = cfg.make_unified_sim_config()
+    nx, ny, nz = case.lattice
+    vel = ((case.u_in, 0, 0), (0, 0, 0), (0, 0, 0), (0, 0, 0), (0, 0, 0), (0, 0, 0))
+    lbm = OracleLBM(nx, ny, nz, niu=sim.lbm_niu, relaxation_semantics=sim.lbm_relaxation_semantics,
+                    open_boundary_semantics=cfg.lbm_open_boundary_semantics, bc=(2, 1, 0, 0, 0, 0),
+                    rho_bc=(1.0,) * 6, vel_bc=vel, limiter_enabled=cfg.open_boundary_limiter_enabled, dtype=dtype)
+    lbm.threads = int(threads)
+    lbm.init_geo_array(solid)
+    lbm.init_simulation()
+    mc = sim.make_mpm_config(gravity=cfg.gravity, **case.material())
+    mpm = OracleMPM(nx, mc.dx, mc.dt, len(parts["x"]), gravity=mc.gravity, young_modulus=mc.young_modulus,
+                    poisson_ratio=mc.poisson_ratio, p_rho=mc.p_rho, dtype=dtype)
+    mpm.init_from_numpy(parts["x"], parts["vol0"], parts["mass"], fixed_mask_np=parts["fixed"])
+    cpl = OracleCoupling(nx, sim.dx_norm, sim.lbm_dt_phys, mb_force_cap_norm=cfg.mb_force_cap_norm)
+    S = case.lbm_substeps if substeps is None else int(substeps)
+    M = case.mpm_substeps if mpm_substeps is None else int(mpm_substeps)
+    return OracleFSIDriver(lbm, mpm, cpl, fsi_exchange_mode="lbm_subcycled_per_fsi_step",
+                           lbm_substeps_per_fsi_step=S, mpm_substeps_per_lbm_step=M)

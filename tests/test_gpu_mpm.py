@@ -138,9 +138,16 @@ def test_one_phase_substeps_match_oracle():
     compare_grid(gpu, ora)
 
 
+# FsiMpmParams.tune: scatter variant | gather variant << 2 (threads per chunk
+# CTA 128 / 256 / 512)
+TUNES = [0, 1 | 1 << 2, 2 | 2 << 2, 2]
+
+
+@pytest.mark.parametrize("tune", TUNES)
 @pytest.mark.parametrize("lock_z,damping", [(False, 0.0), (True, 0.0), (False, 5.0)])
-def test_binned_substeps_match_oracle(lock_z, damping):
+def test_binned_substeps_match_oracle(lock_z, damping, tune):
     gpu, ora = make_solids(lock_z=lock_z, damping=damping)
+    gpu.params.tune = tune
     for s in range(5):  # both grid buffers, and the zeroing of recorded boxes, are exercised
         gpu.substep_binned()
         ora.substep()
@@ -231,9 +238,12 @@ def _oracle_react_stats(st, kind):
 
 
 @pytest.mark.parametrize("kind", [0, 1, 2])
-@pytest.mark.parametrize("path", ["binned", "one_phase"])
+@pytest.mark.parametrize("path", ["binned", "binned_t512", "one_phase"])
 def test_reaction_substeps_match_oracle(kind, path):
     gpu, ora = make_solids(seed=2)
+    if path == "binned_t512":
+        gpu.params.tune = 2 | 2 << 2
+        path = "binned"
     lbm, cpl, olbm, oc = _lbm_and_coupling(kind)
     for _ in range(3):
         if path == "binned":
