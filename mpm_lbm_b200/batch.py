@@ -263,7 +263,7 @@ class FSIBatch:
 
     def _upload(self, slot):
         size = ctypes.sizeof(FsiBatchCase)
-        raw = bytes(memoryview(self.records)[slot * size:(slot + 1) * size].cast("B"))
+        raw = ctypes.string_at(ctypes.addressof(self.records[slot]), size)
         host = torch.frombuffer(bytearray(raw), dtype=torch.uint8)
         self.t_cases[slot * size:(slot + 1) * size].copy_(host)
 
