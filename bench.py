@@ -358,7 +358,9 @@ def main():
                    "population_storage": args.storage,
                    "l2": "flushed (256 MB write) between timed FSI steps", "cuda_graph": True,
                    "launch_variants": None if tuning is None else
-                   {"lbm_tune": tuning["lbm"]["choice"], "mpm_tune": tuning.get("mpm", {}).get("choice")},
+                   {"lbm_tune": tuning["lbm"]["choice"], "mpm_tune": tuning.get("mpm", {}).get("choice"),
+                    "lbm_ms_per_substep": tuning["lbm"]["ms_per_substep"],
+                    "mpm_ms_per_substep": tuning.get("mpm", {}).get("ms_per_substep")},
                    "parallelism": f"replicas x{ws}"},
         "particle_updates_per_s": ws * args.steps * wl.M * n / (total_ms * 1e-3),
         "roofline": roofline,

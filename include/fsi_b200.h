@@ -126,6 +126,8 @@ typedef struct FsiLbmParams {
 enum {
   FSI_TUNE_LBM_OCC3 = 0,  /* registers for 3 CTAs of 256 threads per SM (default) */
   FSI_TUNE_LBM_OCC4 = 1,  /* registers for 4 CTAs per SM (64 per thread) */
+  FSI_TUNE_LBM_PAIR = 2,  /* two x-adjacent cells per thread on the paired FP32 pipe; nx even, and
+                             nx % 64 != 2 with open boundaries (results agree to FP32 rounding) */
 };
 
 typedef struct FsiStepCtl {

@@ -1,10 +1,12 @@
 """Autotuner for the launch variants of the step kernels.
 
-The variants differ only in how a kernel maps onto the SMs: the register
-budget of the LBM step kernel (3 or 4 resident CTAs per SM; bit-identical
-results), and the threads per particle chunk of the binned MPM substep (the
-same arithmetic; the grid sums are float atomics whose order, and so whose
-last-bit rounding, varies from run to run with any variant).  The tuner times each variant with CUDA events
+The variants differ in how a kernel maps onto the SMs: the register budget of
+the one-cell LBM step kernel (3 or 4 resident CTAs per SM; bit-identical
+results), the two-cells-per-thread LBM kernel on the paired FP32 pipe (the
+same operator; its contraction of multiply-adds differs, so results agree to
+FP32 rounding), and the threads per particle chunk of the binned MPM substep
+(the same arithmetic; the grid sums are float atomics whose order, and so
+whose last-bit rounding, varies from run to run with any variant).  The tuner times each variant with CUDA events
 on the caller's own state -- trial steps on a device snapshot that is
 restored afterwards -- and keeps the fastest.  It runs before a CUDA graph of
 the step is captured (a captured graph keeps the variant it was built with).
@@ -14,7 +16,8 @@ from __future__ import annotations
 
 import torch
 
-from ._lib import FSI_TUNE_LBM_OCC3, FSI_TUNE_LBM_OCC4, FSI_TUNE_MPM_T128, FSI_TUNE_MPM_T256, FSI_TUNE_MPM_T512
+from ._lib import (FSI_TUNE_LBM_OCC3, FSI_TUNE_LBM_OCC4, FSI_TUNE_LBM_PAIR, FSI_TUNE_MPM_T128, FSI_TUNE_MPM_T256,
+                   FSI_TUNE_MPM_T512)
 
 
 def _time_ms(fn, steps, reps):
@@ -31,10 +34,21 @@ def _time_ms(fn, steps, reps):
     return best
 
 
-def tune_lbm(lbm, step_fn, candidates=(FSI_TUNE_LBM_OCC3, FSI_TUNE_LBM_OCC4), steps=10, reps=3):
+def lbm_candidates(lbm):
+    """Launch variants valid for this lattice: the paired kernel needs an even
+    nx, and nx % 64 != 2 with open boundaries."""
+    out = [FSI_TUNE_LBM_OCC3, FSI_TUNE_LBM_OCC4]
+    if lbm.nx % 2 == 0 and not ((lbm.bc_x_left or lbm.bc_x_right) and lbm.nx % 64 == 2):
+        out.append(FSI_TUNE_LBM_PAIR)
+    return out
+
+
+def tune_lbm(lbm, step_fn, candidates=None, steps=10, reps=3):
     """Pick lbm.tune among candidates by timing `step_fn` (one LBM substep of
     the caller's kind) on a snapshot of the state.  Returns
     {"choice": tune, "ms_per_substep": {tune: ms}}."""
+    if candidates is None:
+        candidates = lbm_candidates(lbm)
     snap = lbm.snapshot()
     times = {}
     try:

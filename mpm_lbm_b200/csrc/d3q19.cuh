@@ -204,3 +204,130 @@ FSI_HD void mrt_collide(const float* F, float rho, float ux, float uy, float uz,
 }
 
 }  // namespace fsi
+
+#if defined(__CUDACC__)
+#include <cuda_runtime.h>
+namespace fsi {
+
+// ---- paired form: two cells per thread on the sm_100 paired FP32 pipe ----
+// The same operator as mrt_collide, for the populations of two cells held as
+// (cell 0, cell 1) pairs, each operation one paired FP32 instruction.
+__device__ __forceinline__ float2 p2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+// a - b, exact as a subtraction: fma(b, -1, a) rounds once
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.0f, -1.0f), a); }
+
+__device__ __forceinline__ void moments0_2(const float2* F, float2& rho, float2& jx, float2& jy, float2& jz) {
+  float2 s[10], d[10];
+#pragma unroll
+  for (int p = 1; p <= 9; ++p) {
+    s[p] = add2(F[2 * p - 1], F[2 * p]);
+    d[p] = sub2(F[2 * p - 1], F[2 * p]);
+  }
+  rho = add2(add2(F[0], add2(add2(s[1], s[2]), add2(s[3], s[4]))), add2(add2(add2(s[5], s[6]), add2(s[7], s[8])), s[9]));
+  jx = add2(add2(d[1], add2(d[4], d[5])), add2(d[6], d[7]));
+  jy = add2(add2(d[2], sub2(d[4], d[5])), add2(d[8], d[9]));
+  jz = add2(add2(d[3], sub2(d[6], d[7])), sub2(d[8], d[9]));
+}
+
+__device__ __forceinline__ void mrt_collide2(const float2* F, float2 rho, float2 ux, float2 uy, float2 uz, float2 Ax,
+                                             float2 Ay, float2 Az, const MrtK& K, float2* out) {
+  (void)rho;
+  // Guo term, paired over directions: g_a = P + Q, g_b = P - Q
+  const float2 uA = fma2(uz, Az, fma2(uy, Ay, mul2(ux, Ax)));
+  const float2 eA[10] = {p2(0.f), Ax, Ay, Az, add2(Ax, Ay), sub2(Ax, Ay), add2(Ax, Az), sub2(Ax, Az), add2(Ay, Az),
+                         sub2(Ay, Az)};
+  const float2 eU[10] = {p2(0.f), ux, uy, uz, add2(ux, uy), sub2(ux, uy), add2(ux, uz), sub2(ux, uz), add2(uy, uz),
+                         sub2(uy, uz)};
+  const float2 uA3 = mul2(uA, p2(1.0f / 3.0f));
+  // Fg = F + g (kept), and h = F + g/2 reduced at once to its pair sums / differences
+  float2 Fg[19];
+  float2 sg[10], dl[10];
+  {
+    const float2 g0 = mul2(p2(-1.0f / 9.0f), uA);
+    Fg[0] = add2(F[0], g0);
+  }
+  const float2 h0 = fma2(p2(-1.0f / 18.0f), uA, F[0]);
+#pragma unroll
+  for (int p = 1; p <= 9; ++p) {
+    const float w = p <= 3 ? (1.0f / 18.0f) : (1.0f / 36.0f);
+    const float2 P = mul2(p2(w), sub2(mul2(mul2(eU[p], eA[p]), p2(1.0f / 9.0f)), uA3));
+    const float2 Q = mul2(p2(w * (1.0f / 3.0f)), eA[p]);
+    const float2 ga = add2(P, Q), gb = sub2(P, Q);
+    Fg[2 * p - 1] = add2(F[2 * p - 1], ga);
+    Fg[2 * p] = add2(F[2 * p], gb);
+    const float2 ha = fma2(p2(0.5f), ga, F[2 * p - 1]);
+    const float2 hb = fma2(p2(0.5f), gb, F[2 * p]);
+    sg[p] = add2(ha, hb);
+    dl[p] = sub2(ha, hb);
+  }
+  const float2 Sa = add2(add2(sg[1], sg[2]), sg[3]);
+  const float2 Sxy = add2(sg[4], sg[5]), Sxz = add2(sg[6], sg[7]), Syz = add2(sg[8], sg[9]);
+  const float2 Sd = add2(add2(Sxy, Sxz), Syz);
+  const float2 uu = fma2(uz, uz, fma2(uy, uy, mul2(ux, ux)));
+  const float2 r1 = sub2(sub2(Sd, h0), uu);
+  const float2 r2 = add2(fma2(p2(-2.0f), Sa, h0), Sd);
+  const float2 r4 = fma2(p2(-2.0f), dl[1], add2(add2(dl[4], dl[5]), add2(dl[6], dl[7])));
+  const float2 r6 = fma2(p2(-2.0f), dl[2], add2(sub2(dl[4], dl[5]), add2(dl[8], dl[9])));
+  const float2 r8 = fma2(p2(-2.0f), dl[3], add2(sub2(dl[6], dl[7]), sub2(dl[8], dl[9])));
+  const float2 U = sub2(sub2(mul2(p2(2.0f), sg[1]), sg[2]), sg[3]);
+  const float2 T = fma2(p2(-2.0f), Syz, add2(Sxy, Sxz));
+  const float2 r9 = sub2(add2(U, T), sub2(sub2(mul2(p2(2.0f), mul2(ux, ux)), mul2(uy, uy)), mul2(uz, uz)));
+  const float2 r10 = sub2(T, U);
+  const float2 V = sub2(sg[2], sg[3]), Wq = sub2(Sxy, Sxz);
+  const float2 r11 = sub2(add2(V, Wq), sub2(mul2(uy, uy), mul2(uz, uz)));
+  const float2 r12 = sub2(Wq, V);
+  const float2 r13 = sub2(sub2(sg[4], sg[5]), mul2(ux, uy));
+  const float2 r14 = sub2(sub2(sg[8], sg[9]), mul2(uy, uz));
+  const float2 r15 = sub2(sub2(sg[6], sg[7]), mul2(ux, uz));
+  const float2 r16 = sub2(sub2(add2(dl[4], dl[5]), dl[6]), dl[7]);
+  const float2 r17 = add2(add2(sub2(dl[5], dl[4]), dl[8]), dl[9]);
+  const float2 r18 = add2(sub2(sub2(dl[6], dl[7]), dl[8]), dl[9]);
+  // y = K r
+  const float2 y0 = fma2(p2(K.k02), r2, mul2(p2(K.k01), r1));
+  const float2 y1 = fma2(p2(K.k12), r2, mul2(p2(K.k11), r1));
+  const float2 y2 = fma2(p2(K.k22), r2, mul2(p2(K.k21), r1));
+  const float2 y3 = mul2(p2(K.kq0), r4), y4 = mul2(p2(K.kq1), r4);
+  const float2 y5 = mul2(p2(K.kq0), r6), y6 = mul2(p2(K.kq1), r6);
+  const float2 y7 = mul2(p2(K.kq0), r8), y8 = mul2(p2(K.kq1), r8);
+  const float2 y9 = fma2(p2(K.kb), r10, mul2(p2(K.ka), r9)), y10 = fma2(p2(K.ka), r10, mul2(p2(K.kb), r9));
+  const float2 y11 = fma2(p2(K.kd), r12, mul2(p2(K.kc), r11)), y12 = fma2(p2(K.kc), r12, mul2(p2(K.kd), r11));
+  const float2 y13 = mul2(p2(K.ke), r13), y14 = mul2(p2(K.ke), r14), y15 = mul2(p2(K.ke), r15);
+  const float2 y16 = mul2(p2(K.kf), r16), y17 = mul2(p2(K.kf), r17), y18 = mul2(p2(K.kf), r18);
+  // f = F + g - M^T y, paired: f_a = Fg_a - (E + O), f_b = Fg_b - (E - O)
+  const float2 Y012 = add2(add2(y0, y1), y2), B = fma2(p2(-2.0f), y2, y0);
+  const float2 d910 = sub2(y9, y10), s910 = add2(y9, y10), d1112 = sub2(y11, y12), s1112 = add2(y11, y12);
+  const float2 q34 = add2(y3, y4), q56 = add2(y5, y6), q78 = add2(y7, y8);
+  float2 Ev[10], Ov[10];
+  Ev[1] = fma2(p2(2.0f), d910, B);
+  Ov[1] = fma2(p2(-2.0f), y4, y3);
+  Ev[2] = add2(sub2(B, d910), d1112);
+  Ov[2] = fma2(p2(-2.0f), y6, y5);
+  Ev[3] = sub2(sub2(B, d910), d1112);
+  Ov[3] = fma2(p2(-2.0f), y8, y7);
+  const float2 P45 = add2(add2(Y012, s910), s1112), P67 = sub2(add2(Y012, s910), s1112);
+  const float2 P89 = fma2(p2(-2.0f), s910, Y012);
+  Ev[4] = add2(P45, y13);
+  Ov[4] = sub2(add2(add2(q34, q56), y16), y17);
+  Ev[5] = sub2(P45, y13);
+  Ov[5] = add2(add2(sub2(q34, q56), y16), y17);
+  Ev[6] = add2(P67, y15);
+  Ov[6] = add2(sub2(add2(q34, q78), y16), y18);
+  Ev[7] = sub2(P67, y15);
+  Ov[7] = sub2(sub2(sub2(q34, q78), y16), y18);
+  Ev[8] = add2(P89, y14);
+  Ov[8] = sub2(add2(add2(q56, q78), y17), y18);
+  Ev[9] = sub2(P89, y14);
+  Ov[9] = add2(add2(sub2(q56, q78), y17), y18);
+  out[0] = sub2(Fg[0], add2(sub2(y0, y1), y2));
+#pragma unroll
+  for (int p = 1; p <= 9; ++p) {
+    out[2 * p - 1] = sub2(Fg[2 * p - 1], add2(Ev[p], Ov[p]));
+    out[2 * p] = sub2(Fg[2 * p], sub2(Ev[p], Ov[p]));
+  }
+}
+
+}  // namespace fsi
+#endif

@@ -626,6 +626,430 @@ __global__ void __launch_bounds__(256, MINB) k_lbm_step(const Case c) {
   lbm_step_tile<ODD, H, MOVING, BCW, PEN>(c, blockIdx.x, blockIdx.y, acc);
 }
 
+// ------------------------------------------- paired step (2 cells/thread) ----
+// The same step as lbm_step_tile for the two adjacent cells (x0, x0 + 1) of
+// each thread (x0 even; nx even, so that the pair is 8-byte aligned): a warp
+// covers 64 cells of a row, a tile 64 x 4 cells.  Populations of a pair move
+// as float2 / half2 where the AA layout keeps them adjacent (every direction
+// on even steps; directions without an x component on odd steps), and the
+// collision runs on the paired FP32 pipe (mrt_collide2).  Cells next to a
+// solid, penalty forces and open boundaries take the per-cell paths of the
+// one-cell kernel.
+template <bool H>
+struct Pop2;
+
+template <>
+struct Pop2<false> {
+  static __device__ __forceinline__ float2 ld(const Case& c, int s, int64_t cell) {
+    return __ldg(reinterpret_cast<const float2*>(static_cast<const float*>(c.s.pop) + pop_index(c, s, cell)));
+  }
+  static __device__ __forceinline__ void st(const Case& c, int s, int64_t cell, float2 v) {
+    *reinterpret_cast<float2*>(static_cast<float*>(c.s.pop) + pop_index(c, s, cell)) = v;
+  }
+};
+
+template <>
+struct Pop2<true> {
+  static __device__ __forceinline__ float2 ld(const Case& c, int s, int64_t cell) {
+    const __half2 h = *reinterpret_cast<const __half2*>(static_cast<const __half*>(c.s.pop) + pop_index(c, s, cell));
+    const float2 f = __half22float2(h);
+    const float w = lattice_w(s);
+    return make_float2(w * (c.p.rho0 + f.x), w * (c.p.rho0 + f.y));
+  }
+  static __device__ __forceinline__ void st(const Case& c, int s, int64_t cell, float2 v) {
+    const float inv_w = s == 0 ? 3.0f : (s <= 6 ? 18.0f : 36.0f);
+    *reinterpret_cast<__half2*>(static_cast<__half*>(c.s.pop) + pop_index(c, s, cell)) =
+        __floats2half2_rn(v.x * inv_w - c.p.rho0, v.y * inv_w - c.p.rho0);
+  }
+};
+
+__device__ __forceinline__ float comp(const float2& v, int i) { return i ? v.y : v.x; }
+__device__ __forceinline__ void set_comp(float2& v, int i, float a) {
+  if (i)
+    v.y = a;
+  else
+    v.x = a;
+}
+
+// Open boundary of one x face for the warp holding that face cell, pairs
+// layout: face cell, first and second neighbour by (lane, component).
+template <int SIDE>
+__device__ __forceinline__ void bc_face_warp2(const Case& c, int lane, int row, uint8_t fl0, uint8_t fl1,
+                                              float2* F) {
+  const int nx = c.s.nx;
+  const unsigned sb0 = __ballot_sync(kFull, (fl0 & kSolid) != 0), sb1 = __ballot_sync(kFull, (fl1 & kSolid) != 0);
+  const int lr = ((nx - 1) & 63) >> 1;  // lane of x = nx - 1 (component 1) and x = nx - 2 (component 0)
+  const int lf = SIDE == 0 ? 0 : lr, cf = SIDE == 0 ? 0 : 1;
+  const int l1 = SIDE == 0 ? 0 : lr, c1 = SIDE == 0 ? 1 : 0;
+  const int l2 = SIDE == 0 ? 1 : lr - 1, c2 = SIDE == 0 ? 0 : 1;
+  const bool face_solid = ((cf ? sb1 : sb0) >> lf) & 1u;
+  if (face_solid) return;
+  const bool n1_solid = ((c1 ? sb1 : sb0) >> l1) & 1u;
+  const bool n2_fluid = n1_solid ? true : !(((c2 ? sb1 : sb0) >> l2) & 1u);
+  const int src1 = n1_solid ? lf : l1, cs1 = n1_solid ? cf : c1;
+  const int src2 = n1_solid ? lf : l2, cs2 = n1_solid ? cf : c2;
+  float Fn = 0.f, Fn2 = 0.f;
+#pragma unroll
+  for (int q = 0; q < 5; ++q) {
+    const int s = SIDE == 0 ? kUnknownL(q) : kUnknownR(q);
+    const float a = __shfl_sync(kFull, comp(F[s], cs1), src1);
+    const float b = __shfl_sync(kFull, comp(F[s], cs2), src2);
+    if (lane == q) {
+      Fn = a;
+      Fn2 = b;
+    }
+  }
+  float mac_n[4], mac_l[4];
+  load_plane(c, SIDE == 0 ? (n1_solid ? 0 : 1) : (n1_solid ? 3 : 2), row, mac_n);
+  load_plane(c, SIDE == 0 ? (n1_solid ? 1 : 0) : 2, row, mac_l);
+  const FaceVal r = face_population(c.p, c.s.vel_left_dyn, SIDE, lane, Fn, Fn2, n2_fluid, mac_n, mac_l);
+  if (c.p.ob_semantics == FSI_OB_EQUILIBRIUM_RESET) {
+#pragma unroll
+    for (int s = 0; s < 19; ++s) {
+      const float v = __shfl_sync(kFull, r.val, s);
+      if (lane == lf) set_comp(F[s], cf, v);
+    }
+  } else {
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+      const float v = __shfl_sync(kFull, r.val, q);
+      if (lane == lf) set_comp(F[SIDE == 0 ? kUnknownL(q) : kUnknownR(q)], cf, v);
+    }
+    if (c.p.limiter) {
+      const int cnt[5] = {r.packed & 63, (r.packed >> 6) & 63, (r.packed >> 12) & 63, (r.packed >> 18) & 63,
+                          (r.packed >> 24) & 63};
+      flush_counts(c, cnt);
+    }
+  }
+}
+
+// post-streaming populations of one fluid cell next to a solid (per-cell path)
+template <bool ODD, bool H>
+__device__ __forceinline__ void load_near_solid(const Case& c, const Nbh& n, int cell, uint32_t nb, float2* F, int ci) {
+  set_comp(F[0], ci, ldp<H>(c, 0, cell));
+#pragma unroll
+  for (int s = 1; s < 19; ++s) {
+    float v;
+    if (!ODD)
+      v = ldp<H>(c, s, cell);
+    else if ((nb >> kOpp(s)) & 1u)
+      v = ldp<H>(c, s, cell);
+    else
+      v = ldp<H>(c, kOpp(s), n.at(-kEx(s), -kEy(s), -kEz(s)));
+    set_comp(F[s], ci, v);
+  }
+}
+
+// penalty force of one cell (coupling/penalty.py:59-88); returns whether active
+__device__ __forceinline__ bool penalty_cell(const Case& c, int cell, bool fluid, float rho, float ux, float uy,
+                                             float uz, float& f0, float& f1, float& f2) {
+  const int64_t P = c.s.pitch;
+  f0 = f1 = f2 = 0.f;
+  if (!fluid) return false;
+  const float phi = c.s.phi[cell];
+  if (!(phi > c.p.penalty_phi_min)) return false;
+  const float sc = c.p.penalty_beta * phi * rho;
+  f0 = sc * (c.s.svel[cell] - ux);
+  f1 = sc * (c.s.svel[P + cell] - uy);
+  f2 = sc * (c.s.svel[2 * P + cell] - uz);
+  const float nrm = sqrtf(f0 * f0 + f1 * f1 + f2 * f2);
+  if (nrm > c.p.penalty_cap) {
+    const float r = c.p.penalty_cap / nrm;
+    f0 *= r;
+    f1 *= r;
+    f2 *= r;
+  }
+  return true;
+}
+
+template <bool ODD, bool H, bool MOVING, bool BCW, bool PEN>
+__device__ __forceinline__ void lbm_step_tile2(const Case& c, int bx, int by, DirAcc& acc) {
+  const int lane = threadIdx.x;
+  const int nx = c.s.nx, ny = c.s.ny, nz = c.s.nz;
+  const int x0 = bx * 64 + 2 * lane;
+  const int row = by * 4 + threadIdx.y;
+  const bool inrow = row < ny * nz;
+  const bool valid = inrow && x0 < nx;  // nx even: x0 + 1 < nx as well
+  const int j = inrow ? row % ny : 0, k = inrow ? row / ny : 0;
+  const int cell0 = row * nx + x0;
+  const int64_t P = c.s.pitch;
+  const bool dirstats = MOVING && (c.c.mode & FSI_MODE_DIRSTATS);
+  if (dirstats) {
+    const int tid = threadIdx.y * 32 + lane;
+    for (int i = tid; i < 19; i += 128) {
+      acc.cnt[i] = 0;
+      acc.csum[i] = 0.f;
+      acc.cmax[i] = 0.f;
+      acc.imp[i][0] = acc.imp[i][1] = acc.imp[i][2] = 0.f;
+    }
+    if (tid == 0) acc.any = 0;
+    __syncthreads();
+  }
+  uint8_t fl[2];
+  if (valid) {
+    const uint16_t f2 = *reinterpret_cast<const uint16_t*>(c.s.flags + cell0);
+    fl[0] = (uint8_t)(f2 & 0xff);
+    fl[1] = (uint8_t)(f2 >> 8);
+  } else {
+    fl[0] = fl[1] = kSolid;
+  }
+  const bool fluid0 = !(fl[0] & kSolid), fluid1 = !(fl[1] & kSolid);
+  const uint32_t nb0 = (fluid0 && (fl[0] & kNear)) ? c.s.nbr[cell0] : 0u;
+  const uint32_t nb1 = (fluid1 && (fl[1] & kNear)) ? c.s.nbr[cell0 + 1] : 0u;
+  const bool plain = (nb0 | nb1) == 0u;
+  Nbh n0, n1;
+  if (ODD || !plain) {
+    make_nbh(c, valid ? x0 : 0, j, k, n0);
+    n1 = n0;
+    n1.x = valid ? x0 + 1 : 0;
+    n1.xm = valid ? x0 : 0;
+    n1.xp = (valid && x0 + 2 < nx) ? x0 + 2 : 0;
+  }
+
+  // ---- post-streaming populations (AA layout, fluid.py:431-440)
+  float2 F[19];
+  if (fluid0 || fluid1) {
+    if (plain) {
+      if (!ODD) {
+#pragma unroll
+        for (int s = 0; s < 19; ++s) F[s] = Pop2<H>::ld(c, s, cell0);
+      } else {
+        F[0] = Pop2<H>::ld(c, 0, cell0);
+#pragma unroll
+        for (int s = 1; s < 19; ++s) {
+          if (kEx(s) == 0) {
+            F[s] = Pop2<H>::ld(c, kOpp(s), n0.at(0, -kEy(s), -kEz(s)));
+          } else {
+            F[s].x = ldp<H>(c, kOpp(s), n0.at(-kEx(s), -kEy(s), -kEz(s)));
+            F[s].y = ldp<H>(c, kOpp(s), n1.at(-kEx(s), -kEy(s), -kEz(s)));
+          }
+        }
+      }
+    } else {
+#pragma unroll
+      for (int s = 0; s < 19; ++s) F[s] = make_float2(0.f, 0.f);
+      if (fluid0) load_near_solid<ODD, H>(c, n0, cell0, nb0, F, 0);
+      if (fluid1) load_near_solid<ODD, H>(c, n1, cell0 + 1, nb1, F, 1);
+    }
+  } else {
+#pragma unroll
+    for (int s = 0; s < 19; ++s) F[s] = make_float2(0.f, 0.f);
+  }
+
+  // ---- pending open boundary of the previous step (fluid.py:538-569)
+  if (BCW && c.c.bc_pending && inrow) {
+    if (c.p.bc_left != 0 && bx == 0) bc_face_warp2<0>(c, lane, row, fl[0], fl[1], F);
+    if (c.p.bc_right != 0 && bx == ((nx - 1) >> 6)) bc_face_warp2<1>(c, lane, row, fl[0], fl[1], F);
+  }
+
+  // ---- macroscopic state the collision uses (streaming3, fluid.py:1794-1814)
+  float2 cf0 = p2(0.f), cf1 = p2(0.f), cf2 = p2(0.f);
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+    if ((i ? fluid1 : fluid0) && (fl[i] & kCF)) {
+      set_comp(cf0, i, c.s.cell_force[cell0 + i]);
+      set_comp(cf1, i, c.s.cell_force[P + cell0 + i]);
+      set_comp(cf2, i, c.s.cell_force[2 * P + cell0 + i]);
+    }
+  }
+  float2 rho, ux, uy, uz;
+  {
+    float2 jx, jy, jz;
+    moments0_2(F, rho, jx, jy, jz);
+    const float2 inv = make_float2(__frcp_rn(rho.x), __frcp_rn(rho.y));
+    ux = mul2(fma2(p2(0.5f), add2(p2(c.p.force[0]), cf0), jx), inv);
+    uy = mul2(fma2(p2(0.5f), add2(p2(c.p.force[1]), cf1), jy), inv);
+    uz = mul2(fma2(p2(0.5f), add2(p2(c.p.force[2]), cf2), jz), inv);
+  }
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+    const bool fi = i ? fluid1 : fluid0;
+    if (valid && (fl[i] & kOverride)) {
+      set_comp(rho, i, c.s.rho[cell0 + i]);
+      set_comp(ux, i, c.s.vel[cell0 + i]);
+      set_comp(uy, i, c.s.vel[P + cell0 + i]);
+      set_comp(uz, i, c.s.vel[2 * P + cell0 + i]);
+    } else if (!fi) {
+      set_comp(rho, i, c.p.rho0);
+      set_comp(ux, i, 0.f);
+      set_comp(uy, i, 0.f);
+      set_comp(uz, i, 0.f);
+    }
+  }
+  if (BCW) {
+    __syncwarp();
+    if (valid) {
+      const int64_t m = (int64_t)ny * nz;
+      const int pl0 = x0 == 0 ? 0 : (x0 == nx - 2 ? 2 : -1);
+      const int pl1 = x0 + 1 == 1 ? 1 : (x0 + 1 == nx - 1 ? 3 : -1);
+      if (pl0 >= 0) {
+        float* pp = c.s.plane + (int64_t)pl0 * 4 * m;
+        pp[row] = rho.x;
+        pp[m + row] = ux.x;
+        pp[2 * m + row] = uy.x;
+        pp[3 * m + row] = uz.x;
+      }
+      if (pl1 >= 0) {
+        float* pp = c.s.plane + (int64_t)pl1 * 4 * m;
+        pp[row] = rho.y;
+        pp[m + row] = ux.y;
+        pp[2 * m + row] = uy.y;
+        pp[3 * m + row] = uz.y;
+      }
+    }
+  }
+
+  // ---- penalty force built from this state (coupling/penalty.py:59-88)
+  float2 Ax = add2(p2(c.p.force[0]), cf0), Ay = add2(p2(c.p.force[1]), cf1), Az = add2(p2(c.p.force[2]), cf2);
+  uint8_t nfl[2] = {(uint8_t)(fl[0] & (uint8_t)~kOverride), (uint8_t)(fl[1] & (uint8_t)~kOverride)};
+  if (PEN) {
+    int na = 0;
+    float mx = 0.f, s0 = 0.f, s1 = 0.f, s2 = 0.f;
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const int cell = cell0 + i;
+      float f0, f1, f2;
+      const bool active = penalty_cell(c, cell, i ? fluid1 : fluid0, comp(rho, i), comp(ux, i), comp(uy, i),
+                                       comp(uz, i), f0, f1, f2);
+      if (active || (valid && (fl[i] & kCF))) {
+        c.s.cell_force[cell] = f0;
+        c.s.cell_force[P + cell] = f1;
+        c.s.cell_force[2 * P + cell] = f2;
+        c.s.hydro[cell] = -f0;
+        c.s.hydro[P + cell] = -f1;
+        c.s.hydro[2 * P + cell] = -f2;
+      }
+      nfl[i] = active ? (nfl[i] | kCF) : (nfl[i] & (uint8_t)~kCF);
+      set_comp(Ax, i, c.p.force[0] + f0);
+      set_comp(Ay, i, c.p.force[1] + f1);
+      set_comp(Az, i, c.p.force[2] + f2);
+      if (active) {
+        ++na;
+        mx = fmaxf(mx, sqrtf(f0 * f0 + f1 * f1 + f2 * f2));
+        s0 += f0;
+        s1 += f1;
+        s2 += f2;
+      }
+    }
+    if (__any_sync(kFull, na > 0)) {
+      const int nat = (int)__reduce_add_sync(kFull, (unsigned)na);
+      const float wmx = warp_max(mx);
+      const float w0 = warp_sum(s0), w1 = warp_sum(s1), w2 = warp_sum(s2);
+      if (lane == 0) {
+        atomicAdd(&c.s.diag->penalty_active, nat);
+        atomic_max_nonneg(&c.s.diag->penalty_max_norm, wmx);
+        atomicAdd(&c.s.diag->penalty_net[0], w0);
+        atomicAdd(&c.s.diag->penalty_net[1], w1);
+        atomicAdd(&c.s.diag->penalty_net[2], w2);
+      }
+    }
+  }
+  if (valid && (nfl[0] != fl[0] || nfl[1] != fl[1]))
+    *reinterpret_cast<uint16_t*>(c.s.flags + cell0) = (uint16_t)(nfl[0] | (nfl[1] << 8));
+
+  // ---- collision (fluid.py:398-413) and AA streaming
+  if (fluid0 || fluid1) {
+    mrt_collide2(F, rho, ux, uy, uz, Ax, Ay, Az, c.K, F);
+    if (plain) {
+      // a solid member of the pair keeps its slots: write the fluid member alone
+      const bool both = fluid0 && fluid1;
+      if (!ODD) {
+#pragma unroll
+        for (int s = 0; s < 19; ++s) {
+          if (both) {
+            Pop2<H>::st(c, kOpp(s), cell0, F[s]);
+          } else {
+            if (fluid0) stp<H>(c, kOpp(s), cell0, F[s].x);
+            if (fluid1) stp<H>(c, kOpp(s), cell0 + 1, F[s].y);
+          }
+        }
+      } else {
+        if (both) {
+          Pop2<H>::st(c, 0, cell0, F[0]);
+        } else {
+          if (fluid0) stp<H>(c, 0, cell0, F[0].x);
+          if (fluid1) stp<H>(c, 0, cell0 + 1, F[0].y);
+        }
+#pragma unroll
+        for (int s = 1; s < 19; ++s) {
+          if (both && kEx(s) == 0) {
+            Pop2<H>::st(c, s, n0.at(0, kEy(s), kEz(s)), F[s]);
+          } else {
+            if (fluid0) stp<H>(c, s, n0.at(kEx(s), kEy(s), kEz(s)), F[s].x);
+            if (fluid1) stp<H>(c, s, n1.at(kEx(s), kEy(s), kEz(s)), F[s].y);
+          }
+        }
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        if (!(i ? fluid1 : fluid0)) continue;
+        float out[19];
+#pragma unroll
+        for (int s = 0; s < 19; ++s) out[s] = comp(F[s], i);
+        const uint32_t nb = i ? nb1 : nb0;
+        const Nbh& n = i ? n1 : n0;
+        const int cell = cell0 + i;
+        if (nb) {
+          store_near_solid<ODD, H, MOVING>(c, n, cell, nb, comp(rho, i), out, dirstats, &acc);
+        } else if (!ODD) {
+#pragma unroll
+          for (int s = 0; s < 19; ++s) stp<H>(c, kOpp(s), cell, out[s]);
+        } else {
+          stp<H>(c, 0, cell, out[0]);
+#pragma unroll
+          for (int s = 1; s < 19; ++s) stp<H>(c, s, n.at(kEx(s), kEy(s), kEz(s)), out[s]);
+        }
+      }
+    }
+  }
+  if (MOVING && valid) {
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      if ((i ? fluid1 : fluid0) || !(fl[i] & kLink)) continue;
+      // solid cell receiving link forces: recycle last step's ping-pong slot
+      const int cell = cell0 + i;
+      float* prev = c.s.hpp + (int64_t)(c.c.pp ^ 1) * 3 * P;
+      if (c.c.mode & FSI_MODE_SUBCYCLED) {
+        float a[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          a[d] = c.s.accum[d * P + cell] + prev[d * P + cell];
+          c.s.accum[d * P + cell] = a[d];
+          prev[d * P + cell] = 0.f;
+        }
+        atomic_max_nonneg(&c.s.diag->accum_norm_max, sqrtf(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]));
+      } else {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) prev[d * P + cell] = 0.f;
+      }
+    }
+  }
+
+  if (dirstats) {
+    __syncthreads();
+    if (acc.any) {
+      const int tid = threadIdx.y * 32 + lane;
+      for (int i = tid; i < 19; i += 128) {
+        if (acc.cnt[i]) {
+          atomicAdd(&c.s.diag->link_count[i], acc.cnt[i]);
+          atomicAdd(&c.s.diag->corr_abs_sum[i], acc.csum[i]);
+          atomic_max_nonneg(&c.s.diag->corr_abs_max[i], acc.cmax[i]);
+          atomicAdd(&c.s.diag->fluid_impulse[i][0], acc.imp[i][0]);
+          atomicAdd(&c.s.diag->fluid_impulse[i][1], acc.imp[i][1]);
+          atomicAdd(&c.s.diag->fluid_impulse[i][2], acc.imp[i][2]);
+        }
+      }
+    }
+  }
+}
+
+template <bool ODD, bool H, bool MOVING, bool BCW, bool PEN>
+__global__ void __launch_bounds__(128, 4) k_lbm_step2(const Case c) {
+  __shared__ DirAcc acc;
+  lbm_step_tile2<ODD, H, MOVING, BCW, PEN>(c, blockIdx.x, blockIdx.y, acc);
+}
+
 // ------------------------------------------------- init / neighbours ----
 __global__ void k_init(const Case c) {
   const int64_t n = (int64_t)c.s.nx * c.s.ny * c.s.nz;
@@ -1011,11 +1435,20 @@ static int check_state(const FsiLbmState* s, const FsiLbmParams* p) {
   if (s->pitch < (int64_t)s->nx * s->ny * s->nz || (s->pitch % 32) != 0)
     return invalid("pitch must cover nx*ny*nz and be a multiple of 32");
   if (19 * s->pitch > (int64_t)UINT32_MAX) return invalid("lattice too large: 19 * pitch must be below 2^32");
-  if (p->tune != FSI_TUNE_LBM_OCC3 && p->tune != FSI_TUNE_LBM_OCC4) return invalid("unknown FsiLbmParams.tune");
+  if (p->tune != FSI_TUNE_LBM_OCC3 && p->tune != FSI_TUNE_LBM_OCC4 && p->tune != FSI_TUNE_LBM_PAIR)
+    return invalid("unknown FsiLbmParams.tune");
   if ((p->bc_left || p->bc_right) && (s->nx < 4 || (s->nx % 32 == 1) || (s->nx % 32 == 2)))
     return invalid("x open boundaries need nx >= 4 and nx % 32 not in {1, 2}");
   if (!s->pop || !s->flags || !s->nbr || !s->diag) return invalid("null device pointer in FsiLbmState");
   return FSI_OK;
+}
+
+// the paired kernel needs x-adjacent cell pairs aligned (nx even) and, with
+// open boundaries, the three cells next to the x = nx - 1 face in one warp
+static bool pair_ok(const FsiLbmState* s, const FsiLbmParams* p) {
+  if (s->nx % 2) return false;
+  if ((p->bc_left || p->bc_right) && (s->nx % 64 == 2 || s->nx < 4)) return false;
+  return true;
 }
 
 static Case make_case(const FsiLbmState* s, const FsiLbmParams* p, const FsiStepCtl* ctl) {
@@ -1104,8 +1537,13 @@ extern "C" int fsi_lbm_substep(const FsiLbmState* s, const FsiLbmParams* p, cons
   const bool moving = ctl->mode & FSI_MODE_MOVING_BB, pen = ctl->mode & FSI_MODE_PENALTY;
   const bool bcw = p->bc_left != 0 || p->bc_right != 0;
   if (moving && pen) return invalid("penalty steps use static bounce-back (fluid.py:2099-2103)");
+  const dim3 grid2((unsigned)((s->nx + 63) / 64), (unsigned)((s->ny * s->nz + 3) / 4));
+  const dim3 block2(32, 4);
+  if (p->tune == FSI_TUNE_LBM_PAIR && !pair_ok(s, p)) return invalid("FSI_TUNE_LBM_PAIR needs an even nx (and nx % 64 != 2 with open boundaries)");
 #define FSI_LAUNCH(O, HH, M, B, PN)                                        \
-  if (p->tune == FSI_TUNE_LBM_OCC4)                                        \
+  if (p->tune == FSI_TUNE_LBM_PAIR)                                        \
+    k_lbm_step2<O, HH, M, B, PN><<<grid2, block2, 0, st>>>(c);             \
+  else if (p->tune == FSI_TUNE_LBM_OCC4)                                   \
     k_lbm_step<O, HH, M, B, PN, 4><<<grid, block, 0, st>>>(c);             \
   else                                                                     \
     k_lbm_step<O, HH, M, B, PN, 3><<<grid, block, 0, st>>>(c)
@@ -1369,9 +1807,8 @@ extern "C" int fsi_batch_lbm_substep(FsiBatchCase* cases, const FsiBatchDims* d,
   cudaStream_t st = (cudaStream_t)stream;
   k_batch_ctl<<<d->n_cases, 32, 0, st>>>(cases, kBatchLbmPre);
   if ((rc = launch_check("k_batch_ctl"))) return rc;
-  // tiles of all cases: one CTA per tile up to 3 resident CTAs per SM in total
-  const int cap = std::max(1, 148 * 3 * 4 / std::max(1, d->n_cases));
-  const dim3 grid(batch_x(d->max_lbm_tiles, 1, std::max(cap, 8)), d->n_cases);
+  // one CTA per tile of the largest case; CTAs past a smaller case's tiles exit at once
+  const dim3 grid(batch_x(d->max_lbm_tiles, 1, 1 << 20), d->n_cases);
   if (d->store_fp16)
     k_batch_lbm_step<true><<<grid, dim3(32, 8), 0, st>>>(cases);
   else
@@ -1387,8 +1824,7 @@ extern "C" int fsi_batch_mask_rebuild(FsiBatchCase* cases, const FsiBatchDims* d
   cudaStream_t st = (cudaStream_t)stream;
   k_batch_ctl<<<d->n_cases, 32, 0, st>>>(cases, kBatchMaskPre);
   if ((rc = launch_check("k_batch_ctl"))) return rc;
-  const int cap = std::max(8, 148 * 8 / std::max(1, d->n_cases));
-  k_batch_mask_update<<<dim3(batch_x(d->max_cells, 256, cap), d->n_cases), 256, 0, st>>>(cases);
+  k_batch_mask_update<<<dim3(batch_x(d->max_cells, 256, 1 << 20), d->n_cases), 256, 0, st>>>(cases);
   if ((rc = launch_check("k_batch_mask_update"))) return rc;
   const dim3 g2(std::max(1, 148 * 4 / std::max(1, d->n_cases)), d->n_cases);
   if (d->store_fp16)

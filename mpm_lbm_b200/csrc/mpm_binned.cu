@@ -840,8 +840,7 @@ extern "C" int fsi_batch_mpm_bin(FsiBatchCase* cases, const FsiBatchDims* d, voi
   int rc = check_batch_mpm(cases, d);
   if (rc) return rc;
   cudaStream_t st = (cudaStream_t)stream;
-  const int cap = std::max(4, sm_count() * 8 / d->n_cases);
-  const dim3 g((unsigned)std::min<int64_t>(nblk(d->max_particles, 256), cap), d->n_cases);
+  const dim3 g(nblk(d->max_particles, 256), d->n_cases);
   k_batch_bin_count<<<g, 256, 0, st>>>(cases);
   if ((rc = launch_check("k_batch_bin_count"))) return rc;
   k_batch_bin_scan<<<dim3(1, d->n_cases), 1024, 0, st>>>(cases);
@@ -854,11 +853,12 @@ extern "C" int fsi_batch_mpm_substep(FsiBatchCase* cases, const FsiBatchDims* d,
   int rc = check_batch_mpm(cases, d);
   if (rc) return rc;
   cudaStream_t st = (cudaStream_t)stream;
-  const int cap = std::max(4, sm_count() * 8 / d->n_cases);
-  const dim3 gp((unsigned)std::min<int64_t>(nblk(d->max_particles, 128), cap), d->n_cases);
+  const dim3 gp(nblk(d->max_particles, 128), d->n_cases);
   k_batch_p2g_payload<<<gp, 128, 0, st>>>(cases);
   if ((rc = launch_check("k_batch_p2g_payload"))) return rc;
-  const dim3 gc((unsigned)std::min<int64_t>(d->max_chunks, std::max(2, sm_count() * 4 / d->n_cases)), d->n_cases);
+  // about one CTA per chunk of the largest case (a bin's chunks hold <= 128 particles each; bins
+  // partly filled add chunks): CTAs stride over the case's chunk table
+  const dim3 gc((unsigned)std::min<int64_t>(d->max_chunks, 2 * nblk(d->max_particles, kChunk) + 8), d->n_cases);
   const int tsc = d->mpm_tune & 3, tg = (d->mpm_tune >> 2) & 3;
   if (tsc == FSI_TUNE_MPM_T512)
     k_batch_p2g_scatter<512><<<gc, 512, 0, st>>>(cases);

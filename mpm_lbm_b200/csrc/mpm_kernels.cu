@@ -378,7 +378,8 @@ extern "C" int fsi_batch_project(FsiBatchCase* cases, const FsiBatchDims* d, voi
   if (!cases || !d || d->n_cases <= 0 || d->n_cases > 65535 || d->max_cells <= 0 || d->max_particles <= 0)
     return invalid("bad batch arguments");
   cudaStream_t st = (cudaStream_t)stream;
-  const int64_t cap = std::max(8, 148 * 8 / d->n_cases);
+  // one CTA per 256 cells / 128 particles of the largest case (smaller cases' extra CTAs exit at once)
+  const int64_t cap = 1 << 20;
   const unsigned gc = (unsigned)std::min<int64_t>((d->max_cells + 255) / 256, cap);
   k_batch_project_clear<<<dim3(gc, d->n_cases), 256, 0, st>>>(cases);
   int rc = launch_check("k_batch_project_clear");

@@ -72,6 +72,16 @@ def compare(ora, gpu, what=("F", "rho", "v")):
         np.testing.assert_allclose(gpu.v.to_numpy(), ora.v, **VEL_TOL)
 
 
+# FsiLbmParams.tune: 0 one cell per thread (3 CTAs/SM), 2 two x-adjacent cells
+# per thread on the paired FP32 pipe (nx even)
+TUNES = [0, 2]
+
+
+def use_tune(gpu, tune):
+    gpu.tune = tune
+    gpu._sync_params()
+
+
 def channel_with_obstacle(nx, ny, nz):
     s = np.zeros((nx, ny, nz), np.int8)
     s[:, 0, :] = s[:, -1, :] = 1
@@ -80,12 +90,14 @@ def channel_with_obstacle(nx, ny, nz):
     return s
 
 
+@pytest.mark.parametrize("tune", TUNES)
 @pytest.mark.parametrize("collision", ["mrt", "bgk"])
-def test_static_bounceback_steps_match_oracle(collision):
-    nx, ny, nz = 40, 10, 9  # nx > 32: two warps per row
+def test_static_bounceback_steps_match_oracle(collision, tune):
+    nx, ny, nz = 70, 10, 9  # nx > 64: two warps per row in both layouts
     solid = channel_with_obstacle(nx, ny, nz)
     ora, gpu = make_pair(nx, ny, nz, solid, niu=1.0 / 30.0, relaxation_semantics="standard_lattice_kinematic_viscosity",
                          force=(1e-5, 2e-6, -1e-6), collision=collision)
+    use_tune(gpu, tune)
     for step in range(7):  # odd count: ends on the swapped AA layout
         ora.step()
         gpu.step()
@@ -93,10 +105,12 @@ def test_static_bounceback_steps_match_oracle(collision):
             compare(ora, gpu)
 
 
-def test_moving_bounceback_matches_oracle():
-    nx, ny, nz = 33, 8, 7  # nx % 32 == 1 without open boundaries is allowed
+@pytest.mark.parametrize("nx,tune", [(33, 0), (34, 2), (66, 2)])
+def test_moving_bounceback_matches_oracle(nx, tune):
+    ny, nz = 8, 7  # nx % 32 == 1 without open boundaries is allowed
     solid = channel_with_obstacle(nx, ny, nz)
     ora, gpu = make_pair(nx, ny, nz, solid, force=(2e-5, 0.0, 0.0))
+    use_tune(gpu, tune)
     rng = np.random.default_rng(5)
     sv = (0.01 * rng.standard_normal((nx, ny, nz, 3))).astype(np.float32) * solid[..., None]
     ora.solid_vel[...] = sv
@@ -124,9 +138,10 @@ BC_CASES = [
 ]
 
 
+@pytest.mark.parametrize("tune", TUNES)
 @pytest.mark.parametrize("sem,bl,br,lim", BC_CASES)
-@pytest.mark.parametrize("nx", [20, 48])
-def test_open_boundaries_match_oracle(sem, bl, br, lim, nx):
+@pytest.mark.parametrize("nx", [20, 48, 64])
+def test_open_boundaries_match_oracle(sem, bl, br, lim, nx, tune):
     ny, nz = 9, 8
     solid = channel_with_obstacle(nx, ny, nz)
     solid[1, 3, 3] = 1  # neighbour of the inlet face is solid -> ni = face
@@ -135,6 +150,7 @@ def test_open_boundaries_match_oracle(sem, bl, br, lim, nx):
     ora, gpu = make_pair(nx, ny, nz, solid, open_boundary_semantics=sem, bc=(bl, br, 0, 0, 0, 0),
                          rho_bc=(1.01, 0.99, 1, 1, 1, 1), vel_bc=vel, limiter_enabled=lim, ob_u_max=0.035,
                          ob_noneq_cap=0.004, ob_rho_min=0.995, ob_rho_max=1.005, ob_floor=0.0 if lim else None)
+    use_tune(gpu, tune)
     for step in range(6):
         ora.step_moving_bounceback()
         gpu.step_moving_bounceback()
@@ -147,12 +163,14 @@ def test_open_boundaries_match_oracle(sem, bl, br, lim, nx):
             assert go[k] == oo[k], k
 
 
+@pytest.mark.parametrize("tune", TUNES)
 @pytest.mark.parametrize("steps_before", [1, 2])
-def test_dynamic_mask_reinit_matches_oracle(steps_before):
+def test_dynamic_mask_reinit_matches_oracle(steps_before, tune):
     nx, ny, nz = 24, 10, 10
     solid = channel_with_obstacle(nx, ny, nz)
     solid[nx // 2 - 1: nx // 2 + 1, ny // 2 - 1: ny // 2 + 2, nz // 2 - 1: nz // 2 + 1] = 0
     ora, gpu = make_pair(nx, ny, nz, solid, force=(1e-5, 0, 0))
+    use_tune(gpu, tune)
     rng = np.random.default_rng(11)
     sv = (0.01 * rng.standard_normal((nx, ny, nz, 3))).astype(np.float32)
     for phase in range(4):
@@ -178,10 +196,12 @@ def test_dynamic_mask_reinit_matches_oracle(steps_before):
         np.testing.assert_allclose(gpu.hydro_force.to_numpy(), ora.hydro_force, rtol=1e-4, atol=1e-7)
 
 
-def test_subcycled_accumulator_matches_oracle():
+@pytest.mark.parametrize("tune", TUNES)
+def test_subcycled_accumulator_matches_oracle(tune):
     nx, ny, nz = 16, 8, 8
     solid = channel_with_obstacle(nx, ny, nz)
     ora, gpu = make_pair(nx, ny, nz, solid, force=(3e-5, 0, 0))
+    use_tune(gpu, tune)
     for o in (ora, gpu):
         o.clear_moving_boundary_force_accumulator()
     for _ in range(3):
@@ -217,10 +237,12 @@ def test_step115_accumulator_known_answer_gpu():
     assert abs(st["mb_subcycle_force_mean_norm_max"] - 2.0) <= 1e-6
 
 
-def test_penalty_step_matches_oracle():
+@pytest.mark.parametrize("tune", TUNES)
+def test_penalty_step_matches_oracle(tune):
     nx, ny, nz = 16, 10, 9
     solid = channel_with_obstacle(nx, ny, nz)
     ora, gpu = make_pair(nx, ny, nz, solid, force=(1e-5, 0, 0))
+    use_tune(gpu, tune)
     rng = np.random.default_rng(3)
     cpl = orc.OracleCoupling(nx, 1.0 / nx, 4e-3, beta_lbm=0.05, penalty_force_cap=2e-4)
     for step in range(4):

@@ -44,12 +44,14 @@ def fp64_reference():
             "x": drv.solid.x.astype(np.float64), "rho": drv.lbm.rho.astype(np.float64)}
 
 
+@pytest.mark.parametrize("tune", [0, 2])
 @pytest.mark.parametrize("storage", ["fp32", "fp16"])
-def test_storage_form_against_fp64_oracle(storage, fp64_reference):
+def test_storage_form_against_fp64_oracle(storage, tune, fp64_reference):
     import torch
 
     case = _case()
     drv = case.make_driver(storage=storage)
+    drv.lbm.tune = tune  # 0: one cell per thread, 2: two cells per thread (paired FP32)
     for _ in range(FSI_STEPS):
         drv.step_once()
     torch.cuda.synchronize()
@@ -61,7 +63,7 @@ def test_storage_form_against_fp64_oracle(storage, fp64_reference):
     tip_err = np.linalg.norm(tip - ref["tip"]) / np.linalg.norm(ref["tip"])
     rho = drv.lbm.rho.to_numpy().astype(np.float64)
     rho_err = np.abs(rho[fluid] - ref["rho"][fluid]).max()
-    print(f"{storage}: velocity rel L2 {v_err:.3e}, flap-tip displacement rel {tip_err:.3e}, "
+    print(f"{storage} tune {tune}: velocity rel L2 {v_err:.3e}, flap-tip displacement rel {tip_err:.3e}, "
           f"max |rho - rho64| {rho_err:.3e}, tip {tip * case.nx} cells")
     v_tol, tip_tol = TARGETS[storage]
     assert v_err <= v_tol
