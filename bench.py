@@ -265,6 +265,8 @@ def main():
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="default launch variants")
+    ap.add_argument("--lbm-tune", type=int, default=None, help="fixed FsiLbmParams.tune (no autotuning)")
+    ap.add_argument("--mpm-tune", type=int, default=None, help="fixed FsiMpmParams.tune (no autotuning)")
     ap.add_argument("--ref-substeps", type=int, default=30,
                     help="LBM substeps per timed step of the reference arm (bounded CPU sample)")
     args = ap.parse_args()
@@ -285,7 +287,19 @@ def main():
         drv.step_once()
     torch.cuda.synchronize()
     tuning = None
-    if not args.no_autotune:
+    if args.lbm_tune is not None or args.mpm_tune is not None:
+        # fixed launch variants (profiling a given variant); the step graph is recaptured
+        drv._graph = None
+        if args.lbm_tune is not None:
+            drv.lbm.tune = args.lbm_tune
+        if args.mpm_tune is not None:
+            drv.solid.params.tune = args.mpm_tune
+        tuning = {"lbm": {"choice": drv.lbm.tune, "ms_per_substep": None},
+                  "mpm": {"choice": drv.solid.params.tune, "ms_per_substep": None}}
+        for _ in range(2):
+            drv.step_once()
+        torch.cuda.synchronize()
+    elif not args.no_autotune:
         tuning = drv.autotune()  # launch variants timed on this state; the step graph is recaptured
         for _ in range(2):
             drv.step_once()

@@ -218,17 +218,19 @@ typedef struct FsiMpmParams {
   float damping;     /* >0 enables particle_velocity_post_g2p damping */
   int32_t bound;
   int32_t lock_z;
-  int32_t tune;      /* FSI_TUNE_MPM_* of the scatter | FSI_TUNE_MPM_* of the gather << 2 */
+  int32_t tune;      /* FSI_TUNE_P2G_* of the scatter | FSI_TUNE_MPM_* of the gather << 2 */
 } FsiMpmParams;
 
 /* launch variants of fsi_mpm_substep_binned (FsiMpmParams.tune = scatter
- * variant | gather variant << 2); the other MPM entry points ignore it.
- * Scatter: threads per chunk CTA of the P2G scatter.  Gather: threads per
- * chunk CTA of the G2P, with 1, 2 or 4 lanes per particle. */
+ * variant | gather variant << 2); the other MPM entry points ignore it. */
 enum {
-  FSI_TUNE_MPM_T128 = 0,  /* 128 threads per chunk CTA (default) */
-  FSI_TUNE_MPM_T256 = 1,  /* 256 threads */
-  FSI_TUNE_MPM_T512 = 2,  /* 512 threads */
+  /* P2G scatter: lanes per particle of a chunk CTA */
+  FSI_TUNE_P2G_T128 = 0,  /* 128 threads: one lane per particle, all 27 nodes (default) */
+  FSI_TUNE_P2G_T384 = 1,  /* 384 threads: three lanes per particle, one stencil plane each */
+  /* G2P gather: threads per chunk CTA */
+  FSI_TUNE_MPM_T128 = 0,  /* 128 threads: one lane per particle (default) */
+  FSI_TUNE_MPM_T256 = 1,  /* 256 threads: two lanes per particle */
+  FSI_TUNE_MPM_T512 = 2,  /* 512 threads: four lanes per particle */
 };
 
 typedef struct FsiCouplingParams {

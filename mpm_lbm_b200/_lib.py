@@ -19,6 +19,7 @@ FSI_CELL_SOLID, FSI_CELL_NEAR, FSI_CELL_LINK, FSI_CELL_OVERRIDE, FSI_CELL_CF = 1
 FSI_MODE_MOVING_BB, FSI_MODE_SUBCYCLED, FSI_MODE_DIRSTATS, FSI_MODE_PENALTY = 1, 2, 4, 8
 FSI_TUNE_LBM_OCC3, FSI_TUNE_LBM_OCC4, FSI_TUNE_LBM_PAIR = 0, 1, 2
 FSI_TUNE_MPM_T128, FSI_TUNE_MPM_T256, FSI_TUNE_MPM_T512 = 0, 1, 2
+FSI_TUNE_P2G_T128, FSI_TUNE_P2G_T384 = 0, 1
 FSI_MPM_PAYLOAD_ROWS = 32
 
 

@@ -17,7 +17,7 @@ from __future__ import annotations
 import torch
 
 from ._lib import (FSI_TUNE_LBM_OCC3, FSI_TUNE_LBM_OCC4, FSI_TUNE_LBM_PAIR, FSI_TUNE_MPM_T128, FSI_TUNE_MPM_T256,
-                   FSI_TUNE_MPM_T512)
+                   FSI_TUNE_MPM_T512, FSI_TUNE_P2G_T128, FSI_TUNE_P2G_T384)
 
 
 def _time_ms(fn, steps, reps):
@@ -68,7 +68,7 @@ def tune_lbm(lbm, step_fn, candidates=None, steps=10, reps=3):
 
 
 def mpm_tune_value(scatter, gather):
-    """FsiMpmParams.tune for the given FSI_TUNE_MPM_* scatter and gather variants."""
+    """FsiMpmParams.tune for the given FSI_TUNE_P2G_* scatter and FSI_TUNE_MPM_* gather variants."""
     return int(scatter) | (int(gather) << 2)
 
 
@@ -79,7 +79,7 @@ def tune_mpm(solid, substep_fn, extra=(), candidates=None, steps=8, reps=3):
     tensors the substep writes (coupler statistics), restored afterwards.
     Returns {"choice": tune, "ms_per_substep": {tune: ms}}."""
     if candidates is None:
-        candidates = [mpm_tune_value(s, g) for s in (FSI_TUNE_MPM_T128, FSI_TUNE_MPM_T256, FSI_TUNE_MPM_T512)
+        candidates = [mpm_tune_value(s, g) for s in (FSI_TUNE_P2G_T128, FSI_TUNE_P2G_T384)
                       for g in (FSI_TUNE_MPM_T128, FSI_TUNE_MPM_T256, FSI_TUNE_MPM_T512)]
     solid._ensure_binned()
     snap = solid.snapshot(extra)

@@ -378,47 +378,83 @@ __device__ __forceinline__ void p2g_scatter_body(const FsiGrid& g, const FsiMpmP
     const int nv = staged ? bx.vol : 0;
     for (int i = tid; i < 7 * nv; i += T) tile[i] = 0.f;
     __syncthreads();
-    const int npair = ch.y * 27;
-    for (int idx = tid; idx < npair; idx += T) {
-      const int lp = idx / 27, o = idx - lp * 27;
-      const int ox = o / 9, oy = (o / 3) % 3, oz = o % 3;
-      const int I = __float_as_int(sp[kPbase][lp]) + ox, Jj = __float_as_int(sp[kPbase + 1][lp]) + oy,
-                K = __float_as_int(sp[kPbase + 2][lp]) + oz;
-      if (I < 0 || I >= G || Jj < 0 || Jj >= G || K < 0 || K >= G) continue;
-      const float fx[3] = {sp[kPfx][lp], sp[kPfx + 1][lp], sp[kPfx + 2][lp]};
-      // weights of bspline() and offsets as in p2g_node()
-      const float w = sp[kPw + ox][lp] * sp[kPw + 3 + oy][lp] * sp[kPw + 6 + oz][lp];
-      const float dpos[3] = {((float)ox - fx[0]) * mp.dx, ((float)oy - fx[1]) * mp.dx, ((float)oz - fx[2]) * mp.dx};
-      float val[7];
+    // particle-major: lane lp of each group of kChunk threads owns one particle
+    // (its payload in registers); with GL = T / kChunk = 3 lanes per particle,
+    // group `sub` takes the stencil plane ox = sub, otherwise a lane takes all
+    // 27 nodes.  Node order within a lane: ox, oy, oz as in p2g.
+    constexpr int GL = T / kChunk;
+    static_assert(GL == 1 || GL == 3, "scatter CTAs have 128 or 384 threads");
+    const int lp = tid % kChunk, sub = tid / kChunk;
+    if (lp < ch.y) {
+      int base[3];
+      float fx[3], wv[9], mv[3], aff[9], pf[3];
 #pragma unroll
-      for (int a = 0; a < 3; ++a)
-        val[a] = w * (sp[kPmv + a][lp] + (sp[kPaff + 3 * a][lp] * dpos[0] + sp[kPaff + 3 * a + 1][lp] * dpos[1] +
-                                          sp[kPaff + 3 * a + 2][lp] * dpos[2]));
-      val[3] = w * sp[kPmass][lp];
-      int nq = 4;
-      if (REACT) {
-        const float f0 = sp[kPpf][lp], f1 = sp[kPpf + 1][lp], f2 = sp[kPpf + 2][lp];
-        if (f0 != 0.f || f1 != 0.f || f2 != 0.f) {
-          val[4] = w * f0;
-          val[5] = w * f1;
-          val[6] = w * f2;
-          nq = 7;
-          gn[0] += val[4];
-          gn[1] += val[5];
-          gn[2] += val[6];
-          gmax = fmaxf(gmax, sqrtf(val[4] * val[4] + val[5] * val[5] + val[6] * val[6]));
+      for (int q = 0; q < 3; ++q) {
+        base[q] = __float_as_int(sp[kPbase + q][lp]);
+        fx[q] = sp[kPfx + q][lp];
+        mv[q] = sp[kPmv + q][lp];
+        pf[q] = REACT ? sp[kPpf + q][lp] : 0.f;
+      }
+#pragma unroll
+      for (int q = 0; q < 9; ++q) {
+        wv[q] = sp[kPw + q][lp];
+        aff[q] = sp[kPaff + q][lp];
+      }
+      const float mass = sp[kPmass][lp];
+      const bool react = REACT && (pf[0] != 0.f || pf[1] != 0.f || pf[2] != 0.f);
+      const bool inside = base[0] >= 0 && base[1] >= 0 && base[2] >= 0 && base[0] + 2 < G && base[1] + 2 < G &&
+                          base[2] + 2 < G;
+      const float d1[3] = {(0.0f - fx[1]) * mp.dx, (1.0f - fx[1]) * mp.dx, (2.0f - fx[1]) * mp.dx};
+      const float d2[3] = {(0.0f - fx[2]) * mp.dx, (1.0f - fx[2]) * mp.dx, (2.0f - fx[2]) * mp.dx};
+      float gsum[3] = {0.f, 0.f, 0.f}, gm2 = 0.f;
+#pragma unroll
+      for (int oxi = 0; oxi < (GL == 1 ? 3 : 1); ++oxi) {
+        const int ox = GL == 1 ? oxi : sub;
+        const float wx = ox == 0 ? wv[0] : (ox == 1 ? wv[1] : wv[2]);
+        const float d0 = ((float)ox - fx[0]) * mp.dx;
+        const int I = base[0] + ox;
+#pragma unroll
+        for (int oy = 0; oy < 3; ++oy) {
+          const float wxy = wx * wv[3 + oy];
+          const int Jj = base[1] + oy;
+#pragma unroll
+          for (int oz = 0; oz < 3; ++oz) {
+            const int K = base[2] + oz;
+            if (!inside && (I < 0 || I >= G || Jj < 0 || Jj >= G || K < 0 || K >= G)) continue;
+            // weights of bspline() and offsets as in p2g_node()
+            const float w = wxy * wv[6 + oz];
+            float val[7];
+#pragma unroll
+            for (int q = 0; q < 3; ++q)
+              val[q] = w * (mv[q] + (aff[3 * q] * d0 + aff[3 * q + 1] * d1[oy] + aff[3 * q + 2] * d2[oz]));
+            val[3] = w * mass;
+            if (react) {
+#pragma unroll
+              for (int q = 0; q < 3; ++q) {
+                val[4 + q] = w * pf[q];
+                gsum[q] += val[4 + q];
+              }
+              gm2 = fmaxf(gm2, val[4] * val[4] + val[5] * val[5] + val[6] * val[6]);
+            }
+            const int nq = react ? 7 : 4;
+            if (staged) {
+              const int li = ((K - bx.lo[2]) * bx.ext[1] + (Jj - bx.lo[1])) * bx.ext[0] + (I - bx.lo[0]);
+#pragma unroll
+              for (int q = 0; q < 7; ++q)
+                if (q < nq) atomicAdd(&tile[q * nv + li], val[q]);
+            } else {
+              const int64_t node = ((int64_t)K * G + Jj) * G + I;
+#pragma unroll
+              for (int q = 0; q < 7; ++q)
+                if (q < nq) atomicAdd(dst[q] + node, val[q]);
+            }
+          }
         }
       }
-      if (staged) {
-        const int li = ((K - bx.lo[2]) * bx.ext[1] + (Jj - bx.lo[1])) * bx.ext[0] + (I - bx.lo[0]);
+      if (react) {
 #pragma unroll
-        for (int q = 0; q < 7; ++q)
-          if (q < nq) atomicAdd(&tile[q * nv + li], val[q]);
-      } else {
-        const int64_t node = ((int64_t)K * G + Jj) * G + I;
-#pragma unroll
-        for (int q = 0; q < 7; ++q)
-          if (q < nq) atomicAdd(dst[q] + node, val[q]);
+        for (int q = 0; q < 3; ++q) gn[q] += (double)gsum[q];
+        gmax = fmaxf(gmax, sqrtf(gm2));
       }
     }
     __syncthreads();
@@ -444,8 +480,10 @@ __device__ __forceinline__ void p2g_scatter_body(const FsiGrid& g, const FsiMpmP
   }
 }
 
+// register budget: 128-thread CTAs keep 4 per SM, 384-thread CTAs 1 (the
+// payload of a particle stays in registers across its nodes)
 template <bool REACT, int T>
-__global__ __launch_bounds__(T) void k_p2g_scatter(FsiGrid g, FsiMpmParams mp, const float* __restrict__ payload,
+__global__ __launch_bounds__(T, T == 384 ? 1 : 4) void k_p2g_scatter(FsiGrid g, FsiMpmParams mp, const float* __restrict__ payload,
                                                    int n, const int2* __restrict__ chunks, int32_t* meta,
                                                    int32_t* box, int buf, FsiCouplingStats* st) {
   p2g_scatter_body<REACT, T>(g, mp, payload, n, chunks, meta, box, buf, st, blockIdx.x, gridDim.x);
@@ -690,7 +728,7 @@ extern "C" int fsi_mpm_substep_binned(const FsiParticles* pt, const FsiGrid grid
   if ((rc = check_grid(&grid[0])) || (rc = check_grid(&grid[1]))) return rc;
   if (grid[0].n != grid[1].n) return invalid("the two grid buffers differ in size");
   if (buffer != 0 && buffer != 1) return invalid("buffer must be 0 or 1");
-  if (mp->tune < 0 || mp->tune > 15 || (mp->tune & 3) == 3 || ((mp->tune >> 2) & 3) == 3)
+  if (mp->tune < 0 || mp->tune > 15 || (mp->tune & 3) > 1 || ((mp->tune >> 2) & 3) == 3)
     return invalid("unknown FsiMpmParams.tune");
   if ((rc = check_bins(bins, pt->n, grid[0].n))) return rc;
   if (cp) {
@@ -708,7 +746,7 @@ extern "C" int fsi_mpm_substep_binned(const FsiParticles* pt, const FsiGrid grid
   const int2* chunks = reinterpret_cast<const int2*>(bins->chunk);
   const FsiGrid g = grid[buffer], go = grid[1 - buffer];
   const int tsc = mp->tune & 3, tg = (mp->tune >> 2) & 3;
-  const int T = tsc == FSI_TUNE_MPM_T512 ? 512 : (tsc == FSI_TUNE_MPM_T256 ? 256 : 128);
+  const int T = tsc == FSI_TUNE_P2G_T384 ? 384 : 128;
   const int TG = tg == FSI_TUNE_MPM_T512 ? 512 : (tg == FSI_TUNE_MPM_T256 ? 256 : 128);
   const LatView L = cp ? LatView{s->nx, s->ny, s->nz, s->pitch} : LatView{0, 0, 0, 0};
   const float* hy = cp ? hydro : nullptr;
@@ -727,9 +765,9 @@ extern "C" int fsi_mpm_substep_binned(const FsiParticles* pt, const FsiGrid grid
   k_p2g_scatter<R, TT><<<grid_ctas, TT, 0, st>>>(g, *mp, bins->payload, pt->n, chunks, bins->meta, box_b, buffer, \
                                                  stb)
   if (cp) {
-    if (T == 512) FSI_P2G(true, 512); else if (T == 256) FSI_P2G(true, 256); else FSI_P2G(true, 128);
+    if (T == 384) FSI_P2G(true, 384); else FSI_P2G(true, 128);
   } else {
-    if (T == 512) FSI_P2G(false, 512); else if (T == 256) FSI_P2G(false, 256); else FSI_P2G(false, 128);
+    if (T == 384) FSI_P2G(false, 384); else FSI_P2G(false, 128);
   }
 #undef FSI_P2G
   if ((rc = launch_check("k_p2g_scatter"))) return rc;
@@ -798,7 +836,7 @@ __global__ __launch_bounds__(128) void k_batch_p2g_payload(const FsiBatchCase* _
 }
 
 template <int T>
-__global__ __launch_bounds__(T) void k_batch_p2g_scatter(const FsiBatchCase* __restrict__ cases) {
+__global__ __launch_bounds__(T, T == 384 ? 1 : 4) void k_batch_p2g_scatter(const FsiBatchCase* __restrict__ cases) {
   const FsiBatchCase& bc = cases[blockIdx.y];
   if (!bc.active) return;
   const int b = bc.buf;
@@ -828,7 +866,7 @@ int check_batch_mpm(const FsiBatchCase* cases, const FsiBatchDims* d) {
   if (!cases || !d) return invalid("null batch argument");
   if (d->n_cases <= 0 || d->n_cases > 65535) return invalid("n_cases must be in 1..65535");
   if (d->max_particles <= 0 || d->max_chunks <= 0 || d->max_bins <= 0) return invalid("batch MPM dims must be positive");
-  if (d->mpm_tune < 0 || d->mpm_tune > 15 || (d->mpm_tune & 3) == 3 || ((d->mpm_tune >> 2) & 3) == 3)
+  if (d->mpm_tune < 0 || d->mpm_tune > 15 || (d->mpm_tune & 3) > 1 || ((d->mpm_tune >> 2) & 3) == 3)
     return invalid("unknown FsiBatchDims.mpm_tune");
   return FSI_OK;
 }
@@ -860,10 +898,8 @@ extern "C" int fsi_batch_mpm_substep(FsiBatchCase* cases, const FsiBatchDims* d,
   // partly filled add chunks): CTAs stride over the case's chunk table
   const dim3 gc((unsigned)std::min<int64_t>(d->max_chunks, 2 * nblk(d->max_particles, kChunk) + 8), d->n_cases);
   const int tsc = d->mpm_tune & 3, tg = (d->mpm_tune >> 2) & 3;
-  if (tsc == FSI_TUNE_MPM_T512)
-    k_batch_p2g_scatter<512><<<gc, 512, 0, st>>>(cases);
-  else if (tsc == FSI_TUNE_MPM_T256)
-    k_batch_p2g_scatter<256><<<gc, 256, 0, st>>>(cases);
+  if (tsc == FSI_TUNE_P2G_T384)
+    k_batch_p2g_scatter<384><<<gc, 384, 0, st>>>(cases);
   else
     k_batch_p2g_scatter<128><<<gc, 128, 0, st>>>(cases);
   if ((rc = launch_check("k_batch_p2g_scatter"))) return rc;

@@ -95,17 +95,18 @@ __device__ __forceinline__ void p2g_particle(const FsiParticles& pt, int p, cons
   const float c02 = Fp[3] * Fp[7] - Fp[4] * Fp[6];
   const float J = Fp[0] * c00 - Fp[1] * c01 + Fp[2] * c02;
   q.J = J;
-  // (F^-1)^T = cof(F) / det
+  // (F^-1)^T = cof(F) / det, as one correctly rounded reciprocal and nine products
+  const float iJ = __frcp_rn(J);
   float FinvT[9];
-  FinvT[0] = c00 / J;
-  FinvT[1] = -c01 / J;
-  FinvT[2] = c02 / J;
-  FinvT[3] = -(Fp[1] * Fp[8] - Fp[2] * Fp[7]) / J;
-  FinvT[4] = (Fp[0] * Fp[8] - Fp[2] * Fp[6]) / J;
-  FinvT[5] = -(Fp[0] * Fp[7] - Fp[1] * Fp[6]) / J;
-  FinvT[6] = (Fp[1] * Fp[5] - Fp[2] * Fp[4]) / J;
-  FinvT[7] = -(Fp[0] * Fp[5] - Fp[2] * Fp[3]) / J;
-  FinvT[8] = (Fp[0] * Fp[4] - Fp[1] * Fp[3]) / J;
+  FinvT[0] = c00 * iJ;
+  FinvT[1] = -c01 * iJ;
+  FinvT[2] = c02 * iJ;
+  FinvT[3] = -(Fp[1] * Fp[8] - Fp[2] * Fp[7]) * iJ;
+  FinvT[4] = (Fp[0] * Fp[8] - Fp[2] * Fp[6]) * iJ;
+  FinvT[5] = -(Fp[0] * Fp[7] - Fp[1] * Fp[6]) * iJ;
+  FinvT[6] = (Fp[1] * Fp[5] - Fp[2] * Fp[4]) * iJ;
+  FinvT[7] = -(Fp[0] * Fp[5] - Fp[2] * Fp[3]) * iJ;
+  FinvT[8] = (Fp[0] * Fp[4] - Fp[1] * Fp[3]) * iJ;
   const float mu2 = 2.0f * mp.mu, lam = mp.la * (J - 1.0f) * J;
   float P[9];
 #pragma unroll
@@ -179,6 +180,10 @@ __device__ __forceinline__ void reaction_particle(const LatView& L, const float*
                                                   const BSpline& b, float Jp, float vol0, float scale,
                                                   ReactParticle& r) {
   float hs[3] = {0.f, 0.f, 0.f}, ps = 0.f;
+  // stencils wholly inside the lattice (the common case) skip the per-node checks
+  const bool inside = b.base[0] >= 0 && b.base[1] >= 0 && b.base[2] >= 0 && b.base[0] + 2 < L.nx &&
+                      b.base[1] + 2 < L.ny && b.base[2] + 2 < L.nz;
+  const int64_t c000 = inside ? lat_cell(L, b.base[0], b.base[1], b.base[2]) : 0;
 #pragma unroll
   for (int ox = 0; ox < 3; ++ox)
 #pragma unroll
@@ -186,9 +191,9 @@ __device__ __forceinline__ void reaction_particle(const LatView& L, const float*
 #pragma unroll
       for (int oz = 0; oz < 3; ++oz) {
         const int I = b.base[0] + ox, Jj = b.base[1] + oy, K = b.base[2] + oz;
-        if (I < 0 || I >= L.nx || Jj < 0 || Jj >= L.ny || K < 0 || K >= L.nz) continue;
+        if (!inside && (I < 0 || I >= L.nx || Jj < 0 || Jj >= L.ny || K < 0 || K >= L.nz)) continue;
         const float w = b.w[0][ox] * b.w[1][oy] * b.w[2][oz];
-        const int64_t c = lat_cell(L, I, Jj, K);
+        const int64_t c = inside ? c000 + ((int64_t)oz * L.ny + oy) * L.nx + ox : lat_cell(L, I, Jj, K);
         hs[0] += w * hydro[c];
         hs[1] += w * hydro[L.pitch + c];
         hs[2] += w * hydro[2 * L.pitch + c];

@@ -96,13 +96,21 @@ FSI_HD2 void polar_rotation_jacobi_d(const double F[9], double R[9]) {
     for (int j = 0; j < 3; ++j) R[i * 3 + j] = U[i][0] * Vs[j][0] + U[i][1] * Vs[j][1] + U[i][2] * Vs[j][2];
 }
 
-// Scaled Newton iteration; returns false (R untouched) when det F <= 0 or the
-// iteration has not converged, so that the caller falls back to Jacobi.
+// Scaled Newton iteration X <- a X + b X^-T (X^-T = cof(X) / det X); returns
+// false (R untouched) when det F <= 0 or the iteration has not converged, so
+// that the caller falls back to Jacobi.  With X = R S, a X + b X^-T =
+// R (a S + b S^-1): the polar factor R is kept exactly for any positive a, b,
+// which only steer the convergence.  So the matrix arithmetic is FP64 while the
+// scaling a = g/2, b = 1/(2 g det) with g = (|X^-1|_F / |X|_F)^(1/2) is formed
+// in FP32 (square roots and division on the fast FP32 path); once the steps are
+// small the iteration switches to the unscaled a = 1/2, b = 1/(2 det) in FP64,
+// which drives S to I quadratically (and removes the FP32 rounding of the
+// scalars from the scale of X).
 FSI_HD2 bool polar_rotation_newton_d(const double F[9], double R[9]) {
   double X[9];
   for (int a = 0; a < 9; ++a) X[a] = F[a];
-  bool scale = true;
-  for (int it = 0; it < 16; ++it) {
+  bool scaled = true;
+  for (int it = 0; it < 20; ++it) {
     // cofactor matrix C = det(X) X^-T
     const double C0 = X[4] * X[8] - X[5] * X[7], C1 = X[5] * X[6] - X[3] * X[8], C2 = X[3] * X[7] - X[4] * X[6];
     const double C3 = X[2] * X[7] - X[1] * X[8], C4 = X[0] * X[8] - X[2] * X[6], C5 = X[1] * X[6] - X[0] * X[7];
@@ -110,17 +118,22 @@ FSI_HD2 bool polar_rotation_newton_d(const double F[9], double R[9]) {
     const double det = X[0] * C0 + X[1] * C1 + X[2] * C2;
     if (!(det > 0.0)) return false;
     const double C[9] = {C0, C1, C2, C3, C4, C5, C6, C7, C8};
-    double g = 1.0;
-    if (scale) {
+    double a0, b0;
+    if (scaled) {
       double nx = 0.0, nc = 0.0;
       for (int a = 0; a < 9; ++a) {
         nx += X[a] * X[a];
         nc += C[a] * C[a];
       }
-      // g = sqrt(|X^-1|_F / |X|_F), |X^-1|_F = |C|_F / det
-      g = sqrt(sqrt(nc / (nx * det * det)));
+      const float detf = (float)det;
+      const float g = sqrtf(sqrtf((float)nc / ((float)nx * detf * detf)));
+      if (!(g > 0.0f) || !(g < 3.0e38f)) return false;
+      a0 = (double)(0.5f * g);
+      b0 = (double)(0.5f / (g * detf));
+    } else {
+      a0 = 0.5;
+      b0 = 0.5 / det;
     }
-    const double a0 = 0.5 * g, b0 = 0.5 / (g * det);
     double d2 = 0.0;
     for (int a = 0; a < 9; ++a) {
       const double xn = a0 * X[a] + b0 * C[a];
@@ -129,9 +142,9 @@ FSI_HD2 bool polar_rotation_newton_d(const double F[9], double R[9]) {
       X[a] = xn;
     }
     // near convergence the scale factor is 1 to first order: drop it
-    if (d2 < 1e-6) scale = false;
-    // quadratic convergence: a step of size e leaves an error of order e^2
-    if (d2 < 1e-18) {
+    if (d2 < 1e-6) scaled = false;
+    // quadratic convergence of the unscaled steps: a step of size e leaves an error of order e^2
+    if (!scaled && d2 < 1e-18) {
       const double tr = X[0] + X[4] + X[8];
       if (!(tr - tr == 0.0)) return false;  // inf or NaN
       for (int a = 0; a < 9; ++a) R[a] = X[a];

@@ -138,9 +138,9 @@ def test_one_phase_substeps_match_oracle():
     compare_grid(gpu, ora)
 
 
-# FsiMpmParams.tune: scatter variant | gather variant << 2 (threads per chunk
-# CTA 128 / 256 / 512)
-TUNES = [0, 1 | 1 << 2, 2 | 2 << 2, 2]
+# FsiMpmParams.tune: scatter variant (128 / 384 threads per chunk CTA) |
+# gather variant (128 / 256 / 512 threads) << 2
+TUNES = [0, 1 | 1 << 2, 1 | 2 << 2, 2 << 2]
 
 
 @pytest.mark.parametrize("tune", TUNES)
@@ -242,7 +242,7 @@ def _oracle_react_stats(st, kind):
 def test_reaction_substeps_match_oracle(kind, path):
     gpu, ora = make_solids(seed=2)
     if path == "binned_t512":
-        gpu.params.tune = 2 | 2 << 2
+        gpu.params.tune = 1 | 2 << 2
         path = "binned"
     lbm, cpl, olbm, oc = _lbm_and_coupling(kind)
     for _ in range(3):
