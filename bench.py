@@ -222,6 +222,77 @@ def run_reference(args, wl, ws, rank):
           flush=True)
 
 
+def run_batched(args):
+    """Batching form: 64 cases of the batching configuration (per-axis edges in
+    {32, 48, 64, 96}, tau ~ U[0.52, 0.8], block or plate of 4^3-16^3 cells,
+    E ~ U[0.01, 0.1], penalty or moving_boundary), one batched launch per
+    phase replayed as one CUDA graph per FSI step, against the same cases
+    advanced one at a time (each with its own CUDA-graph step) on the same GPU.
+    A step is one FSI step (one LBM step + 10 MPM substeps) of every case."""
+    import torch
+
+    from mpm_lbm_b200.batch import FSIBatch, sample_box_cases
+
+    cases = sample_box_cases(args.cases, seed=0)
+    cells = sum(c.cells for c in cases)
+    batch = FSIBatch(capacity=len(cases), storage=args.storage, mpm_substeps=10)
+    for c in cases:
+        batch.add(c.make_driver(storage=args.storage))
+    for _ in range(max(args.warmup, 3)):
+        batch.step(use_graph=True)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        batch.step(use_graph=True)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    out = {"metric": "batched coupled-FSI MLUPS", "value": cells / (ms * 1e-3) / 1e6, "unit": "MLUPS",
+           "form": "batched", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+           "higher_is_better": True, "dtype": "f32" if args.storage == "fp32" else "f16-storage/f32-compute",
+           "data": "synthetic", "config": {"workload": f"batch_{len(cases)}_box_cases", "cases": len(cases),
+                                           "cells": cells, "kernels_per_step": batch.graph_kernels,
+                                           "lbm_tune": batch.dims.lbm_tune, "mpm_tune": batch.dims.mpm_tune}}
+    del batch
+    if not args.no_one_by_one:
+        tot = 0.0
+        for c in cases:
+            drv = c.make_driver(storage=args.storage)
+            drv.use_cuda_graph = True
+            for _ in range(3):
+                drv.step_once()
+            torch.cuda.synchronize()
+            e0.record()
+            for _ in range(args.steps):
+                drv.step_once()
+            e1.record()
+            torch.cuda.synchronize()
+            tot += e0.elapsed_time(e1) / args.steps
+            del drv
+        out["one_by_one"] = {"ms_per_step": tot, "value": cells / (tot * 1e-3) / 1e6, "unit": "MLUPS"}
+    print(json.dumps(out), flush=True)
+
+
+def run_served(args):
+    """Serving form: a Poisson stream (20 requests/s) of FSI solves, cubic
+    grids from {32, 48, 64, 96, 128} with weights {.3, .3, .2, .15, .05}, 100-2000
+    LBM steps each, solid / tau / mode as in the batching form, admitted into a
+    continuous batch under a 150 GB HBM budget."""
+    from mpm_lbm_b200.serve import FSIServer, poisson_requests
+
+    reqs = poisson_requests(args.requests, rate_per_s=20.0, seed=1, steps=(100, 2000))
+    srv = FSIServer(slots=64, hbm_budget_bytes=150e9, storage=args.storage)
+    srv.run(reqs, time_limit_s=1800)
+    rep = srv.report()
+    out = {"metric": "served coupled-FSI MLUPS", "value": rep["aggregate_mlups"], "unit": "MLUPS", "form": "served",
+           "n_gpus": 1, "higher_is_better": True,
+           "dtype": "f32" if args.storage == "fp32" else "f16-storage/f32-compute", "data": "synthetic",
+           "p50_latency_s": rep["p50_latency_s"], "p99_latency_s": rep["p99_latency_s"],
+           "config": {"workload": f"poisson_20ps_{args.requests}_requests", **rep}}
+    print(json.dumps(out), flush=True)
+
+
 def time_lbm_kernel(drv, storage, n_k1=40, reps=5):
     """Average duration of the fused LBM step kernel: a CUDA graph of n_k1
     back-to-back moving-boundary substeps, replayed reps times between events on
@@ -269,7 +340,18 @@ def main():
     ap.add_argument("--mpm-tune", type=int, default=None, help="fixed FsiMpmParams.tune (no autotuning)")
     ap.add_argument("--ref-substeps", type=int, default=30,
                     help="LBM substeps per timed step of the reference arm (bounded CPU sample)")
+    ap.add_argument("--form", default="single", choices=["single", "batched", "served"],
+                    help="single: the metric's case; batched / served: the batching and serving forms")
+    ap.add_argument("--cases", type=int, default=64)
+    ap.add_argument("--requests", type=int, default=100)
+    ap.add_argument("--no-one-by-one", action="store_true")
     args = ap.parse_args()
+    if args.form == "batched":
+        run_batched(args)
+        return
+    if args.form == "served":
+        run_served(args)
+        return
     wl = Workload(args.workload)
     ws, rank, local = dist_setup()
     if args.impl == "reference":

@@ -225,8 +225,8 @@ typedef struct FsiMpmParams {
  * variant | gather variant << 2); the other MPM entry points ignore it. */
 enum {
   /* P2G scatter: lanes per particle of a chunk CTA */
-  FSI_TUNE_P2G_T128 = 0,  /* 128 threads: one lane per particle, all 27 nodes (default) */
-  FSI_TUNE_P2G_T384 = 1,  /* 384 threads: three lanes per particle, one stencil plane each */
+  FSI_TUNE_P2G_T128 = 0,  /* 128 threads: 4 warps, each scattering one particle at a time (default) */
+  FSI_TUNE_P2G_T384 = 1,  /* 384 threads: 12 warps */
   /* G2P gather: threads per chunk CTA */
   FSI_TUNE_MPM_T128 = 0,  /* 128 threads: one lane per particle (default) */
   FSI_TUNE_MPM_T256 = 1,  /* 256 threads: two lanes per particle */
@@ -381,7 +381,7 @@ typedef struct FsiBatchDims {
   int32_t max_chunks;             /* max FsiMpmBins.max_chunks */
   int32_t max_bins;               /* max FsiMpmBins.n_bins */
   int32_t mpm_tune;               /* FsiMpmParams.tune of the batched MPM substep (all cases) */
-  int32_t pad;
+  int32_t lbm_tune;               /* FSI_TUNE_LBM_OCC3, or FSI_TUNE_LBM_PAIR when every case has an even nx */
 } FsiBatchDims;
 
 /* MPMToLBMProjector3D.project per case (coupling/projection.py:21-97). */

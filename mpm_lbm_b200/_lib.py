@@ -101,7 +101,7 @@ class FsiBatchCase(ctypes.Structure):
 class FsiBatchDims(ctypes.Structure):
     _fields_ = [("n_cases", c_i32), ("store_fp16", c_i32), ("max_lbm_tiles", c_i32), ("max_particles", c_i32),
                 ("max_cells", c_i64), ("max_chunks", c_i32), ("max_bins", c_i32), ("mpm_tune", c_i32),
-                ("pad", c_i32)]
+                ("lbm_tune", c_i32)]
 
 
 FSI_BATCH_PENALTY, FSI_BATCH_MOVING = 0, 1

@@ -21,16 +21,28 @@ from ._lib import (FSI_TUNE_LBM_OCC3, FSI_TUNE_LBM_OCC4, FSI_TUNE_LBM_PAIR, FSI_
 
 
 def _time_ms(fn, steps, reps):
+    """Device time per call of fn: `steps` calls captured in a CUDA graph (so
+    that host launch overhead does not enter), replayed `reps` times between
+    events; the best replay counts.  steps must return the state's alternating
+    layouts (AA parity, ping-pong slots, grid buffers) to their start, i.e. be
+    even."""
+    torch.cuda.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        for _ in range(steps):
+            fn()
+    graph.replay()
+    torch.cuda.synchronize()
     stream = torch.cuda.current_stream()
     best = float("inf")
     for _ in range(reps):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        for _ in range(steps):
-            fn()
+        graph.replay()
         e1.record(stream)
         torch.cuda.synchronize()
         best = min(best, e0.elapsed_time(e1) / steps)
+    del graph
     return best
 
 
@@ -89,7 +101,7 @@ def tune_mpm(solid, substep_fn, extra=(), candidates=None, steps=8, reps=3):
             solid.params.tune = int(t)
             substep_fn()
             torch.cuda.synchronize()
-            times[int(t)] = _time_ms(substep_fn, steps, reps)
+            times[int(t)] = _time_ms(substep_fn, steps + steps % 2, reps)
             solid.restore(snap)
     finally:
         solid.restore(snap)

@@ -34,7 +34,8 @@ import numpy as np
 import torch
 
 from ._lib import (FSI_BATCH_MOVING, FSI_BATCH_PENALTY, FSI_MODE_DIRSTATS, FSI_MODE_MOVING_BB, FSI_MODE_PENALTY,
-                   FsiBatchCase, FsiBatchDims, call, launch_count, stream_handle)
+                   FSI_TUNE_LBM_OCC3, FSI_TUNE_LBM_PAIR, FsiBatchCase, FsiBatchDims, call, launch_count,
+                   stream_handle)
 from .config import FSIDriverConfig
 from .geometry import jittered_block, walled_channel
 
@@ -159,12 +160,15 @@ def sample_box_cases(n, seed=0, edges=(32, 48, 64, 96), lbm_steps=200, mpm_subst
 class FSIBatch:
     """Up to `capacity` independent FSI cases, advanced together."""
 
-    def __init__(self, capacity, storage="fp32", mpm_substeps=10, device="cuda", mpm_tune=0):
+    def __init__(self, capacity, storage="fp32", mpm_substeps=10, device="cuda", mpm_tune=0, lbm_tune=None):
+        """lbm_tune: FSI_TUNE_LBM_OCC3 (0) or FSI_TUNE_LBM_PAIR (2, every case's nx
+        even); None picks the paired kernel while every case allows it."""
         self.capacity = int(capacity)
         self.storage = storage
         self.M = int(mpm_substeps)
         self.device = torch.device(device)
         self.mpm_tune = int(mpm_tune)
+        self.lbm_tune = lbm_tune
         self.slots = [None] * self.capacity          # FSIDriver3D per slot
         self.records = (FsiBatchCase * self.capacity)()
         self.t_cases = torch.zeros(ctypes.sizeof(self.records), dtype=torch.uint8, device=self.device)
@@ -273,6 +277,13 @@ class FSIBatch:
         d.n_cases = self.capacity
         d.store_fp16 = int(self.storage == "fp16")
         d.mpm_tune = self.mpm_tune
+        all_even = all(x.lbm.nx % 2 == 0 for x in act)
+        if self.lbm_tune is None:
+            d.lbm_tune = FSI_TUNE_LBM_PAIR if all_even else FSI_TUNE_LBM_OCC3
+        else:
+            if self.lbm_tune == FSI_TUNE_LBM_PAIR and not all_even:
+                raise ValueError("the paired LBM kernel needs an even nx in every case")
+            d.lbm_tune = int(self.lbm_tune)
         if not act:
             d.max_lbm_tiles = d.max_particles = d.max_chunks = d.max_bins = 1
             d.max_cells = 1

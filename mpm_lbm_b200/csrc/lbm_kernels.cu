@@ -384,7 +384,7 @@ __device__ __forceinline__ void stp(const Case& c, int s, int idx, float v) {
 // (fluid.py:431-440, 488-519).
 template <bool ODD, bool H, bool MOVING>
 __device__ __forceinline__ void store_near_solid(const Case& c, const Nbh& n, int cell, uint32_t nb, float rho,
-                                              const float* out, bool dirstats, DirAcc* acc) {
+                                              const float* out) {
   float* hpp = c.s.hpp + (int64_t)c.c.pp * 3 * c.s.pitch;
   const int64_t P = c.s.pitch;
 #pragma unroll
@@ -401,16 +401,6 @@ __device__ __forceinline__ void store_near_solid(const Case& c, const Nbh& n, in
       if (kEx(s)) atomicAdd(hpp + ip, (float)kEx(s) * tot);
       if (kEy(s)) atomicAdd(hpp + P + ip, (float)kEy(s) * tot);
       if (kEz(s)) atomicAdd(hpp + 2 * P + ip, (float)kEz(s) * tot);
-      if (dirstats) {
-        const float ac = fabsf(corr);
-        atomicAdd(&acc->cnt[s], 1);
-        atomicAdd(&acc->csum[s], ac);
-        atomic_max_nonneg(&acc->cmax[s], ac);
-        if (kEx(s)) atomicAdd(&acc->imp[s][0], -(float)kEx(s) * tot);
-        if (kEy(s)) atomicAdd(&acc->imp[s][1], -(float)kEy(s) * tot);
-        if (kEz(s)) atomicAdd(&acc->imp[s][2], -(float)kEz(s) * tot);
-        acc->any = 1;
-      }
     }
     if (!ODD || s == 0 || bb)
       stp<H>(c, kOpp(s), cell, val);
@@ -423,6 +413,45 @@ __device__ __forceinline__ void store_near_solid(const Case& c, const Nbh& n, in
 // (bx, by).  Called by the single-case kernel (c in the parameter bank) and by
 // the batched kernel (c staged in shared memory); acc: the CTA's shared
 // per-direction accumulator.
+// Per-direction bounce-back reductions of one step (fluid.py:488-536: link
+// counts, |correction| sum and max, fluid impulse), called by every lane of
+// the warp together after the streaming stores: per direction the warp's link
+// contributions are combined with shuffles and one lane adds them to the CTA's
+// shared accumulator (float atomics to one shared address serialise, so that
+// each direction sees at most one per warp).  nb: the lane's cell's solid
+// neighbour mask (0 for no cell, solid or plain fluid); out: the cell's
+// post-collision populations; rho: its density.
+__device__ __forceinline__ void dirstats_warp(const Case& c, const Nbh& n, uint32_t nb, float rho, const float* out,
+                                              DirAcc& acc) {
+  const int64_t P = c.s.pitch;
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int s = 1; s < 19; ++s) {
+    const bool link = (nb >> s) & 1u;
+    const unsigned m = __ballot_sync(kFull, link);
+    if (m == 0u) continue;
+    float ac = 0.f, tot = 0.f;
+    if (link) {
+      const int ip = n.at(kEx(s), kEy(s), kEz(s));
+      const float ew = (float)kEx(s) * c.s.svel[ip] + (float)kEy(s) * c.s.svel[P + ip] + (float)kEz(s) * c.s.svel[2 * P + ip];
+      const float corr = -6.0f * lattice_w(s) * rho * ew;
+      const float f0 = out[s];
+      tot = (f0 + corr) + f0;  // solid force = e_s (bounced + f)
+      ac = fabsf(corr);
+    }
+    const float sum = warp_sum(ac), mx = warp_max(ac), ts = warp_sum(tot);
+    if (lane == 0) {
+      atomicAdd(&acc.cnt[s], __popc(m));
+      atomicAdd(&acc.csum[s], sum);
+      atomic_max_nonneg(&acc.cmax[s], mx);
+      if (kEx(s)) atomicAdd(&acc.imp[s][0], -(float)kEx(s) * ts);
+      if (kEy(s)) atomicAdd(&acc.imp[s][1], -(float)kEy(s) * ts);
+      if (kEz(s)) atomicAdd(&acc.imp[s][2], -(float)kEz(s) * ts);
+      acc.any = 1;
+    }
+  }
+}
+
 template <bool ODD, bool H, bool MOVING, bool BCW, bool PEN>
 __device__ __forceinline__ void lbm_step_tile(const Case& c, int bx, int by, DirAcc& acc) {
   const int lane = threadIdx.x;
@@ -579,7 +608,7 @@ __device__ __forceinline__ void lbm_step_tile(const Case& c, int bx, int by, Dir
         for (int s = 1; s < 19; ++s) stp<H>(c, s, n.at(kEx(s), kEy(s), kEz(s)), F[s]);
       }
     } else {
-      store_near_solid<ODD, H, MOVING>(c, n, cell, nb, rho, F, dirstats, &acc);
+      store_near_solid<ODD, H, MOVING>(c, n, cell, nb, rho, F);
     }
   } else if (MOVING && valid && (fl & kLink)) {
     // solid cell receiving link forces: recycle last step's ping-pong slot
@@ -600,6 +629,7 @@ __device__ __forceinline__ void lbm_step_tile(const Case& c, int bx, int by, Dir
   }
 
   if (dirstats) {
+    dirstats_warp(c, n, fluid ? nb : 0u, rho, F, acc);
     __syncthreads();
     if (acc.any) {
       const int tid = threadIdx.y * 32 + lane;
@@ -725,18 +755,16 @@ __device__ __forceinline__ void bc_face_warp2(const Case& c, int lane, int row, 
 
 // post-streaming populations of one fluid cell next to a solid (per-cell path)
 template <bool ODD, bool H>
-__device__ __forceinline__ void load_near_solid(const Case& c, const Nbh& n, int cell, uint32_t nb, float2* F, int ci) {
-  set_comp(F[0], ci, ldp<H>(c, 0, cell));
+__device__ __forceinline__ void set_near_solid_loads(const Case& c, const Nbh& n, int cell, uint32_t nb, float* F) {
+  F[0] = ldp<H>(c, 0, cell);
 #pragma unroll
   for (int s = 1; s < 19; ++s) {
-    float v;
     if (!ODD)
-      v = ldp<H>(c, s, cell);
+      F[s] = ldp<H>(c, s, cell);
     else if ((nb >> kOpp(s)) & 1u)
-      v = ldp<H>(c, s, cell);
+      F[s] = ldp<H>(c, s, cell);
     else
-      v = ldp<H>(c, kOpp(s), n.at(-kEx(s), -kEy(s), -kEz(s)));
-    set_comp(F[s], ci, v);
+      F[s] = ldp<H>(c, kOpp(s), n.at(-kEx(s), -kEy(s), -kEz(s)));
   }
 }
 
@@ -760,6 +788,25 @@ __device__ __forceinline__ bool penalty_cell(const Case& c, int cell, bool fluid
     f2 *= r;
   }
   return true;
+}
+
+// The paired kernel keeps its rare paths (cells next to a solid, the face
+// cells of open boundaries) out of line, so that the instruction footprint of
+// the common path stays small.
+template <bool ODD, bool H, bool MOVING>
+__device__ __noinline__ void store_near_solid_nl(const Case& c, const Nbh& n, int cell, uint32_t nb, float rho,
+                                                 const float* out) {
+  store_near_solid<ODD, H, MOVING>(c, n, cell, nb, rho, out);
+}
+
+template <bool ODD, bool H>
+__device__ __noinline__ void load_near_solid_nl(const Case& c, const Nbh& n, int cell, uint32_t nb, float* F) {
+  set_near_solid_loads<ODD, H>(c, n, cell, nb, F);
+}
+
+template <int SIDE>
+__device__ __noinline__ void bc_face_warp2_nl(const Case& c, int lane, int row, uint8_t fl0, uint8_t fl1, float2* F) {
+  bc_face_warp2<SIDE>(c, lane, row, fl0, fl1, F);
 }
 
 template <bool ODD, bool H, bool MOVING, bool BCW, bool PEN>
@@ -826,10 +873,13 @@ __device__ __forceinline__ void lbm_step_tile2(const Case& c, int bx, int by, Di
         }
       }
     } else {
+      float a[19], b[19];
 #pragma unroll
-      for (int s = 0; s < 19; ++s) F[s] = make_float2(0.f, 0.f);
-      if (fluid0) load_near_solid<ODD, H>(c, n0, cell0, nb0, F, 0);
-      if (fluid1) load_near_solid<ODD, H>(c, n1, cell0 + 1, nb1, F, 1);
+      for (int s = 0; s < 19; ++s) a[s] = b[s] = 0.f;
+      if (fluid0) load_near_solid_nl<ODD, H>(c, n0, cell0, nb0, a);
+      if (fluid1) load_near_solid_nl<ODD, H>(c, n1, cell0 + 1, nb1, b);
+#pragma unroll
+      for (int s = 0; s < 19; ++s) F[s] = make_float2(a[s], b[s]);
     }
   } else {
 #pragma unroll
@@ -838,8 +888,8 @@ __device__ __forceinline__ void lbm_step_tile2(const Case& c, int bx, int by, Di
 
   // ---- pending open boundary of the previous step (fluid.py:538-569)
   if (BCW && c.c.bc_pending && inrow) {
-    if (c.p.bc_left != 0 && bx == 0) bc_face_warp2<0>(c, lane, row, fl[0], fl[1], F);
-    if (c.p.bc_right != 0 && bx == ((nx - 1) >> 6)) bc_face_warp2<1>(c, lane, row, fl[0], fl[1], F);
+    if (c.p.bc_left != 0 && bx == 0) bc_face_warp2_nl<0>(c, lane, row, fl[0], fl[1], F);
+    if (c.p.bc_right != 0 && bx == ((nx - 1) >> 6)) bc_face_warp2_nl<1>(c, lane, row, fl[0], fl[1], F);
   }
 
   // ---- macroscopic state the collision uses (streaming3, fluid.py:1794-1814)
@@ -981,7 +1031,7 @@ __device__ __forceinline__ void lbm_step_tile2(const Case& c, int bx, int by, Di
         }
       }
     } else {
-#pragma unroll
+#pragma unroll 1
       for (int i = 0; i < 2; ++i) {
         if (!(i ? fluid1 : fluid0)) continue;
         float out[19];
@@ -991,7 +1041,7 @@ __device__ __forceinline__ void lbm_step_tile2(const Case& c, int bx, int by, Di
         const Nbh& n = i ? n1 : n0;
         const int cell = cell0 + i;
         if (nb) {
-          store_near_solid<ODD, H, MOVING>(c, n, cell, nb, comp(rho, i), out, dirstats, &acc);
+          store_near_solid_nl<ODD, H, MOVING>(c, n, cell, nb, comp(rho, i), out);
         } else if (!ODD) {
 #pragma unroll
           for (int s = 0; s < 19; ++s) stp<H>(c, kOpp(s), cell, out[s]);
@@ -1027,6 +1077,14 @@ __device__ __forceinline__ void lbm_step_tile2(const Case& c, int bx, int by, Di
   }
 
   if (dirstats) {
+    float o0[19], o1[19];
+#pragma unroll
+    for (int s = 0; s < 19; ++s) {
+      o0[s] = F[s].x;
+      o1[s] = F[s].y;
+    }
+    dirstats_warp(c, n0, fluid0 ? nb0 : 0u, rho.x, o0, acc);
+    dirstats_warp(c, n1, fluid1 ? nb1 : 0u, rho.y, o1, acc);
     __syncthreads();
     if (acc.any) {
       const int tid = threadIdx.y * 32 + lane;
@@ -1045,7 +1103,7 @@ __device__ __forceinline__ void lbm_step_tile2(const Case& c, int bx, int by, Di
 }
 
 template <bool ODD, bool H, bool MOVING, bool BCW, bool PEN>
-__global__ void __launch_bounds__(128, 4) k_lbm_step2(const Case c) {
+__global__ void __launch_bounds__(128, 4) k_lbm_step2(const __grid_constant__ Case c) {
   __shared__ DirAcc acc;
   lbm_step_tile2<ODD, H, MOVING, BCW, PEN>(c, blockIdx.x, blockIdx.y, acc);
 }
@@ -1736,6 +1794,33 @@ __global__ void __launch_bounds__(256, 3) k_batch_lbm_step(const FsiBatchCase* _
   }
 }
 
+// the same with two cells per thread (lbm_step_tile2): tiles of 64 x 4 cells
+template <bool H>
+__global__ void __launch_bounds__(128, 4) k_batch_lbm_step2(const FsiBatchCase* __restrict__ cases) {
+  __shared__ Case sc;
+  __shared__ DirAcc acc;
+  const FsiBatchCase& bc = cases[blockIdx.y];
+  const int gx = (bc.lbm.nx + 63) / 64, nt = gx * ((bc.lbm.ny * bc.lbm.nz + 3) / 4);
+  if ((int)blockIdx.x >= nt || !stage_case(bc, sc, true)) return;
+  const bool moving = sc.c.mode & FSI_MODE_MOVING_BB;
+  const bool odd = sc.c.parity != 0;
+  for (int t = blockIdx.x; t < nt; t += gridDim.x) {
+    const int bx = t % gx, by = t / gx;
+    if (moving) {
+      if (odd)
+        lbm_step_tile2<true, H, true, false, false>(sc, bx, by, acc);
+      else
+        lbm_step_tile2<false, H, true, false, false>(sc, bx, by, acc);
+    } else {
+      if (odd)
+        lbm_step_tile2<true, H, false, false, true>(sc, bx, by, acc);
+      else
+        lbm_step_tile2<false, H, false, false, true>(sc, bx, by, acc);
+    }
+    __syncthreads();  // acc is reused by the next tile
+  }
+}
+
 __global__ void k_batch_mask_update(const FsiBatchCase* __restrict__ cases) {
   __shared__ Case sc;
   const FsiBatchCase& bc = cases[blockIdx.y];
@@ -1791,6 +1876,8 @@ int check_batch(const FsiBatchCase* cases, const FsiBatchDims* d) {
   if (!cases || !d) return invalid("null batch argument");
   if (d->n_cases <= 0 || d->n_cases > 65535) return invalid("n_cases must be in 1..65535");
   if (d->max_lbm_tiles <= 0 || d->max_cells <= 0) return invalid("batch dims must be positive");
+  if (d->lbm_tune != FSI_TUNE_LBM_OCC3 && d->lbm_tune != FSI_TUNE_LBM_PAIR)
+    return invalid("FsiBatchDims.lbm_tune must be FSI_TUNE_LBM_OCC3 or FSI_TUNE_LBM_PAIR (every case nx even)");
   return FSI_OK;
 }
 
@@ -1808,11 +1895,20 @@ extern "C" int fsi_batch_lbm_substep(FsiBatchCase* cases, const FsiBatchDims* d,
   k_batch_ctl<<<d->n_cases, 32, 0, st>>>(cases, kBatchLbmPre);
   if ((rc = launch_check("k_batch_ctl"))) return rc;
   // one CTA per tile of the largest case; CTAs past a smaller case's tiles exit at once
-  const dim3 grid(batch_x(d->max_lbm_tiles, 1, 1 << 20), d->n_cases);
-  if (d->store_fp16)
-    k_batch_lbm_step<true><<<grid, dim3(32, 8), 0, st>>>(cases);
-  else
-    k_batch_lbm_step<false><<<grid, dim3(32, 8), 0, st>>>(cases);
+  if (d->lbm_tune == FSI_TUNE_LBM_PAIR) {
+    // max_lbm_tiles counts 32 x 8 tiles; a 64 x 4 tile covers as many cells
+    const dim3 grid(batch_x((int64_t)d->max_lbm_tiles + 64, 1, 1 << 20), d->n_cases);
+    if (d->store_fp16)
+      k_batch_lbm_step2<true><<<grid, dim3(32, 4), 0, st>>>(cases);
+    else
+      k_batch_lbm_step2<false><<<grid, dim3(32, 4), 0, st>>>(cases);
+  } else {
+    const dim3 grid(batch_x(d->max_lbm_tiles, 1, 1 << 20), d->n_cases);
+    if (d->store_fp16)
+      k_batch_lbm_step<true><<<grid, dim3(32, 8), 0, st>>>(cases);
+    else
+      k_batch_lbm_step<false><<<grid, dim3(32, 8), 0, st>>>(cases);
+  }
   if ((rc = launch_check("k_batch_lbm_step"))) return rc;
   k_batch_ctl<<<d->n_cases, 32, 0, st>>>(cases, kBatchLbmPost);
   return launch_check("k_batch_ctl");

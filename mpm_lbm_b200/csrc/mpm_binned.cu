@@ -239,7 +239,6 @@ __device__ __forceinline__ void p2g_payload_body(const FsiParticles& pt, const F
                                                  FsiCouplingStats* st, const FsiLbmDiag* diag, int vb, int vg) {
   __shared__ float s_scale;
   const int n = pt.n;
-  const int slot = vb * blockDim.x + threadIdx.x;
   if (REACT) {
     if (threadIdx.x == 0) {
       float raw = 1.f;
@@ -254,38 +253,54 @@ __device__ __forceinline__ void p2g_payload_body(const FsiParticles& pt, const F
   int n_act = 0;
   float pmax = 0.f;
   double pn[3] = {0.0, 0.0, 0.0};
-  if (slot < n) {
-    const int p = perm[slot];
-    const float X[3] = {pt.x[p], pt.x[n + p], pt.x[2 * n + p]};
-    BSpline b;
-    bspline(X, mp.inv_dx, b);
-    P2GParticle q;
-    p2g_particle(pt, p, mp, q);
-    pt.Jp[p] = q.J;
-    float pf[3] = {0.f, 0.f, 0.f};
-    if (REACT) {
-      ReactParticle r;
-      reaction_particle(L, hydro, phi, cp, b, q.J, pt.vol0[p], s_scale, r);
-      n_act = r.act ? 1 : 0;
-      pmax = r.pnorm;
-      if (r.gated)
-        for (int a = 0; a < 3; ++a) pn[a] = (double)r.pf[a];
-      if (r.scatter)
-        for (int a = 0; a < 3; ++a) pf[a] = r.pf[a];
+  // two lanes per particle slot, in different warps of the CTA so that the two
+  // halves of the work run side by side instead of one after the other:
+  // warps of role 0 the stress and affine momentum (FP64 polar rotation),
+  // warps of role 1 the B-spline data and the reaction force (with its own
+  // det F for the volume).  Warp w of the CTA covers slots
+  // (vb * blockDim.x / 2) + (w / 2) * 32 + lane with role w % 2.
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int pslot = vb * (blockDim.x >> 1) + (wid >> 1) * 32 + lane, role = wid & 1;
+  if (pslot < n) {
+    const int p = perm[pslot];
+    float* const col = payload + pslot;
+    if (role == 0) {
+      P2GParticle q;
+      p2g_particle(pt, p, mp, q);
+      pt.Jp[p] = q.J;
+#pragma unroll
+      for (int a = 0; a < 3; ++a) col[(int64_t)(kPmv + a) * n] = q.mv[a];
+#pragma unroll
+      for (int a = 0; a < 9; ++a) col[(int64_t)(kPaff + a) * n] = q.aff[a];
+      col[(int64_t)kPmass * n] = q.mass;
+    } else {
+      const float X[3] = {pt.x[p], pt.x[n + p], pt.x[2 * n + p]};
+      BSpline b;
+      bspline(X, mp.inv_dx, b);
+      float pf[3] = {0.f, 0.f, 0.f};
+      if (REACT) {
+        float Fp[9];
+#pragma unroll
+        for (int a = 0; a < 9; ++a) Fp[a] = pt.F[(int64_t)a * n + p];
+        const float J = det3(Fp);
+        ReactParticle r;
+        reaction_particle(L, hydro, phi, cp, b, J, pt.vol0[p], s_scale, r);
+        n_act = r.act ? 1 : 0;
+        pmax = r.pnorm;
+        if (r.gated)
+          for (int a = 0; a < 3; ++a) pn[a] = (double)r.pf[a];
+        if (r.scatter)
+          for (int a = 0; a < 3; ++a) pf[a] = r.pf[a];
+      }
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        col[(int64_t)(kPfx + a) * n] = b.fx[a];
+        col[(int64_t)(kPbase + a) * n] = __int_as_float(b.base[a]);
+        col[(int64_t)(kPpf + a) * n] = pf[a];
+#pragma unroll
+        for (int o = 0; o < 3; ++o) col[(int64_t)(kPw + 3 * a + o) * n] = b.w[a][o];
+      }
     }
-    float* const col = payload + slot;
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      col[(int64_t)(kPfx + a) * n] = b.fx[a];
-      col[(int64_t)(kPbase + a) * n] = __int_as_float(b.base[a]);
-      col[(int64_t)(kPmv + a) * n] = q.mv[a];
-      col[(int64_t)(kPpf + a) * n] = pf[a];
-#pragma unroll
-      for (int o = 0; o < 3; ++o) col[(int64_t)(kPw + 3 * a + o) * n] = b.w[a][o];
-    }
-#pragma unroll
-    for (int a = 0; a < 9; ++a) col[(int64_t)(kPaff + a) * n] = q.aff[a];
-    col[(int64_t)kPmass * n] = q.mass;
   }
   if (REACT) {
     // diagnostics reductions (penalty.py:202-240, moving_boundary.py:312-374)
@@ -314,9 +329,9 @@ __global__ __launch_bounds__(128) void k_p2g_payload(FsiParticles pt, FsiMpmPara
 
 // P2G scatter of the chunks of this CTA into grid buffer g, from the payload:
 //  stage the chunk's payload columns and find its node box;
-//  the 27 x chunk (particle, node) pairs spread over the T threads, so that
-//  the lanes of one shared-memory atomic touch distinct nodes (pair order:
-//  particle-major, offsets ox, oy, oz as in p2g);
+//  each warp scatters one particle at a time, lane o on stencil node o, so
+//  that the lanes of one shared-memory atomic touch distinct nodes (float
+//  atomics to one shared address serialise);
 //  one global atomic per touched node value.
 // Chunks whose box exceeds the tile (bins gone stale) scatter with global
 // atomics directly.
@@ -378,84 +393,58 @@ __device__ __forceinline__ void p2g_scatter_body(const FsiGrid& g, const FsiMpmP
     const int nv = staged ? bx.vol : 0;
     for (int i = tid; i < 7 * nv; i += T) tile[i] = 0.f;
     __syncthreads();
-    // particle-major: lane lp of each group of kChunk threads owns one particle
-    // (its payload in registers); with GL = T / kChunk = 3 lanes per particle,
-    // group `sub` takes the stencil plane ox = sub, otherwise a lane takes all
-    // 27 nodes.  Node order within a lane: ox, oy, oz as in p2g.
-    constexpr int GL = T / kChunk;
-    static_assert(GL == 1 || GL == 3, "scatter CTAs have 128 or 384 threads");
-    const int lp = tid % kChunk, sub = tid / kChunk;
-    if (lp < ch.y) {
-      int base[3];
-      float fx[3], wv[9], mv[3], aff[9], pf[3];
+    // one warp per particle, lane o < 27 on stencil node o (ox, oy, oz = o / 9,
+    // o / 3 % 3, o % 3): the particle's payload is a broadcast read and the
+    // warp's shared-memory atomics land on 27 distinct nodes
+    const int lane = tid & 31, warp = tid >> 5;
+    const int ox = lane / 9, oy = (lane / 3) % 3, oz = lane % 3;
+    const float dox = (float)ox, doy = (float)oy, doz = (float)oz;
+    float gsum[3] = {0.f, 0.f, 0.f}, gm2 = 0.f;
+    for (int lp = warp; lp < ch.y; lp += T / 32) {
+      if (lane >= 27) continue;
+      const int I = __float_as_int(sp[kPbase][lp]) + ox, Jj = __float_as_int(sp[kPbase + 1][lp]) + oy,
+                K = __float_as_int(sp[kPbase + 2][lp]) + oz;
+      if (I < 0 || I >= G || Jj < 0 || Jj >= G || K < 0 || K >= G) continue;
+      // weights of bspline() (staged by the payload) and offsets as in p2g_node()
+      const float w = sp[kPw + ox][lp] * sp[kPw + 3 + oy][lp] * sp[kPw + 6 + oz][lp];
+      const float dpos[3] = {(dox - sp[kPfx][lp]) * mp.dx, (doy - sp[kPfx + 1][lp]) * mp.dx,
+                             (doz - sp[kPfx + 2][lp]) * mp.dx};
+      float val[7];
 #pragma unroll
-      for (int q = 0; q < 3; ++q) {
-        base[q] = __float_as_int(sp[kPbase + q][lp]);
-        fx[q] = sp[kPfx + q][lp];
-        mv[q] = sp[kPmv + q][lp];
-        pf[q] = REACT ? sp[kPpf + q][lp] : 0.f;
-      }
+      for (int q = 0; q < 3; ++q)
+        val[q] = w * (sp[kPmv + q][lp] + (sp[kPaff + 3 * q][lp] * dpos[0] + sp[kPaff + 3 * q + 1][lp] * dpos[1] +
+                                          sp[kPaff + 3 * q + 2][lp] * dpos[2]));
+      val[3] = w * sp[kPmass][lp];
+      bool react = false;
+      if (REACT) {
+        const float f0 = sp[kPpf][lp], f1 = sp[kPpf + 1][lp], f2 = sp[kPpf + 2][lp];
+        react = f0 != 0.f || f1 != 0.f || f2 != 0.f;
+        if (react) {
+          val[4] = w * f0;
+          val[5] = w * f1;
+          val[6] = w * f2;
 #pragma unroll
-      for (int q = 0; q < 9; ++q) {
-        wv[q] = sp[kPw + q][lp];
-        aff[q] = sp[kPaff + q][lp];
-      }
-      const float mass = sp[kPmass][lp];
-      const bool react = REACT && (pf[0] != 0.f || pf[1] != 0.f || pf[2] != 0.f);
-      const bool inside = base[0] >= 0 && base[1] >= 0 && base[2] >= 0 && base[0] + 2 < G && base[1] + 2 < G &&
-                          base[2] + 2 < G;
-      const float d1[3] = {(0.0f - fx[1]) * mp.dx, (1.0f - fx[1]) * mp.dx, (2.0f - fx[1]) * mp.dx};
-      const float d2[3] = {(0.0f - fx[2]) * mp.dx, (1.0f - fx[2]) * mp.dx, (2.0f - fx[2]) * mp.dx};
-      float gsum[3] = {0.f, 0.f, 0.f}, gm2 = 0.f;
-#pragma unroll
-      for (int oxi = 0; oxi < (GL == 1 ? 3 : 1); ++oxi) {
-        const int ox = GL == 1 ? oxi : sub;
-        const float wx = ox == 0 ? wv[0] : (ox == 1 ? wv[1] : wv[2]);
-        const float d0 = ((float)ox - fx[0]) * mp.dx;
-        const int I = base[0] + ox;
-#pragma unroll
-        for (int oy = 0; oy < 3; ++oy) {
-          const float wxy = wx * wv[3 + oy];
-          const int Jj = base[1] + oy;
-#pragma unroll
-          for (int oz = 0; oz < 3; ++oz) {
-            const int K = base[2] + oz;
-            if (!inside && (I < 0 || I >= G || Jj < 0 || Jj >= G || K < 0 || K >= G)) continue;
-            // weights of bspline() and offsets as in p2g_node()
-            const float w = wxy * wv[6 + oz];
-            float val[7];
-#pragma unroll
-            for (int q = 0; q < 3; ++q)
-              val[q] = w * (mv[q] + (aff[3 * q] * d0 + aff[3 * q + 1] * d1[oy] + aff[3 * q + 2] * d2[oz]));
-            val[3] = w * mass;
-            if (react) {
-#pragma unroll
-              for (int q = 0; q < 3; ++q) {
-                val[4 + q] = w * pf[q];
-                gsum[q] += val[4 + q];
-              }
-              gm2 = fmaxf(gm2, val[4] * val[4] + val[5] * val[5] + val[6] * val[6]);
-            }
-            const int nq = react ? 7 : 4;
-            if (staged) {
-              const int li = ((K - bx.lo[2]) * bx.ext[1] + (Jj - bx.lo[1])) * bx.ext[0] + (I - bx.lo[0]);
-#pragma unroll
-              for (int q = 0; q < 7; ++q)
-                if (q < nq) atomicAdd(&tile[q * nv + li], val[q]);
-            } else {
-              const int64_t node = ((int64_t)K * G + Jj) * G + I;
-#pragma unroll
-              for (int q = 0; q < 7; ++q)
-                if (q < nq) atomicAdd(dst[q] + node, val[q]);
-            }
-          }
+          for (int q = 0; q < 3; ++q) gsum[q] += val[4 + q];
+          gm2 = fmaxf(gm2, val[4] * val[4] + val[5] * val[5] + val[6] * val[6]);
         }
       }
-      if (react) {
+      const int nq = react ? 7 : 4;
+      if (staged) {
+        const int li = ((K - bx.lo[2]) * bx.ext[1] + (Jj - bx.lo[1])) * bx.ext[0] + (I - bx.lo[0]);
 #pragma unroll
-        for (int q = 0; q < 3; ++q) gn[q] += (double)gsum[q];
-        gmax = fmaxf(gmax, sqrtf(gm2));
+        for (int q = 0; q < 7; ++q)
+          if (q < nq) atomicAdd(&tile[q * nv + li], val[q]);
+      } else {
+        const int64_t node = ((int64_t)K * G + Jj) * G + I;
+#pragma unroll
+        for (int q = 0; q < 7; ++q)
+          if (q < nq) atomicAdd(dst[q] + node, val[q]);
       }
+    }
+    if (REACT) {
+#pragma unroll
+      for (int q = 0; q < 3; ++q) gn[q] += (double)gsum[q];
+      gmax = fmaxf(gmax, sqrtf(gm2));
     }
     __syncthreads();
     for (int li = tid; li < nv; li += T) {
@@ -480,8 +469,7 @@ __device__ __forceinline__ void p2g_scatter_body(const FsiGrid& g, const FsiMpmP
   }
 }
 
-// register budget: 128-thread CTAs keep 4 per SM, 384-thread CTAs 1 (the
-// payload of a particle stays in registers across its nodes)
+// register budget: 128-thread CTAs keep 4 per SM, 384-thread CTAs 1
 template <bool REACT, int T>
 __global__ __launch_bounds__(T, T == 384 ? 1 : 4) void k_p2g_scatter(FsiGrid g, FsiMpmParams mp, const float* __restrict__ payload,
                                                    int n, const int2* __restrict__ chunks, int32_t* meta,
@@ -755,11 +743,11 @@ extern "C" int fsi_mpm_substep_binned(const FsiParticles* pt, const FsiGrid grid
   FsiCouplingStats* stb = cp ? &stats[buffer] : nullptr;
   const FsiLbmDiag* dg = cp ? s->diag : nullptr;
   if (cp)
-    k_p2g_payload<true><<<nblk(pt->n, 128), 128, 0, st>>>(*pt, *mp, bins->perm, bins->payload, L, hy, ph, cpv, stb,
-                                                          dg);
+    k_p2g_payload<true><<<nblk(2 * (int64_t)pt->n, 128), 128, 0, st>>>(*pt, *mp, bins->perm, bins->payload, L, hy,
+                                                                         ph, cpv, stb, dg);
   else
-    k_p2g_payload<false><<<nblk(pt->n, 128), 128, 0, st>>>(*pt, *mp, bins->perm, bins->payload, L, hy, ph, cpv, stb,
-                                                           dg);
+    k_p2g_payload<false><<<nblk(2 * (int64_t)pt->n, 128), 128, 0, st>>>(*pt, *mp, bins->perm, bins->payload, L, hy,
+                                                                          ph, cpv, stb, dg);
   if ((rc = launch_check("k_p2g_payload"))) return rc;
 #define FSI_P2G(R, TT)                                                                                            \
   k_p2g_scatter<R, TT><<<grid_ctas, TT, 0, st>>>(g, *mp, bins->payload, pt->n, chunks, bins->meta, box_b, buffer, \
@@ -828,7 +816,7 @@ __global__ __launch_bounds__(128) void k_batch_p2g_payload(const FsiBatchCase* _
   const FsiBatchCase& bc = cases[blockIdx.y];
   if (!bc.active) return;
   const LatView L{bc.lbm.nx, bc.lbm.ny, bc.lbm.nz, bc.lbm.pitch};
-  const int nvb = (bc.pt.n + blockDim.x - 1) / blockDim.x;
+  const int nvb = (2 * bc.pt.n + blockDim.x - 1) / blockDim.x;  // two lanes per particle
   const float* hydro = batch_hydro(bc);
   for (int vb = blockIdx.x; vb < nvb; vb += gridDim.x)
     p2g_payload_body<true>(bc.pt, bc.mp, bc.bins.perm, bc.bins.payload, L, hydro, bc.lbm.phi, bc.cp,
@@ -891,7 +879,7 @@ extern "C" int fsi_batch_mpm_substep(FsiBatchCase* cases, const FsiBatchDims* d,
   int rc = check_batch_mpm(cases, d);
   if (rc) return rc;
   cudaStream_t st = (cudaStream_t)stream;
-  const dim3 gp(nblk(d->max_particles, 128), d->n_cases);
+  const dim3 gp(nblk(2 * (int64_t)d->max_particles, 128), d->n_cases);
   k_batch_p2g_payload<<<gp, 128, 0, st>>>(cases);
   if ((rc = launch_check("k_batch_p2g_payload"))) return rc;
   // about one CTA per chunk of the largest case (a bin's chunks hold <= 128 particles each; bins

@@ -59,12 +59,15 @@ def alone():
     return out
 
 
+@pytest.mark.parametrize("lbm_tune", [0, 2])
 @pytest.mark.parametrize("use_graph", [False, True])
-def test_batched_cases_match_single_case_runs(alone, use_graph):
+def test_batched_cases_match_single_case_runs(alone, use_graph, lbm_tune):
+    """lbm_tune 0: one cell per thread (the single runs' kernel); 2: two cells
+    per thread on the paired FP32 pipe (agrees to FP32 rounding)."""
     from mpm_lbm_b200.batch import FSIBatch
 
     cases = _cases()
-    batch = FSIBatch(capacity=4, mpm_substeps=4)
+    batch = FSIBatch(capacity=4, mpm_substeps=4, lbm_tune=lbm_tune)
     slots = [batch.add(c.make_driver()) for c in cases]
     for _ in range(STEPS):
         batch.step(use_graph=use_graph)
