@@ -321,9 +321,15 @@ def time_lbm_kernel(drv, storage, n_k1=40, reps=5):
     return k1_ms
 
 
-# DRAM bytes (read + write) of one k_lbm_step launch from an ncu capture of the
-# same workload's kernel (the profiles/ summary named below), per launch
-NCU_LBM_TRAFFIC = {}
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one k_lbm_step
+# launch, from an ncu capture of the same workload's kernel
+# (profiles/k_lbm_step_<workload>.md).  The 128x64x64 lattice fits in L2: the
+# capture (caches flushed before the launch) reads the populations from DRAM
+# and its writes stay in L2.
+NCU_LBM_TRAFFIC = {
+    ("duct_plate_128x64x64", "fp32"): 42.34e6,
+    ("duct_plate_256x128x128", "fp32"): 590.7e6,
+}
 
 
 def main():
@@ -413,8 +419,16 @@ def main():
     rows_ok = bool(np.isfinite(drv.lbm.get_stats()["rho_max"]))
     kernels_per_step = drv.graph_kernels_per_step
 
-    # ---- dominant kernel: the fused LBM step
-    k1_ms = time_lbm_kernel(drv, args.storage)
+    # ---- dominant kernel: the fused LBM step (the chosen variant; every valid variant listed)
+    from mpm_lbm_b200.autotune import lbm_candidates
+
+    chosen = drv.lbm.tune
+    variant_ms = {}
+    for t in lbm_candidates(drv.lbm):
+        drv.lbm.tune = t
+        variant_ms[int(t)] = time_lbm_kernel(drv, args.storage)
+    drv.lbm.tune = chosen
+    k1_ms = variant_ms[int(chosen)]
     pop_bytes = 2 if args.storage == "fp16" else 4
     alg_bytes = fluid_cells * 19 * 2 * pop_bytes + wl.cells * 1
     peak, peak_kind = measured_peak()
@@ -422,7 +436,8 @@ def main():
     traffic = NCU_LBM_TRAFFIC.get((wl.name, args.storage))
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic, "peak_source": f"{peak_kind} (hbm_gbs)", "kernel": "k_lbm_step",
-                "kernel_ms": k1_ms, "alg_bytes_per_launch": alg_bytes,
+                "kernel_ms": k1_ms, "kernel_variant": int(chosen),
+                "kernel_ms_by_variant": variant_ms, "alg_bytes_per_launch": alg_bytes,
                 "alg_bytes_per_cell": f"2*19*{pop_bytes} per fluid cell + 1 (flags) per cell"}
 
     # ---- end to end through the public API with host buffers

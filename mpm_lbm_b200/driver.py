@@ -204,7 +204,15 @@ class FSIDriver3D:
         self._graph = None
         self._graph_steps = 0
         step = self.lbm.step_moving_bounceback if self.config.coupling_mode == "moving_boundary" else self.lbm.step
-        self.tuning = {"lbm": tune_lbm(self.lbm, step)}
+        # time the substep the FSI step runs most: subcycled steps produce the
+        # per-direction reductions only on their last substep
+        subcycled = self.config.fsi_exchange_mode == "lbm_subcycled_per_fsi_step"
+        saved = self.lbm.dirstats_enabled
+        self.lbm.dirstats_enabled = not subcycled
+        try:
+            self.tuning = {"lbm": tune_lbm(self.lbm, step)}
+        finally:
+            self.lbm.dirstats_enabled = saved
         if self.mpm_path == "binned":
             mode = self.config.coupling_mode
             coupler = {"penalty": self.penalty_coupler, "none": None}.get(mode)

@@ -629,3 +629,27 @@ def fsi_driver_for_case(case, dtype=np.float32, substeps=None, mpm_substeps=None
     M = case.mpm_substeps if mpm_substeps is None else int(mpm_substeps)
     return OracleFSIDriver(lbm, mpm, cpl, fsi_exchange_mode="lbm_subcycled_per_fsi_step",
                            lbm_substeps_per_fsi_step=S, mpm_substeps_per_lbm_step=M)
+
+
+def fsi_driver_for_box_case(case, dtype=np.float32, threads=1):
+    """The oracle set up on a box case of ``mpm_lbm_b200.batch.BoxCase``: the
+    same walls, particles, material, unit mapping, body force and coupling
+    mode as ``case.make_driver()``, one LBM step per FSI step."""
+    cfg = case.config()
+    solid, parts = case.geometry()
+    sim = cfg.make_unified_sim_config()
+    nx, ny, nz = case.lattice
+    lbm = OracleLBM(nx, ny, nz, niu=sim.lbm_niu, relaxation_semantics=sim.lbm_relaxation_semantics, dtype=dtype)
+    lbm.threads = int(threads)
+    lbm.init_geo_array(solid)
+    lbm.init_simulation()
+    lbm.set_force(case.body_force)
+    mc = sim.make_mpm_config(gravity=cfg.gravity, **case.material())
+    mpm = OracleMPM(case.n_grid, mc.dx, mc.dt, len(parts["x"]), gravity=mc.gravity, young_modulus=mc.young_modulus,
+                    poisson_ratio=mc.poisson_ratio, p_rho=mc.p_rho, dtype=dtype)
+    mpm.init_from_numpy(parts["x"], parts["vol0"], parts["mass"], fixed_mask_np=parts["fixed"])
+    cpl = OracleCoupling(case.n_grid, sim.dx_norm, sim.lbm_dt_phys, beta_lbm=cfg.beta_lbm,
+                         penalty_force_cap=cfg.penalty_force_cap_lbm, mb_force_cap_norm=cfg.mb_force_cap_norm)
+    return OracleFSIDriver(lbm, mpm, cpl, coupling_mode=case.mode,
+                           mpm_substeps_per_lbm_step=case.mpm_substeps,
+                           dynamic_solid_threshold=cfg.dynamic_solid_threshold)
