@@ -110,26 +110,31 @@ FSI_HD void moments0(const float* F, float& rho, float& jx, float& jy, float& jz
 // the macroscopic state the reference collides with (streaming3 output,
 // fluid.py:1799-1810); (Ax,Ay,Az): body force + cell force (fluid.py:393-396).
 // Writes the post-collision populations to out (may alias F).
+// FORCED = false: the caller knows Ax = Ay = Az = 0, so the Guo term vanishes
+// (g = 0, h = F) and is not evaluated.
+template <bool FORCED = true>
 FSI_HD void mrt_collide(const float* F, float rho, float ux, float uy, float uz, float Ax, float Ay, float Az,
                         const MrtK& K, float* out) {
   // Guo term, paired: g_a = P + Q, g_b = P - Q
-  const float uA = ux * Ax + uy * Ay + uz * Az;
-  const float eA[10] = {0.f, Ax, Ay, Az, Ax + Ay, Ax - Ay, Ax + Az, Ax - Az, Ay + Az, Ay - Az};
-  const float eU[10] = {0.f, ux, uy, uz, ux + uy, ux - uy, ux + uz, ux - uz, uy + uz, uy - uz};
   float g[19];
-  g[0] = (-1.0f / 9.0f) * uA;  // w0 * (-uA/3)
+  if (FORCED) {
+    const float uA = ux * Ax + uy * Ay + uz * Az;
+    const float eA[10] = {0.f, Ax, Ay, Az, Ax + Ay, Ax - Ay, Ax + Az, Ax - Az, Ay + Az, Ay - Az};
+    const float eU[10] = {0.f, ux, uy, uz, ux + uy, ux - uy, ux + uz, ux - uz, uy + uz, uy - uz};
+    g[0] = (-1.0f / 9.0f) * uA;  // w0 * (-uA/3)
 #pragma unroll
-  for (int p = 1; p <= 9; ++p) {
-    const float w = p <= 3 ? (1.0f / 18.0f) : (1.0f / 36.0f);
-    const float P = w * ((eU[p] * eA[p]) * (1.0f / 9.0f) - uA * (1.0f / 3.0f));
-    const float Q = w * (1.0f / 3.0f) * eA[p];
-    g[2 * p - 1] = P + Q;
-    g[2 * p] = P - Q;
+    for (int p = 1; p <= 9; ++p) {
+      const float w = p <= 3 ? (1.0f / 18.0f) : (1.0f / 36.0f);
+      const float P = w * ((eU[p] * eA[p]) * (1.0f / 9.0f) - uA * (1.0f / 3.0f));
+      const float Q = w * (1.0f / 3.0f) * eA[p];
+      g[2 * p - 1] = P + Q;
+      g[2 * p] = P - Q;
+    }
   }
   // h = F + g/2 and its non-conserved moments
   float h[19];
 #pragma unroll
-  for (int s = 0; s < 19; ++s) h[s] = F[s] + 0.5f * g[s];
+  for (int s = 0; s < 19; ++s) h[s] = FORCED ? F[s] + 0.5f * g[s] : F[s];
   float sg[10], dl[10];
 #pragma unroll
   for (int p = 1; p <= 9; ++p) {
@@ -193,11 +198,11 @@ FSI_HD void mrt_collide(const float* F, float rho, float ux, float uy, float uz,
   Ov[8] = q56 + q78 + y17 - y18;
   Ev[9] = P89 - y14;
   Ov[9] = q56 - q78 + y17 + y18;
-  out[0] = F[0] + g[0] - (y0 - y1 + y2);
+  out[0] = (FORCED ? F[0] + g[0] : F[0]) - (y0 - y1 + y2);
 #pragma unroll
   for (int p = 1; p <= 9; ++p) {
-    const float a = F[2 * p - 1] + g[2 * p - 1];
-    const float b = F[2 * p] + g[2 * p];
+    const float a = FORCED ? F[2 * p - 1] + g[2 * p - 1] : F[2 * p - 1];
+    const float b = FORCED ? F[2 * p] + g[2 * p] : F[2 * p];
     out[2 * p - 1] = a - (Ev[p] + Ov[p]);
     out[2 * p] = b - (Ev[p] - Ov[p]);
   }
@@ -232,36 +237,48 @@ __device__ __forceinline__ void moments0_2(const float2* F, float2& rho, float2&
   jz = add2(add2(d[3], sub2(d[6], d[7])), sub2(d[8], d[9]));
 }
 
+// FORCED = false: the caller knows the force vanishes for both cells (g = 0)
+template <bool FORCED = true>
 __device__ __forceinline__ void mrt_collide2(const float2* F, float2 rho, float2 ux, float2 uy, float2 uz, float2 Ax,
                                              float2 Ay, float2 Az, const MrtK& K, float2* out) {
   (void)rho;
-  // Guo term, paired over directions: g_a = P + Q, g_b = P - Q
-  const float2 uA = fma2(uz, Az, fma2(uy, Ay, mul2(ux, Ax)));
-  const float2 eA[10] = {p2(0.f), Ax, Ay, Az, add2(Ax, Ay), sub2(Ax, Ay), add2(Ax, Az), sub2(Ax, Az), add2(Ay, Az),
-                         sub2(Ay, Az)};
-  const float2 eU[10] = {p2(0.f), ux, uy, uz, add2(ux, uy), sub2(ux, uy), add2(ux, uz), sub2(ux, uz), add2(uy, uz),
-                         sub2(uy, uz)};
-  const float2 uA3 = mul2(uA, p2(1.0f / 3.0f));
   // Fg = F + g (kept), and h = F + g/2 reduced at once to its pair sums / differences
   float2 Fg[19];
   float2 sg[10], dl[10];
-  {
-    const float2 g0 = mul2(p2(-1.0f / 9.0f), uA);
-    Fg[0] = add2(F[0], g0);
-  }
-  const float2 h0 = fma2(p2(-1.0f / 18.0f), uA, F[0]);
+  float2 h0;
+  if (FORCED) {
+    // Guo term, paired over directions: g_a = P + Q, g_b = P - Q
+    const float2 uA = fma2(uz, Az, fma2(uy, Ay, mul2(ux, Ax)));
+    const float2 eA[10] = {p2(0.f), Ax, Ay, Az, add2(Ax, Ay), sub2(Ax, Ay), add2(Ax, Az), sub2(Ax, Az), add2(Ay, Az),
+                           sub2(Ay, Az)};
+    const float2 eU[10] = {p2(0.f), ux, uy, uz, add2(ux, uy), sub2(ux, uy), add2(ux, uz), sub2(ux, uz), add2(uy, uz),
+                           sub2(uy, uz)};
+    const float2 uA3 = mul2(uA, p2(1.0f / 3.0f));
+    Fg[0] = add2(F[0], mul2(p2(-1.0f / 9.0f), uA));
+    h0 = fma2(p2(-1.0f / 18.0f), uA, F[0]);
 #pragma unroll
-  for (int p = 1; p <= 9; ++p) {
-    const float w = p <= 3 ? (1.0f / 18.0f) : (1.0f / 36.0f);
-    const float2 P = mul2(p2(w), sub2(mul2(mul2(eU[p], eA[p]), p2(1.0f / 9.0f)), uA3));
-    const float2 Q = mul2(p2(w * (1.0f / 3.0f)), eA[p]);
-    const float2 ga = add2(P, Q), gb = sub2(P, Q);
-    Fg[2 * p - 1] = add2(F[2 * p - 1], ga);
-    Fg[2 * p] = add2(F[2 * p], gb);
-    const float2 ha = fma2(p2(0.5f), ga, F[2 * p - 1]);
-    const float2 hb = fma2(p2(0.5f), gb, F[2 * p]);
-    sg[p] = add2(ha, hb);
-    dl[p] = sub2(ha, hb);
+    for (int p = 1; p <= 9; ++p) {
+      const float w = p <= 3 ? (1.0f / 18.0f) : (1.0f / 36.0f);
+      const float2 P = mul2(p2(w), sub2(mul2(mul2(eU[p], eA[p]), p2(1.0f / 9.0f)), uA3));
+      const float2 Q = mul2(p2(w * (1.0f / 3.0f)), eA[p]);
+      const float2 ga = add2(P, Q), gb = sub2(P, Q);
+      Fg[2 * p - 1] = add2(F[2 * p - 1], ga);
+      Fg[2 * p] = add2(F[2 * p], gb);
+      const float2 ha = fma2(p2(0.5f), ga, F[2 * p - 1]);
+      const float2 hb = fma2(p2(0.5f), gb, F[2 * p]);
+      sg[p] = add2(ha, hb);
+      dl[p] = sub2(ha, hb);
+    }
+  } else {
+    Fg[0] = F[0];
+    h0 = F[0];
+#pragma unroll
+    for (int p = 1; p <= 9; ++p) {
+      Fg[2 * p - 1] = F[2 * p - 1];
+      Fg[2 * p] = F[2 * p];
+      sg[p] = add2(F[2 * p - 1], F[2 * p]);
+      dl[p] = sub2(F[2 * p - 1], F[2 * p]);
+    }
   }
   const float2 Sa = add2(add2(sg[1], sg[2]), sg[3]);
   const float2 Sxy = add2(sg[4], sg[5]), Sxz = add2(sg[6], sg[7]), Syz = add2(sg[8], sg[9]);

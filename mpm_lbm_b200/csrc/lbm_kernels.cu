@@ -596,8 +596,14 @@ __device__ __forceinline__ void lbm_step_tile(const Case& c, int bx, int by, Dir
   if (valid && nfl != fl) c.s.flags[cell] = nfl;
 
   // ---- collision (fluid.py:398-413) and AA streaming
+  // the Guo term only where some fluid cell of the warp is forced (body force,
+  // penalty or cell force); with no force it vanishes exactly
+  const bool forced = __any_sync(kFull, fluid && (Ax != 0.f || Ay != 0.f || Az != 0.f));
   if (fluid) {
-    mrt_collide(F, rho, ux, uy, uz, Ax, Ay, Az, c.K, F);
+    if (forced)
+      mrt_collide<true>(F, rho, ux, uy, uz, Ax, Ay, Az, c.K, F);
+    else
+      mrt_collide<false>(F, rho, ux, uy, uz, Ax, Ay, Az, c.K, F);
     if (nb == 0) {
       if (!ODD) {
 #pragma unroll
@@ -998,8 +1004,13 @@ __device__ __forceinline__ void lbm_step_tile2(const Case& c, int bx, int by, Di
     *reinterpret_cast<uint16_t*>(c.s.flags + cell0) = (uint16_t)(nfl[0] | (nfl[1] << 8));
 
   // ---- collision (fluid.py:398-413) and AA streaming
+  const bool forced = __any_sync(kFull, (fluid0 && (Ax.x != 0.f || Ay.x != 0.f || Az.x != 0.f)) ||
+                                           (fluid1 && (Ax.y != 0.f || Ay.y != 0.f || Az.y != 0.f)));
   if (fluid0 || fluid1) {
-    mrt_collide2(F, rho, ux, uy, uz, Ax, Ay, Az, c.K, F);
+    if (forced)
+      mrt_collide2<true>(F, rho, ux, uy, uz, Ax, Ay, Az, c.K, F);
+    else
+      mrt_collide2<false>(F, rho, ux, uy, uz, Ax, Ay, Az, c.K, F);
     if (plain) {
       // a solid member of the pair keeps its slots: write the fluid member alone
       const bool both = fluid0 && fluid1;

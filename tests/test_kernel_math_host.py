@@ -21,6 +21,10 @@ extern "C" void host_collide(const float* F, float rho, const float* u, const fl
   const fsi::MrtK K = fsi::make_mrt_k(s_v, s_o);
   fsi::mrt_collide(F, rho, u[0], u[1], u[2], A[0], A[1], A[2], K, out);
 }
+extern "C" void host_collide_unforced(const float* F, float rho, const float* u, float s_v, float s_o, float* out) {
+  const fsi::MrtK K = fsi::make_mrt_k(s_v, s_o);
+  fsi::mrt_collide<false>(F, rho, u[0], u[1], u[2], 0.f, 0.f, 0.f, K, out);
+}
 extern "C" void host_moments(const float* F, float* m) { fsi::moments0(F, m[0], m[1], m[2], m[3]); }
 extern "C" void host_polar(const double* F, double* R) { fsi::polar_rotation_d(F, R); }
 extern "C" void host_polar_jacobi(const double* F, double* R) { fsi::polar_rotation_jacobi_d(F, R); }
@@ -124,3 +128,21 @@ def test_polar_newton_agrees_with_jacobi(hostlib):
         Rref = F @ U @ np.diag(w ** -0.5) @ U.T
         np.testing.assert_allclose(R, Rref, atol=1e-6)
     assert used > 1500
+
+
+def test_unforced_collision_equals_forced_with_zero_force(hostlib):
+    """mrt_collide<false> (no Guo term evaluated) gives the same populations as
+    the forced form with a zero force, bit for bit."""
+    rng = np.random.default_rng(21)
+    w = np.array([1 / 3] + [1 / 18] * 6 + [1 / 36] * 12, np.float32)
+    for _ in range(200):
+        F = (w * (1.0 + 0.05 * rng.standard_normal(19))).astype(np.float32)
+        u = (0.05 * rng.standard_normal(3)).astype(np.float32)
+        rho = np.float32(F.sum())
+        A = np.zeros(3, np.float32)
+        a, b = np.zeros(19, np.float32), np.zeros(19, np.float32)
+        hostlib.host_collide(P(F), ctypes.c_float(rho), P(u), P(A), ctypes.c_float(1 / 0.6),
+                             ctypes.c_float(1.4), P(a))
+        hostlib.host_collide_unforced(P(F), ctypes.c_float(rho), P(u), ctypes.c_float(1 / 0.6),
+                                      ctypes.c_float(1.4), P(b))
+        np.testing.assert_array_equal(a, b)
