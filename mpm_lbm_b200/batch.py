@@ -161,8 +161,8 @@ class FSIBatch:
     """Up to `capacity` independent FSI cases, advanced together."""
 
     def __init__(self, capacity, storage="fp32", mpm_substeps=10, device="cuda", mpm_tune=0, lbm_tune=None):
-        """lbm_tune: FSI_TUNE_LBM_OCC3 (0) or FSI_TUNE_LBM_PAIR (2, every case's nx
-        even); None picks the paired kernel while every case allows it."""
+        """lbm_tune: FSI_TUNE_LBM_OCC3 (0, default) or FSI_TUNE_LBM_PAIR (2, every
+        case's nx even)."""
         self.capacity = int(capacity)
         self.storage = storage
         self.M = int(mpm_substeps)
@@ -279,7 +279,7 @@ class FSIBatch:
         d.mpm_tune = self.mpm_tune
         all_even = all(x.lbm.nx % 2 == 0 for x in act)
         if self.lbm_tune is None:
-            d.lbm_tune = FSI_TUNE_LBM_PAIR if all_even else FSI_TUNE_LBM_OCC3
+            d.lbm_tune = FSI_TUNE_LBM_OCC3  # the faster of the two on B200 (see profiles/)
         else:
             if self.lbm_tune == FSI_TUNE_LBM_PAIR and not all_even:
                 raise ValueError("the paired LBM kernel needs an even nx in every case")

@@ -5,6 +5,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <string>
+#include <utility>
 
 #include "../../include/fsi_b200.h"
 
@@ -33,6 +34,16 @@ inline int invalid(const std::string& msg) {
 }
 
 #if defined(__CUDACC__)
+// Programmatic dependent launch (sm_90+): a kernel launched with
+// launch_pdl() may be scheduled while the kernel before it in the stream is
+// still running; it must call griddep_wait() before touching memory that
+// kernel writes (the wait returns once that grid has completed and its writes
+// are visible; in a kernel launched normally it returns at once).
+// griddep_launch() lets the next such kernel be scheduled; every CTA calls it
+// after its own wait, so the chain never runs more than one grid ahead.
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void griddep_launch() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 // max of non-negative floats through their integer bit patterns
 __device__ __forceinline__ void atomic_max_nonneg(float* addr, float v) {
   atomicMax(reinterpret_cast<int*>(addr), __float_as_int(v));
@@ -54,6 +65,25 @@ __device__ __forceinline__ double warp_sum_d(double v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
+}
+#endif
+
+#if defined(__CUDACC__)
+// launch with programmatic stream serialization (see griddep_wait)
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                              Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
 }
 #endif
 

@@ -659,6 +659,8 @@ __device__ __forceinline__ void lbm_step_tile(const Case& c, int bx, int by, Dir
 template <bool ODD, bool H, bool MOVING, bool BCW, bool PEN, int MINB>
 __global__ void __launch_bounds__(256, MINB) k_lbm_step(const Case c) {
   __shared__ DirAcc acc;
+  griddep_wait();
+  griddep_launch();
   lbm_step_tile<ODD, H, MOVING, BCW, PEN>(c, blockIdx.x, blockIdx.y, acc);
 }
 
@@ -796,25 +798,6 @@ __device__ __forceinline__ bool penalty_cell(const Case& c, int cell, bool fluid
   return true;
 }
 
-// The paired kernel keeps its rare paths (cells next to a solid, the face
-// cells of open boundaries) out of line, so that the instruction footprint of
-// the common path stays small.
-template <bool ODD, bool H, bool MOVING>
-__device__ __noinline__ void store_near_solid_nl(const Case& c, const Nbh& n, int cell, uint32_t nb, float rho,
-                                                 const float* out) {
-  store_near_solid<ODD, H, MOVING>(c, n, cell, nb, rho, out);
-}
-
-template <bool ODD, bool H>
-__device__ __noinline__ void load_near_solid_nl(const Case& c, const Nbh& n, int cell, uint32_t nb, float* F) {
-  set_near_solid_loads<ODD, H>(c, n, cell, nb, F);
-}
-
-template <int SIDE>
-__device__ __noinline__ void bc_face_warp2_nl(const Case& c, int lane, int row, uint8_t fl0, uint8_t fl1, float2* F) {
-  bc_face_warp2<SIDE>(c, lane, row, fl0, fl1, F);
-}
-
 template <bool ODD, bool H, bool MOVING, bool BCW, bool PEN>
 __device__ __forceinline__ void lbm_step_tile2(const Case& c, int bx, int by, DirAcc& acc) {
   const int lane = threadIdx.x;
@@ -882,8 +865,8 @@ __device__ __forceinline__ void lbm_step_tile2(const Case& c, int bx, int by, Di
       float a[19], b[19];
 #pragma unroll
       for (int s = 0; s < 19; ++s) a[s] = b[s] = 0.f;
-      if (fluid0) load_near_solid_nl<ODD, H>(c, n0, cell0, nb0, a);
-      if (fluid1) load_near_solid_nl<ODD, H>(c, n1, cell0 + 1, nb1, b);
+      if (fluid0) set_near_solid_loads<ODD, H>(c, n0, cell0, nb0, a);
+      if (fluid1) set_near_solid_loads<ODD, H>(c, n1, cell0 + 1, nb1, b);
 #pragma unroll
       for (int s = 0; s < 19; ++s) F[s] = make_float2(a[s], b[s]);
     }
@@ -894,8 +877,8 @@ __device__ __forceinline__ void lbm_step_tile2(const Case& c, int bx, int by, Di
 
   // ---- pending open boundary of the previous step (fluid.py:538-569)
   if (BCW && c.c.bc_pending && inrow) {
-    if (c.p.bc_left != 0 && bx == 0) bc_face_warp2_nl<0>(c, lane, row, fl[0], fl[1], F);
-    if (c.p.bc_right != 0 && bx == ((nx - 1) >> 6)) bc_face_warp2_nl<1>(c, lane, row, fl[0], fl[1], F);
+    if (c.p.bc_left != 0 && bx == 0) bc_face_warp2<0>(c, lane, row, fl[0], fl[1], F);
+    if (c.p.bc_right != 0 && bx == ((nx - 1) >> 6)) bc_face_warp2<1>(c, lane, row, fl[0], fl[1], F);
   }
 
   // ---- macroscopic state the collision uses (streaming3, fluid.py:1794-1814)
@@ -1042,7 +1025,7 @@ __device__ __forceinline__ void lbm_step_tile2(const Case& c, int bx, int by, Di
         }
       }
     } else {
-#pragma unroll 1
+#pragma unroll
       for (int i = 0; i < 2; ++i) {
         if (!(i ? fluid1 : fluid0)) continue;
         float out[19];
@@ -1052,7 +1035,7 @@ __device__ __forceinline__ void lbm_step_tile2(const Case& c, int bx, int by, Di
         const Nbh& n = i ? n1 : n0;
         const int cell = cell0 + i;
         if (nb) {
-          store_near_solid_nl<ODD, H, MOVING>(c, n, cell, nb, comp(rho, i), out);
+          store_near_solid<ODD, H, MOVING>(c, n, cell, nb, comp(rho, i), out);
         } else if (!ODD) {
 #pragma unroll
           for (int s = 0; s < 19; ++s) stp<H>(c, kOpp(s), cell, out[s]);
@@ -1114,8 +1097,10 @@ __device__ __forceinline__ void lbm_step_tile2(const Case& c, int bx, int by, Di
 }
 
 template <bool ODD, bool H, bool MOVING, bool BCW, bool PEN>
-__global__ void __launch_bounds__(128, 4) k_lbm_step2(const __grid_constant__ Case c) {
+__global__ void __launch_bounds__(128, 3) k_lbm_step2(const __grid_constant__ Case c) {
   __shared__ DirAcc acc;
+  griddep_wait();
+  griddep_launch();
   lbm_step_tile2<ODD, H, MOVING, BCW, PEN>(c, blockIdx.x, blockIdx.y, acc);
 }
 
@@ -1585,15 +1570,19 @@ extern "C" int fsi_lbm_substep(const FsiLbmState* s, const FsiLbmParams* p, cons
   if (rc) return rc;
   if (!ctl) return invalid("null step control");
   cudaStream_t st = (cudaStream_t)stream;
+  bool memset_before = false;
   if (ctl->bc_pending && p->limiter) {
     rc = cuda_check(cudaMemsetAsync(s->diag->ob_step, 0, sizeof(s->diag->ob_step), st), "memset ob_step");
     if (rc) return rc;
+    memset_before = true;
   }
   if ((ctl->mode & FSI_MODE_DIRSTATS) && (ctl->mode & FSI_MODE_MOVING_BB)) {
     rc = cuda_check(cudaMemsetAsync(s->diag, 0, offsetof(FsiLbmDiag, accum_norm_max), st), "memset dirstats");
     if (rc) return rc;
+    memset_before = true;
   }
   if (ctl->mode & FSI_MODE_PENALTY) {
+    memset_before = true;
     rc = cuda_check(cudaMemsetAsync(&s->diag->penalty_active, 0,
                                     offsetof(FsiLbmDiag, change_count) - offsetof(FsiLbmDiag, penalty_active), st),
                     "memset penalty stats");
@@ -1609,13 +1598,23 @@ extern "C" int fsi_lbm_substep(const FsiLbmState* s, const FsiLbmParams* p, cons
   const dim3 grid2((unsigned)((s->nx + 63) / 64), (unsigned)((s->ny * s->nz + 3) / 4));
   const dim3 block2(32, 4);
   if (p->tune == FSI_TUNE_LBM_PAIR && !pair_ok(s, p)) return invalid("FSI_TUNE_LBM_PAIR needs an even nx (and nx % 64 != 2 with open boundaries)");
+  // back-to-back steps overlap the launch of the next with the tail of the
+  // previous (programmatic dependent launch) unless a memset came in between
+  const bool pdl = !memset_before;
+  cudaError_t lerr = cudaSuccess;
+#define FSI_KLAUNCH(K, G, BL)                          \
+  if (pdl)                                             \
+    lerr = launch_pdl(K, G, BL, 0, st, c);             \
+  else                                                 \
+    K<<<G, BL, 0, st>>>(c)
 #define FSI_LAUNCH(O, HH, M, B, PN)                                        \
-  if (p->tune == FSI_TUNE_LBM_PAIR)                                        \
-    k_lbm_step2<O, HH, M, B, PN><<<grid2, block2, 0, st>>>(c);             \
-  else if (p->tune == FSI_TUNE_LBM_OCC4)                                   \
-    k_lbm_step<O, HH, M, B, PN, 4><<<grid, block, 0, st>>>(c);             \
-  else                                                                     \
-    k_lbm_step<O, HH, M, B, PN, 3><<<grid, block, 0, st>>>(c)
+  if (p->tune == FSI_TUNE_LBM_PAIR) {                                      \
+    FSI_KLAUNCH((k_lbm_step2<O, HH, M, B, PN>), grid2, block2);            \
+  } else if (p->tune == FSI_TUNE_LBM_OCC4) {                               \
+    FSI_KLAUNCH((k_lbm_step<O, HH, M, B, PN, 4>), grid, block);            \
+  } else {                                                                 \
+    FSI_KLAUNCH((k_lbm_step<O, HH, M, B, PN, 3>), grid, block);            \
+  }
 #define FSI_BY_H(O, M, B, PN) \
   if (h) { FSI_LAUNCH(O, true, M, B, PN); } else { FSI_LAUNCH(O, false, M, B, PN); }
 #define FSI_BY_O(M, B, PN) \
@@ -1630,6 +1629,8 @@ extern "C" int fsi_lbm_substep(const FsiLbmState* s, const FsiLbmParams* p, cons
 #undef FSI_BY_O
 #undef FSI_BY_H
 #undef FSI_LAUNCH
+#undef FSI_KLAUNCH
+  if ((rc = cuda_check(lerr, "k_lbm_step (launch)"))) return rc;
   return launch_check("k_lbm_step");
 }
 

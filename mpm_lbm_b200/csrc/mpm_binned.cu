@@ -324,6 +324,8 @@ __global__ __launch_bounds__(128) void k_p2g_payload(FsiParticles pt, FsiMpmPara
                                                      LatView L, const float* __restrict__ hydro,
                                                      const float* __restrict__ phi, FsiCouplingParams cp,
                                                      FsiCouplingStats* st, const FsiLbmDiag* diag) {
+  griddep_wait();
+  griddep_launch();
   p2g_payload_body<REACT>(pt, mp, perm, payload, L, hydro, phi, cp, st, diag, blockIdx.x, gridDim.x);
 }
 
@@ -474,6 +476,8 @@ template <bool REACT, int T>
 __global__ __launch_bounds__(T, T == 384 ? 1 : 4) void k_p2g_scatter(FsiGrid g, FsiMpmParams mp, const float* __restrict__ payload,
                                                    int n, const int2* __restrict__ chunks, int32_t* meta,
                                                    int32_t* box, int buf, FsiCouplingStats* st) {
+  griddep_wait();
+  griddep_launch();
   p2g_scatter_body<REACT, T>(g, mp, payload, n, chunks, meta, box, buf, st, blockIdx.x, gridDim.x);
 }
 
@@ -606,6 +610,8 @@ __global__ __launch_bounds__(T) void k_g2p_binned(FsiParticles pt, FsiGrid g, Fs
                                                   const int32_t* __restrict__ box_b,
                                                   const int32_t* __restrict__ box_o, int buf,
                                                   FsiCouplingStats* st_other) {
+  griddep_wait();
+  griddep_launch();
   g2p_binned_body<T>(pt, g, go, mp, perm, chunks, meta, box_b, box_o, buf, st_other, blockIdx.x, gridDim.x);
 }
 
@@ -742,29 +748,35 @@ extern "C" int fsi_mpm_substep_binned(const FsiParticles* pt, const FsiGrid grid
   const FsiCouplingParams cpv = cp ? *cp : FsiCouplingParams{};
   FsiCouplingStats* stb = cp ? &stats[buffer] : nullptr;
   const FsiLbmDiag* dg = cp ? s->diag : nullptr;
+  // the three kernels of a substep, and the substeps, follow each other with
+  // programmatic dependent launch (each waits for its predecessor's writes)
+  const unsigned gp = nblk(2 * (int64_t)pt->n, 128);
+  cudaError_t lerr;
   if (cp)
-    k_p2g_payload<true><<<nblk(2 * (int64_t)pt->n, 128), 128, 0, st>>>(*pt, *mp, bins->perm, bins->payload, L, hy,
-                                                                         ph, cpv, stb, dg);
+    lerr = launch_pdl(k_p2g_payload<true>, dim3(gp), dim3(128), 0, st, *pt, *mp, (const int32_t*)bins->perm,
+                      bins->payload, L, hy, ph, cpv, stb, dg);
   else
-    k_p2g_payload<false><<<nblk(2 * (int64_t)pt->n, 128), 128, 0, st>>>(*pt, *mp, bins->perm, bins->payload, L, hy,
-                                                                          ph, cpv, stb, dg);
-  if ((rc = launch_check("k_p2g_payload"))) return rc;
-#define FSI_P2G(R, TT)                                                                                            \
-  k_p2g_scatter<R, TT><<<grid_ctas, TT, 0, st>>>(g, *mp, bins->payload, pt->n, chunks, bins->meta, box_b, buffer, \
-                                                 stb)
+    lerr = launch_pdl(k_p2g_payload<false>, dim3(gp), dim3(128), 0, st, *pt, *mp, (const int32_t*)bins->perm,
+                      bins->payload, L, hy, ph, cpv, stb, dg);
+  if ((rc = cuda_check(lerr, "k_p2g_payload (launch)")) || (rc = launch_check("k_p2g_payload"))) return rc;
+#define FSI_P2G(R, TT)                                                                                        \
+  lerr = launch_pdl(k_p2g_scatter<R, TT>, dim3(grid_ctas), dim3(TT), 0, st, g, *mp,                         \
+                    (const float*)bins->payload, pt->n, chunks, bins->meta, box_b, buffer, stb)
   if (cp) {
     if (T == 384) FSI_P2G(true, 384); else FSI_P2G(true, 128);
   } else {
     if (T == 384) FSI_P2G(false, 384); else FSI_P2G(false, 128);
   }
 #undef FSI_P2G
-  if ((rc = launch_check("k_p2g_scatter"))) return rc;
+  if ((rc = cuda_check(lerr, "k_p2g_scatter (launch)")) || (rc = launch_check("k_p2g_scatter"))) return rc;
   FsiCouplingStats* sto = cp ? &stats[1 - buffer] : nullptr;
-#define FSI_G2P(TT)                                                                                                \
-  k_g2p_binned<TT><<<grid_ctas, TT, 0, st>>>(*pt, g, go, *mp, bins->perm, chunks, bins->meta, box_b, box_o, buffer, \
-                                             sto)
+#define FSI_G2P(TT)                                                                                       \
+  lerr = launch_pdl(k_g2p_binned<TT>, dim3(grid_ctas), dim3(TT), 0, st, *pt, g, go, *mp,                   \
+                    (const int32_t*)bins->perm, chunks, (const int32_t*)bins->meta, (const int32_t*)box_b, \
+                    (const int32_t*)box_o, buffer, sto)
   if (TG == 512) FSI_G2P(512); else if (TG == 256) FSI_G2P(256); else FSI_G2P(128);
 #undef FSI_G2P
+  if ((rc = cuda_check(lerr, "k_g2p_binned (launch)"))) return rc;
   return launch_check("k_g2p_binned");
 }
 
