@@ -253,7 +253,7 @@ def run_batched(args):
            "higher_is_better": True, "dtype": "f32" if args.storage == "fp32" else "f16-storage/f32-compute",
            "data": "synthetic", "config": {"workload": f"batch_{len(cases)}_box_cases", "cases": len(cases),
                                            "cells": cells, "kernels_per_step": batch.graph_kernels,
-                                           "lbm_tune": batch.dims.lbm_tune, "mpm_tune": batch.dims.mpm_tune}}
+                                           "lbm_tune": batch.dims.lbm_tune}}
     del batch
     if not args.no_one_by_one:
         tot = 0.0
@@ -321,6 +321,33 @@ def time_lbm_kernel(drv, storage, n_k1=40, reps=5):
     return k1_ms
 
 
+def time_mpm_phase(drv, reps=5):
+    """Average duration of one binned MPM substep with its reaction transfer:
+    a CUDA graph of the FSI step's MPM phase (re-binning, then the M substeps
+    of fsi_mpm_substeps_binned), replayed reps times between events."""
+    import torch
+
+    solid, lbm = drv.solid, drv.lbm
+    coupler = drv.mb_coupler if drv.mb_coupler is not None else drv.link_area_coupler
+    M = drv.config.mpm_substeps_per_lbm_step
+    stream = torch.cuda.current_stream()
+    graph = torch.cuda.CUDAGraph()
+    torch.cuda.synchronize()
+    with torch.cuda.graph(graph):
+        solid.rebin()
+        solid.substeps_binned(M, coupler, lbm)
+    graph.replay()  # warm
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        graph.replay()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    del graph
+    return e0.elapsed_time(e1) / (reps * M)
+
+
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one k_lbm_step
 # launch, from an ncu capture of the same workload's kernel
 # (profiles/k_lbm_step_<workload>.md).  The 128x64x64 lattice fits in L2: the
@@ -343,7 +370,6 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="default launch variants")
     ap.add_argument("--lbm-tune", type=int, default=None, help="fixed FsiLbmParams.tune (no autotuning)")
-    ap.add_argument("--mpm-tune", type=int, default=None, help="fixed FsiMpmParams.tune (no autotuning)")
     ap.add_argument("--ref-substeps", type=int, default=30,
                     help="LBM substeps per timed step of the reference arm (bounded CPU sample)")
     ap.add_argument("--form", default="single", choices=["single", "batched", "served"],
@@ -375,15 +401,11 @@ def main():
         drv.step_once()
     torch.cuda.synchronize()
     tuning = None
-    if args.lbm_tune is not None or args.mpm_tune is not None:
-        # fixed launch variants (profiling a given variant); the step graph is recaptured
+    if args.lbm_tune is not None:
+        # a fixed launch variant (profiling a given variant); the step graph is recaptured
         drv._graph = None
-        if args.lbm_tune is not None:
-            drv.lbm.tune = args.lbm_tune
-        if args.mpm_tune is not None:
-            drv.solid.params.tune = args.mpm_tune
-        tuning = {"lbm": {"choice": drv.lbm.tune, "ms_per_substep": None},
-                  "mpm": {"choice": drv.solid.params.tune, "ms_per_substep": None}}
+        drv.lbm.tune = args.lbm_tune
+        tuning = {"lbm": {"choice": drv.lbm.tune, "ms_per_substep": None}}
         for _ in range(2):
             drv.step_once()
         torch.cuda.synchronize()
@@ -440,6 +462,11 @@ def main():
                 "kernel_ms_by_variant": variant_ms, "alg_bytes_per_launch": alg_bytes,
                 "alg_bytes_per_cell": f"2*19*{pop_bytes} per fluid cell + 1 (flags) per cell"}
 
+    # ---- the MPM phase (second in the step after the LBM substeps)
+    mpm_ms = time_mpm_phase(drv)
+    mpm = {"kernel": "k_mpm_seq", "ms_per_substep": mpm_ms, "launches_per_substep": (wl.M + 2) / wl.M,
+           "share_of_step": wl.M * mpm_ms / ms_step}
+
     # ---- end to end through the public API with host buffers
     pinned_in = torch.tensor([wl.case.u_in, 0.0, 0.0], dtype=torch.float32).pin_memory()
     n = drv.solid.n_particles
@@ -469,12 +496,11 @@ def main():
                    "population_storage": args.storage,
                    "l2": "flushed (256 MB write) between timed FSI steps", "cuda_graph": True,
                    "launch_variants": None if tuning is None else
-                   {"lbm_tune": tuning["lbm"]["choice"], "mpm_tune": tuning.get("mpm", {}).get("choice"),
-                    "lbm_ms_per_substep": tuning["lbm"]["ms_per_substep"],
-                    "mpm_ms_per_substep": tuning.get("mpm", {}).get("ms_per_substep")},
+                   {"lbm_tune": tuning["lbm"]["choice"], "lbm_ms_per_substep": tuning["lbm"]["ms_per_substep"]},
                    "parallelism": f"replicas x{ws}"},
         "particle_updates_per_s": ws * args.steps * wl.M * n / (total_ms * 1e-3),
         "roofline": roofline,
+        "mpm": mpm,
         "clocks": clk.summary(),
         "e2e": {"value": e2e_value, "unit": "MLUPS", "h2d_bytes_per_step": 12, "d2h_bytes_per_step": 12 * n,
                 "api": "FSIDriver3D.step_once + inlet velocity H2D from pinned host + particle positions D2H"},

@@ -218,20 +218,9 @@ typedef struct FsiMpmParams {
   float damping;     /* >0 enables particle_velocity_post_g2p damping */
   int32_t bound;
   int32_t lock_z;
-  int32_t tune;      /* FSI_TUNE_P2G_* of the scatter | FSI_TUNE_MPM_* of the gather << 2 */
+  int32_t pad;
 } FsiMpmParams;
 
-/* launch variants of fsi_mpm_substep_binned (FsiMpmParams.tune = scatter
- * variant | gather variant << 2); the other MPM entry points ignore it. */
-enum {
-  /* P2G scatter: lanes per particle of a chunk CTA */
-  FSI_TUNE_P2G_T128 = 0,  /* 128 threads: 4 warps, each scattering one particle at a time (default) */
-  FSI_TUNE_P2G_T384 = 1,  /* 384 threads: 12 warps */
-  /* G2P gather: threads per chunk CTA */
-  FSI_TUNE_MPM_T128 = 0,  /* 128 threads: one lane per particle (default) */
-  FSI_TUNE_MPM_T256 = 1,  /* 256 threads: two lanes per particle */
-  FSI_TUNE_MPM_T512 = 2,  /* 512 threads: four lanes per particle */
-};
 
 typedef struct FsiCouplingParams {
   float inv_dx_norm, cell_volume_norm, vel_scale, eps_mass;
@@ -278,37 +267,35 @@ int fsi_mpm_grid_update(const FsiGrid* g, const FsiMpmParams* mp, void* stream);
  * F update, damping / z-lock controls, fixed-base reset. */
 int fsi_mpm_g2p(const FsiParticles* pt, const FsiGrid* g, const FsiMpmParams* mp, void* stream);
 
-/* ---- binned MPM substep --------------------------------------------------
+/* ---- binned MPM substeps ------------------------------------------------
  * The same substep as clear -> p2g -> reaction -> grid_update -> g2p above
  * (one call of MPMSolid3D.substep plus the coupler's reaction transfer, as
  * driven by fsi_driver.py's MPM loops), organised around particle bins:
  *   - fsi_mpm_bin sorts particle ids by 4x4x4-cell block of their B-spline
  *     base cell and cuts every bin into chunks of at most FSI_BIN_CHUNK
  *     particles (bins may go stale between calls: that costs speed only);
- *   - fsi_mpm_substep_binned scatters each chunk into a shared-memory tile
- *     covering the chunk's stencil box and flushes the tile with one atomic
- *     per touched node value, then gathers with the grid update evaluated per
- *     node while staging.  It alternates between two grid buffers: a substep
- *     with buffer b leaves momentum (not velocity), mass and f_ext in grid[b]
- *     and zeroes the boxes recorded by the previous substep in grid[1 - b],
- *     so no dense pass over the grid is made. */
+ *   - fsi_mpm_substeps_binned runs substeps chunk by chunk: each chunk is
+ *     scattered into a shared-memory tile covering its stencil box and the
+ *     tile is flushed with one atomic per touched node value; the gather
+ *     evaluates the grid update per node while staging the chunk's box.  A
+ *     substep leaves momentum (not velocity), mass and f_ext in its grid
+ *     buffer; three buffers rotate, and only the boxes recorded for a buffer
+ *     are zeroed before it is reused, so no dense pass over the grid is made. */
 #define FSI_BIN_CHUNK 128
 #define FSI_BIN_EDGE 4
-#define FSI_MPM_PAYLOAD_ROWS 32
 
 /* count, start and chunk must be 16-byte aligned */
 typedef struct FsiMpmBins {
   int32_t n_bins;       /* ceil(n_grid / FSI_BIN_EDGE)^3 */
-  int32_t max_chunks;   /* capacity of chunk[] and of each half of box[] */
+  int32_t max_chunks;   /* capacity of chunk[] and of each third of box[] */
   int32_t* key;         /* [n_particles] bin of each particle */
   int32_t* count;       /* [n_bins] zero before the first fsi_mpm_bin; kept zero after each call */
   int32_t* start;       /* [n_bins] end offset of each bin in perm after fsi_mpm_bin */
   int32_t* perm;        /* [n_particles] particle ids ordered by bin */
   int32_t* chunk;       /* [max_chunks][2] (first slot in perm, particle count) */
-  int32_t* box;         /* [2][max_chunks][6] node box (lo xyz, hi xyz) touched per chunk and buffer */
-  int32_t* meta;        /* [4] chunk count, records in box[0], records in box[1], overflowed chunks;
-                           zero before the first call */
-  float* payload;       /* [FSI_MPM_PAYLOAD_ROWS][n_particles] scratch: per-particle P2G data in bin order */
+  int32_t* box;         /* [3][max_chunks][6] node box (lo xyz, hi xyz) touched per chunk and buffer */
+  int32_t* meta;        /* [8] chunk count, records in box[0..2], chunks scattered without the tile,
+                           buffer 0..2 holds unzeroed boxes; zero before the first call */
 } FsiMpmBins;
 
 /* n_bins and max_chunks for a particle count and grid edge */
@@ -318,14 +305,21 @@ int fsi_mpm_bins_layout(int32_t n_particles, int32_t n_grid, int32_t* n_bins, in
 int fsi_mpm_bin(const FsiParticles* pt, const FsiGrid* g, const FsiMpmParams* mp, const FsiMpmBins* bins,
                 void* stream);
 
-/* One MPM substep into grid[buffer] (buffer 0 or 1; grid[buffer] must be zero
- * apart from the boxes recorded for it, which the previous substep with the
- * other buffer cleared).  With cp != NULL the reaction transfer of kind
- * cp->kind is added (s, hydro as for fsi_reaction_to_grid) and its reductions
- * go to stats[buffer]; the reaction part of stats[1 - buffer] is zeroed. */
-int fsi_mpm_substep_binned(const FsiParticles* pt, const FsiGrid grid[2], const FsiMpmBins* bins,
-                           const FsiMpmParams* mp, int32_t buffer, const FsiLbmState* s, const float* hydro,
-                           const FsiCouplingParams* cp, FsiCouplingStats stats[2], void* stream);
+/* n_substeps binned MPM substeps (each one call of MPMSolid3D.substep plus,
+ * with cp != NULL, the reaction transfer of kind cp->kind from s and hydro as
+ * for fsi_reaction_to_grid, whose reductions go to stats[substep % 3]) as
+ * n_substeps + 2 launches: launch s gathers substep s - 1 and, for the same
+ * chunk of particles, builds and scatters substep s, rotating over three grid
+ * buffers (substep s scatters into grid[s % 3]).
+ *   - On entry every buffer must be zero apart from the boxes recorded in the
+ *     bins (any earlier call of this function leaves it so).
+ *   - On return grid[(n_substeps - 1) % 3] holds the last substep's momentum,
+ *     mass and f_ext, and stats[(n_substeps - 1) % 3] its reaction reductions.
+ *   - Zero the three buffers and bins->meta[1..7] after using grid[0] with
+ *     the one-phase entry points (fsi_mpm_p2g etc.). */
+int fsi_mpm_substeps_binned(const FsiParticles* pt, const FsiGrid grid[3], const FsiMpmBins* bins,
+                            const FsiMpmParams* mp, int32_t n_substeps, const FsiLbmState* s, const float* hydro,
+                            const FsiCouplingParams* cp, FsiCouplingStats stats[3], void* stream);
 
 /* grid velocity after a binned substep (the grid_v of the reference after
  * grid_update) from grid's momentum, mass and f_ext, into out [3][n^3] */
@@ -340,9 +334,9 @@ int fsi_mpm_grid_velocity(const FsiGrid* g, const FsiMpmParams* mp, float* out, 
  * a batch of N cases performs, per case, exactly the phases of
  * FSIDriver3D.step_once with one LBM step per FSI step:
  *   penalty:          fsi_batch_project, fsi_batch_lbm_substep (penalty force
- *                     built in the step), then M x fsi_batch_mpm_substep
+ *                     built in the step), then fsi_batch_mpm_substeps (M)
  *   moving_boundary:  fsi_batch_project, fsi_batch_mask_rebuild,
- *                     fsi_batch_lbm_substep, then M x fsi_batch_mpm_substep
+ *                     fsi_batch_lbm_substep, then fsi_batch_mpm_substeps (M)
  * with fsi_batch_mpm_bin before the MPM substeps.  Cases must have no open
  * boundaries (bc_left = bc_right = 0) and equal population storage.
  *
@@ -360,16 +354,15 @@ typedef struct FsiBatchCase {
   FsiLbmParams lp;
   FsiStepCtl ctl;                 /* parity, pp advanced by fsi_batch_lbm_substep */
   FsiParticles pt;
-  FsiGrid grid[2];                /* MPM grid buffers of the binned substep */
+  FsiGrid grid[3];                /* MPM grid buffers of the binned substeps */
   FsiMpmBins bins;
   FsiMpmParams mp;
   FsiCouplingParams cp;           /* reaction kind 0 penalty, 1 engineering, 2 link-area */
   FsiCouplingStats* proj_stats;   /* device [1] */
-  FsiCouplingStats* react_stats;  /* device [2], zero before the first substep */
+  FsiCouplingStats* react_stats;  /* device [3] (as stats of fsi_mpm_substeps_binned) */
   float mask_threshold;           /* dynamic_solid_threshold */
   int32_t mode;                   /* FSI_BATCH_* */
   int32_t active;                 /* 0: empty slot, skipped */
-  int32_t buf;                    /* grid buffer of the next MPM substep, advanced on the device */
 } FsiBatchCase;
 
 typedef struct FsiBatchDims {
@@ -380,7 +373,6 @@ typedef struct FsiBatchDims {
   int64_t max_cells;              /* max nx * ny * nz */
   int32_t max_chunks;             /* max FsiMpmBins.max_chunks */
   int32_t max_bins;               /* max FsiMpmBins.n_bins */
-  int32_t mpm_tune;               /* FsiMpmParams.tune of the batched MPM substep (all cases) */
   int32_t lbm_tune;               /* FSI_TUNE_LBM_OCC3, or FSI_TUNE_LBM_PAIR when every case has an even nx */
 } FsiBatchDims;
 
@@ -395,10 +387,11 @@ int fsi_batch_mask_rebuild(FsiBatchCase* cases, const FsiBatchDims* dims, void* 
 int fsi_batch_lbm_substep(FsiBatchCase* cases, const FsiBatchDims* dims, void* stream);
 /* fsi_mpm_bin per case. */
 int fsi_batch_mpm_bin(FsiBatchCase* cases, const FsiBatchDims* dims, void* stream);
-/* One binned MPM substep per case with its reaction transfer (penalty.py:
- * 90-129 / moving_boundary.py:58-110 / link_area.py:139-193) from the last
- * LBM step's force field; then the case's grid buffer advances. */
-int fsi_batch_mpm_substep(FsiBatchCase* cases, const FsiBatchDims* dims, void* stream);
+/* n_substeps binned MPM substeps per case with its reaction transfer
+ * (penalty.py:90-129 / moving_boundary.py:58-110 / link_area.py:139-193) from
+ * the last LBM step's force field, as fsi_mpm_substeps_binned does for one
+ * case: n_substeps + 2 launches for the whole batch. */
+int fsi_batch_mpm_substeps(FsiBatchCase* cases, const FsiBatchDims* dims, int32_t n_substeps, void* stream);
 
 /* ---- misc --------------------------------------------------------------- */
 int fsi_abi_version(void);

@@ -18,9 +18,6 @@ c_i32, c_i64, c_f32, c_f64, c_p = ctypes.c_int32, ctypes.c_int64, ctypes.c_float
 FSI_CELL_SOLID, FSI_CELL_NEAR, FSI_CELL_LINK, FSI_CELL_OVERRIDE, FSI_CELL_CF = 1, 2, 4, 8, 16
 FSI_MODE_MOVING_BB, FSI_MODE_SUBCYCLED, FSI_MODE_DIRSTATS, FSI_MODE_PENALTY = 1, 2, 4, 8
 FSI_TUNE_LBM_OCC3, FSI_TUNE_LBM_OCC4, FSI_TUNE_LBM_PAIR = 0, 1, 2
-FSI_TUNE_MPM_T128, FSI_TUNE_MPM_T256, FSI_TUNE_MPM_T512 = 0, 1, 2
-FSI_TUNE_P2G_T128, FSI_TUNE_P2G_T384 = 0, 1
-FSI_MPM_PAYLOAD_ROWS = 32
 
 
 class FsiLbmDiag(ctypes.Structure):
@@ -68,12 +65,12 @@ class FsiGrid(ctypes.Structure):
 
 class FsiMpmBins(ctypes.Structure):
     _fields_ = [("n_bins", c_i32), ("max_chunks", c_i32), ("key", c_p), ("count", c_p), ("start", c_p),
-                ("perm", c_p), ("chunk", c_p), ("box", c_p), ("meta", c_p), ("payload", c_p)]
+                ("perm", c_p), ("chunk", c_p), ("box", c_p), ("meta", c_p)]
 
 
 class FsiMpmParams(ctypes.Structure):
     _fields_ = [("dx", c_f32), ("inv_dx", c_f32), ("dt", c_f32), ("mu", c_f32), ("la", c_f32),
-                ("gravity", c_f32 * 3), ("damping", c_f32), ("bound", c_i32), ("lock_z", c_i32), ("tune", c_i32)]
+                ("gravity", c_f32 * 3), ("damping", c_f32), ("bound", c_i32), ("lock_z", c_i32), ("pad", c_i32)]
 
 
 class FsiCouplingParams(ctypes.Structure):
@@ -93,14 +90,14 @@ class FsiCouplingStats(ctypes.Structure):
 
 class FsiBatchCase(ctypes.Structure):
     _fields_ = [("lbm", FsiLbmState), ("lp", FsiLbmParams), ("ctl", FsiStepCtl), ("pt", FsiParticles),
-                ("grid", FsiGrid * 2), ("bins", FsiMpmBins), ("mp", FsiMpmParams), ("cp", FsiCouplingParams),
+                ("grid", FsiGrid * 3), ("bins", FsiMpmBins), ("mp", FsiMpmParams), ("cp", FsiCouplingParams),
                 ("proj_stats", c_p), ("react_stats", c_p), ("mask_threshold", c_f32), ("mode", c_i32),
-                ("active", c_i32), ("buf", c_i32)]
+                ("active", c_i32)]
 
 
 class FsiBatchDims(ctypes.Structure):
     _fields_ = [("n_cases", c_i32), ("store_fp16", c_i32), ("max_lbm_tiles", c_i32), ("max_particles", c_i32),
-                ("max_cells", c_i64), ("max_chunks", c_i32), ("max_bins", c_i32), ("mpm_tune", c_i32),
+                ("max_cells", c_i64), ("max_chunks", c_i32), ("max_bins", c_i32),
                 ("lbm_tune", c_i32)]
 
 
@@ -132,14 +129,14 @@ SIGNATURES = {
     "fsi_mpm_g2p": [_P(FsiParticles), _P(FsiGrid), _P(FsiMpmParams), c_p],
     "fsi_mpm_bins_layout": [c_i32, c_i32, _P(c_i32), _P(c_i32)],
     "fsi_mpm_bin": [_P(FsiParticles), _P(FsiGrid), _P(FsiMpmParams), _P(FsiMpmBins), c_p],
-    "fsi_mpm_substep_binned": [_P(FsiParticles), _P(FsiGrid), _P(FsiMpmBins), _P(FsiMpmParams), c_i32,
-                               _P(FsiLbmState), c_p, _P(FsiCouplingParams), c_p, c_p],
+    "fsi_mpm_substeps_binned": [_P(FsiParticles), _P(FsiGrid), _P(FsiMpmBins), _P(FsiMpmParams), c_i32,
+                                _P(FsiLbmState), c_p, _P(FsiCouplingParams), c_p, c_p],
     "fsi_mpm_grid_velocity": [_P(FsiGrid), _P(FsiMpmParams), c_p, c_p],
     "fsi_batch_project": [c_p, _P(FsiBatchDims), c_p],
     "fsi_batch_mask_rebuild": [c_p, _P(FsiBatchDims), c_p],
     "fsi_batch_lbm_substep": [c_p, _P(FsiBatchDims), c_p],
     "fsi_batch_mpm_bin": [c_p, _P(FsiBatchDims), c_p],
-    "fsi_batch_mpm_substep": [c_p, _P(FsiBatchDims), c_p],
+    "fsi_batch_mpm_substeps": [c_p, _P(FsiBatchDims), c_i32, c_p],
     "fsi_abi_version": [],
     "fsi_last_error": [ctypes.c_char_p, ctypes.c_size_t],
     "fsi_launch_count": [],

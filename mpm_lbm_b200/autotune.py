@@ -2,11 +2,9 @@
 
 The variants differ in how a kernel maps onto the SMs: the register budget of
 the one-cell LBM step kernel (3 or 4 resident CTAs per SM; bit-identical
-results), the two-cells-per-thread LBM kernel on the paired FP32 pipe (the
+results) and the two-cells-per-thread LBM kernel on the paired FP32 pipe (the
 same operator; its contraction of multiply-adds differs, so results agree to
-FP32 rounding), and the threads per particle chunk of the binned MPM substep
-(the same arithmetic; the grid sums are float atomics whose order, and so
-whose last-bit rounding, varies from run to run with any variant).  The tuner times each variant with CUDA events
+FP32 rounding).  The tuner times each variant with CUDA events
 on the caller's own state -- trial steps on a device snapshot that is
 restored afterwards -- and keeps the fastest.  It runs before a CUDA graph of
 the step is captured (a captured graph keeps the variant it was built with).
@@ -16,15 +14,14 @@ from __future__ import annotations
 
 import torch
 
-from ._lib import (FSI_TUNE_LBM_OCC3, FSI_TUNE_LBM_OCC4, FSI_TUNE_LBM_PAIR, FSI_TUNE_MPM_T128, FSI_TUNE_MPM_T256,
-                   FSI_TUNE_MPM_T512, FSI_TUNE_P2G_T128, FSI_TUNE_P2G_T384)
+from ._lib import FSI_TUNE_LBM_OCC3, FSI_TUNE_LBM_OCC4, FSI_TUNE_LBM_PAIR
 
 
 def _time_ms(fn, steps, reps):
     """Device time per call of fn: `steps` calls captured in a CUDA graph (so
     that host launch overhead does not enter), replayed `reps` times between
     events; the best replay counts.  steps must return the state's alternating
-    layouts (AA parity, ping-pong slots, grid buffers) to their start, i.e. be
+    layouts (AA parity, ping-pong slots) to their start, i.e. be
     even."""
     torch.cuda.synchronize()
     graph = torch.cuda.CUDAGraph()
@@ -76,35 +73,4 @@ def tune_lbm(lbm, step_fn, candidates=None, steps=10, reps=3):
     best = min(times, key=times.get)
     lbm.tune = best
     lbm._sync_params()
-    return {"choice": best, "ms_per_substep": times}
-
-
-def mpm_tune_value(scatter, gather):
-    """FsiMpmParams.tune for the given FSI_TUNE_P2G_* scatter and FSI_TUNE_MPM_* gather variants."""
-    return int(scatter) | (int(gather) << 2)
-
-
-def tune_mpm(solid, substep_fn, extra=(), candidates=None, steps=8, reps=3):
-    """Pick solid.params.tune (threads per chunk CTA of the binned P2G scatter
-    and G2P gather) by timing `substep_fn` (one binned substep as the caller
-    runs it) on a snapshot of the particle / grid / bin state.  extra: further
-    tensors the substep writes (coupler statistics), restored afterwards.
-    Returns {"choice": tune, "ms_per_substep": {tune: ms}}."""
-    if candidates is None:
-        candidates = [mpm_tune_value(s, g) for s in (FSI_TUNE_P2G_T128, FSI_TUNE_P2G_T384)
-                      for g in (FSI_TUNE_MPM_T128, FSI_TUNE_MPM_T256, FSI_TUNE_MPM_T512)]
-    solid._ensure_binned()
-    snap = solid.snapshot(extra)
-    times = {}
-    try:
-        for t in candidates:
-            solid.params.tune = int(t)
-            substep_fn()
-            torch.cuda.synchronize()
-            times[int(t)] = _time_ms(substep_fn, steps + steps % 2, reps)
-            solid.restore(snap)
-    finally:
-        solid.restore(snap)
-    best = min(times, key=times.get)
-    solid.params.tune = best
     return {"choice": best, "ms_per_substep": times}

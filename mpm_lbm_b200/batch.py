@@ -160,14 +160,13 @@ def sample_box_cases(n, seed=0, edges=(32, 48, 64, 96), lbm_steps=200, mpm_subst
 class FSIBatch:
     """Up to `capacity` independent FSI cases, advanced together."""
 
-    def __init__(self, capacity, storage="fp32", mpm_substeps=10, device="cuda", mpm_tune=0, lbm_tune=None):
+    def __init__(self, capacity, storage="fp32", mpm_substeps=10, device="cuda", lbm_tune=None):
         """lbm_tune: FSI_TUNE_LBM_OCC3 (0, default) or FSI_TUNE_LBM_PAIR (2, every
         case's nx even)."""
         self.capacity = int(capacity)
         self.storage = storage
         self.M = int(mpm_substeps)
         self.device = torch.device(device)
-        self.mpm_tune = int(mpm_tune)
         self.lbm_tune = lbm_tune
         self.slots = [None] * self.capacity          # FSIDriver3D per slot
         self.records = (FsiBatchCase * self.capacity)()
@@ -229,11 +228,12 @@ class FSIBatch:
         # open boundary (none here), make the readout state current
         lbm.flush_open_boundary()
         solid._ensure_binned()
-        if not solid._binned_clean:
-            for t in solid._buffers(0) + solid._buffers(1):
-                t.zero_()
-            solid._bins["t"]["meta"][1:3].zero_()
-            solid._buf, solid._binned_last, solid._binned_clean = 0, None, True
+        if not solid._binned_clean or solid._binned_mode != "seq":
+            for b in range(3):
+                for t in solid._buffers(b):
+                    t.zero_()
+            solid._bins["t"]["meta"][1:].zero_()
+            solid._binned_last, solid._binned_clean, solid._binned_mode = None, True, "seq"
         if moving:
             coupler = drv.mb_coupler if drv.mb_coupler is not None else drv.link_area_coupler
             mode = FSI_MODE_MOVING_BB | FSI_MODE_DIRSTATS
@@ -249,7 +249,8 @@ class FSIBatch:
         rec.lp = lbm.params
         rec.ctl.parity, rec.ctl.bc_pending, rec.ctl.pp, rec.ctl.mode = lbm.parity, 0, lbm.pp, mode
         rec.pt = solid.particles
-        rec.grid[0], rec.grid[1] = solid._bins["grids"][0], solid._bins["grids"][1]
+        for b in range(3):
+            rec.grid[b] = solid._bins["grids"][b]
         rec.bins = solid._bins["struct"]
         rec.mp = solid.params
         rec.cp = coupler.params
@@ -258,7 +259,6 @@ class FSIBatch:
         rec.mask_threshold = float(drv.config.dynamic_solid_threshold)
         rec.mode = FSI_BATCH_MOVING if moving else FSI_BATCH_PENALTY
         rec.active = 1
-        rec.buf = solid._buf
         self.records[slot] = rec
         self._coupler = getattr(self, "_coupler", {})
         self._coupler[slot] = coupler
@@ -276,7 +276,6 @@ class FSIBatch:
         act = [drv for drv in self.slots if drv is not None]
         d.n_cases = self.capacity
         d.store_fp16 = int(self.storage == "fp16")
-        d.mpm_tune = self.mpm_tune
         all_even = all(x.lbm.nx % 2 == 0 for x in act)
         if self.lbm_tune is None:
             d.lbm_tune = FSI_TUNE_LBM_OCC3  # the faster of the two on B200 (see profiles/)
@@ -306,8 +305,7 @@ class FSIBatch:
         call("fsi_batch_mask_rebuild", self._ptr(), d, st)
         call("fsi_batch_lbm_substep", self._ptr(), d, st)
         call("fsi_batch_mpm_bin", self._ptr(), d, st)
-        for _ in range(self.M):
-            call("fsi_batch_mpm_substep", self._ptr(), d, st)
+        call("fsi_batch_mpm_substeps", self._ptr(), d, self.M, st)
 
     def capture(self):
         """Capture one batched FSI step in a CUDA graph (for the current slots)."""
@@ -356,12 +354,12 @@ class FSIBatch:
         lbm.steps += k - getattr(lbm, "_batch_steps_seen", 0)
         lbm._batch_steps_seen = k
         lbm._version += 1
-        solid._buf = int(rec.buf)
-        solid._binned_last = solid._buf ^ 1 if k > 0 else solid._binned_last
+        if k > 0 and self.M > 0:
+            solid._binned_last = (self.M - 1) % 3
         solid._since_bin = 0
         coupler = self._coupler[slot]
-        if k > 0:
-            coupler._binned_slot = solid._buf ^ 1
+        if k > 0 and self.M > 0:
+            coupler._binned_slot = (self.M - 1) % 3
         drv.current_lbm_step = k
         drv.total_lbm_substeps = k
         drv.total_mpm_substeps = k * self.M

@@ -30,11 +30,11 @@ class _StatsBuffer:
 
 
 class _BinnedReaction:
-    """Reaction transfer fused into MPMSolid3D.substep_binned: the kernel
+    """Reaction transfer fused into MPMSolid3D.substeps_binned: the kernel
     writes the reductions of a substep with grid buffer b to record b."""
 
     def _init_binned(self, device):
-        self.binned_stats = _StatsBuffer(device, count=2)
+        self.binned_stats = _StatsBuffer(device, count=3)
         self._binned_slot = None
 
     def _binned_args(self, lbm):

@@ -1,7 +1,11 @@
-// Binned MPM substep: particles sorted by 4x4x4-cell block, P2G (+ reaction
-// transfer) staged in a shared-memory tile per chunk of a bin, G2P with the
-// grid update evaluated while staging the chunk's node box, and two grid
-// buffers so that only the boxes touched one substep earlier are zeroed.
+// Binned MPM substeps: particles sorted by 4x4x4-cell block and cut into
+// chunks; one launch per substep, in which each CTA takes whole chunks
+// through the G2P gather of the previous substep (grid update evaluated while
+// the chunk's node box is staged), the P2G stress / reaction payload and the
+// P2G scatter staged in a shared-memory tile, flushed with one global atomic
+// per touched node value.  Three grid buffers rotate so that only the boxes
+// touched two substeps earlier are zeroed, by the launch after their last
+// reader.
 //
 // The per-particle and per-node arithmetic is the one of the one-phase
 // kernels (mpm_common.cuh): solid.py:212-315 and the reaction transfers of
@@ -157,6 +161,47 @@ __global__ void k_bin_scatter(int n, const int32_t* __restrict__ key, int32_t* _
   bin_scatter_body(n, key, cursor, perm, blockIdx.x, gridDim.x);
 }
 
+// Orders the particles of each chunk by B-spline base node (ties by particle
+// id), so that particles sharing a stencil are adjacent within the chunk: one
+// CTA of kChunk threads per chunk, each particle's rank counted against the
+// chunk's other keys.
+__device__ __forceinline__ void chunk_sort_body(const FsiParticles& pt, float inv_dx, int G,
+                                                const int2* __restrict__ chunks, const int32_t* __restrict__ meta,
+                                                int32_t* __restrict__ perm, int vb, int vg) {
+  __shared__ unsigned long long key[kChunk];
+  const int t = threadIdx.x, n = pt.n;
+  const int nch = meta[0];
+  for (int c = vb; c < nch; c += vg) {
+    const int2 ch = chunks[c];
+    int p = 0;
+    unsigned long long k = ~0ull;
+    if (t < ch.y) {
+      p = perm[ch.x + t];
+      unsigned long long cell = 0;
+      for (int a = 2; a >= 0; --a) {
+        const float Xp = __fmul_rn(pt.x[a * n + p], inv_dx);
+        cell = cell * (unsigned long long)(G + 2) + (unsigned long long)(clampi((int)(Xp - 0.5f), -1, G) + 1);
+      }
+      k = (cell << 32) | (unsigned long long)(unsigned)p;
+    }
+    key[t] = k;
+    __syncthreads();
+    if (t < ch.y) {
+      int rank = 0;
+      for (int j = 0; j < ch.y; ++j) rank += key[j] < k;
+      perm[ch.x + rank] = p;
+    }
+    __syncthreads();
+  }
+}
+
+__global__ __launch_bounds__(kChunk) void k_bin_sort_chunks(FsiParticles pt, float inv_dx, int G,
+                                                             const int2* __restrict__ chunks,
+                                                             const int32_t* __restrict__ meta,
+                                                             int32_t* __restrict__ perm) {
+  chunk_sort_body(pt, inv_dx, G, chunks, meta, perm, blockIdx.x, gridDim.x);
+}
+
 struct Box {
   int lo[3], ext[3];
   int vol;
@@ -173,13 +218,6 @@ __device__ __forceinline__ Box load_box(const int32_t* r) {
   }
   b.vol = v > INT_MAX ? INT_MAX : (int)v;
   return b;
-}
-
-__device__ __forceinline__ int64_t box_node(const Box& b, int li, int G) {
-  const int i = b.lo[0] + li % b.ext[0];
-  const int j = b.lo[1] + (li / b.ext[0]) % b.ext[1];
-  const int k = b.lo[2] + li / (b.ext[0] * b.ext[1]);
-  return ((int64_t)k * G + j) * G + i;
 }
 
 // quadratic B-spline weight of offset o for the fractional position f (the
@@ -219,290 +257,73 @@ __device__ __forceinline__ void g2p_gather_global(const FsiGrid& g, const FsiMpm
   }
 }
 
-// Per-particle P2G payload, one row per quantity, one column per particle slot
-// (the particle's position in the bin order perm): fractional position, base
-// node, momentum, affine matrix, mass, reaction force, and the B-spline
-// weights [axis][offset].
+// P2G payload of a particle, one row per quantity, one column per particle of
+// the chunk (shared memory): fractional position, base node, momentum, affine
+// matrix, mass, reaction force, and the B-spline weights [axis][offset].
 enum { kPfx = 0, kPbase = 3, kPmv = 6, kPaff = 9, kPmass = 18, kPpf = 19, kPw = 22, kPn = 31 };
-static_assert(kPn <= FSI_MPM_PAYLOAD_ROWS, "payload rows exceed the caller's buffer");
 
-// P2G, per particle (one thread per slot): fixed-corotated stress and affine
-// momentum with the FP64 polar rotation (solid.py:231-249), the reaction force
-// gathered from the lattice hydro force (penalty.py:90-129,
-// moving_boundary.py:58-110, link_area.py:139-193) and its reductions, and the
-// particle's B-spline data -- written to the payload for the scatter kernel.
-template <bool REACT>
-__device__ __forceinline__ void p2g_payload_body(const FsiParticles& pt, const FsiMpmParams& mp,
-                                                 const int32_t* __restrict__ perm, float* __restrict__ payload,
-                                                 const LatView& L, const float* __restrict__ hydro,
-                                                 const float* __restrict__ phi, const FsiCouplingParams& cp,
-                                                 FsiCouplingStats* st, const FsiLbmDiag* diag, int vb, int vg) {
-  __shared__ float s_scale;
-  const int n = pt.n;
-  if (REACT) {
-    if (threadIdx.x == 0) {
-      float raw = 1.f;
-      s_scale = cp.kind == 2 ? link_area_scale(diag, cp, &raw) : 1.0f;
-      if (vb == 0 && cp.kind == 2) {
-        st->area_scale = s_scale;
-        st->raw_area_scale = raw;
-      }
-    }
-    __syncthreads();
-  }
-  int n_act = 0;
-  float pmax = 0.f;
-  double pn[3] = {0.0, 0.0, 0.0};
-  // two lanes per particle slot, in different warps of the CTA so that the two
-  // halves of the work run side by side instead of one after the other:
-  // warps of role 0 the stress and affine momentum (FP64 polar rotation),
-  // warps of role 1 the B-spline data and the reaction force (with its own
-  // det F for the volume).  Warp w of the CTA covers slots
-  // (vb * blockDim.x / 2) + (w / 2) * 32 + lane with role w % 2.
-  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int pslot = vb * (blockDim.x >> 1) + (wid >> 1) * 32 + lane, role = wid & 1;
-  if (pslot < n) {
-    const int p = perm[pslot];
-    float* const col = payload + pslot;
-    if (role == 0) {
-      P2GParticle q;
-      p2g_particle(pt, p, mp, q);
-      pt.Jp[p] = q.J;
-#pragma unroll
-      for (int a = 0; a < 3; ++a) col[(int64_t)(kPmv + a) * n] = q.mv[a];
-#pragma unroll
-      for (int a = 0; a < 9; ++a) col[(int64_t)(kPaff + a) * n] = q.aff[a];
-      col[(int64_t)kPmass * n] = q.mass;
-    } else {
-      const float X[3] = {pt.x[p], pt.x[n + p], pt.x[2 * n + p]};
-      BSpline b;
-      bspline(X, mp.inv_dx, b);
-      float pf[3] = {0.f, 0.f, 0.f};
-      if (REACT) {
-        float Fp[9];
-#pragma unroll
-        for (int a = 0; a < 9; ++a) Fp[a] = pt.F[(int64_t)a * n + p];
-        const float J = det3(Fp);
-        ReactParticle r;
-        reaction_particle(L, hydro, phi, cp, b, J, pt.vol0[p], s_scale, r);
-        n_act = r.act ? 1 : 0;
-        pmax = r.pnorm;
-        if (r.gated)
-          for (int a = 0; a < 3; ++a) pn[a] = (double)r.pf[a];
-        if (r.scatter)
-          for (int a = 0; a < 3; ++a) pf[a] = r.pf[a];
-      }
-#pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        col[(int64_t)(kPfx + a) * n] = b.fx[a];
-        col[(int64_t)(kPbase + a) * n] = __int_as_float(b.base[a]);
-        col[(int64_t)(kPpf + a) * n] = pf[a];
-#pragma unroll
-        for (int o = 0; o < 3; ++o) col[(int64_t)(kPw + 3 * a + o) * n] = b.w[a][o];
-      }
-    }
-  }
-  if (REACT) {
-    // diagnostics reductions (penalty.py:202-240, moving_boundary.py:312-374)
-    const int na = __reduce_add_sync(0xffffffffu, (unsigned)n_act);
-    const float pm = warp_max(pmax);
-    double sp3[3];
-#pragma unroll
-    for (int a = 0; a < 3; ++a) sp3[a] = warp_sum_d(pn[a]);
-    if ((threadIdx.x & 31) == 0) {
-      if (na) atomicAdd(&st->active_reaction_particle_count, na);
-      if (pm > 0.f) atomic_max_nonneg(&st->max_particle_reaction_norm, pm);
-      for (int a = 0; a < 3; ++a)
-        if (sp3[a] != 0.0) atomicAdd(&st->net_particle_reaction[a], sp3[a]);
-    }
-  }
+// ---- fused substep sequence --------------------------------------------------
+// M substeps in M + 1 launches (after a prologue).  Launch s, for each chunk of
+// its CTA: the gather of substep s - 1 (G2P from grid buffer (s - 1) % 3, the
+// new particle state written to the particle fields and kept in shared
+// memory), then the P2G payload of substep s from that state and its scatter
+// into buffer s % 3.  A chunk's particles belong to one CTA for the launch, so
+// gather, payload and scatter of a chunk follow each other without any
+// grid-wide synchronisation; the launch boundary is the one grid-wide step
+// (every scatter of substep s is complete before any gather of it).  The
+// launch also zeroes the boxes substep s - 2 recorded in buffer (s + 1) % 3,
+// whose last reader (the gather of substep s - 2) ran in the launch before:
+// three buffers, so that no launch zeroes a buffer that another CTA of the
+// same launch still reads or writes.  The arithmetic is the one of the
+// three-kernel substep above (p2g_particle, reaction_particle, g2p_node and
+// g2p_finish on the same values).
+
+enum { kSx = 0, kSv = 3, kSC = 6, kSF = 15, kSn = 24 };  // staged particle state rows
+// bins->meta: [0] chunks, [1 + b] records in box[b], [4] chunks scattered
+// without the tile, [5 + b] buffer b holds recorded boxes not yet zeroed
+enum { kMetaChunks = 0, kMetaRec = 1, kMetaOverflow = 4, kMetaDirty = 5 };
+constexpr int kSeqT = 256;
+constexpr size_t kSeqSmem = sizeof(float) * (7 * kTileCap + (kPn + kSn) * kChunk);
+
+struct SeqArgs {
+  FsiParticles pt;
+  FsiGrid grid[3];
+  FsiMpmParams mp;
+  const int32_t* perm;
+  const int2* chunks;
+  int32_t* meta;
+  int32_t* box;        // [3][max_chunks][6]
+  int64_t box_stride;  // 6 * max_chunks
+  LatView L;
+  const float* hydro;
+  const float* phi;
+  FsiCouplingParams cp;
+  FsiCouplingStats* stats;  // [3]; null without the reaction transfer
+  const FsiLbmDiag* diag;
+  int32_t s, M;             // launch index (0..M) and substeps in the sequence
+};
+
+// lattice coordinates of entry li of a box (two divisions)
+__device__ __forceinline__ void box_ijk(const Box& b, int li, int& i, int& j, int& k) {
+  const int e0 = b.ext[0], e01 = b.ext[0] * b.ext[1];
+  k = li / e01;
+  const int r = li - k * e01;
+  j = r / e0;
+  i = r - j * e0 + b.lo[0];
+  j += b.lo[1];
+  k += b.lo[2];
 }
 
-template <bool REACT>
-__global__ __launch_bounds__(128) void k_p2g_payload(FsiParticles pt, FsiMpmParams mp,
-                                                     const int32_t* __restrict__ perm, float* __restrict__ payload,
-                                                     LatView L, const float* __restrict__ hydro,
-                                                     const float* __restrict__ phi, FsiCouplingParams cp,
-                                                     FsiCouplingStats* st, const FsiLbmDiag* diag) {
-  griddep_wait();
-  griddep_launch();
-  p2g_payload_body<REACT>(pt, mp, perm, payload, L, hydro, phi, cp, st, diag, blockIdx.x, gridDim.x);
-}
-
-// P2G scatter of the chunks of this CTA into grid buffer g, from the payload:
-//  stage the chunk's payload columns and find its node box;
-//  each warp scatters one particle at a time, lane o on stencil node o, so
-//  that the lanes of one shared-memory atomic touch distinct nodes (float
-//  atomics to one shared address serialise);
-//  one global atomic per touched node value.
-// Chunks whose box exceeds the tile (bins gone stale) scatter with global
-// atomics directly.
-template <bool REACT, int T>
-__device__ __forceinline__ void p2g_scatter_body(const FsiGrid& g, const FsiMpmParams& mp,
-                                                 const float* __restrict__ payload, int n,
-                                                 const int2* __restrict__ chunks, int32_t* meta, int32_t* box, int buf,
-                                                 FsiCouplingStats* st, int vb, int vg) {
-  __shared__ float tile[7 * kTileCap];
-  __shared__ float sp[kPn][kChunk];
-  __shared__ int s_lo[3], s_hi[3];
-  const int tid = threadIdx.x;
-  const int G = g.n;
+__device__ __forceinline__ void zero_boxes(const FsiGrid& go, const int32_t* __restrict__ rec, int nrec, int vb,
+                                           int vg) {
+  const int G = go.n;
   const int64_t N = (int64_t)G * G * G;
-  const int nch = meta[0];
-  if (vb == 0 && tid == 0) meta[1 + buf] = nch;
-  float* const dst[7] = {g.v, g.v + N, g.v + 2 * N, g.m, g.f_ext, g.f_ext + N, g.f_ext + 2 * N};
-  float gmax = 0.f;
-  double gn[3] = {0.0, 0.0, 0.0};
-  for (int c = vb; c < nch; c += vg) {
-    __syncthreads();  // the previous chunk's flush has read the tile and sp
-    if (tid < 3) {
-      s_lo[tid] = INT_MAX;
-      s_hi[tid] = INT_MIN;
-    }
-    const int2 ch = chunks[c];
-    for (int i = tid; i < kPn * ch.y; i += T) {
-      const int r = i / ch.y, k = i - r * ch.y;
-      sp[r][k] = payload[(int64_t)r * n + ch.x + k];
-    }
-    __syncthreads();
-    if (tid < 32 * ((ch.y + 31) / 32)) {
-      const bool live = tid < ch.y;
-#pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        const int bs = live ? __float_as_int(sp[kPbase + a][tid]) : 0;
-        const int lo = __reduce_min_sync(0xffffffffu, live ? bs : INT_MAX);
-        const int hi = __reduce_max_sync(0xffffffffu, live ? bs : INT_MIN);
-        if ((tid & 31) == 0) {
-          atomicMin(&s_lo[a], lo);
-          atomicMax(&s_hi[a], hi);
-        }
-      }
-    }
-    __syncthreads();
-    int32_t rec[6];
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      rec[a] = max(s_lo[a], 0);
-      rec[3 + a] = s_hi[a] == INT_MIN ? -1 : min(min(s_hi[a], G) + 2, G - 1);
-    }
-    const Box bx = load_box(rec);
-    const bool staged = bx.vol <= kTileCap;
-    if (tid == 0) {
-#pragma unroll
-      for (int a = 0; a < 6; ++a) box[6 * c + a] = rec[a];
-      if (!staged) atomicAdd(meta + 3, 1);
-    }
-    const int nv = staged ? bx.vol : 0;
-    for (int i = tid; i < 7 * nv; i += T) tile[i] = 0.f;
-    __syncthreads();
-    // one warp per particle, lane o < 27 on stencil node o (ox, oy, oz = o / 9,
-    // o / 3 % 3, o % 3): the particle's payload is a broadcast read and the
-    // warp's shared-memory atomics land on 27 distinct nodes
-    const int lane = tid & 31, warp = tid >> 5;
-    const int ox = lane / 9, oy = (lane / 3) % 3, oz = lane % 3;
-    const float dox = (float)ox, doy = (float)oy, doz = (float)oz;
-    float gsum[3] = {0.f, 0.f, 0.f}, gm2 = 0.f;
-    for (int lp = warp; lp < ch.y; lp += T / 32) {
-      if (lane >= 27) continue;
-      const int I = __float_as_int(sp[kPbase][lp]) + ox, Jj = __float_as_int(sp[kPbase + 1][lp]) + oy,
-                K = __float_as_int(sp[kPbase + 2][lp]) + oz;
-      if (I < 0 || I >= G || Jj < 0 || Jj >= G || K < 0 || K >= G) continue;
-      // weights of bspline() (staged by the payload) and offsets as in p2g_node()
-      const float w = sp[kPw + ox][lp] * sp[kPw + 3 + oy][lp] * sp[kPw + 6 + oz][lp];
-      const float dpos[3] = {(dox - sp[kPfx][lp]) * mp.dx, (doy - sp[kPfx + 1][lp]) * mp.dx,
-                             (doz - sp[kPfx + 2][lp]) * mp.dx};
-      float val[7];
-#pragma unroll
-      for (int q = 0; q < 3; ++q)
-        val[q] = w * (sp[kPmv + q][lp] + (sp[kPaff + 3 * q][lp] * dpos[0] + sp[kPaff + 3 * q + 1][lp] * dpos[1] +
-                                          sp[kPaff + 3 * q + 2][lp] * dpos[2]));
-      val[3] = w * sp[kPmass][lp];
-      bool react = false;
-      if (REACT) {
-        const float f0 = sp[kPpf][lp], f1 = sp[kPpf + 1][lp], f2 = sp[kPpf + 2][lp];
-        react = f0 != 0.f || f1 != 0.f || f2 != 0.f;
-        if (react) {
-          val[4] = w * f0;
-          val[5] = w * f1;
-          val[6] = w * f2;
-#pragma unroll
-          for (int q = 0; q < 3; ++q) gsum[q] += val[4 + q];
-          gm2 = fmaxf(gm2, val[4] * val[4] + val[5] * val[5] + val[6] * val[6]);
-        }
-      }
-      const int nq = react ? 7 : 4;
-      if (staged) {
-        const int li = ((K - bx.lo[2]) * bx.ext[1] + (Jj - bx.lo[1])) * bx.ext[0] + (I - bx.lo[0]);
-#pragma unroll
-        for (int q = 0; q < 7; ++q)
-          if (q < nq) atomicAdd(&tile[q * nv + li], val[q]);
-      } else {
-        const int64_t node = ((int64_t)K * G + Jj) * G + I;
-#pragma unroll
-        for (int q = 0; q < 7; ++q)
-          if (q < nq) atomicAdd(dst[q] + node, val[q]);
-      }
-    }
-    if (REACT) {
-#pragma unroll
-      for (int q = 0; q < 3; ++q) gn[q] += (double)gsum[q];
-      gmax = fmaxf(gmax, sqrtf(gm2));
-    }
-    __syncthreads();
-    for (int li = tid; li < nv; li += T) {
-      const int64_t node = box_node(bx, li, G);
-#pragma unroll
-      for (int q = 0; q < 7; ++q) {
-        const float v = tile[q * nv + li];
-        if (v != 0.f) atomicAdd(dst[q] + node, v);
-      }
-    }
-  }
-  if (REACT) {
-    const float gm = warp_max(gmax);
-    double sg[3];
-#pragma unroll
-    for (int a = 0; a < 3; ++a) sg[a] = warp_sum_d(gn[a]);
-    if ((tid & 31) == 0) {
-      if (gm > 0.f) atomic_max_nonneg(&st->max_grid_reaction_norm, gm);
-      for (int a = 0; a < 3; ++a)
-        if (sg[a] != 0.0) atomicAdd(&st->net_grid_reaction[a], sg[a]);
-    }
-  }
-}
-
-// register budget: 128-thread CTAs keep 4 per SM, 384-thread CTAs 1
-template <bool REACT, int T>
-__global__ __launch_bounds__(T, T == 384 ? 1 : 4) void k_p2g_scatter(FsiGrid g, FsiMpmParams mp, const float* __restrict__ payload,
-                                                   int n, const int2* __restrict__ chunks, int32_t* meta,
-                                                   int32_t* box, int buf, FsiCouplingStats* st) {
-  griddep_wait();
-  griddep_launch();
-  p2g_scatter_body<REACT, T>(g, mp, payload, n, chunks, meta, box, buf, st, blockIdx.x, gridDim.x);
-}
-
-// G2P of the chunks of this CTA from grid buffer g; zeroes the boxes the
-// previous substep recorded in the other buffer go.  T threads per CTA: each
-// particle's 27 nodes are split over T / kChunk adjacent lanes (offsets o =
-// sub, sub + T/kChunk, ...), whose partial sums are combined with shuffles
-// before the first of them finishes the particle.
-template <int T>
-__device__ __forceinline__ void g2p_binned_body(const FsiParticles& pt, const FsiGrid& g, const FsiGrid& go,
-                                                const FsiMpmParams& mp, const int32_t* __restrict__ perm,
-                                                const int2* __restrict__ chunks, const int32_t* meta,
-                                                const int32_t* __restrict__ box_b, const int32_t* __restrict__ box_o,
-                                                int buf, FsiCouplingStats* st_other, int vb, int vg) {
-  constexpr int GP = T / kChunk;  // lanes per particle: 1, 2 or 4
-  static_assert(GP == 1 || GP == 2 || GP == 4, "T must be 128, 256 or 512");
-  __shared__ float vt[3 * kTileCap];
-  const int tid = threadIdx.x;
-  const int G = g.n;
-  const int64_t N = (int64_t)G * G * G;
-  const int nrec = meta[1 + (1 - buf)];
   for (int r = vb; r < nrec; r += vg) {
-    const Box bx = load_box(box_o + 6 * r);
-    for (int li = tid; li < bx.vol; li += T) {
-      const int64_t node = box_node(bx, li, G);
+    const Box bx = load_box(rec + 6 * r);
+    for (int li = threadIdx.x; li < bx.vol; li += blockDim.x) {
+      int i, j, k;
+      box_ijk(bx, li, i, j, k);
+      const int64_t node = ((int64_t)k * G + j) * G + i;
       go.v[node] = 0.f;
       go.v[N + node] = 0.f;
       go.v[2 * N + node] = 0.f;
@@ -512,107 +333,469 @@ __device__ __forceinline__ void g2p_binned_body(const FsiParticles& pt, const Fs
       go.f_ext[2 * N + node] = 0.f;
     }
   }
-  if (st_other && vb == 0 && tid == 0) {
-    st_other->active_reaction_particle_count = 0;
-    st_other->max_particle_reaction_norm = 0.f;
-    st_other->max_grid_reaction_norm = 0.f;
-    st_other->area_scale = 0.f;
-    st_other->raw_area_scale = 0.f;
-    for (int a = 0; a < 3; ++a) {
-      st_other->net_particle_reaction[a] = 0.0;
-      st_other->net_grid_reaction[a] = 0.0;
+}
+
+__device__ __forceinline__ void zero_reaction_stats(FsiCouplingStats* st) {
+  st->active_reaction_particle_count = 0;
+  st->max_particle_reaction_norm = 0.f;
+  st->max_grid_reaction_norm = 0.f;
+  st->area_scale = 0.f;
+  st->raw_area_scale = 0.f;
+  for (int a = 0; a < 3; ++a) {
+    st->net_particle_reaction[a] = 0.0;
+    st->net_grid_reaction[a] = 0.0;
+  }
+}
+
+// grid buffer b by value (a select, not an indexed access, so that a
+// SeqArgs held in registers needs no local memory)
+__device__ __forceinline__ FsiGrid grid_of(const SeqArgs& A, int b) {
+  return b == 0 ? A.grid[0] : (b == 1 ? A.grid[1] : A.grid[2]);
+}
+
+// zeroes every buffer with boxes left from an earlier sequence, and the
+// reaction record of the first substep
+__device__ __forceinline__ void seq_prologue_body(const SeqArgs& A, int vb, int vg) {
+  for (int b = 0; b < 3; ++b)
+    if (A.meta[kMetaDirty + b]) zero_boxes(grid_of(A, b), A.box + b * A.box_stride, A.meta[kMetaRec + b], vb, vg);
+  if (A.stats && vb == 0 && threadIdx.x == 0) zero_reaction_stats(A.stats);
+}
+
+// reaction_particle() from the chunk's lattice box staged in shared memory
+// (lat[q * nv + li], q = 0..2 the force field, 3 phi; li the index in the box
+// bx, which holds every stencil node of the chunk inside the grid): the same
+// nodes, weights and summation order
+__device__ __forceinline__ void reaction_particle_staged(const float* __restrict__ lat, const Box& bx, int nv,
+                                                         const LatView& L, const FsiCouplingParams& cp,
+                                                         const BSpline& b, float Jp, float vol0, float scale,
+                                                         ReactParticle& r) {
+  float hs[3] = {0.f, 0.f, 0.f}, ps = 0.f;
+  const bool inside = b.base[0] >= 0 && b.base[1] >= 0 && b.base[2] >= 0 && b.base[0] + 2 < L.nx &&
+                      b.base[1] + 2 < L.ny && b.base[2] + 2 < L.nz;
+  const int l000 = ((b.base[2] - bx.lo[2]) * bx.ext[1] + (b.base[1] - bx.lo[1])) * bx.ext[0] + (b.base[0] - bx.lo[0]);
+#pragma unroll
+  for (int ox = 0; ox < 3; ++ox)
+#pragma unroll
+    for (int oy = 0; oy < 3; ++oy)
+#pragma unroll
+      for (int oz = 0; oz < 3; ++oz) {
+        const int I = b.base[0] + ox, Jj = b.base[1] + oy, K = b.base[2] + oz;
+        if (!inside && (I < 0 || I >= L.nx || Jj < 0 || Jj >= L.ny || K < 0 || K >= L.nz)) continue;
+        const float w = b.w[0][ox] * b.w[1][oy] * b.w[2][oz];
+        const int li = l000 + (oz * bx.ext[1] + oy) * bx.ext[0] + ox;
+        hs[0] += w * lat[li];
+        hs[1] += w * lat[nv + li];
+        hs[2] += w * lat[2 * nv + li];
+        if (cp.kind != 0) ps += w * lat[3 * nv + li];
+      }
+  reaction_from_sums(cp, hs, ps, Jp, vol0, scale, r);
+}
+
+__device__ __forceinline__ int base_of(float x, float inv_dx) { return (int)(__fmul_rn(x, inv_dx) - 0.5f); }
+
+// the chunk's node box: min / max base node over the live threads (every
+// thread of the CTA calls this, live or not)
+__device__ __forceinline__ void box_reduce(bool live, const int nb[3], int* s_lo, int* s_hi) {
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+    const int lo = __reduce_min_sync(0xffffffffu, live ? nb[r] : INT_MAX);
+    const int hi = __reduce_max_sync(0xffffffffu, live ? nb[r] : INT_MIN);
+    if ((threadIdx.x & 31) == 0) {
+      if (lo != INT_MAX) atomicMin(&s_lo[r], lo);
+      if (hi != INT_MIN) atomicMax(&s_hi[r], hi);
     }
   }
-  const int nch = meta[0];
-  const float s4 = 4.0f * mp.inv_dx * mp.inv_dx;
-  const int lp = tid / GP, sub = tid % GP;
-  for (int c = vb; c < nch; c += vg) {
-    __syncthreads();  // the previous chunk's gathers are done
-    const Box bx = load_box(box_b + 6 * c);
-    const bool staged = bx.vol <= kTileCap;
-    const int nv = staged ? bx.vol : 0;
-    for (int li = tid; li < nv; li += T) {
-      const int64_t node = box_node(bx, li, G);
-      const float m = g.m[node];
-      const float P[3] = {g.v[node], g.v[N + node], g.v[2 * N + node]};
-      float v[3] = {P[0], P[1], P[2]};
-      if (m > 0.0f) {
-        const float f[3] = {g.f_ext[node], g.f_ext[N + node], g.f_ext[2 * N + node]};
-        const int i = (int)(node % G), j = (int)((node / G) % G), k = (int)(node / ((int64_t)G * G));
-        grid_node_velocity(P, m, f, i, j, k, G, mp, v);
-      }
-      vt[li] = v[0];
-      vt[nv + li] = v[1];
-      vt[2 * nv + li] = v[2];
+}
+
+constexpr int kRun = kChunk / (kSeqT / 32);  // particles per warp in the scatter
+
+// launch A.s of the sequence for the chunks vb, vb + vg, ... (kSeqT threads,
+// kSeqSmem bytes of dynamic shared memory)
+template <bool REACT>
+__device__ __forceinline__ void mpm_seq_body(const SeqArgs& A, int vb, int vg) {
+  constexpr int T = kSeqT, GP = T / kChunk, NW = T / 32;  // G2P: two lanes per particle
+  extern __shared__ float4 seq_smem4[];
+  // G2P: [3][nv] node velocities; payload: [4][nv] lattice box; scatter: [7][nv] tile
+  float* const tile = reinterpret_cast<float*>(seq_smem4);
+  float* const sp = tile + 7 * kTileCap;  // [kPn][kChunk] P2G payload
+  float* const ss = sp + kPn * kChunk;    // [kSn][kChunk] particle state
+  __shared__ int s_lo[3], s_hi[3];
+  __shared__ float s_scale;
+  __shared__ int s_cnt[NW];
+  __shared__ float s_fmax[NW][2];
+  __shared__ double s_dsum[NW][6];
+  const FsiParticles& pt = A.pt;
+  const FsiMpmParams& mp = A.mp;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int s = A.s;
+  const bool do_g2p = s > 0, do_p2g = s < A.M;
+  const int bg = (s + 2) % 3, bs = s % 3, bz = (s + 1) % 3;
+  const int G = A.grid[0].n;
+  const int64_t N = (int64_t)G * G * G;
+  const int nch = A.meta[kMetaChunks];
+  FsiCouplingStats* const st = REACT ? A.stats + bs : nullptr;
+  if (vb == 0 && tid == 0) {
+    if (s == 0) {  // the prologue zeroed every buffer
+      A.meta[kMetaDirty + 1] = 0;
+      A.meta[kMetaDirty + 2] = 0;
     }
-    __syncthreads();
-    const int2 ch = chunks[c];
-    // all GP lanes of a particle take the same branch (lp < ch.y is uniform
-    // over them), so the shuffles below see all their partners
-    if (lp < ch.y) {
-      const int p = perm[ch.x + lp];
-      const int n = pt.n;
-      float X[3] = {pt.x[p], pt.x[n + p], pt.x[2 * n + p]};
-      BSpline b;
-      bspline(X, mp.inv_dx, b);
-      float nvl[3] = {0.f, 0.f, 0.f}, nC[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-      if (!staged) {
-        if (sub == 0) g2p_gather_global(g, mp, b, nvl, nC);
-      } else {
+    if (s >= 2) A.meta[kMetaDirty + bz] = 0;
+    if (do_p2g) {
+      A.meta[kMetaRec + bs] = nch;
+      A.meta[kMetaDirty + bs] = 1;
+    }
+    if (REACT) zero_reaction_stats(A.stats + bz);  // the record of substep s + 1
+  }
+  if (REACT && do_p2g && tid == 0) {
+    float raw = 1.f;
+    s_scale = A.cp.kind == 2 ? link_area_scale(A.diag, A.cp, &raw) : 1.0f;
+    if (vb == 0 && A.cp.kind == 2) {
+      st->area_scale = s_scale;
+      st->raw_area_scale = raw;
+    }
+  }
+  if (s >= 2) zero_boxes(grid_of(A, bz), A.box + bz * A.box_stride, A.meta[kMetaRec + bz], vb, vg);
+
+  const float s4 = 4.0f * mp.inv_dx * mp.inv_dx;
+  const int n = pt.n;
+  int n_act = 0;
+  float pmax = 0.f, gmax = 0.f;
+  double pn[3] = {0.0, 0.0, 0.0}, gn[3] = {0.0, 0.0, 0.0};
+  for (int c = vb; c < nch; c += vg) {
+    __syncthreads();  // the previous chunk is done with the tile, the stages and the box
+    if (tid < 3) {
+      s_lo[tid] = INT_MAX;
+      s_hi[tid] = INT_MIN;
+    }
+    const int2 ch = A.chunks[c];
+    int nb[3] = {0, 0, 0};  // base node of this thread's particle after the gather
+    bool nb_live = false;
+    if (do_g2p) {
+      // ---- G2P of substep s - 1 from buffer bg
+      const FsiGrid g = grid_of(A, bg);
+      const Box bx = load_box(A.box + bg * A.box_stride + 6 * c);
+      const bool staged = bx.vol <= kTileCap;
+      const int nv = staged ? bx.vol : 0;
+      for (int li = tid; li < nv; li += T) {
+        int i, j, k;
+        box_ijk(bx, li, i, j, k);
+        const int64_t node = ((int64_t)k * G + j) * G + i;
+        const float m = g.m[node];
+        const float P[3] = {g.v[node], g.v[N + node], g.v[2 * N + node]};
+        float v[3] = {P[0], P[1], P[2]};
+        if (m > 0.0f) {
+          const float f[3] = {g.f_ext[node], g.f_ext[N + node], g.f_ext[2 * N + node]};
+          grid_node_velocity(P, m, f, i, j, k, G, mp, v);
+        }
+        tile[li] = v[0];
+        tile[nv + li] = v[1];
+        tile[2 * nv + li] = v[2];
+      }
+      __syncthreads();  // also publishes the s_lo / s_hi reset
+      const int lp = tid / GP, sub = tid % GP;
+      if (lp < ch.y) {  // uniform over a particle's GP lanes
+        const int p = A.perm[ch.x + lp];
+        float X[3] = {pt.x[p], pt.x[n + p], pt.x[2 * n + p]};
+        BSpline b;
+        bspline(X, mp.inv_dx, b);
+        float nvl[3] = {0.f, 0.f, 0.f}, nC[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        if (!staged) {
+          if (sub == 0) g2p_gather_global(g, mp, b, nvl, nC);
+        } else {
 #pragma unroll
-        for (int o0 = 0; o0 < 27; o0 += GP) {
-          const int o = o0 + sub;
-          if (o < 27) {
-            const int ox = o / 9, oy = (o / 3) % 3, oz = o % 3;
-            const int I = b.base[0] + ox, Jj = b.base[1] + oy, K = b.base[2] + oz;
-            if (I >= 0 && I < G && Jj >= 0 && Jj < G && K >= 0 && K < G) {
-              const int li = ((K - bx.lo[2]) * bx.ext[1] + (Jj - bx.lo[1])) * bx.ext[0] + (I - bx.lo[0]);
-              const float gv[3] = {vt[li], vt[nv + li], vt[2 * nv + li]};
-              if (GP == 1) {
-                g2p_node(b, ox, oy, oz, mp.dx, s4, gv, nvl, nC);
-              } else {
-                // the offsets of this lane are not compile-time constants: weights by
-                // value instead of indexing b.w (g2p_node's arithmetic otherwise)
+          for (int o0 = 0; o0 < 27; o0 += GP) {
+            const int o = o0 + sub;
+            if (o < 27) {
+              const int ox = o / 9, oy = (o / 3) % 3, oz = o % 3;
+              const int I = b.base[0] + ox, Jj = b.base[1] + oy, K = b.base[2] + oz;
+              if (I >= 0 && I < G && Jj >= 0 && Jj < G && K >= 0 && K < G) {
+                const int li = ((K - bx.lo[2]) * bx.ext[1] + (Jj - bx.lo[1])) * bx.ext[0] + (I - bx.lo[0]);
+                const float gv[3] = {tile[li], tile[nv + li], tile[2 * nv + li]};
                 const float dpos[3] = {((float)ox - b.fx[0]) * mp.dx, ((float)oy - b.fx[1]) * mp.dx,
                                        ((float)oz - b.fx[2]) * mp.dx};
                 const float w = bspline_w(b.fx[0], ox) * bspline_w(b.fx[1], oy) * bspline_w(b.fx[2], oz);
 #pragma unroll
-                for (int a = 0; a < 3; ++a) {
-                  nvl[a] += w * gv[a];
+                for (int q = 0; q < 3; ++q) {
+                  nvl[q] += w * gv[q];
 #pragma unroll
-                  for (int cc = 0; cc < 3; ++cc) nC[a * 3 + cc] += (w * gv[a]) * dpos[cc] * s4;
+                  for (int cc = 0; cc < 3; ++cc) nC[q * 3 + cc] += (w * gv[q]) * dpos[cc] * s4;
                 }
               }
             }
           }
         }
-      }
-      if (GP > 1) {
-        // partners of a particle are adjacent lanes, aligned to GP
-        const unsigned grp = ((1u << GP) - 1u) << ((tid & 31) & ~(GP - 1));
+        const unsigned grp = ((1u << GP) - 1u) << (lane & ~(GP - 1));
 #pragma unroll
         for (int w = 1; w < GP; w <<= 1) {
 #pragma unroll
-          for (int a = 0; a < 3; ++a) nvl[a] += __shfl_xor_sync(grp, nvl[a], w, GP);
+          for (int q = 0; q < 3; ++q) nvl[q] += __shfl_xor_sync(grp, nvl[q], w, GP);
 #pragma unroll
-          for (int a = 0; a < 9; ++a) nC[a] += __shfl_xor_sync(grp, nC[a], w, GP);
+          for (int q = 0; q < 9; ++q) nC[q] += __shfl_xor_sync(grp, nC[q], w, GP);
+        }
+        if (sub == 0) {
+          g2p_finish(pt, p, mp, X, nvl, nC, do_p2g ? ss : nullptr, kChunk, lp);
+#pragma unroll
+          for (int r = 0; r < 3; ++r) nb[r] = base_of(X[r], mp.inv_dx);
+          nb_live = true;
         }
       }
-      if (sub == 0) g2p_finish(pt, p, mp, X, nvl, nC);
+    } else {
+      __syncthreads();  // publishes the s_lo / s_hi reset
+      if (tid < ch.y) {
+        // ---- first launch: stage the state from the particle fields
+        const int p = A.perm[ch.x + tid];
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+          const float x = pt.x[q * n + p];
+          ss[(kSx + q) * kChunk + tid] = x;
+          ss[(kSv + q) * kChunk + tid] = pt.v[q * n + p];
+          nb[q] = base_of(x, mp.inv_dx);
+        }
+#pragma unroll
+        for (int q = 0; q < 9; ++q) {
+          ss[(kSC + q) * kChunk + tid] = pt.C[(int64_t)q * n + p];
+          ss[(kSF + q) * kChunk + tid] = pt.F[(int64_t)q * n + p];
+        }
+        nb_live = true;
+      }
+    }
+    if (!do_p2g) continue;
+    box_reduce(nb_live, nb, s_lo, s_hi);
+    __syncthreads();  // the state stage and the box of substep s are complete
+    int32_t rec[6];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      rec[r] = max(s_lo[r], 0);
+      rec[3 + r] = s_hi[r] == INT_MIN ? -1 : min(min(s_hi[r], G) + 2, G - 1);
+    }
+    const Box bx = load_box(rec);
+    const bool staged = bx.vol <= kTileCap;
+    const int nv = staged ? bx.vol : 0;
+    if (tid == 0) {
+      int32_t* const out = A.box + bs * A.box_stride + 6 * c;
+#pragma unroll
+      for (int r = 0; r < 6; ++r) out[r] = rec[r];
+      if (!staged) atomicAdd(A.meta + kMetaOverflow, 1);
+    }
+    // ---- P2G payload of substep s: warps of role 0 the stress and affine
+    // momentum, warps of role 1 the B-spline data and the reaction force
+    {
+      const int role = wid & 1, slot = (wid >> 1) * 32 + lane;
+      if (role == 0) {
+        if (slot < ch.y) {
+          const int p = A.perm[ch.x + slot];
+          P2GParticle q;
+          p2g_particle_rows(ss + kSF * kChunk, ss + kSC * kChunk, ss + kSv * kChunk, kChunk, slot, pt.mass[p],
+                            pt.vol0[p], mp, q);
+          pt.Jp[p] = q.J;
+#pragma unroll
+          for (int r = 0; r < 3; ++r) sp[(kPmv + r) * kChunk + slot] = q.mv[r];
+#pragma unroll
+          for (int r = 0; r < 9; ++r) sp[(kPaff + r) * kChunk + slot] = q.aff[r];
+          sp[kPmass * kChunk + slot] = q.mass;
+        }
+      } else {
+        if (REACT && staged) {
+          // the chunk's lattice box (force field, phi) into shared memory, by
+          // the role-1 warps only (named barrier 1)
+          for (int li = slot; li < nv; li += T / 2) {
+            int i, j, k;
+            box_ijk(bx, li, i, j, k);
+            float h0 = 0.f, h1 = 0.f, h2 = 0.f, ph = 0.f;
+            if (i < A.L.nx && j < A.L.ny && k < A.L.nz) {
+              const int64_t cl = lat_cell(A.L, i, j, k);
+              h0 = A.hydro[cl];
+              h1 = A.hydro[A.L.pitch + cl];
+              h2 = A.hydro[2 * A.L.pitch + cl];
+              if (A.cp.kind != 0) ph = A.phi[cl];
+            }
+            tile[li] = h0;
+            tile[nv + li] = h1;
+            tile[2 * nv + li] = h2;
+            tile[3 * nv + li] = ph;
+          }
+          asm volatile("bar.sync 1, %0;" ::"n"(kSeqT / 2) : "memory");
+        }
+        if (slot < ch.y) {
+          const int p = A.perm[ch.x + slot];
+          const float X[3] = {ss[kSx * kChunk + slot], ss[(kSx + 1) * kChunk + slot], ss[(kSx + 2) * kChunk + slot]};
+          BSpline b;
+          bspline(X, mp.inv_dx, b);
+          float pf[3] = {0.f, 0.f, 0.f};
+          if (REACT) {
+            float Fp[9];
+#pragma unroll
+            for (int r = 0; r < 9; ++r) Fp[r] = ss[(kSF + r) * kChunk + slot];
+            const float J = det3(Fp);
+            ReactParticle rp;
+            if (staged)
+              reaction_particle_staged(tile, bx, nv, A.L, A.cp, b, J, pt.vol0[p], s_scale, rp);
+            else
+              reaction_particle(A.L, A.hydro, A.phi, A.cp, b, J, pt.vol0[p], s_scale, rp);
+            if (rp.act) ++n_act;
+            pmax = fmaxf(pmax, rp.pnorm);
+            if (rp.gated)
+              for (int r = 0; r < 3; ++r) pn[r] += (double)rp.pf[r];
+            if (rp.scatter)
+              for (int r = 0; r < 3; ++r) pf[r] = rp.pf[r];
+          }
+#pragma unroll
+          for (int r = 0; r < 3; ++r) {
+            sp[(kPfx + r) * kChunk + slot] = b.fx[r];
+            sp[(kPbase + r) * kChunk + slot] = __int_as_float(b.base[r]);
+            sp[(kPpf + r) * kChunk + slot] = pf[r];
+#pragma unroll
+            for (int o = 0; o < 3; ++o) sp[(kPw + 3 * r + o) * kChunk + slot] = b.w[r][o];
+          }
+        }
+      }
+    }
+    __syncthreads();  // payload complete; the lattice box is no longer needed
+    for (int i = tid; i < 7 * nv; i += T) tile[i] = 0.f;
+    __syncthreads();
+    // ---- P2G scatter of substep s into buffer bs.  Warp w takes kRun
+    // consecutive particles of the chunk, one at a time, lane o on stencil node
+    // o; particles are sorted by base node within the chunk (fsi_mpm_bin), so
+    // a run of particles with the same base is summed in registers and added
+    // to the tile with one shared-memory atomic per node value.
+    const FsiGrid g = grid_of(A, bs);
+    float* const dst[7] = {g.v, g.v + N, g.v + 2 * N, g.m, g.f_ext, g.f_ext + N, g.f_ext + 2 * N};
+    {
+      constexpr int NQ = REACT ? 7 : 4;
+      const int ox = lane / 9, oy = (lane / 3) % 3, oz = lane % 3;
+      const float dox = (float)ox, doy = (float)oy, doz = (float)oz;
+      float gsum[3] = {0.f, 0.f, 0.f}, gm2 = 0.f;
+      float acc[NQ];
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) acc[q] = 0.f;
+      int cb0 = INT_MIN, cb1 = 0, cb2 = 0;  // base of the run (warp-uniform)
+      // adds the run's sums of this lane's node to the tile (or the grid)
+      auto flush_run = [&]() {
+        const int I = cb0 + ox, Jj = cb1 + oy, K = cb2 + oz;
+        if (lane < 27 && I >= 0 && I < G && Jj >= 0 && Jj < G && K >= 0 && K < G) {
+          if (staged) {
+            const int li = ((K - bx.lo[2]) * bx.ext[1] + (Jj - bx.lo[1])) * bx.ext[0] + (I - bx.lo[0]);
+#pragma unroll
+            for (int q = 0; q < NQ; ++q)
+              if (acc[q] != 0.f) atomicAdd(&tile[q * nv + li], acc[q]);
+          } else {
+            const int64_t node = ((int64_t)K * G + Jj) * G + I;
+#pragma unroll
+            for (int q = 0; q < NQ; ++q)
+              if (acc[q] != 0.f) atomicAdd(dst[q] + node, acc[q]);
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) acc[q] = 0.f;
+      };
+      const int p1 = min(wid * kRun + kRun, ch.y);
+      for (int lp = wid * kRun; lp < p1; ++lp) {
+        const int b0 = __float_as_int(sp[kPbase * kChunk + lp]), b1 = __float_as_int(sp[(kPbase + 1) * kChunk + lp]),
+                  b2 = __float_as_int(sp[(kPbase + 2) * kChunk + lp]);
+        if (b0 != cb0 || b1 != cb1 || b2 != cb2) {
+          if (cb0 != INT_MIN) flush_run();
+          cb0 = b0;
+          cb1 = b1;
+          cb2 = b2;
+        }
+        if (lane < 27) {
+          // weights of bspline() (staged by the payload) and offsets as in p2g_node()
+          const float w = sp[(kPw + ox) * kChunk + lp] * sp[(kPw + 3 + oy) * kChunk + lp] *
+                          sp[(kPw + 6 + oz) * kChunk + lp];
+          const float dpos[3] = {(dox - sp[kPfx * kChunk + lp]) * mp.dx, (doy - sp[(kPfx + 1) * kChunk + lp]) * mp.dx,
+                                 (doz - sp[(kPfx + 2) * kChunk + lp]) * mp.dx};
+#pragma unroll
+          for (int q = 0; q < 3; ++q)
+            acc[q] += w * (sp[(kPmv + q) * kChunk + lp] + (sp[(kPaff + 3 * q) * kChunk + lp] * dpos[0] +
+                                                           sp[(kPaff + 3 * q + 1) * kChunk + lp] * dpos[1] +
+                                                           sp[(kPaff + 3 * q + 2) * kChunk + lp] * dpos[2]));
+          acc[3] += w * sp[kPmass * kChunk + lp];
+          if (REACT) {
+            const float f0 = sp[kPpf * kChunk + lp], f1 = sp[(kPpf + 1) * kChunk + lp],
+                        f2 = sp[(kPpf + 2) * kChunk + lp];
+            if (f0 != 0.f || f1 != 0.f || f2 != 0.f) {
+              const float v4 = w * f0, v5 = w * f1, v6 = w * f2;
+              acc[NQ - 3] += v4;
+              acc[NQ - 2] += v5;
+              acc[NQ - 1] += v6;
+              gsum[0] += v4;
+              gsum[1] += v5;
+              gsum[2] += v6;
+              gm2 = fmaxf(gm2, v4 * v4 + v5 * v5 + v6 * v6);
+            }
+          }
+        }
+      }
+      if (cb0 != INT_MIN) flush_run();
+      if (REACT) {
+#pragma unroll
+        for (int q = 0; q < 3; ++q) gn[q] += (double)gsum[q];
+        gmax = fmaxf(gmax, sqrtf(gm2));
+      }
+    }
+    __syncthreads();
+    for (int li = tid; li < nv; li += T) {
+      int i, j, k;
+      box_ijk(bx, li, i, j, k);
+      const int64_t node = ((int64_t)k * G + j) * G + i;
+#pragma unroll
+      for (int q = 0; q < 7; ++q) {
+        const float v = tile[q * nv + li];
+        if (v != 0.f) atomicAdd(dst[q] + node, v);
+      }
+    }
+  }
+  if (REACT && do_p2g) {
+    // diagnostics reductions (penalty.py:202-240, moving_boundary.py:312-374):
+    // warp, then CTA, then one global atomic per CTA and quantity
+    const int na = __reduce_add_sync(0xffffffffu, (unsigned)n_act);
+    const float pm = warp_max(pmax), gm = warp_max(gmax);
+    double r6[6];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      r6[r] = warp_sum_d(pn[r]);
+      r6[3 + r] = warp_sum_d(gn[r]);
+    }
+    if (lane == 0) {
+      s_cnt[wid] = na;
+      s_fmax[wid][0] = pm;
+      s_fmax[wid][1] = gm;
+#pragma unroll
+      for (int r = 0; r < 6; ++r) s_dsum[wid][r] = r6[r];
+    }
+    __syncthreads();
+    if (tid == 0) {
+      int ca = 0;
+      float m0 = 0.f, m1 = 0.f;
+      double d[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+      for (int w = 0; w < NW; ++w) {
+        ca += s_cnt[w];
+        m0 = fmaxf(m0, s_fmax[w][0]);
+        m1 = fmaxf(m1, s_fmax[w][1]);
+        for (int r = 0; r < 6; ++r) d[r] += s_dsum[w][r];
+      }
+      if (ca) atomicAdd(&st->active_reaction_particle_count, ca);
+      if (m0 > 0.f) atomic_max_nonneg(&st->max_particle_reaction_norm, m0);
+      if (m1 > 0.f) atomic_max_nonneg(&st->max_grid_reaction_norm, m1);
+      for (int r = 0; r < 3; ++r) {
+        if (d[r] != 0.0) atomicAdd(&st->net_particle_reaction[r], d[r]);
+        if (d[3 + r] != 0.0) atomicAdd(&st->net_grid_reaction[r], d[3 + r]);
+      }
     }
   }
 }
 
-template <int T>
-__global__ __launch_bounds__(T) void k_g2p_binned(FsiParticles pt, FsiGrid g, FsiGrid go, FsiMpmParams mp,
-                                                  const int32_t* __restrict__ perm,
-                                                  const int2* __restrict__ chunks, const int32_t* meta,
-                                                  const int32_t* __restrict__ box_b,
-                                                  const int32_t* __restrict__ box_o, int buf,
-                                                  FsiCouplingStats* st_other) {
+__global__ __launch_bounds__(kSeqT) void k_mpm_seq_prologue(const __grid_constant__ SeqArgs A) {
   griddep_wait();
   griddep_launch();
-  g2p_binned_body<T>(pt, g, go, mp, perm, chunks, meta, box_b, box_o, buf, st_other, blockIdx.x, gridDim.x);
+  seq_prologue_body(A, blockIdx.x, gridDim.x);
+}
+
+template <bool REACT>
+__global__ __launch_bounds__(kSeqT, 2) void k_mpm_seq(const __grid_constant__ SeqArgs A) {
+  griddep_wait();
+  griddep_launch();
+  mpm_seq_body<REACT>(A, blockIdx.x, gridDim.x);
 }
 
 __global__ void k_grid_velocity(FsiGrid g, FsiMpmParams mp, float* __restrict__ out) {
@@ -634,10 +817,11 @@ __global__ void k_grid_velocity(FsiGrid g, FsiMpmParams mp, float* __restrict__ 
 
 int layout(int32_t n_particles, int32_t n_grid, int32_t* n_bins, int32_t* max_chunks) {
   if (n_particles <= 0 || n_grid <= 0) return invalid("n_particles and n_grid must be positive");
+  if (n_grid > 1600) return invalid("n_grid above 1600 is not supported by the binned substeps");
   const int64_t nb = (n_grid + kEdge - 1) / kEdge;
   const int64_t bins = nb * nb * nb;
   const int64_t mc = ((int64_t)n_particles + kChunk - 1) / kChunk + std::min<int64_t>(n_particles, bins);
-  if (bins > INT_MAX || mc > INT_MAX / 12) return invalid("grid or particle count too large for binning");
+  if (bins > INT_MAX || mc > INT_MAX / 18) return invalid("grid or particle count too large for binning");
   *n_bins = (int32_t)bins;
   *max_chunks = (int32_t)mc;
   return FSI_OK;
@@ -645,8 +829,7 @@ int layout(int32_t n_particles, int32_t n_grid, int32_t* n_bins, int32_t* max_ch
 
 int check_bins(const FsiMpmBins* bins, int32_t n_particles, int32_t n_grid) {
   if (!bins) return invalid("null bins");
-  if (!bins->key || !bins->count || !bins->start || !bins->perm || !bins->chunk || !bins->box || !bins->meta ||
-      !bins->payload)
+  if (!bins->key || !bins->count || !bins->start || !bins->perm || !bins->chunk || !bins->box || !bins->meta)
     return invalid("null bins array");
   int32_t nb = 0, mc = 0;
   const int rc = layout(n_particles, n_grid, &nb, &mc);
@@ -685,6 +868,28 @@ int sm_count() {
 
 inline unsigned nblk(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
+// CTAs of a fused-sequence launch: one resident wave (at most one CTA per chunk)
+int seq_ctas(bool react, int max_chunks, int* ctas) {
+  static int occ[64][2] = {};
+  int dev = 0;
+  int rc = cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+  if (rc) return rc;
+  if (dev < 0 || dev >= 64) return invalid("device ordinal out of range");
+  int& o = occ[dev][react ? 1 : 0];
+  if (!o) {
+    void (*k)(const SeqArgs) = react ? k_mpm_seq<true> : k_mpm_seq<false>;
+    if ((rc = cuda_check(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSeqSmem),
+                         "k_mpm_seq shared memory")))
+      return rc;
+    int b = 0;
+    if ((rc = cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k, kSeqT, kSeqSmem), "k_mpm_seq occupancy")))
+      return rc;
+    o = b > 0 ? b : 1;
+  }
+  *ctas = std::max(1, std::min(max_chunks, sm_count() * o));
+  return FSI_OK;
+}
+
 }  // namespace
 }  // namespace fsi
 
@@ -709,21 +914,23 @@ extern "C" int fsi_mpm_bin(const FsiParticles* pt, const FsiGrid* g, const FsiMp
                                  bins->meta);
   if ((rc = launch_check("k_bin_scan"))) return rc;
   k_bin_scatter<<<nblk(pt->n, 256), 256, 0, st>>>(pt->n, bins->key, bins->start, bins->perm);
-  return launch_check("k_bin_scatter");
+  if ((rc = launch_check("k_bin_scatter"))) return rc;
+  k_bin_sort_chunks<<<(unsigned)std::min(bins->max_chunks, sm_count() * 8), kChunk, 0, st>>>(
+      *pt, mp->inv_dx, g->n, reinterpret_cast<const int2*>(bins->chunk), bins->meta, bins->perm);
+  return launch_check("k_bin_sort_chunks");
 }
 
-extern "C" int fsi_mpm_substep_binned(const FsiParticles* pt, const FsiGrid grid[2], const FsiMpmBins* bins,
-                                      const FsiMpmParams* mp, int32_t buffer, const FsiLbmState* s,
-                                      const float* hydro, const FsiCouplingParams* cp, FsiCouplingStats stats[2],
-                                      void* stream) {
+extern "C" int fsi_mpm_substeps_binned(const FsiParticles* pt, const FsiGrid grid[3], const FsiMpmBins* bins,
+                                       const FsiMpmParams* mp, int32_t n_substeps, const FsiLbmState* s,
+                                       const float* hydro, const FsiCouplingParams* cp, FsiCouplingStats stats[3],
+                                       void* stream) {
   int rc = check_particles(pt);
   if (rc) return rc;
   if (!grid || !mp) return invalid("null grid or params");
-  if ((rc = check_grid(&grid[0])) || (rc = check_grid(&grid[1]))) return rc;
-  if (grid[0].n != grid[1].n) return invalid("the two grid buffers differ in size");
-  if (buffer != 0 && buffer != 1) return invalid("buffer must be 0 or 1");
-  if (mp->tune < 0 || mp->tune > 15 || (mp->tune & 3) > 1 || ((mp->tune >> 2) & 3) == 3)
-    return invalid("unknown FsiMpmParams.tune");
+  for (int b = 0; b < 3; ++b)
+    if ((rc = check_grid(&grid[b]))) return rc;
+  if (grid[0].n != grid[1].n || grid[0].n != grid[2].n) return invalid("the three grid buffers differ in size");
+  if (n_substeps < 0) return invalid("n_substeps must be >= 0");
   if ((rc = check_bins(bins, pt->n, grid[0].n))) return rc;
   if (cp) {
     if (!s || !hydro || !stats) return invalid("reaction transfer needs the lattice state, hydro and stats");
@@ -733,51 +940,37 @@ extern "C" int fsi_mpm_substep_binned(const FsiParticles* pt, const FsiGrid grid
     if (cp->inv_dx_norm != mp->inv_dx)
       return invalid("binned substep needs the coupling and MPM grids to share dx (inv_dx_norm == inv_dx)");
   }
-  cudaStream_t st = (cudaStream_t)stream;
-  const int grid_ctas = (int)std::min<int64_t>(bins->max_chunks, (int64_t)sm_count() * 4);
-  int32_t* box_b = bins->box + (int64_t)6 * bins->max_chunks * buffer;
-  int32_t* box_o = bins->box + (int64_t)6 * bins->max_chunks * (1 - buffer);
-  const int2* chunks = reinterpret_cast<const int2*>(bins->chunk);
-  const FsiGrid g = grid[buffer], go = grid[1 - buffer];
-  const int tsc = mp->tune & 3, tg = (mp->tune >> 2) & 3;
-  const int T = tsc == FSI_TUNE_P2G_T384 ? 384 : 128;
-  const int TG = tg == FSI_TUNE_MPM_T512 ? 512 : (tg == FSI_TUNE_MPM_T256 ? 256 : 128);
-  const LatView L = cp ? LatView{s->nx, s->ny, s->nz, s->pitch} : LatView{0, 0, 0, 0};
-  const float* hy = cp ? hydro : nullptr;
-  const float* ph = cp ? s->phi : nullptr;
-  const FsiCouplingParams cpv = cp ? *cp : FsiCouplingParams{};
-  FsiCouplingStats* stb = cp ? &stats[buffer] : nullptr;
-  const FsiLbmDiag* dg = cp ? s->diag : nullptr;
-  // the three kernels of a substep, and the substeps, follow each other with
-  // programmatic dependent launch (each waits for its predecessor's writes)
-  const unsigned gp = nblk(2 * (int64_t)pt->n, 128);
-  cudaError_t lerr;
-  if (cp)
-    lerr = launch_pdl(k_p2g_payload<true>, dim3(gp), dim3(128), 0, st, *pt, *mp, (const int32_t*)bins->perm,
-                      bins->payload, L, hy, ph, cpv, stb, dg);
-  else
-    lerr = launch_pdl(k_p2g_payload<false>, dim3(gp), dim3(128), 0, st, *pt, *mp, (const int32_t*)bins->perm,
-                      bins->payload, L, hy, ph, cpv, stb, dg);
-  if ((rc = cuda_check(lerr, "k_p2g_payload (launch)")) || (rc = launch_check("k_p2g_payload"))) return rc;
-#define FSI_P2G(R, TT)                                                                                        \
-  lerr = launch_pdl(k_p2g_scatter<R, TT>, dim3(grid_ctas), dim3(TT), 0, st, g, *mp,                         \
-                    (const float*)bins->payload, pt->n, chunks, bins->meta, box_b, buffer, stb)
+  if (n_substeps == 0) return FSI_OK;
+  SeqArgs A{};
+  A.pt = *pt;
+  for (int b = 0; b < 3; ++b) A.grid[b] = grid[b];
+  A.mp = *mp;
+  A.perm = bins->perm;
+  A.chunks = reinterpret_cast<const int2*>(bins->chunk);
+  A.meta = bins->meta;
+  A.box = bins->box;
+  A.box_stride = (int64_t)6 * bins->max_chunks;
   if (cp) {
-    if (T == 384) FSI_P2G(true, 384); else FSI_P2G(true, 128);
-  } else {
-    if (T == 384) FSI_P2G(false, 384); else FSI_P2G(false, 128);
+    A.L = LatView{s->nx, s->ny, s->nz, s->pitch};
+    A.hydro = hydro;
+    A.phi = s->phi;
+    A.cp = *cp;
+    A.stats = stats;
+    A.diag = s->diag;
   }
-#undef FSI_P2G
-  if ((rc = cuda_check(lerr, "k_p2g_scatter (launch)")) || (rc = launch_check("k_p2g_scatter"))) return rc;
-  FsiCouplingStats* sto = cp ? &stats[1 - buffer] : nullptr;
-#define FSI_G2P(TT)                                                                                       \
-  lerr = launch_pdl(k_g2p_binned<TT>, dim3(grid_ctas), dim3(TT), 0, st, *pt, g, go, *mp,                   \
-                    (const int32_t*)bins->perm, chunks, (const int32_t*)bins->meta, (const int32_t*)box_b, \
-                    (const int32_t*)box_o, buffer, sto)
-  if (TG == 512) FSI_G2P(512); else if (TG == 256) FSI_G2P(256); else FSI_G2P(128);
-#undef FSI_G2P
-  if ((rc = cuda_check(lerr, "k_g2p_binned (launch)"))) return rc;
-  return launch_check("k_g2p_binned");
+  A.M = n_substeps;
+  int ctas = 0;
+  if ((rc = seq_ctas(cp != nullptr, bins->max_chunks, &ctas))) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaError_t lerr = launch_pdl(k_mpm_seq_prologue, dim3(ctas), dim3(kSeqT), 0, st, A);
+  if ((rc = cuda_check(lerr, "k_mpm_seq_prologue (launch)")) || (rc = launch_check("k_mpm_seq_prologue"))) return rc;
+  for (int i = 0; i <= n_substeps; ++i) {
+    A.s = i;
+    lerr = cp ? launch_pdl(k_mpm_seq<true>, dim3(ctas), dim3(kSeqT), kSeqSmem, st, A)
+              : launch_pdl(k_mpm_seq<false>, dim3(ctas), dim3(kSeqT), kSeqSmem, st, A);
+    if ((rc = cuda_check(lerr, "k_mpm_seq (launch)")) || (rc = launch_check("k_mpm_seq"))) return rc;
+  }
+  return FSI_OK;
 }
 
 extern "C" int fsi_mpm_grid_velocity(const FsiGrid* g, const FsiMpmParams* mp, float* out, void* stream) {
@@ -824,50 +1017,56 @@ __global__ void k_batch_bin_scatter(const FsiBatchCase* __restrict__ cases) {
     bin_scatter_body(bc.pt.n, bc.bins.key, bc.bins.start, bc.bins.perm, vb, nvb);
 }
 
-__global__ __launch_bounds__(128) void k_batch_p2g_payload(const FsiBatchCase* __restrict__ cases) {
-  const FsiBatchCase& bc = cases[blockIdx.y];
-  if (!bc.active) return;
-  const LatView L{bc.lbm.nx, bc.lbm.ny, bc.lbm.nz, bc.lbm.pitch};
-  const int nvb = (2 * bc.pt.n + blockDim.x - 1) / blockDim.x;  // two lanes per particle
-  const float* hydro = batch_hydro(bc);
-  for (int vb = blockIdx.x; vb < nvb; vb += gridDim.x)
-    p2g_payload_body<true>(bc.pt, bc.mp, bc.bins.perm, bc.bins.payload, L, hydro, bc.lbm.phi, bc.cp,
-                           &bc.react_stats[bc.buf], bc.lbm.diag, vb, nvb);
+// the sequence arguments of a batched case (one thread, into shared memory)
+__device__ __forceinline__ void load_batch_seq(const FsiBatchCase& bc, int s, int M, SeqArgs* A) {
+  A->pt = bc.pt;
+#pragma unroll
+  for (int b = 0; b < 3; ++b) A->grid[b] = bc.grid[b];
+  A->mp = bc.mp;
+  A->perm = bc.bins.perm;
+  A->chunks = reinterpret_cast<const int2*>(bc.bins.chunk);
+  A->meta = bc.bins.meta;
+  A->box = bc.bins.box;
+  A->box_stride = (int64_t)6 * bc.bins.max_chunks;
+  A->L = LatView{bc.lbm.nx, bc.lbm.ny, bc.lbm.nz, bc.lbm.pitch};
+  A->hydro = batch_hydro(bc);
+  A->phi = bc.lbm.phi;
+  A->cp = bc.cp;
+  A->stats = bc.react_stats;
+  A->diag = bc.lbm.diag;
+  A->s = s;
+  A->M = M;
 }
 
-template <int T>
-__global__ __launch_bounds__(T, T == 384 ? 1 : 4) void k_batch_p2g_scatter(const FsiBatchCase* __restrict__ cases) {
+__global__ __launch_bounds__(kSeqT) void k_batch_mpm_seq_prologue(const FsiBatchCase* __restrict__ cases) {
+  __shared__ SeqArgs A;
   const FsiBatchCase& bc = cases[blockIdx.y];
   if (!bc.active) return;
-  const int b = bc.buf;
-  int32_t* box_b = bc.bins.box + (int64_t)6 * bc.bins.max_chunks * b;
-  p2g_scatter_body<true, T>(bc.grid[b], bc.mp, bc.bins.payload, bc.pt.n, reinterpret_cast<const int2*>(bc.bins.chunk),
-                            bc.bins.meta, box_b, b, &bc.react_stats[b], blockIdx.x, gridDim.x);
+  if (threadIdx.x == 0) load_batch_seq(bc, 0, 1, &A);
+  __syncthreads();
+  seq_prologue_body(A, blockIdx.x, gridDim.x);
 }
 
-template <int T>
-__global__ __launch_bounds__(T) void k_batch_g2p(const FsiBatchCase* __restrict__ cases) {
+__global__ __launch_bounds__(kSeqT, 2) void k_batch_mpm_seq(const FsiBatchCase* __restrict__ cases, int s, int M) {
+  __shared__ SeqArgs A;
   const FsiBatchCase& bc = cases[blockIdx.y];
   if (!bc.active) return;
-  const int b = bc.buf;
-  const int32_t* box_b = bc.bins.box + (int64_t)6 * bc.bins.max_chunks * b;
-  const int32_t* box_o = bc.bins.box + (int64_t)6 * bc.bins.max_chunks * (1 - b);
-  g2p_binned_body<T>(bc.pt, bc.grid[b], bc.grid[1 - b], bc.mp, bc.bins.perm,
-                     reinterpret_cast<const int2*>(bc.bins.chunk), bc.bins.meta, box_b, box_o, b,
-                     &bc.react_stats[1 - b], blockIdx.x, gridDim.x);
+  if (threadIdx.x == 0) load_batch_seq(bc, s, M, &A);
+  __syncthreads();
+  mpm_seq_body<true>(A, blockIdx.x, gridDim.x);
 }
 
-__global__ void k_batch_mpm_post(FsiBatchCase* cases) {
-  FsiBatchCase& bc = cases[blockIdx.x];
-  if (bc.active && threadIdx.x == 0) bc.buf ^= 1;
+__global__ __launch_bounds__(kChunk) void k_batch_bin_sort_chunks(const FsiBatchCase* __restrict__ cases) {
+  const FsiBatchCase& bc = cases[blockIdx.y];
+  if (!bc.active) return;
+  chunk_sort_body(bc.pt, bc.mp.inv_dx, bc.grid[0].n, reinterpret_cast<const int2*>(bc.bins.chunk), bc.bins.meta,
+                  bc.bins.perm, blockIdx.x, gridDim.x);
 }
 
 int check_batch_mpm(const FsiBatchCase* cases, const FsiBatchDims* d) {
   if (!cases || !d) return invalid("null batch argument");
   if (d->n_cases <= 0 || d->n_cases > 65535) return invalid("n_cases must be in 1..65535");
   if (d->max_particles <= 0 || d->max_chunks <= 0 || d->max_bins <= 0) return invalid("batch MPM dims must be positive");
-  if (d->mpm_tune < 0 || d->mpm_tune > 15 || (d->mpm_tune & 3) > 1 || ((d->mpm_tune >> 2) & 3) == 3)
-    return invalid("unknown FsiBatchDims.mpm_tune");
   return FSI_OK;
 }
 
@@ -884,32 +1083,43 @@ extern "C" int fsi_batch_mpm_bin(FsiBatchCase* cases, const FsiBatchDims* d, voi
   k_batch_bin_scan<<<dim3(1, d->n_cases), 1024, 0, st>>>(cases);
   if ((rc = launch_check("k_batch_bin_scan"))) return rc;
   k_batch_bin_scatter<<<g, 256, 0, st>>>(cases);
-  return launch_check("k_batch_bin_scatter");
+  if ((rc = launch_check("k_batch_bin_scatter"))) return rc;
+  k_batch_bin_sort_chunks<<<dim3((unsigned)std::min(d->max_chunks, 2 * (int)nblk(d->max_particles, kChunk) + 8),
+                                 d->n_cases),
+                            kChunk, 0, st>>>(cases);
+  return launch_check("k_batch_bin_sort_chunks");
 }
 
-extern "C" int fsi_batch_mpm_substep(FsiBatchCase* cases, const FsiBatchDims* d, void* stream) {
+extern "C" int fsi_batch_mpm_substeps(FsiBatchCase* cases, const FsiBatchDims* d, int32_t n_substeps,
+                                      void* stream) {
   int rc = check_batch_mpm(cases, d);
   if (rc) return rc;
+  if (n_substeps < 0) return invalid("n_substeps must be >= 0");
+  if (n_substeps == 0) return FSI_OK;
   cudaStream_t st = (cudaStream_t)stream;
-  const dim3 gp(nblk(2 * (int64_t)d->max_particles, 128), d->n_cases);
-  k_batch_p2g_payload<<<gp, 128, 0, st>>>(cases);
-  if ((rc = launch_check("k_batch_p2g_payload"))) return rc;
+  {
+    // once per device (not during stream capture of a later call)
+    static bool attr_set[64] = {};
+    int dev = 0;
+    if ((rc = cuda_check(cudaGetDevice(&dev), "cudaGetDevice"))) return rc;
+    if (dev < 0 || dev >= 64) return invalid("device ordinal out of range");
+    if (!attr_set[dev]) {
+      if ((rc = cuda_check(cudaFuncSetAttribute(k_batch_mpm_seq, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                (int)kSeqSmem),
+                           "k_batch_mpm_seq shared memory")))
+        return rc;
+      attr_set[dev] = true;
+    }
+  }
   // about one CTA per chunk of the largest case (a bin's chunks hold <= 128 particles each; bins
   // partly filled add chunks): CTAs stride over the case's chunk table
-  const dim3 gc((unsigned)std::min<int64_t>(d->max_chunks, 2 * nblk(d->max_particles, kChunk) + 8), d->n_cases);
-  const int tsc = d->mpm_tune & 3, tg = (d->mpm_tune >> 2) & 3;
-  if (tsc == FSI_TUNE_P2G_T384)
-    k_batch_p2g_scatter<384><<<gc, 384, 0, st>>>(cases);
-  else
-    k_batch_p2g_scatter<128><<<gc, 128, 0, st>>>(cases);
-  if ((rc = launch_check("k_batch_p2g_scatter"))) return rc;
-  if (tg == FSI_TUNE_MPM_T512)
-    k_batch_g2p<512><<<gc, 512, 0, st>>>(cases);
-  else if (tg == FSI_TUNE_MPM_T256)
-    k_batch_g2p<256><<<gc, 256, 0, st>>>(cases);
-  else
-    k_batch_g2p<128><<<gc, 128, 0, st>>>(cases);
-  if ((rc = launch_check("k_batch_g2p"))) return rc;
-  k_batch_mpm_post<<<d->n_cases, 32, 0, st>>>(cases);
-  return launch_check("k_batch_mpm_post");
+  const unsigned gx = (unsigned)std::min<int64_t>(d->max_chunks, 2 * nblk(d->max_particles, kChunk) + 8);
+  const dim3 gc(gx, d->n_cases);
+  k_batch_mpm_seq_prologue<<<gc, kSeqT, 0, st>>>(cases);
+  if ((rc = launch_check("k_batch_mpm_seq_prologue"))) return rc;
+  for (int i = 0; i <= n_substeps; ++i) {
+    k_batch_mpm_seq<<<gc, kSeqT, kSeqSmem, st>>>(cases, i, n_substeps);
+    if ((rc = launch_check("k_batch_mpm_seq"))) return rc;
+  }
+  return FSI_OK;
 }

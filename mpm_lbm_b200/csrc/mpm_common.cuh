@@ -1,6 +1,6 @@
 // Per-particle and per-node pieces of the MPM substep and of the reaction
 // transfer, shared by the one-phase-per-launch kernels (mpm_kernels.cu) and
-// the binned, shared-memory-staged substep (mpm_fused.cu) so that both paths
+// the binned, shared-memory-staged substep (mpm_binned.cu) so that both paths
 // perform the same arithmetic.
 //
 // Reference semantics:
@@ -79,14 +79,17 @@ struct P2GParticle {
   float aff[9];  // -dt vol0 P F^T inv_dx^2 + m C (solid.py:239: no factor 4)
 };
 
-__device__ __forceinline__ void p2g_particle(const FsiParticles& pt, int p, const FsiMpmParams& mp, P2GParticle& q) {
-  const int n = pt.n;
+// the particle's state read from rows of stride `ld` (global SoA fields with
+// ld = n, or a shared-memory stage with ld = chunk size), column `col`
+__device__ __forceinline__ void p2g_particle_rows(const float* __restrict__ Frow, const float* __restrict__ Crow,
+                                                  const float* __restrict__ vrow, int64_t ld, int col, float mass,
+                                                  float vol0, const FsiMpmParams& mp, P2GParticle& q) {
   float Fp[9], Cp[9];
   double Fd[9], Rd[9];
 #pragma unroll
   for (int a = 0; a < 9; ++a) {
-    Fp[a] = pt.F[(int64_t)a * n + p];
-    Cp[a] = pt.C[(int64_t)a * n + p];
+    Fp[a] = Frow[a * ld + col];
+    Cp[a] = Crow[a * ld + col];
     Fd[a] = (double)Fp[a];
   }
   polar_rotation_d(Fd, Rd);
@@ -111,8 +114,7 @@ __device__ __forceinline__ void p2g_particle(const FsiParticles& pt, int p, cons
   float P[9];
 #pragma unroll
   for (int a = 0; a < 9; ++a) P[a] = mu2 * (Fp[a] - (float)Rd[a]) + lam * FinvT[a];
-  const float pre = -mp.dt * pt.vol0[p];
-  const float mass = pt.mass[p];
+  const float pre = -mp.dt * vol0;
   q.mass = mass;
 #pragma unroll
   for (int i = 0; i < 3; ++i)
@@ -123,7 +125,11 @@ __device__ __forceinline__ void p2g_particle(const FsiParticles& pt, int p, cons
       q.aff[i * 3 + j] = pf * mp.inv_dx * mp.inv_dx + mass * Cp[i * 3 + j];
     }
 #pragma unroll
-  for (int a = 0; a < 3; ++a) q.mv[a] = mass * pt.v[(int64_t)a * n + p];
+  for (int a = 0; a < 3; ++a) q.mv[a] = mass * vrow[a * ld + col];
+}
+
+__device__ __forceinline__ void p2g_particle(const FsiParticles& pt, int p, const FsiMpmParams& mp, P2GParticle& q) {
+  p2g_particle_rows(pt.F, pt.C, pt.v, pt.n, p, pt.mass[p], pt.vol0[p], mp, q);
 }
 
 // momentum carried to the node at stencil offset (ox, oy, oz)
@@ -225,9 +231,12 @@ __device__ __forceinline__ float det3(const float (&M)[9]) {
 }
 
 // advect, clamp, update F and apply the step-112 controls, then store
-// (solid.py:261-315); nv and nC are the gathered velocity and affine matrix
+// (solid.py:261-315); nv and nC are the gathered velocity and affine matrix.
+// With a stage (rows x 3, v 3, C 9, F 9 of stride ld, column col) the new
+// state is also written there.
 __device__ __forceinline__ void g2p_finish(const FsiParticles& pt, int p, const FsiMpmParams& mp, float X[3],
-                                           const float nv[3], float nC[9]) {
+                                           const float nv[3], float nC[9], float* stage = nullptr, int ld = 0,
+                                           int col = 0) {
   const int n = pt.n;
   float v[3];
 #pragma unroll
@@ -303,6 +312,18 @@ __device__ __forceinline__ void g2p_finish(const FsiParticles& pt, int p, const 
     pt.F[(int64_t)a * n + p] = Fn[a];
   }
   pt.Jp[p] = J;
+  if (stage) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      stage[a * ld + col] = X[a];
+      stage[(3 + a) * ld + col] = v[a];
+    }
+#pragma unroll
+    for (int a = 0; a < 9; ++a) {
+      stage[(6 + a) * ld + col] = nC[a];
+      stage[(15 + a) * ld + col] = Fn[a];
+    }
+  }
 }
 
 // one gathered node's contribution to the particle velocity and affine matrix

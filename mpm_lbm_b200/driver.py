@@ -46,7 +46,7 @@ class FSIDriver3D:
                  lattice_shape=None, material=None, static_solid=None, initial_particles=None, use_cuda_graph=False,
                  mpm_path="binned", device=None):
         if mpm_path not in ("binned", "one_phase"):
-            raise ValueError("mpm_path must be 'binned' (fsi_mpm_substep_binned) or 'one_phase' (one kernel per phase)")
+            raise ValueError("mpm_path must be 'binned' (fsi_mpm_substeps_binned) or 'one_phase' (one kernel per phase)")
         self.mpm_path = mpm_path
         self.config = config
         self.out_dir = out_dir
@@ -197,7 +197,7 @@ class FSIDriver3D:
         """Time the launch variants of the step kernels on this case's state and
         keep the fastest (results are identical across variants).  Drops a
         captured step graph so that the next step recaptures with the choice."""
-        from .autotune import tune_lbm, tune_mpm
+        from .autotune import tune_lbm
 
         if not self.initialized:
             self.initialize()
@@ -213,14 +213,6 @@ class FSIDriver3D:
             self.tuning = {"lbm": tune_lbm(self.lbm, step)}
         finally:
             self.lbm.dirstats_enabled = saved
-        if self.mpm_path == "binned":
-            mode = self.config.coupling_mode
-            coupler = {"penalty": self.penalty_coupler, "none": None}.get(mode)
-            if mode == "moving_boundary":
-                coupler = self.mb_coupler if self.mb_coupler is not None else self.link_area_coupler
-            lbm = self.lbm if coupler is not None else None
-            extra = () if coupler is None else (coupler.binned_stats.t,)
-            self.tuning["mpm"] = tune_mpm(self.solid, lambda: self.solid.substep_binned(coupler, lbm), extra=extra)
         return self.tuning
 
     # ------------------------------------------------------------ steps
@@ -230,11 +222,10 @@ class FSIDriver3D:
         self.timing[key] += time.perf_counter() - t0
 
     def _graph_period(self):
-        # the captured sequence must return the AA layout parity, the ping-pong slot and the binned
-        # substep's grid buffer to their start values
+        # the captured sequence must return the AA layout parity and the ping-pong slot to their
+        # start values (the binned MPM substeps of every FSI step start from the same buffers)
         S = self.config.lbm_substeps_per_fsi_step if self.config.fsi_exchange_mode == "lbm_subcycled_per_fsi_step" else 1
-        M = self.config.mpm_substeps_per_lbm_step if self.mpm_path == "binned" else 0
-        return 2 if S % 2 or M % 2 else 1
+        return 2 if S % 2 else 1
 
     def step_once(self):
         if not self.initialized:
@@ -314,9 +305,8 @@ class FSIDriver3D:
         M = self.config.mpm_substeps_per_lbm_step
         if self.mpm_path == "binned":
             self.solid.rebin()
-            for _ in range(M):
-                self.solid.substep_binned(coupler, self.lbm if coupler is not None else None)
-                self.total_mpm_substeps += 1
+            self.solid.substeps_binned(M, coupler, self.lbm if coupler is not None else None)
+            self.total_mpm_substeps += M
         else:
             for _ in range(M):
                 self.solid.clear_grid()

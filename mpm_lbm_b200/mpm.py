@@ -14,7 +14,7 @@ import os
 import numpy as np
 import torch
 
-from ._lib import (FSI_MPM_PAYLOAD_ROWS, FsiCouplingStats, FsiGrid, FsiMpmBins, FsiMpmParams, FsiParticles, call,
+from ._lib import (FsiCouplingStats, FsiGrid, FsiMpmBins, FsiMpmParams, FsiParticles, call,
                    ptr, stream_handle)
 from .config import MPMConfig
 from .fields import ParticleField
@@ -120,11 +120,11 @@ class MPMSolid3D:
         self.grid_v = _GridField(self._grid_velocity, self.n_grid, 3, lambda: self._one_phase_grid()[0])
         self.grid_m = _GridField(lambda: self._last_grid()[1], self.n_grid, 0, lambda: self._one_phase_grid()[1])
         self.grid_f_ext = _GridField(lambda: self._last_grid()[2], self.n_grid, 3, lambda: self._one_phase_grid()[2])
-        # binned substep (fsi_mpm_substep_binned): second grid buffer and bins, made on first use
+        # binned substeps (fsi_mpm_substeps_binned): three grid buffers and bins, made on first use
         self._bins = None
-        self._buf = 0             # buffer the next binned substep scatters into
         self._binned_last = None  # buffer of the last binned substep while the grid holds its result
-        self._binned_clean = True  # both buffers zero outside the recorded boxes
+        self._binned_clean = True  # the buffers are zero outside the recorded boxes
+        self._binned_mode = "seq"
         self._since_bin = 0
         self.rebin_interval = 64  # binned substeps between automatic re-binnings
 
@@ -246,20 +246,21 @@ class MPMSolid3D:
         i32 = lambda *s: torch.zeros(*s, dtype=torch.int32, device=dev)  # noqa: E731
         f32 = lambda *s: torch.zeros(*s, dtype=torch.float32, device=dev)  # noqa: E731
         t = {"key": i32(n), "count": i32(nb.value), "start": i32(nb.value), "perm": i32(n),
-             "chunk": i32(mc.value, 2), "box": i32(2, mc.value, 6), "meta": i32(4),
-             "payload": f32(FSI_MPM_PAYLOAD_ROWS, n)}
+             "chunk": i32(mc.value, 2), "box": i32(3, mc.value, 6), "meta": i32(8)}
         self.t_gv1, self.t_gm1, self.t_gf1 = f32(3, G), f32(G), f32(3, G)
-        grids = (FsiGrid * 2)()
+        self.t_gv2, self.t_gm2, self.t_gf2 = f32(3, G), f32(G), f32(3, G)
+        grids = (FsiGrid * 3)()
         grids[0] = self.grid
         grids[1] = FsiGrid(n=self.n_grid, v=ptr(self.t_gv1), m=ptr(self.t_gm1), f_ext=ptr(self.t_gf1))
+        grids[2] = FsiGrid(n=self.n_grid, v=ptr(self.t_gv2), m=ptr(self.t_gm2), f_ext=ptr(self.t_gf2))
         bins = FsiMpmBins(n_bins=nb.value, max_chunks=mc.value, **{k: ptr(v) for k, v in t.items()})
         self._bins = {"t": t, "grids": grids, "struct": bins}
         self._binned_clean = True
-        self._buf = 0
         self._since_bin = None
 
     def _buffers(self, b):
-        return (self.t_gv, self.t_gm, self.t_gf) if b == 0 else (self.t_gv1, self.t_gm1, self.t_gf1)
+        return ((self.t_gv, self.t_gm, self.t_gf), (self.t_gv1, self.t_gm1, self.t_gf1),
+                (self.t_gv2, self.t_gm2, self.t_gf2))[b]
 
     def _last_grid(self):
         """(momentum or velocity, mass, f_ext) tensors of the last grid state."""
@@ -290,14 +291,14 @@ class MPMSolid3D:
 
     # ---- state snapshots (trial substeps, e.g. autotuning) ----------------
     _SNAPSHOT = ("t_x", "t_v", "t_C", "t_F", "t_Jp", "t_gv", "t_gm", "t_gf")
-    _SNAPSHOT_ATTRS = ("_buf", "_binned_last", "_binned_clean", "_since_bin")
+    _SNAPSHOT_ATTRS = ("_binned_last", "_binned_clean", "_binned_mode", "_since_bin")
 
     def snapshot(self, extra=()):
         """Device copies of the mutable particle, grid and bin state (plus the
         given extra tensors)."""
         names = list(self._SNAPSHOT)
         if self._bins is not None:
-            names += ["t_gv1", "t_gm1", "t_gf1"]
+            names += ["t_gv1", "t_gm1", "t_gf1", "t_gv2", "t_gm2", "t_gf2"]
         tensors = {k: getattr(self, k).clone() for k in names}
         bins = {} if self._bins is None else {k: v.clone() for k, v in self._bins["t"].items()}
         return (tensors, bins, [(t, t.clone()) for t in extra], {k: getattr(self, k) for k in self._SNAPSHOT_ATTRS})
@@ -321,15 +322,24 @@ class MPMSolid3D:
         self._since_bin = 0
 
     def substep_binned(self, coupler=None, lbm=None):
-        """One substep through fsi_mpm_substep_binned: the same update as
-        substep() (plus the coupler's reaction transfer when given, as the
-        driver's MPM loops call it), with binned, shared-memory-staged P2G."""
+        """One substep through the binned path: the same update as substep()
+        (plus the coupler's reaction transfer when given, as the driver's MPM
+        loops call it), with binned, shared-memory-staged P2G."""
+        self.substeps_binned(1, coupler, lbm)
+
+    def substeps_binned(self, count, coupler=None, lbm=None):
+        """`count` substeps through fsi_mpm_substeps_binned (one launch per
+        substep: the gather of one substep, the stress, reaction and scatter
+        of the next), re-binning first when the bins are due."""
+        if count <= 0:
+            return
         self._ensure_binned()
-        if not self._binned_clean:
-            for t in self._buffers(0) + self._buffers(1):
-                t.zero_()
-            self._bins["t"]["meta"][1:3].zero_()  # no recorded boxes; the chunk table stays valid
-            self._buf, self._binned_last, self._binned_clean = 0, None, True
+        if self._binned_mode != "seq" or not self._binned_clean:
+            for b in range(3):
+                for t in self._buffers(b):
+                    t.zero_()
+            self._bins["t"]["meta"][1:].zero_()  # no recorded boxes; the chunk table stays valid
+            self._binned_last, self._binned_clean, self._binned_mode = None, True, "seq"
         if self._since_bin is None or self._since_bin >= self.rebin_interval:
             self.rebin()
         if coupler is not None:
@@ -337,13 +347,13 @@ class MPMSolid3D:
             args = (ctypes.byref(state), ptr(hydro), ctypes.byref(cp), stats)
         else:
             args = (None, None, None, None)
-        call("fsi_mpm_substep_binned", ctypes.byref(self.particles), self._bins["grids"],
-             ctypes.byref(self._bins["struct"]), ctypes.byref(self.params), self._buf, *args, self._stream())
+        call("fsi_mpm_substeps_binned", ctypes.byref(self.particles), self._bins["grids"],
+             ctypes.byref(self._bins["struct"]), ctypes.byref(self.params), int(count), *args, self._stream())
+        last = (count - 1) % 3
         if coupler is not None:
-            coupler._binned_slot = self._buf
-        self._binned_last = self._buf
-        self._buf ^= 1
-        self._since_bin += 1
+            coupler._binned_slot = last
+        self._binned_last = last
+        self._since_bin += count
 
     def inside_grid(self, I):
         return all(0 <= int(i) < self.n_grid for i in I)

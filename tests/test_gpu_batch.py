@@ -74,8 +74,8 @@ def test_batched_cases_match_single_case_runs(alone, use_graph, lbm_tune):
     for slot, ref in zip(slots, alone):
         _compare(_fields(batch.sync_case(slot)), ref)
     if use_graph:
-        # one launch per phase: project 3, mask 4, LBM 3, bin 3, M x (payload, scatter, gather, post)
-        assert batch.graph_kernels == 3 + 4 + 3 + 3 + 4 * 4
+        # one launch per phase: project 3, mask 4, LBM 3, bin 4, MPM prologue + M + 1
+        assert batch.graph_kernels == 3 + 4 + 3 + 4 + 4 + 2
 
 
 def test_slot_reuse_and_empty_slots(alone):

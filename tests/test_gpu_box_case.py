@@ -28,16 +28,15 @@ def _case(mode):
                    mpm_substeps=10, dt_lbm=4e-3, seed=0)
 
 
-@pytest.mark.parametrize("variants", [(0, 0, False), (1, 1, True), (2, 1 | 2 << 2, True)])
+@pytest.mark.parametrize("variants", [(0, False), (1, True), (2, True)])
 @pytest.mark.parametrize("mode", ["moving_boundary", "penalty"])
 def test_box_case_matches_oracle(mode, variants):
     import torch
 
-    lbm_tune, mpm_tune, graph = variants
+    lbm_tune, graph = variants
     case = _case(mode)
     drv = case.make_driver()
     drv.lbm.tune = lbm_tune
-    drv.solid.params.tune = mpm_tune
     drv.use_cuda_graph = graph
     ora = orc.fsi_driver_for_box_case(case, threads=4)
     for _ in range(STEPS):

@@ -2,7 +2,7 @@
 
 Covers the one-phase kernels (fsi_mpm_p2g / grid_update / g2p and
 fsi_reaction_to_grid, mpm/solid.py:212-315, coupling/*.py reaction
-transfers), the binned substep (fsi_mpm_bin + fsi_mpm_substep_binned) and the
+transfers), the binned substeps (fsi_mpm_bin + fsi_mpm_substeps_binned) and the
 particle binning itself, which is integer work and must be bit-exact.
 
 Tolerances: grid sums are FP32 atomics whose order differs between the GPU and
@@ -127,6 +127,14 @@ def test_binning_is_bit_exact(case):
     for b in np.nonzero(counts)[0]:
         got = np.sort(perm[start[b]: start[b] + counts[b]])
         np.testing.assert_array_equal(got, np.nonzero(key == b)[0])
+    # within each chunk the particles are ordered by (base node z, y, x, particle id)
+    xp = (x.astype(np.float32) * np.float32(N_GRID)).astype(np.float32)
+    base = np.clip((xp - np.float32(0.5)).astype(np.int32), -1, N_GRID) + 1
+    cell = (base[:, 2].astype(np.int64) * (N_GRID + 2) + base[:, 1]) * (N_GRID + 2) + base[:, 0]
+    for first, cnt in chunks:
+        ids = perm[first: first + cnt]
+        order = np.lexsort((ids, cell[ids]))
+        np.testing.assert_array_equal(order, np.arange(cnt))
 
 
 def test_one_phase_substeps_match_oracle():
@@ -138,24 +146,24 @@ def test_one_phase_substeps_match_oracle():
     compare_grid(gpu, ora)
 
 
-# FsiMpmParams.tune: scatter variant (128 / 384 threads per chunk CTA) |
-# gather variant (128 / 256 / 512 threads) << 2
-TUNES = [0, 1 | 1 << 2, 1 | 2 << 2, 2 << 2]
+META_OVERFLOW = 4  # bins->meta[4]: chunks scattered without the shared-memory tile
 
 
-@pytest.mark.parametrize("tune", TUNES)
+@pytest.mark.parametrize("calls", [[1] * 5, [5], [2, 4, 1], [7]])
 @pytest.mark.parametrize("lock_z,damping", [(False, 0.0), (True, 0.0), (False, 5.0)])
-def test_binned_substeps_match_oracle(lock_z, damping, tune):
+def test_binned_substeps_match_oracle(lock_z, damping, calls):
+    """fsi_mpm_substeps_binned called with the given substep counts in turn:
+    every buffer of the rotation, the zeroing of recorded boxes within a call
+    and by the next call's prologue are exercised."""
     gpu, ora = make_solids(lock_z=lock_z, damping=damping)
-    gpu.params.tune = tune
-    for s in range(5):  # both grid buffers, and the zeroing of recorded boxes, are exercised
-        gpu.substep_binned()
-        ora.substep()
-        if s == 2:
-            compare_grid(gpu, ora)
+    for count in calls:
+        gpu.substeps_binned(count)
+        for _ in range(count):
+            ora.substep()
+        compare_grid(gpu, ora)
     compare_particles(gpu, ora)
     compare_grid(gpu, ora)
-    assert int(gpu._bins["t"]["meta"][3]) == 0  # every chunk was staged in shared memory
+    assert int(gpu._bins["t"]["meta"][META_OVERFLOW]) == 0  # every chunk was staged in shared memory
 
 
 def test_binned_then_one_phase_switches_grid_layout():
@@ -182,10 +190,10 @@ def test_binned_with_stale_bins_takes_the_unstaged_path():
     x = np.clip(x, 4 * DX, 1 - 4 * DX).astype(np.float32)
     ora.x[...] = x
     gpu.x.from_numpy(x)
+    gpu.substeps_binned(3)
     for _ in range(3):
-        gpu.substep_binned()
         ora.substep()
-    assert int(gpu._bins["t"]["meta"][3]) > 0
+    assert int(gpu._bins["t"]["meta"][META_OVERFLOW]) > 0
     compare_particles(gpu, ora)
     compare_grid(gpu, ora)
 
@@ -238,16 +246,17 @@ def _oracle_react_stats(st, kind):
 
 
 @pytest.mark.parametrize("kind", [0, 1, 2])
-@pytest.mark.parametrize("path", ["binned", "binned_t512", "one_phase"])
+@pytest.mark.parametrize("path", ["binned", "binned_sequence", "one_phase"])
 def test_reaction_substeps_match_oracle(kind, path):
     gpu, ora = make_solids(seed=2)
-    if path == "binned_t512":
-        gpu.params.tune = 1 | 2 << 2
-        path = "binned"
     lbm, cpl, olbm, oc = _lbm_and_coupling(kind)
+    if path == "binned_sequence":
+        gpu.substeps_binned(3, cpl, lbm)
     for _ in range(3):
         if path == "binned":
             gpu.substep_binned(cpl, lbm)
+        elif path == "binned_sequence":
+            pass
         else:
             gpu.clear_grid()
             gpu.p2g()
@@ -292,6 +301,11 @@ def test_binned_layout_and_argument_checks():
     with pytest.raises(FsiError, match="max_chunks"):
         call("fsi_mpm_bin", ctypes.byref(gpu.particles), ctypes.byref(gpu.grid), ctypes.byref(gpu.params),
              ctypes.byref(bad), None)
-    with pytest.raises(FsiError, match="buffer"):
-        call("fsi_mpm_substep_binned", ctypes.byref(gpu.particles), gpu._bins["grids"],
-             ctypes.byref(gpu._bins["struct"]), ctypes.byref(gpu.params), 2, None, None, None, None, None)
+    with pytest.raises(FsiError, match="n_substeps"):
+        call("fsi_mpm_substeps_binned", ctypes.byref(gpu.particles), gpu._bins["grids"],
+             ctypes.byref(gpu._bins["struct"]), ctypes.byref(gpu.params), -1, None, None, None, None, None)
+    bad_grids = (type(gpu._bins["grids"][0]) * 3)(*gpu._bins["grids"])
+    bad_grids[2].n = gpu.n_grid + 1
+    with pytest.raises(FsiError, match="differ in size"):
+        call("fsi_mpm_substeps_binned", ctypes.byref(gpu.particles), bad_grids,
+             ctypes.byref(gpu._bins["struct"]), ctypes.byref(gpu.params), 1, None, None, None, None, None)
