@@ -271,9 +271,10 @@ int fsi_mpm_g2p(const FsiParticles* pt, const FsiGrid* g, const FsiMpmParams* mp
  * The same substep as clear -> p2g -> reaction -> grid_update -> g2p above
  * (one call of MPMSolid3D.substep plus the coupler's reaction transfer, as
  * driven by fsi_driver.py's MPM loops), organised around particle bins:
- *   - fsi_mpm_bin sorts particle ids by 4x4x4-cell block of their B-spline
- *     base cell and cuts every bin into chunks of at most FSI_BIN_CHUNK
- *     particles (bins may go stale between calls: that costs speed only);
+ *   - fsi_mpm_bin sorts particle ids by FSI_BIN_EDGE^3-cell block of their
+ *     B-spline base cell, and within a block by base cell, and cuts every bin
+ *     into chunks of at most FSI_BIN_CHUNK particles (bins may go stale
+ *     between calls: that costs speed only);
  *   - fsi_mpm_substeps_binned runs substeps chunk by chunk: each chunk is
  *     scattered into a shared-memory tile covering its stencil box and the
  *     tile is flushed with one atomic per touched node value; the gather
@@ -282,13 +283,13 @@ int fsi_mpm_g2p(const FsiParticles* pt, const FsiGrid* g, const FsiMpmParams* mp
  *     buffer; three buffers rotate, and only the boxes recorded for a buffer
  *     are zeroed before it is reused, so no dense pass over the grid is made. */
 #define FSI_BIN_CHUNK 128
-#define FSI_BIN_EDGE 4
+#define FSI_BIN_EDGE 8
 
 /* count, start and chunk must be 16-byte aligned */
 typedef struct FsiMpmBins {
   int32_t n_bins;       /* ceil(n_grid / FSI_BIN_EDGE)^3 */
   int32_t max_chunks;   /* capacity of chunk[] and of each third of box[] */
-  int32_t* key;         /* [n_particles] bin of each particle */
+  int32_t* key;         /* [n_particles] scratch (bin keys, then the in-bin sort) */
   int32_t* count;       /* [n_bins] zero before the first fsi_mpm_bin; kept zero after each call */
   int32_t* start;       /* [n_bins] end offset of each bin in perm after fsi_mpm_bin */
   int32_t* perm;        /* [n_particles] particle ids ordered by bin */

@@ -26,10 +26,10 @@ namespace {
 
 constexpr int kChunk = FSI_BIN_CHUNK;  // particles per chunk
 constexpr int kEdge = FSI_BIN_EDGE;
-// nodes staged per CTA: a chunk of one bin spans (4 + 3)^3 = 343 nodes; the
-// rest absorbs drift since the last binning (a 10^3 box).  7 floats per node
-// in P2G = 28 KB.
-constexpr int kTileCap = 1000;
+// nodes staged per CTA: the stencils of a chunk of one bin span at most
+// (8 + 2)^3 = 1000 nodes; the rest absorbs drift since the last binning (a
+// 13^3 box).  7 floats per node in P2G = 61.5 KB.
+constexpr int kTileCap = 2197;
 
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
@@ -161,45 +161,76 @@ __global__ void k_bin_scatter(int n, const int32_t* __restrict__ key, int32_t* _
   bin_scatter_body(n, key, cursor, perm, blockIdx.x, gridDim.x);
 }
 
-// Orders the particles of each chunk by B-spline base node (ties by particle
-// id), so that particles sharing a stencil are adjacent within the chunk: one
-// CTA of kChunk threads per chunk, each particle's rank counted against the
-// chunk's other keys.
-__device__ __forceinline__ void chunk_sort_body(const FsiParticles& pt, float inv_dx, int G,
-                                                const int2* __restrict__ chunks, const int32_t* __restrict__ meta,
-                                                int32_t* __restrict__ perm, int vb, int vg) {
-  __shared__ unsigned long long key[kChunk];
-  const int t = threadIdx.x, n = pt.n;
-  const int nch = meta[0];
-  for (int c = vb; c < nch; c += vg) {
-    const int2 ch = chunks[c];
-    int p = 0;
-    unsigned long long k = ~0ull;
-    if (t < ch.y) {
-      p = perm[ch.x + t];
-      unsigned long long cell = 0;
-      for (int a = 2; a >= 0; --a) {
-        const float Xp = __fmul_rn(pt.x[a * n + p], inv_dx);
-        cell = cell * (unsigned long long)(G + 2) + (unsigned long long)(clampi((int)(Xp - 0.5f), -1, G) + 1);
-      }
-      k = (cell << 32) | (unsigned long long)(unsigned)p;
-    }
-    key[t] = k;
+// Orders the particles of each bin by B-spline base node (counting sort over
+// the bin's kEdge^3 base cells; order within a cell unspecified), so that the
+// chunks cut from a bin are compact slabs and particles sharing a stencil are
+// adjacent.  One CTA per bin (grid-stride); the bin's range of perm is sorted
+// through the same range of `tmp`.  After fsi_mpm_bin's scatter, end[b] is the
+// end offset of bin b in perm (its start is end[b - 1]).
+constexpr int kBinCells = kEdge * kEdge * kEdge;
+constexpr int kSortT = 256;
+
+__device__ __forceinline__ int local_base_cell(const FsiParticles& pt, int p, float inv_dx, int G) {
+  int l = 0;
+  for (int a = 2; a >= 0; --a) {
+    const float Xp = __fmul_rn(pt.x[a * pt.n + p], inv_dx);
+    l = l * kEdge + clampi((int)(Xp - 0.5f), 0, G - 1) % kEdge;
+  }
+  return l;
+}
+
+__device__ __forceinline__ void bin_sort_body(const FsiParticles& pt, float inv_dx, int G, int nbins,
+                                              const int32_t* __restrict__ end, int32_t* __restrict__ perm,
+                                              int32_t* __restrict__ tmp, int vb, int vg) {
+  __shared__ int cnt[kBinCells];
+  __shared__ int wsum[kSortT / 32];
+  const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
+  constexpr int PER = kBinCells / kSortT;  // counters per thread
+  static_assert(kBinCells % kSortT == 0, "bin cells must be a multiple of the sort CTA");
+  for (int b = vb; b < nbins; b += vg) {
+    const int lo = b ? end[b - 1] : 0, hi = end[b];
+    if (hi - lo < 2) continue;  // uniform over the CTA
+    for (int i = t; i < kBinCells; i += kSortT) cnt[i] = 0;
     __syncthreads();
-    if (t < ch.y) {
-      int rank = 0;
-      for (int j = 0; j < ch.y; ++j) rank += key[j] < k;
-      perm[ch.x + rank] = p;
+    for (int i = lo + t; i < hi; i += kSortT) atomicAdd(&cnt[local_base_cell(pt, perm[i], inv_dx, G)], 1);
+    __syncthreads();
+    // exclusive scan of the counters: PER per thread, then warps, then CTA
+    int v[PER], sum = 0;
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+      v[q] = cnt[t * PER + q];
+      sum += v[q];
     }
+    int inc = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += y;
+    }
+    if (lane == 31) wsum[wid] = inc;
+    __syncthreads();
+    int off = inc - sum;
+    for (int w = 0; w < wid; ++w) off += wsum[w];
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+      cnt[t * PER + q] = off;  // becomes the cell's cursor
+      off += v[q];
+    }
+    __syncthreads();
+    for (int i = lo + t; i < hi; i += kSortT) {
+      const int p = perm[i];
+      tmp[lo + atomicAdd(&cnt[local_base_cell(pt, p, inv_dx, G)], 1)] = p;
+    }
+    __syncthreads();
+    for (int i = lo + t; i < hi; i += kSortT) perm[i] = tmp[i];
     __syncthreads();
   }
 }
 
-__global__ __launch_bounds__(kChunk) void k_bin_sort_chunks(FsiParticles pt, float inv_dx, int G,
-                                                             const int2* __restrict__ chunks,
-                                                             const int32_t* __restrict__ meta,
-                                                             int32_t* __restrict__ perm) {
-  chunk_sort_body(pt, inv_dx, G, chunks, meta, perm, blockIdx.x, gridDim.x);
+__global__ __launch_bounds__(kSortT) void k_bin_sort(FsiParticles pt, float inv_dx, int G, int nbins,
+                                                      const int32_t* __restrict__ end, int32_t* __restrict__ perm,
+                                                      int32_t* __restrict__ tmp) {
+  bin_sort_body(pt, inv_dx, G, nbins, end, perm, tmp, blockIdx.x, gridDim.x);
 }
 
 struct Box {
@@ -257,10 +288,15 @@ __device__ __forceinline__ void g2p_gather_global(const FsiGrid& g, const FsiMpm
   }
 }
 
-// P2G payload of a particle, one row per quantity, one column per particle of
-// the chunk (shared memory): fractional position, base node, momentum, affine
-// matrix, mass, reaction force, and the B-spline weights [axis][offset].
-enum { kPfx = 0, kPbase = 3, kPmv = 6, kPaff = 9, kPmass = 18, kPpf = 19, kPw = 22, kPn = 31 };
+// P2G payload of a particle (shared memory), one record of kQn floats per
+// particle of the chunk, in float4 groups so that the scatter reads the
+// values every lane needs as 128-bit broadcasts:
+//   [0]  mv0 mv1 mv2 mass      [4]  aff0..3      [8]  aff4..7     [12] aff8
+//   [16] base0 base1 base2 fx0 [20] fx1 fx2 pf0 pf1
+//   [24] w[0][0..2] pf2        [28] w[1][0..2]   [32] w[2][0..2]
+// (base as int bits; w the B-spline weights [axis][offset]).  A record of 36
+// floats keeps the 128-bit stores of 8 consecutive particles on distinct banks.
+enum { kQmv = 0, kQaff = 4, kQbase = 16, kQfx1 = 20, kQwx = 24, kQwy = 28, kQwz = 32, kQn = 36 };
 
 // ---- fused substep sequence --------------------------------------------------
 // M substeps in M + 1 launches (after a prologue).  Launch s, for each chunk of
@@ -283,7 +319,8 @@ enum { kSx = 0, kSv = 3, kSC = 6, kSF = 15, kSn = 24 };  // staged particle stat
 // without the tile, [5 + b] buffer b holds recorded boxes not yet zeroed
 enum { kMetaChunks = 0, kMetaRec = 1, kMetaOverflow = 4, kMetaDirty = 5 };
 constexpr int kSeqT = 256;
-constexpr size_t kSeqSmem = sizeof(float) * (7 * kTileCap + (kPn + kSn) * kChunk);
+constexpr int kTileFloats = (7 * kTileCap + 3) & ~3;  // keeps the payload 16-byte aligned
+constexpr size_t kSeqSmem = sizeof(float) * (kTileFloats + (kQn + kSn) * kChunk);
 
 struct SeqArgs {
   FsiParticles pt;
@@ -417,8 +454,8 @@ __device__ __forceinline__ void mpm_seq_body(const SeqArgs& A, int vb, int vg) {
   extern __shared__ float4 seq_smem4[];
   // G2P: [3][nv] node velocities; payload: [4][nv] lattice box; scatter: [7][nv] tile
   float* const tile = reinterpret_cast<float*>(seq_smem4);
-  float* const sp = tile + 7 * kTileCap;  // [kPn][kChunk] P2G payload
-  float* const ss = sp + kPn * kChunk;    // [kSn][kChunk] particle state
+  float* const sp = tile + kTileFloats;  // [kChunk][kQn] P2G payload
+  float* const ss = sp + kQn * kChunk;   // [kSn][kChunk] particle state
   __shared__ int s_lo[3], s_hi[3];
   __shared__ float s_scale;
   __shared__ int s_cnt[NW];
@@ -470,12 +507,36 @@ __device__ __forceinline__ void mpm_seq_body(const SeqArgs& A, int vb, int vg) {
     const int2 ch = A.chunks[c];
     int nb[3] = {0, 0, 0};  // base node of this thread's particle after the gather
     bool nb_live = false;
+    // particle reads of the payload, issued ahead of the gather
+    const int pslot = (wid >> 1) * 32 + lane;
+    int pq = 0;
+    float pmass = 0.f, pvol0 = 0.f;
+    if (do_p2g && pslot < ch.y) {
+      pq = A.perm[ch.x + pslot];
+      pmass = pt.mass[pq];
+      pvol0 = pt.vol0[pq];
+    }
     if (do_g2p) {
       // ---- G2P of substep s - 1 from buffer bg
       const FsiGrid g = grid_of(A, bg);
       const Box bx = load_box(A.box + bg * A.box_stride + 6 * c);
       const bool staged = bx.vol <= kTileCap;
       const int nv = staged ? bx.vol : 0;
+      // this lane's particle, read ahead of the staging barrier
+      const int lp = tid / GP, sub = tid % GP;
+      int p = 0;
+      float X[3] = {0.f, 0.f, 0.f}, Fo[9];
+#pragma unroll
+      for (int a = 0; a < 9; ++a) Fo[a] = 0.f;
+      if (lp < ch.y) {
+        p = A.perm[ch.x + lp];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) X[a] = pt.x[a * n + p];
+        if (sub == 0) {
+#pragma unroll
+          for (int a = 0; a < 9; ++a) Fo[a] = pt.F[(int64_t)a * n + p];
+        }
+      }
       for (int li = tid; li < nv; li += T) {
         int i, j, k;
         box_ijk(bx, li, i, j, k);
@@ -492,10 +553,7 @@ __device__ __forceinline__ void mpm_seq_body(const SeqArgs& A, int vb, int vg) {
         tile[2 * nv + li] = v[2];
       }
       __syncthreads();  // also publishes the s_lo / s_hi reset
-      const int lp = tid / GP, sub = tid % GP;
       if (lp < ch.y) {  // uniform over a particle's GP lanes
-        const int p = A.perm[ch.x + lp];
-        float X[3] = {pt.x[p], pt.x[n + p], pt.x[2 * n + p]};
         BSpline b;
         bspline(X, mp.inv_dx, b);
         float nvl[3] = {0.f, 0.f, 0.f}, nC[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
@@ -533,7 +591,7 @@ __device__ __forceinline__ void mpm_seq_body(const SeqArgs& A, int vb, int vg) {
           for (int q = 0; q < 9; ++q) nC[q] += __shfl_xor_sync(grp, nC[q], w, GP);
         }
         if (sub == 0) {
-          g2p_finish(pt, p, mp, X, nvl, nC, do_p2g ? ss : nullptr, kChunk, lp);
+          g2p_finish_f(pt, p, mp, X, nvl, nC, Fo, do_p2g ? ss : nullptr, kChunk, lp);
 #pragma unroll
           for (int r = 0; r < 3; ++r) nb[r] = base_of(X[r], mp.inv_dx);
           nb_live = true;
@@ -580,19 +638,19 @@ __device__ __forceinline__ void mpm_seq_body(const SeqArgs& A, int vb, int vg) {
     // ---- P2G payload of substep s: warps of role 0 the stress and affine
     // momentum, warps of role 1 the B-spline data and the reaction force
     {
-      const int role = wid & 1, slot = (wid >> 1) * 32 + lane;
+      const int role = wid & 1, slot = pslot;
       if (role == 0) {
         if (slot < ch.y) {
-          const int p = A.perm[ch.x + slot];
+          const int p = pq;
           P2GParticle q;
-          p2g_particle_rows(ss + kSF * kChunk, ss + kSC * kChunk, ss + kSv * kChunk, kChunk, slot, pt.mass[p],
-                            pt.vol0[p], mp, q);
+          p2g_particle_rows(ss + kSF * kChunk, ss + kSC * kChunk, ss + kSv * kChunk, kChunk, slot, pmass, pvol0, mp,
+                            q);
           pt.Jp[p] = q.J;
-#pragma unroll
-          for (int r = 0; r < 3; ++r) sp[(kPmv + r) * kChunk + slot] = q.mv[r];
-#pragma unroll
-          for (int r = 0; r < 9; ++r) sp[(kPaff + r) * kChunk + slot] = q.aff[r];
-          sp[kPmass * kChunk + slot] = q.mass;
+          float* const rq = sp + slot * kQn;
+          *reinterpret_cast<float4*>(rq + kQmv) = make_float4(q.mv[0], q.mv[1], q.mv[2], q.mass);
+          *reinterpret_cast<float4*>(rq + kQaff) = make_float4(q.aff[0], q.aff[1], q.aff[2], q.aff[3]);
+          *reinterpret_cast<float4*>(rq + kQaff + 4) = make_float4(q.aff[4], q.aff[5], q.aff[6], q.aff[7]);
+          rq[kQaff + 8] = q.aff[8];
         }
       } else {
         if (REACT && staged) {
@@ -617,7 +675,6 @@ __device__ __forceinline__ void mpm_seq_body(const SeqArgs& A, int vb, int vg) {
           asm volatile("bar.sync 1, %0;" ::"n"(kSeqT / 2) : "memory");
         }
         if (slot < ch.y) {
-          const int p = A.perm[ch.x + slot];
           const float X[3] = {ss[kSx * kChunk + slot], ss[(kSx + 1) * kChunk + slot], ss[(kSx + 2) * kChunk + slot]};
           BSpline b;
           bspline(X, mp.inv_dx, b);
@@ -629,9 +686,9 @@ __device__ __forceinline__ void mpm_seq_body(const SeqArgs& A, int vb, int vg) {
             const float J = det3(Fp);
             ReactParticle rp;
             if (staged)
-              reaction_particle_staged(tile, bx, nv, A.L, A.cp, b, J, pt.vol0[p], s_scale, rp);
+              reaction_particle_staged(tile, bx, nv, A.L, A.cp, b, J, pvol0, s_scale, rp);
             else
-              reaction_particle(A.L, A.hydro, A.phi, A.cp, b, J, pt.vol0[p], s_scale, rp);
+              reaction_particle(A.L, A.hydro, A.phi, A.cp, b, J, pvol0, s_scale, rp);
             if (rp.act) ++n_act;
             pmax = fmaxf(pmax, rp.pnorm);
             if (rp.gated)
@@ -639,14 +696,13 @@ __device__ __forceinline__ void mpm_seq_body(const SeqArgs& A, int vb, int vg) {
             if (rp.scatter)
               for (int r = 0; r < 3; ++r) pf[r] = rp.pf[r];
           }
-#pragma unroll
-          for (int r = 0; r < 3; ++r) {
-            sp[(kPfx + r) * kChunk + slot] = b.fx[r];
-            sp[(kPbase + r) * kChunk + slot] = __int_as_float(b.base[r]);
-            sp[(kPpf + r) * kChunk + slot] = pf[r];
-#pragma unroll
-            for (int o = 0; o < 3; ++o) sp[(kPw + 3 * r + o) * kChunk + slot] = b.w[r][o];
-          }
+          float* const rq = sp + slot * kQn;
+          *reinterpret_cast<float4*>(rq + kQbase) =
+              make_float4(__int_as_float(b.base[0]), __int_as_float(b.base[1]), __int_as_float(b.base[2]), b.fx[0]);
+          *reinterpret_cast<float4*>(rq + kQfx1) = make_float4(b.fx[1], b.fx[2], pf[0], pf[1]);
+          *reinterpret_cast<float4*>(rq + kQwx) = make_float4(b.w[0][0], b.w[0][1], b.w[0][2], pf[2]);
+          *reinterpret_cast<float4*>(rq + kQwy) = make_float4(b.w[1][0], b.w[1][1], b.w[1][2], 0.f);
+          *reinterpret_cast<float4*>(rq + kQwz) = make_float4(b.w[2][0], b.w[2][1], b.w[2][2], 0.f);
         }
       }
     }
@@ -690,8 +746,9 @@ __device__ __forceinline__ void mpm_seq_body(const SeqArgs& A, int vb, int vg) {
       };
       const int p1 = min(wid * kRun + kRun, ch.y);
       for (int lp = wid * kRun; lp < p1; ++lp) {
-        const int b0 = __float_as_int(sp[kPbase * kChunk + lp]), b1 = __float_as_int(sp[(kPbase + 1) * kChunk + lp]),
-                  b2 = __float_as_int(sp[(kPbase + 2) * kChunk + lp]);
+        const float* const rq = sp + lp * kQn;
+        const float4 q4 = *reinterpret_cast<const float4*>(rq + kQbase);
+        const int b0 = __float_as_int(q4.x), b1 = __float_as_int(q4.y), b2 = __float_as_int(q4.z);
         if (b0 != cb0 || b1 != cb1 || b2 != cb2) {
           if (cb0 != INT_MIN) flush_run();
           cb0 = b0;
@@ -700,19 +757,21 @@ __device__ __forceinline__ void mpm_seq_body(const SeqArgs& A, int vb, int vg) {
         }
         if (lane < 27) {
           // weights of bspline() (staged by the payload) and offsets as in p2g_node()
-          const float w = sp[(kPw + ox) * kChunk + lp] * sp[(kPw + 3 + oy) * kChunk + lp] *
-                          sp[(kPw + 6 + oz) * kChunk + lp];
-          const float dpos[3] = {(dox - sp[kPfx * kChunk + lp]) * mp.dx, (doy - sp[(kPfx + 1) * kChunk + lp]) * mp.dx,
-                                 (doz - sp[(kPfx + 2) * kChunk + lp]) * mp.dx};
+          const float4 q5 = *reinterpret_cast<const float4*>(rq + kQfx1);
+          const float w = rq[kQwx + ox] * rq[kQwy + oy] * rq[kQwz + oz];
+          const float dpos[3] = {(dox - q4.w) * mp.dx, (doy - q5.x) * mp.dx, (doz - q5.y) * mp.dx};
+          const float4 m4 = *reinterpret_cast<const float4*>(rq + kQmv);
+          const float4 a0 = *reinterpret_cast<const float4*>(rq + kQaff);
+          const float4 a1 = *reinterpret_cast<const float4*>(rq + kQaff + 4);
+          const float a8 = rq[kQaff + 8];
+          const float mv[3] = {m4.x, m4.y, m4.z};
+          const float aff[9] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w, a8};
 #pragma unroll
           for (int q = 0; q < 3; ++q)
-            acc[q] += w * (sp[(kPmv + q) * kChunk + lp] + (sp[(kPaff + 3 * q) * kChunk + lp] * dpos[0] +
-                                                           sp[(kPaff + 3 * q + 1) * kChunk + lp] * dpos[1] +
-                                                           sp[(kPaff + 3 * q + 2) * kChunk + lp] * dpos[2]));
-          acc[3] += w * sp[kPmass * kChunk + lp];
+            acc[q] += w * (mv[q] + (aff[3 * q] * dpos[0] + aff[3 * q + 1] * dpos[1] + aff[3 * q + 2] * dpos[2]));
+          acc[3] += w * m4.w;
           if (REACT) {
-            const float f0 = sp[kPpf * kChunk + lp], f1 = sp[(kPpf + 1) * kChunk + lp],
-                        f2 = sp[(kPpf + 2) * kChunk + lp];
+            const float f0 = q5.z, f1 = q5.w, f2 = rq[kQwx + 3];
             if (f0 != 0.f || f1 != 0.f || f2 != 0.f) {
               const float v4 = w * f0, v5 = w * f1, v6 = w * f2;
               acc[NQ - 3] += v4;
@@ -915,9 +974,10 @@ extern "C" int fsi_mpm_bin(const FsiParticles* pt, const FsiGrid* g, const FsiMp
   if ((rc = launch_check("k_bin_scan"))) return rc;
   k_bin_scatter<<<nblk(pt->n, 256), 256, 0, st>>>(pt->n, bins->key, bins->start, bins->perm);
   if ((rc = launch_check("k_bin_scatter"))) return rc;
-  k_bin_sort_chunks<<<(unsigned)std::min(bins->max_chunks, sm_count() * 8), kChunk, 0, st>>>(
-      *pt, mp->inv_dx, g->n, reinterpret_cast<const int2*>(bins->chunk), bins->meta, bins->perm);
-  return launch_check("k_bin_sort_chunks");
+  // the bin keys are no longer needed: key[] is the sort's scratch
+  k_bin_sort<<<(unsigned)std::min(bins->n_bins, sm_count() * 8), kSortT, 0, st>>>(
+      *pt, mp->inv_dx, g->n, bins->n_bins, bins->start, bins->perm, bins->key);
+  return launch_check("k_bin_sort");
 }
 
 extern "C" int fsi_mpm_substeps_binned(const FsiParticles* pt, const FsiGrid grid[3], const FsiMpmBins* bins,
@@ -1056,11 +1116,11 @@ __global__ __launch_bounds__(kSeqT, 2) void k_batch_mpm_seq(const FsiBatchCase* 
   mpm_seq_body<true>(A, blockIdx.x, gridDim.x);
 }
 
-__global__ __launch_bounds__(kChunk) void k_batch_bin_sort_chunks(const FsiBatchCase* __restrict__ cases) {
+__global__ __launch_bounds__(kSortT) void k_batch_bin_sort(const FsiBatchCase* __restrict__ cases) {
   const FsiBatchCase& bc = cases[blockIdx.y];
   if (!bc.active) return;
-  chunk_sort_body(bc.pt, bc.mp.inv_dx, bc.grid[0].n, reinterpret_cast<const int2*>(bc.bins.chunk), bc.bins.meta,
-                  bc.bins.perm, blockIdx.x, gridDim.x);
+  bin_sort_body(bc.pt, bc.mp.inv_dx, bc.grid[0].n, bc.bins.n_bins, bc.bins.start, bc.bins.perm, bc.bins.key,
+                blockIdx.x, gridDim.x);
 }
 
 int check_batch_mpm(const FsiBatchCase* cases, const FsiBatchDims* d) {
@@ -1084,10 +1144,8 @@ extern "C" int fsi_batch_mpm_bin(FsiBatchCase* cases, const FsiBatchDims* d, voi
   if ((rc = launch_check("k_batch_bin_scan"))) return rc;
   k_batch_bin_scatter<<<g, 256, 0, st>>>(cases);
   if ((rc = launch_check("k_batch_bin_scatter"))) return rc;
-  k_batch_bin_sort_chunks<<<dim3((unsigned)std::min(d->max_chunks, 2 * (int)nblk(d->max_particles, kChunk) + 8),
-                                 d->n_cases),
-                            kChunk, 0, st>>>(cases);
-  return launch_check("k_batch_bin_sort_chunks");
+  k_batch_bin_sort<<<dim3((unsigned)std::min(d->max_bins, 64), d->n_cases), kSortT, 0, st>>>(cases);
+  return launch_check("k_batch_bin_sort");
 }
 
 extern "C" int fsi_batch_mpm_substeps(FsiBatchCase* cases, const FsiBatchDims* d, int32_t n_substeps,

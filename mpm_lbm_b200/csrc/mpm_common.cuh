@@ -234,9 +234,10 @@ __device__ __forceinline__ float det3(const float (&M)[9]) {
 // (solid.py:261-315); nv and nC are the gathered velocity and affine matrix.
 // With a stage (rows x 3, v 3, C 9, F 9 of stride ld, column col) the new
 // state is also written there.
-__device__ __forceinline__ void g2p_finish(const FsiParticles& pt, int p, const FsiMpmParams& mp, float X[3],
-                                           const float nv[3], float nC[9], float* stage = nullptr, int ld = 0,
-                                           int col = 0) {
+// Fo: the particle's deformation gradient before the substep
+__device__ __forceinline__ void g2p_finish_f(const FsiParticles& pt, int p, const FsiMpmParams& mp, float X[3],
+                                             const float nv[3], float nC[9], const float Fo[9],
+                                             float* stage = nullptr, int ld = 0, int col = 0) {
   const int n = pt.n;
   float v[3];
 #pragma unroll
@@ -256,9 +257,7 @@ __device__ __forceinline__ void g2p_finish(const FsiParticles& pt, int p, const 
       if (v[a] > 0.f) v[a] = 0.f;
     }
   }
-  float Fo[9], Fn[9];
-#pragma unroll
-  for (int a = 0; a < 9; ++a) Fo[a] = pt.F[(int64_t)a * n + p];
+  float Fn[9];
 #pragma unroll
   for (int a = 0; a < 3; ++a)
 #pragma unroll
@@ -324,6 +323,14 @@ __device__ __forceinline__ void g2p_finish(const FsiParticles& pt, int p, const 
       stage[(15 + a) * ld + col] = Fn[a];
     }
   }
+}
+
+__device__ __forceinline__ void g2p_finish(const FsiParticles& pt, int p, const FsiMpmParams& mp, float X[3],
+                                           const float nv[3], float nC[9]) {
+  float Fo[9];
+#pragma unroll
+  for (int a = 0; a < 9; ++a) Fo[a] = pt.F[(int64_t)a * pt.n + p];
+  g2p_finish_f(pt, p, mp, X, nv, nC, Fo);
 }
 
 // one gathered node's contribution to the particle velocity and affine matrix
