@@ -128,6 +128,8 @@ enum {
   FSI_TUNE_LBM_OCC4 = 1,  /* registers for 4 CTAs per SM (64 per thread) */
   FSI_TUNE_LBM_PAIR = 2,  /* two x-adjacent cells per thread on the paired FP32 pipe; nx even, and
                              nx % 64 != 2 with open boundaries (results agree to FP32 rounding) */
+  FSI_TUNE_LBM_OCC3_PF = 3, /* OCC3, each CTA prefetching into L2 the tile one resident wave later */
+  FSI_TUNE_LBM_OCC4_PF = 4, /* OCC4 with the same L2 prefetch */
 };
 
 typedef struct FsiStepCtl {
@@ -369,7 +371,7 @@ typedef struct FsiBatchCase {
 typedef struct FsiBatchDims {
   int32_t n_cases;                /* slots in `cases` (active or not) */
   int32_t store_fp16;             /* population storage of every case */
-  int32_t max_lbm_tiles;          /* max over cases of ceil(nx / 32) * ceil(ny * nz / 8) */
+  int32_t max_lbm_tiles;          /* max over cases of ceil(nx / 32) * ceil(ny / 8) * nz */
   int32_t max_particles;
   int64_t max_cells;              /* max nx * ny * nz */
   int32_t max_chunks;             /* max FsiMpmBins.max_chunks */

@@ -17,7 +17,7 @@ c_i32, c_i64, c_f32, c_f64, c_p = ctypes.c_int32, ctypes.c_int64, ctypes.c_float
 
 FSI_CELL_SOLID, FSI_CELL_NEAR, FSI_CELL_LINK, FSI_CELL_OVERRIDE, FSI_CELL_CF = 1, 2, 4, 8, 16
 FSI_MODE_MOVING_BB, FSI_MODE_SUBCYCLED, FSI_MODE_DIRSTATS, FSI_MODE_PENALTY = 1, 2, 4, 8
-FSI_TUNE_LBM_OCC3, FSI_TUNE_LBM_OCC4, FSI_TUNE_LBM_PAIR = 0, 1, 2
+FSI_TUNE_LBM_OCC3, FSI_TUNE_LBM_OCC4, FSI_TUNE_LBM_PAIR, FSI_TUNE_LBM_OCC3_PF, FSI_TUNE_LBM_OCC4_PF = 0, 1, 2, 3, 4
 
 
 class FsiLbmDiag(ctypes.Structure):

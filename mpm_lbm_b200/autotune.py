@@ -1,8 +1,9 @@
 """Autotuner for the launch variants of the step kernels.
 
 The variants differ in how a kernel maps onto the SMs: the register budget of
-the one-cell LBM step kernel (3 or 4 resident CTAs per SM; bit-identical
-results) and the two-cells-per-thread LBM kernel on the paired FP32 pipe (the
+the one-cell LBM step kernel (3 or 4 resident CTAs per SM), with or without an
+L2 prefetch of the tile one resident wave ahead (bit-identical results), and
+the two-cells-per-thread LBM kernel on the paired FP32 pipe (the
 same operator; its contraction of multiply-adds differs, so results agree to
 FP32 rounding).  The tuner times each variant with CUDA events
 on the caller's own state -- trial steps on a device snapshot that is
@@ -14,7 +15,7 @@ from __future__ import annotations
 
 import torch
 
-from ._lib import FSI_TUNE_LBM_OCC3, FSI_TUNE_LBM_OCC4, FSI_TUNE_LBM_PAIR
+from ._lib import FSI_TUNE_LBM_OCC3, FSI_TUNE_LBM_OCC3_PF, FSI_TUNE_LBM_OCC4, FSI_TUNE_LBM_OCC4_PF, FSI_TUNE_LBM_PAIR
 
 
 def _time_ms(fn, steps, reps):
@@ -46,7 +47,7 @@ def _time_ms(fn, steps, reps):
 def lbm_candidates(lbm):
     """Launch variants valid for this lattice: the paired kernel needs an even
     nx, and nx % 64 != 2 with open boundaries."""
-    out = [FSI_TUNE_LBM_OCC3, FSI_TUNE_LBM_OCC4]
+    out = [FSI_TUNE_LBM_OCC3, FSI_TUNE_LBM_OCC4, FSI_TUNE_LBM_OCC3_PF, FSI_TUNE_LBM_OCC4_PF]
     if lbm.nx % 2 == 0 and not ((lbm.bc_x_left or lbm.bc_x_right) and lbm.nx % 64 == 2):
         out.append(FSI_TUNE_LBM_PAIR)
     return out

@@ -287,7 +287,7 @@ class FSIBatch:
             d.max_lbm_tiles = d.max_particles = d.max_chunks = d.max_bins = 1
             d.max_cells = 1
             return
-        d.max_lbm_tiles = max(((l.nx + 31) // 32) * ((l.ny * l.nz + 7) // 8) for l in (x.lbm for x in act))
+        d.max_lbm_tiles = max(((l.nx + 31) // 32) * ((l.ny + 7) // 8) * l.nz for l in (x.lbm for x in act))
         d.max_cells = max(x.lbm.ncell for x in act)
         d.max_particles = max(x.solid.n_particles for x in act)
         d.max_chunks = max(x.solid._bins["struct"].max_chunks for x in act)

@@ -36,6 +36,7 @@ struct Case {
   FsiLbmParams p;
   FsiStepCtl c;
   MrtK K;
+  int pf_dist;  // tiles between a CTA's tile and the one it prefetches into L2 (0: none)
 };
 
 // ------------------------------------------------------------ storage ----
@@ -453,14 +454,15 @@ __device__ __forceinline__ void dirstats_warp(const Case& c, const Nbh& n, uint3
 }
 
 template <bool ODD, bool H, bool MOVING, bool BCW, bool PEN>
-__device__ __forceinline__ void lbm_step_tile(const Case& c, int bx, int by, DirAcc& acc) {
+__device__ __forceinline__ void lbm_step_tile(const Case& c, int bx, int by, int bz, DirAcc& acc) {
   const int lane = threadIdx.x;
   const int nx = c.s.nx, ny = c.s.ny, nz = c.s.nz;
   const int x = bx * 32 + lane;
-  const int row = by * 8 + threadIdx.y;
-  const bool inrow = row < ny * nz;
+  const int jr = by * 8 + threadIdx.y;
+  const bool inrow = jr < ny;
   const bool valid = inrow && x < nx;
-  const int j = inrow ? row % ny : 0, k = inrow ? row / ny : 0;
+  const int j = inrow ? jr : 0, k = bz;
+  const int row = k * ny + j;
   const int cell = row * nx + x;
   const bool dirstats = MOVING && (c.c.mode & FSI_MODE_DIRSTATS);
   if (dirstats) {
@@ -653,15 +655,40 @@ __device__ __forceinline__ void lbm_step_tile(const Case& c, int bx, int by, Dir
   }
 }
 
+// L2 prefetch of the populations of tile (bx, by, bz) of a 32 x 8 x 1 tiling:
+// its 8 rows of 32 cells in the 19 planes, one 128-byte line per thread.
+template <bool H>
+__device__ __forceinline__ void prefetch_tile_l2(const Case& c, int bx, int by, int bz) {
+  const int tid = threadIdx.y * 32 + threadIdx.x;
+  if (tid >= 19 * 8) return;
+  const int s = tid >> 3, j = by * 8 + (tid & 7);
+  if (j >= c.s.ny) return;
+  const uint32_t idx = pop_index(c, s, (int64_t)(bz * c.s.ny + j) * c.s.nx + bx * 32);
+  const void* ptr = H ? static_cast<const void*>(static_cast<const __half*>(c.s.pop) + idx)
+                      : static_cast<const void*>(static_cast<const float*>(c.s.pop) + idx);
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(ptr));
+}
+
 // MINB: resident CTAs per SM the register allocation must allow (3: no
-// spills; 4: 64 registers with a few spilled words).  The host picks it from
-// FsiLbmParams.tune (chosen by the autotuner of the Python layer).
-template <bool ODD, bool H, bool MOVING, bool BCW, bool PEN, int MINB>
+// spills; 4: 64 registers with a few spilled words).  PF: each CTA first
+// prefetches into L2 the tile c.pf_dist tiles after its own in launch order
+// (about one resident wave later), so that the populations of the next wave
+// are read from L2.  The host picks both from FsiLbmParams.tune (chosen by the
+// autotuner of the Python layer).  Grid: (ceil(nx / 32), ceil(ny / 8), nz).
+template <bool ODD, bool H, bool MOVING, bool BCW, bool PEN, int MINB, bool PF>
 __global__ void __launch_bounds__(256, MINB) k_lbm_step(const Case c) {
   __shared__ DirAcc acc;
   griddep_wait();
   griddep_launch();
-  lbm_step_tile<ODD, H, MOVING, BCW, PEN>(c, blockIdx.x, blockIdx.y, acc);
+  if (PF) {
+    const unsigned gx = gridDim.x, gy = gridDim.y;
+    const unsigned t = blockIdx.x + gx * (blockIdx.y + gy * blockIdx.z) + (unsigned)c.pf_dist;
+    if (t < gx * gy * gridDim.z) {
+      const unsigned r = t / gx;
+      prefetch_tile_l2<H>(c, (int)(t - r * gx), (int)(r % gy), (int)(r / gy));
+    }
+  }
+  lbm_step_tile<ODD, H, MOVING, BCW, PEN>(c, blockIdx.x, blockIdx.y, blockIdx.z, acc);
 }
 
 // ------------------------------------------- paired step (2 cells/thread) ----
@@ -1489,8 +1516,7 @@ static int check_state(const FsiLbmState* s, const FsiLbmParams* p) {
   if (s->pitch < (int64_t)s->nx * s->ny * s->nz || (s->pitch % 32) != 0)
     return invalid("pitch must cover nx*ny*nz and be a multiple of 32");
   if (19 * s->pitch > (int64_t)UINT32_MAX) return invalid("lattice too large: 19 * pitch must be below 2^32");
-  if (p->tune != FSI_TUNE_LBM_OCC3 && p->tune != FSI_TUNE_LBM_OCC4 && p->tune != FSI_TUNE_LBM_PAIR)
-    return invalid("unknown FsiLbmParams.tune");
+  if (p->tune < FSI_TUNE_LBM_OCC3 || p->tune > FSI_TUNE_LBM_OCC4_PF) return invalid("unknown FsiLbmParams.tune");
   if ((p->bc_left || p->bc_right) && (s->nx < 4 || (s->nx % 32 == 1) || (s->nx % 32 == 2)))
     return invalid("x open boundaries need nx >= 4 and nx % 32 not in {1, 2}");
   if (!s->pop || !s->flags || !s->nbr || !s->diag) return invalid("null device pointer in FsiLbmState");
@@ -1514,7 +1540,20 @@ static Case make_case(const FsiLbmState* s, const FsiLbmParams* p, const FsiStep
   else
     c.c = FsiStepCtl{0, 0, 0, 0};
   c.K = make_mrt_k(p->s_v, p->s_o);
+  c.pf_dist = 0;
   return c;
+}
+
+static int lbm_sm_count() {
+  static int cached[64] = {0};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+  if (!cached[dev]) {
+    int n = 0;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+    cached[dev] = n;
+  }
+  return cached[dev];
 }
 
 static inline unsigned blocks_for(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
@@ -1588,9 +1627,11 @@ extern "C" int fsi_lbm_substep(const FsiLbmState* s, const FsiLbmParams* p, cons
                     "memset penalty stats");
     if (rc) return rc;
   }
-  const Case c = make_case(s, p, ctl);
+  Case c = make_case(s, p, ctl);
   dim3 block(32, 8);
-  dim3 grid((unsigned)((s->nx + 31) / 32), (unsigned)((s->ny * s->nz + 7) / 8));
+  dim3 grid((unsigned)((s->nx + 31) / 32), (unsigned)((s->ny + 7) / 8), (unsigned)s->nz);
+  if (p->tune == FSI_TUNE_LBM_OCC3_PF || p->tune == FSI_TUNE_LBM_OCC4_PF)
+    c.pf_dist = lbm_sm_count() * (p->tune == FSI_TUNE_LBM_OCC4_PF ? 4 : 3);
   const bool odd = ctl->parity != 0, h = s->store_fp16 != 0;
   const bool moving = ctl->mode & FSI_MODE_MOVING_BB, pen = ctl->mode & FSI_MODE_PENALTY;
   const bool bcw = p->bc_left != 0 || p->bc_right != 0;
@@ -1611,9 +1652,13 @@ extern "C" int fsi_lbm_substep(const FsiLbmState* s, const FsiLbmParams* p, cons
   if (p->tune == FSI_TUNE_LBM_PAIR) {                                      \
     FSI_KLAUNCH((k_lbm_step2<O, HH, M, B, PN>), grid2, block2);            \
   } else if (p->tune == FSI_TUNE_LBM_OCC4) {                               \
-    FSI_KLAUNCH((k_lbm_step<O, HH, M, B, PN, 4>), grid, block);            \
+    FSI_KLAUNCH((k_lbm_step<O, HH, M, B, PN, 4, false>), grid, block);     \
+  } else if (p->tune == FSI_TUNE_LBM_OCC4_PF) {                            \
+    FSI_KLAUNCH((k_lbm_step<O, HH, M, B, PN, 4, true>), grid, block);      \
+  } else if (p->tune == FSI_TUNE_LBM_OCC3_PF) {                            \
+    FSI_KLAUNCH((k_lbm_step<O, HH, M, B, PN, 3, true>), grid, block);      \
   } else {                                                                 \
-    FSI_KLAUNCH((k_lbm_step<O, HH, M, B, PN, 3>), grid, block);            \
+    FSI_KLAUNCH((k_lbm_step<O, HH, M, B, PN, 3, false>), grid, block);     \
   }
 #define FSI_BY_H(O, M, B, PN) \
   if (h) { FSI_LAUNCH(O, true, M, B, PN); } else { FSI_LAUNCH(O, false, M, B, PN); }
@@ -1775,7 +1820,10 @@ __device__ __forceinline__ bool stage_case(const FsiBatchCase& bc, Case& sc, boo
   copy_words(&sc.s, &bc.lbm, (int)sizeof(FsiLbmState), tid, nt);
   copy_words(&sc.p, &bc.lp, (int)sizeof(FsiLbmParams), tid, nt);
   copy_words(&sc.c, &bc.ctl, (int)sizeof(FsiStepCtl), tid, nt);
-  if (with_k && tid == 0) sc.K = make_mrt_k(bc.lp.s_v, bc.lp.s_o);
+  if (with_k && tid == 0) {
+    sc.K = make_mrt_k(bc.lp.s_v, bc.lp.s_o);
+    sc.pf_dist = 0;
+  }
   __syncthreads();
   return true;
 }
@@ -1785,22 +1833,22 @@ __global__ void __launch_bounds__(256, 3) k_batch_lbm_step(const FsiBatchCase* _
   __shared__ Case sc;
   __shared__ DirAcc acc;
   const FsiBatchCase& bc = cases[blockIdx.y];
-  const int gx = (bc.lbm.nx + 31) / 32, nt = gx * ((bc.lbm.ny * bc.lbm.nz + 7) / 8);
+  const int gx = (bc.lbm.nx + 31) / 32, gy = (bc.lbm.ny + 7) / 8, nt = gx * gy * bc.lbm.nz;
   if ((int)blockIdx.x >= nt || !stage_case(bc, sc, true)) return;
   const bool moving = sc.c.mode & FSI_MODE_MOVING_BB;
   const bool odd = sc.c.parity != 0;
   for (int t = blockIdx.x; t < nt; t += gridDim.x) {
-    const int bx = t % gx, by = t / gx;
+    const int r = t / gx, bx = t - r * gx, by = r % gy, bz = r / gy;
     if (moving) {
       if (odd)
-        lbm_step_tile<true, H, true, false, false>(sc, bx, by, acc);
+        lbm_step_tile<true, H, true, false, false>(sc, bx, by, bz, acc);
       else
-        lbm_step_tile<false, H, true, false, false>(sc, bx, by, acc);
+        lbm_step_tile<false, H, true, false, false>(sc, bx, by, bz, acc);
     } else {
       if (odd)
-        lbm_step_tile<true, H, false, false, true>(sc, bx, by, acc);
+        lbm_step_tile<true, H, false, false, true>(sc, bx, by, bz, acc);
       else
-        lbm_step_tile<false, H, false, false, true>(sc, bx, by, acc);
+        lbm_step_tile<false, H, false, false, true>(sc, bx, by, bz, acc);
     }
     __syncthreads();  // acc is reused by the next tile
   }
@@ -1908,7 +1956,7 @@ extern "C" int fsi_batch_lbm_substep(FsiBatchCase* cases, const FsiBatchDims* d,
   if ((rc = launch_check("k_batch_ctl"))) return rc;
   // one CTA per tile of the largest case; CTAs past a smaller case's tiles exit at once
   if (d->lbm_tune == FSI_TUNE_LBM_PAIR) {
-    // max_lbm_tiles counts 32 x 8 tiles; a 64 x 4 tile covers as many cells
+    // max_lbm_tiles counts 32 x 8 x 1 tiles; a 64 x 4 tile covers as many cells
     const dim3 grid(batch_x((int64_t)d->max_lbm_tiles + 64, 1, 1 << 20), d->n_cases);
     if (d->store_fp16)
       k_batch_lbm_step2<true><<<grid, dim3(32, 4), 0, st>>>(cases);

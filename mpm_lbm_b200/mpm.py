@@ -315,7 +315,8 @@ class MPMSolid3D:
             setattr(self, k, v)
 
     def rebin(self):
-        """Sort particle ids by 4x4x4-cell block (fsi_mpm_bin)."""
+        """Sort particle ids by 8x8x8 block of base cells, and by base cell
+        within a block (fsi_mpm_bin)."""
         self._ensure_binned()
         call("fsi_mpm_bin", ctypes.byref(self.particles), ctypes.byref(self.grid), ctypes.byref(self.params),
              ctypes.byref(self._bins["struct"]), self._stream())

@@ -263,14 +263,14 @@ def test_penalty_step_matches_oracle(tune):
 
 @pytest.mark.parametrize("moving", [False, True])
 def test_launch_variants_are_bit_identical(moving):
-    """FsiLbmParams.tune only changes the register budget of the step kernel:
-    populations and macroscopic fields agree bit for bit; the link forces are
-    float atomic sums whose order (and last-bit rounding) varies between any
-    two launches."""
+    """FsiLbmParams.tune 0, 1, 3, 4 only change the register budget of the step
+    kernel and whether it prefetches the next wave's tiles into L2: populations
+    and macroscopic fields agree bit for bit; the link forces are float atomic
+    sums whose order (and last-bit rounding) varies between any two launches."""
     nx, ny, nz = 40, 12, 10
     solid = channel_with_obstacle(nx, ny, nz)
     outs = []
-    for tune in (0, 1):
+    for tune in (0, 1, 3, 4):
         _, gpu = make_pair(nx, ny, nz, solid, force=(2e-5, 0.0, 0.0), seed=7)
         gpu.tune = tune
         rng = np.random.default_rng(9)
@@ -279,6 +279,7 @@ def test_launch_variants_are_bit_identical(moving):
         for _ in range(5):
             gpu.step_moving_bounceback() if moving else gpu.step()
         outs.append((gpu.F.to_numpy(), gpu.rho.to_numpy(), gpu.v.to_numpy(), gpu.hydro_force.to_numpy()))
-    for a, b in zip(outs[0][:3], outs[1][:3]):
-        np.testing.assert_array_equal(a, b)
-    np.testing.assert_allclose(outs[0][3], outs[1][3], rtol=1e-5, atol=1e-9)
+    for other in outs[1:]:
+        for a, b in zip(outs[0][:3], other[:3]):
+            np.testing.assert_array_equal(a, b)
+        np.testing.assert_allclose(outs[0][3], other[3], rtol=1e-5, atol=1e-9)
