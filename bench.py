@@ -354,8 +354,8 @@ def time_mpm_phase(drv, reps=5):
 # capture (caches flushed before the launch) reads the populations from DRAM
 # and its writes stay in L2.
 NCU_LBM_TRAFFIC = {
-    ("duct_plate_128x64x64", "fp32"): 42.34e6,
-    ("duct_plate_256x128x128", "fp32"): 590.7e6,
+    ("duct_plate_128x64x64", "fp32"): 42.6e6,
+    ("duct_plate_256x128x128", "fp32"): 590.1e6,
 }
 
 
