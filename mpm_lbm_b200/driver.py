@@ -81,6 +81,7 @@ class FSIDriver3D:
         self.use_cuda_graph = bool(use_cuda_graph)
         self._graph = None
         self._graph_steps = 0
+        self._graph_warm = False
         self.graph_kernels_per_step = None
         self.tuning = None
 
@@ -237,8 +238,12 @@ class FSIDriver3D:
 
     def _step_graph(self):
         """Replay a CUDA graph of whole FSI steps (captured after one eager step)."""
-        if self._graph is None and self.current_lbm_step == 0:
-            self._step_eager()  # warm-up: allocates lazily created buffers, leaves bc_pending set
+        if self._graph is None and not self._graph_warm:
+            # warm-up: allocates lazily created buffers (bins, grid buffers, readout
+            # arrays) outside any capture, and leaves bc_pending set; also the first
+            # step of a driver restored from a restart file
+            self._step_eager()
+            self._graph_warm = True
             return
         period = self._graph_period()
         if self._graph is None:

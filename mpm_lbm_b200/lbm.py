@@ -174,7 +174,7 @@ class LBMFluid3D:
         self.rho = CellField(d, 0, np.float32, lambda: self._readout()[1], self._put_rho, "rho")
         self.v = CellField(d, 3, np.float32, lambda: self._readout()[2], self._put_vel, "v")
         self.solid = CellField(d, 0, np.int8, lambda: (self.t_flags & FSI_CELL_SOLID), self._put_solid, "solid")
-        self.static_solid = CellField(d, 0, np.int8, lambda: self.t_static, None, "static_solid")
+        self.static_solid = CellField(d, 0, np.int8, lambda: self.t_static, self._put_static, "static_solid")
         self.old_solid = CellField(d, 0, np.int8,
                                    lambda: (self.t_flags & FSI_CELL_SOLID) if self._old_equals_solid else self.t_old,
                                    None, "old_solid")
@@ -277,6 +277,12 @@ class LBMFluid3D:
     def _put_solid(self, arr):
         s = (np.asarray(arr) > 0).astype(np.uint8)
         self._set_solid(s, keep_static=True)
+
+    def _put_static(self, arr):
+        """static_solid.from_numpy (a restart load, restart.py:76): the mask the
+        dynamic solid update starts from; the current solid mask is unchanged."""
+        ref_to_lattice((np.asarray(arr) > 0).astype(np.uint8), self.dims, 0, self.t_static)
+        self._version += 1
 
     def _put_hydro(self, arr):
         ref_to_lattice(arr, self.dims, 3, self._hydro_tensor())
