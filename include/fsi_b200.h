@@ -190,6 +190,26 @@ int fsi_force_accum_finalize(const FsiLbmState* s, const FsiStepCtl* ctl, int32_
 int fsi_lbm_readout(const FsiLbmState* s, const FsiLbmParams* p, const FsiStepCtl* ctl, float* out_pop,
                     float* out_rho, float* out_vel, void* stream);
 
+/* Per-FSI-step reductions of the subcycled flow campaign
+ * (solvers/official_subcycled_flow_solver.py:352-365 copies rho, v, f and
+ * solid to the host every step; 443-515 then sums them in FP64).  One pass
+ * over the readout state of every cell (as fsi_lbm_readout returns it),
+ * FP64 sums, ~100 bytes of output instead of the four fields:
+ *   - over fluid cells: sum of rho, the cell count, and the number of cells
+ *     with a non-finite rho, v or population;
+ *   - over the cells whose regions[i] has bit r set (any solid state; NULL:
+ *     none): sum of rho * v_x.
+ * regions: [nx * ny * nz] in lattice order (x fastest).  out: device. */
+#define FSI_CAMPAIGN_REGIONS 8
+typedef struct FsiCampaignSums {
+  double fluid_mass;
+  double region_flux[FSI_CAMPAIGN_REGIONS];
+  int32_t fluid_cells;
+  int32_t nonfinite_rho, nonfinite_vel, nonfinite_pop;
+} FsiCampaignSums;
+int fsi_campaign_sums(const FsiLbmState* s, const FsiLbmParams* p, const FsiStepCtl* ctl, const uint8_t* regions,
+                      FsiCampaignSums* out, void* stream);
+
 /* ---- particles, projection, reaction transfer, MPM ---------------------- */
 
 typedef struct FsiParticles {

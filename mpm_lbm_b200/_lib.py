@@ -20,6 +20,14 @@ FSI_MODE_MOVING_BB, FSI_MODE_SUBCYCLED, FSI_MODE_DIRSTATS, FSI_MODE_PENALTY = 1,
 FSI_TUNE_LBM_OCC3, FSI_TUNE_LBM_OCC4, FSI_TUNE_LBM_PAIR, FSI_TUNE_LBM_OCC3_PF, FSI_TUNE_LBM_OCC4_PF = 0, 1, 2, 3, 4
 
 
+FSI_CAMPAIGN_REGIONS = 8
+
+
+class FsiCampaignSums(ctypes.Structure):
+    _fields_ = [("fluid_mass", ctypes.c_double), ("region_flux", ctypes.c_double * FSI_CAMPAIGN_REGIONS),
+                ("fluid_cells", c_i32), ("nonfinite_rho", c_i32), ("nonfinite_vel", c_i32), ("nonfinite_pop", c_i32)]
+
+
 class FsiLbmDiag(ctypes.Structure):
     _fields_ = [
         ("link_count", c_i32 * 19), ("corr_abs_sum", c_f32 * 19), ("corr_abs_max", c_f32 * 19),
@@ -107,7 +115,7 @@ STRUCTS = {
     "FsiLbmDiag": FsiLbmDiag, "FsiLbmState": FsiLbmState, "FsiLbmParams": FsiLbmParams, "FsiStepCtl": FsiStepCtl,
     "FsiParticles": FsiParticles, "FsiGrid": FsiGrid, "FsiMpmParams": FsiMpmParams,
     "FsiCouplingParams": FsiCouplingParams, "FsiCouplingStats": FsiCouplingStats, "FsiMpmBins": FsiMpmBins,
-    "FsiBatchCase": FsiBatchCase, "FsiBatchDims": FsiBatchDims,
+    "FsiBatchCase": FsiBatchCase, "FsiBatchDims": FsiBatchDims, "FsiCampaignSums": FsiCampaignSums,
 }
 
 # entry point -> argtypes (all return int)
@@ -122,6 +130,7 @@ SIGNATURES = {
     "fsi_mask_rebuild_static_scratch": [_P(FsiLbmState), _P(FsiLbmParams), _P(FsiStepCtl), c_f32, c_p],
     "fsi_force_accum_finalize": [_P(FsiLbmState), _P(FsiStepCtl), c_i32, c_p],
     "fsi_lbm_readout": [_P(FsiLbmState), _P(FsiLbmParams), _P(FsiStepCtl), c_p, c_p, c_p, c_p],
+    "fsi_campaign_sums": [_P(FsiLbmState), _P(FsiLbmParams), _P(FsiStepCtl), c_p, c_p, c_p],
     "fsi_project": [_P(FsiLbmState), _P(FsiParticles), _P(FsiCouplingParams), c_p, c_p],
     "fsi_reaction_to_grid": [_P(FsiLbmState), c_p, _P(FsiParticles), _P(FsiGrid), _P(FsiCouplingParams), c_p, c_p],
     "fsi_mpm_p2g": [_P(FsiParticles), _P(FsiGrid), _P(FsiMpmParams), c_p],

@@ -1423,15 +1423,15 @@ __global__ void k_flush_bc(const Case c) {
   if (c.p.limiter) flush_counts(c, cnt);
 }
 
+// The readout state of cell i (what F, rho, v .to_numpy() return): the 19
+// populations in natural order with a pending open boundary applied, and the
+// macroscopic fields of streaming3 (fluid.py:1794-1814), or the stored ones
+// for cells whose collision uses them.  Returns the cell's flags.
 template <bool H>
-__global__ void k_readout(const Case c, float* out_pop, float* out_rho, float* out_vel) {
-  const int64_t n = (int64_t)c.s.nx * c.s.ny * c.s.nz;
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+__device__ __forceinline__ uint8_t readout_cell(const Case& c, int64_t i, float F[19], float& rho, float u[3]) {
   const Coord q = coord_of(c, i);
   const uint8_t fl = c.s.flags[i];
   const uint32_t nb = (fl & kNear) ? c.s.nbr[i] : 0u;
-  float F[19];
 #pragma unroll
   for (int s = 0; s < 19; ++s) {
     int ss;
@@ -1453,8 +1453,8 @@ __global__ void k_readout(const Case c, float* out_pop, float* out_rho, float* o
     }
   }
   const int64_t P = c.s.pitch;
-  for (int s = 0; s < 19; ++s) out_pop[(int64_t)s * P + i] = F[s];
-  float rho = c.p.rho0, u[3] = {0.f, 0.f, 0.f};
+  rho = c.p.rho0;
+  u[0] = u[1] = u[2] = 0.f;
   if (!fluid && (fl & kOverride)) {
     rho = c.s.rho[i];
     for (int a = 0; a < 3; ++a) u[a] = c.s.vel[a * P + i];
@@ -1473,8 +1473,90 @@ __global__ void k_readout(const Case c, float* out_pop, float* out_rho, float* o
       }
     }
   }
+  return fl;
+}
+
+template <bool H>
+__global__ void k_readout(const Case c, float* out_pop, float* out_rho, float* out_vel) {
+  const int64_t n = (int64_t)c.s.nx * c.s.ny * c.s.nz;
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float F[19], rho, u[3];
+  readout_cell<H>(c, i, F, rho, u);
+  const int64_t P = c.s.pitch;
+  for (int s = 0; s < 19; ++s) out_pop[(int64_t)s * P + i] = F[s];
   out_rho[i] = rho;
   for (int a = 0; a < 3; ++a) out_vel[a * P + i] = u[a];
+}
+
+// Reductions of the subcycled-flow campaign over the readout state, one pass
+// (official_subcycled_flow_solver.py:443-515 computes them in FP64 on host
+// copies of rho, v, f and solid): over fluid cells the mass sum(rho), the
+// cell count and the counts of cells with a non-finite rho, v or population;
+// over the cells of region r (bit r of regions[i], any solid state) the flux
+// sum(rho * u_x).  Products and sums in FP64; one atomic per CTA and value.
+template <bool H>
+__global__ void __launch_bounds__(256) k_campaign_sums(const Case c, const uint8_t* __restrict__ regions,
+                                                       FsiCampaignSums* out) {
+  __shared__ double s_d[8][1 + FSI_CAMPAIGN_REGIONS];
+  __shared__ int s_i[8][4];
+  const int64_t n = (int64_t)c.s.nx * c.s.ny * c.s.nz;
+  double mass = 0.0, flux[FSI_CAMPAIGN_REGIONS];
+#pragma unroll
+  for (int r = 0; r < FSI_CAMPAIGN_REGIONS; ++r) flux[r] = 0.0;
+  int cells = 0, bad_rho = 0, bad_vel = 0, bad_pop = 0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    float F[19], rho, u[3];
+    const uint8_t fl = readout_cell<H>(c, i, F, rho, u);
+    if (!(fl & kSolid)) {
+      ++cells;
+      mass += (double)rho;
+      bad_rho += isfinite(rho) ? 0 : 1;
+      bad_vel += (isfinite(u[0]) && isfinite(u[1]) && isfinite(u[2])) ? 0 : 1;
+      bool pf = true;
+#pragma unroll
+      for (int s = 0; s < 19; ++s) pf = pf && isfinite(F[s]);
+      bad_pop += pf ? 0 : 1;
+    }
+    const unsigned rg = regions ? regions[i] : 0u;
+    if (rg) {
+      const double jx = (double)rho * (double)u[0];
+#pragma unroll
+      for (int r = 0; r < FSI_CAMPAIGN_REGIONS; ++r)
+        if ((rg >> r) & 1u) flux[r] += jx;
+    }
+  }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  mass = warp_sum_d(mass);
+#pragma unroll
+  for (int r = 0; r < FSI_CAMPAIGN_REGIONS; ++r) flux[r] = warp_sum_d(flux[r]);
+  cells = __reduce_add_sync(0xffffffffu, (unsigned)cells);
+  bad_rho = __reduce_add_sync(0xffffffffu, (unsigned)bad_rho);
+  bad_vel = __reduce_add_sync(0xffffffffu, (unsigned)bad_vel);
+  bad_pop = __reduce_add_sync(0xffffffffu, (unsigned)bad_pop);
+  if (lane == 0) {
+    s_d[wid][0] = mass;
+#pragma unroll
+    for (int r = 0; r < FSI_CAMPAIGN_REGIONS; ++r) s_d[wid][1 + r] = flux[r];
+    s_i[wid][0] = cells;
+    s_i[wid][1] = bad_rho;
+    s_i[wid][2] = bad_vel;
+    s_i[wid][3] = bad_pop;
+  }
+  __syncthreads();
+  const int nw = blockDim.x >> 5;
+  if (threadIdx.x < 1 + FSI_CAMPAIGN_REGIONS) {
+    double v = 0.0;
+    for (int w = 0; w < nw; ++w) v += s_d[w][threadIdx.x];
+    double* dst = threadIdx.x == 0 ? &out->fluid_mass : &out->region_flux[threadIdx.x - 1];
+    if (v != 0.0) atomicAdd(dst, v);
+  } else if (threadIdx.x >= 32 && threadIdx.x < 36) {
+    const int k = threadIdx.x - 32;
+    int v = 0;
+    for (int w = 0; w < nw; ++w) v += s_i[w][k];
+    int32_t* dst = k == 0 ? &out->fluid_cells : (k == 1 ? &out->nonfinite_rho : (k == 2 ? &out->nonfinite_vel : &out->nonfinite_pop));
+    if (v) atomicAdd(dst, v);
+  }
 }
 
 // finalize_moving_boundary_force_accumulator (fluid.py:475-486)
@@ -1749,6 +1831,23 @@ extern "C" int fsi_lbm_readout(const FsiLbmState* s, const FsiLbmParams* p, cons
   else
     k_readout<false><<<blocks_for(n, 256), 256, 0, (cudaStream_t)stream>>>(c, out_pop, out_rho, out_vel);
   return launch_check("k_readout");
+}
+
+extern "C" int fsi_campaign_sums(const FsiLbmState* s, const FsiLbmParams* p, const FsiStepCtl* ctl,
+                                 const uint8_t* regions, FsiCampaignSums* out, void* stream) {
+  int rc = check_state(s, p);
+  if (rc) return rc;
+  if (!ctl || !out) return invalid("null step control or output");
+  cudaStream_t st = (cudaStream_t)stream;
+  if ((rc = cuda_check(cudaMemsetAsync(out, 0, sizeof(FsiCampaignSums), st), "memset campaign sums"))) return rc;
+  const Case c = make_case(s, p, ctl);
+  const int64_t n = (int64_t)s->nx * s->ny * s->nz;
+  const unsigned blocks = (unsigned)std::min<int64_t>(blocks_for(n, 256), (int64_t)lbm_sm_count() * 8);
+  if (s->store_fp16)
+    k_campaign_sums<true><<<blocks, 256, 0, st>>>(c, regions, out);
+  else
+    k_campaign_sums<false><<<blocks, 256, 0, st>>>(c, regions, out);
+  return launch_check("k_campaign_sums");
 }
 
 // ---- mask rebuild with a built-in change list ----------------------------
