@@ -282,4 +282,6 @@ def test_launch_variants_are_bit_identical(moving):
     for other in outs[1:]:
         for a, b in zip(outs[0][:3], other[:3]):
             np.testing.assert_array_equal(a, b)
-        np.testing.assert_allclose(outs[0][3], other[3], rtol=1e-5, atol=1e-9)
+        # link forces: float atomic sums of terms up to ~0.3 that cancel to ~1e-4;
+        # their order varies, so compare within one ulp of the largest term
+        np.testing.assert_allclose(outs[0][3], other[3], rtol=1e-5, atol=2e-8)
