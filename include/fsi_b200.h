@@ -48,12 +48,23 @@ enum {
   FSI_CELL_CF = 16,       /* cell_force / hydro hold a non-zero penalty force */
 };
 
-/* open-boundary semantics (src/mpm_lbm/sim/lbm/fluid.py:16-19) */
+/* open-boundary semantics (src/mpm_lbm/sim/lbm/fluid.py:16-25, Boundary_condition 538-569).
+ * 4-9 differ from 1 only at a right-face pressure outlet (bc_right == 1): a
+ * repaired regularized population (4, 6, 8) or its blend with the convective
+ * one (5, 7, 9), fed back from the neighbour's density and velocity (4-7) or
+ * from the plane-flux controller (8, 9: update_open_boundary_plane_flux_controller,
+ * fluid.py:1141-1263, run once per step after the step kernel). */
 enum {
   FSI_OB_EQUILIBRIUM_RESET = 0,
   FSI_OB_REGULARIZED = 1,
   FSI_OB_REGULARIZED_LIMITED = 2,
   FSI_OB_CONVECTIVE = 3,
+  FSI_OB_REG_MASS_BALANCED = 4,     /* regularized_mass_balanced_pressure_outlet */
+  FSI_OB_CONV_MASS_BALANCED = 5,    /* convective_mass_balanced_pressure_outlet */
+  FSI_OB_REG_FLUX_MATCHED = 6,      /* regularized_flux_matched_pressure_outlet */
+  FSI_OB_CONV_FLUX_MATCHED = 7,     /* convective_flux_matched_damped_outlet */
+  FSI_OB_REG_PLANE_FLUX = 8,        /* regularized_plane_flux_controlled_pressure_outlet */
+  FSI_OB_CONV_PLANE_FLUX = 9,       /* convective_plane_flux_controlled_damped_outlet */
 };
 
 /* step mode bits */
@@ -80,6 +91,28 @@ typedef struct FsiLbmDiag {
   int32_t change_count;              /* cells whose solid bit flipped in the last mask rebuild */
   int32_t status;                    /* non-zero: device-side error code */
   int32_t pad[2];
+  /* open-boundary repair of semantics 4-9 (fluid.py:1115-1140): the last BC
+   * (cleared before each) and cumulative: mass_balance_correction_count /
+   * _abs_sum, unknown_population_delta_abs_sum, flow_correction_delta_abs_sum,
+   * flow_correction_gain_effective_step, flow_outlet_flux_error_filtered_run */
+  int32_t obr_count_step;
+  float obr_corr_step, obr_delta_step, obf_delta_step, obf_gain_step;
+  int32_t obr_count_run;
+  float obr_corr_run, obr_delta_run, obf_delta_run, obf_err_filtered_run;
+  /* plane-flux controller (fluid.py:1141-1263): sums the step kernel accumulates
+   * from its macroscopic state (rho * u_x of the fluid cells of x = 0, the
+   * measure plane, x = nx-1, nx-2, nx-3, nx-4; fluid cells of the measure plane;
+   * total fluid mass), consumed and cleared by the controller update */
+  float pc_acc[8];
+  float pc_target, pc_measured, pc_area, pc_true_outlet;
+  float pc_near[3];
+  float pc_err_filtered, pc_u_fb, pc_rho_fb, pc_guard_ref;
+  int32_t pc_guard_step, pc_guard_run;
+  int32_t pc_update_step, pc_update_run, pc_sat_step, pc_sat_run;
+  float mn_mass, mn_reference, mn_error, mn_rho_fb;
+  int32_t mn_initialized;
+  int32_t mn_update_step, mn_update_run, mn_sat_step, mn_sat_run;
+  int32_t pad2;
 } FsiLbmDiag;
 
 typedef struct FsiLbmState {
@@ -101,7 +134,8 @@ typedef struct FsiLbmState {
   float* hydro;             /* [3][pitch] hydro_force (penalty / subcycled mean) */
   float* hpp;               /* [2][3][pitch] per-step link forces, ping-pong */
   float* accum;             /* [3][pitch] hydro_force_accum */
-  float* plane;             /* [4][4][ny*nz] rho,ux,uy,uz of x = 0, 1, nx-2, nx-1 of the last step */
+  float* plane;             /* [5][4][ny*nz]: planes 0-3 rho,ux,uy,uz of x = 0, 1, nx-2, nx-1 of the last
+                               step; plane 4 scratch of the outlet flow filter (semantics 6, 7), zeroed */
   int32_t* change_list;     /* [pitch] scratch for the mask rebuild */
   FsiLbmDiag* diag;         /* device */
   const float* vel_left_dyn;  /* optional [3]: x-min inlet velocity read on the device each step
@@ -120,6 +154,13 @@ typedef struct FsiLbmParams {
   float ob_rho_min, ob_rho_max, ob_u_max, ob_noneq_cap, ob_floor;
   float penalty_beta, penalty_phi_min, penalty_cap;
   int32_t tune;             /* FSI_TUNE_LBM_*: launch variant of the step kernel (results are identical) */
+  /* open-boundary semantics 4-9 (LBMConfig.open_boundary_*, lbm/config.py:53-69) */
+  float ob_gain_u, ob_gain_rho, ob_filter_alpha, ob_cap_u, ob_delta_cap_u, ob_slew_alpha, ob_blend;
+  float ob_target_scale, ob_guard_min_ratio, ob_mn_gain, ob_mn_cap, ob_mn_blend;
+  int32_t ob_measure_offset;  /* 0..2: the controller measures x = nx - 1 - offset */
+  int32_t ob_guard;           /* outlet flux drop guard */
+  int32_t ob_mass_neutral;    /* mass-neutral density offset (mode global_mass_error_density_offset) */
+  int32_t ob_pad;
 } FsiLbmParams;
 
 /* launch variants of fsi_lbm_substep (FsiLbmParams.tune) */
@@ -159,6 +200,17 @@ int fsi_lbm_to_natural(const FsiLbmState* s, void* stream);
  * collision (398-413) -> AA streaming with static or moving half-way
  * bounce-back and momentum-exchange link forces (431-440 / 488-536). */
 int fsi_lbm_substep(const FsiLbmState* s, const FsiLbmParams* p, const FsiStepCtl* ctl, void* stream);
+/* Under semantics 4-9 fsi_lbm_substep launches one more small kernel after the
+ * step: the clear of the repair step counters and, under 8 and 9, the outlet
+ * flux controller (update_open_boundary_plane_flux_controller, fluid.py:1141-1263)
+ * from plane sums the step accumulated, ahead of the step's pending open boundary. */
+
+/* update_open_boundary_plane_flux_controller (fluid.py:1141-1263) called on its
+ * own, from given macroscopic fields rho [pitch] and vel [3][pitch] (the
+ * readout of the state, or fields the caller set) and the solid bits of the
+ * state.  Replaces LBMFluid3D.update_open_boundary_plane_flux_controller. */
+int fsi_ob_controller_update(const FsiLbmState* s, const FsiLbmParams* p, const float* rho, const float* vel,
+                             void* stream);
 
 /* Apply a pending open-boundary step into the state (so that a mask rebuild
  * sees the same populations as the reference). */

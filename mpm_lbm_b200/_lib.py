@@ -34,6 +34,16 @@ class FsiLbmDiag(ctypes.Structure):
         ("fluid_impulse", (c_f32 * 3) * 19), ("accum_norm_max", c_f32), ("mean_norm_max", c_f32),
         ("ob_step", c_i32 * 5), ("ob_run", c_i32 * 5), ("penalty_active", c_i32), ("penalty_max_norm", c_f32),
         ("penalty_net", c_f32 * 3), ("change_count", c_i32), ("status", c_i32), ("pad", c_i32 * 2),
+        ("obr_count_step", c_i32), ("obr_corr_step", c_f32), ("obr_delta_step", c_f32), ("obf_delta_step", c_f32),
+        ("obf_gain_step", c_f32), ("obr_count_run", c_i32), ("obr_corr_run", c_f32), ("obr_delta_run", c_f32),
+        ("obf_delta_run", c_f32), ("obf_err_filtered_run", c_f32), ("pc_acc", c_f32 * 8),
+        ("pc_target", c_f32), ("pc_measured", c_f32), ("pc_area", c_f32), ("pc_true_outlet", c_f32),
+        ("pc_near", c_f32 * 3), ("pc_err_filtered", c_f32), ("pc_u_fb", c_f32), ("pc_rho_fb", c_f32),
+        ("pc_guard_ref", c_f32), ("pc_guard_step", c_i32), ("pc_guard_run", c_i32), ("pc_update_step", c_i32),
+        ("pc_update_run", c_i32), ("pc_sat_step", c_i32), ("pc_sat_run", c_i32), ("mn_mass", c_f32),
+        ("mn_reference", c_f32), ("mn_error", c_f32), ("mn_rho_fb", c_f32), ("mn_initialized", c_i32),
+        ("mn_update_step", c_i32), ("mn_update_run", c_i32), ("mn_sat_step", c_i32), ("mn_sat_run", c_i32),
+        ("pad2", c_i32),
     ]
 
 
@@ -55,6 +65,10 @@ class FsiLbmParams(ctypes.Structure):
         ("ob_rho_min", c_f32), ("ob_rho_max", c_f32), ("ob_u_max", c_f32), ("ob_noneq_cap", c_f32),
         ("ob_floor", c_f32), ("penalty_beta", c_f32), ("penalty_phi_min", c_f32), ("penalty_cap", c_f32),
         ("tune", c_i32),
+        ("ob_gain_u", c_f32), ("ob_gain_rho", c_f32), ("ob_filter_alpha", c_f32), ("ob_cap_u", c_f32),
+        ("ob_delta_cap_u", c_f32), ("ob_slew_alpha", c_f32), ("ob_blend", c_f32), ("ob_target_scale", c_f32),
+        ("ob_guard_min_ratio", c_f32), ("ob_mn_gain", c_f32), ("ob_mn_cap", c_f32), ("ob_mn_blend", c_f32),
+        ("ob_measure_offset", c_i32), ("ob_guard", c_i32), ("ob_mass_neutral", c_i32), ("ob_pad", c_i32),
     ]
 
 
@@ -125,6 +139,7 @@ SIGNATURES = {
     "fsi_lbm_set_solid": [_P(FsiLbmState), c_p, c_p],
     "fsi_lbm_to_natural": [_P(FsiLbmState), c_p],
     "fsi_lbm_substep": [_P(FsiLbmState), _P(FsiLbmParams), _P(FsiStepCtl), c_p],
+    "fsi_ob_controller_update": [_P(FsiLbmState), _P(FsiLbmParams), c_p, c_p, c_p],
     "fsi_lbm_flush_bc": [_P(FsiLbmState), _P(FsiLbmParams), _P(FsiStepCtl), c_p],
     "fsi_mask_rebuild": [_P(FsiLbmState), _P(FsiLbmParams), _P(FsiStepCtl), c_f32, c_p],
     "fsi_mask_rebuild_static_scratch": [_P(FsiLbmState), _P(FsiLbmParams), _P(FsiStepCtl), c_f32, c_p],

@@ -195,6 +195,8 @@ class FSIBatch:
         lbm = drv.lbm
         if lbm.bc_x_left or lbm.bc_x_right:
             raise ValueError("batched cases have no open boundaries")
+        if lbm.params.ob_semantics >= 8:
+            raise ValueError("batched cases run no outlet flux controller (open-boundary semantics 8 and 9)")
         if slot is None:
             free = self.free_slots()
             if not free:

@@ -45,13 +45,15 @@ OPEN_BOUNDARY_SEMANTICS = (
     "regularized_plane_flux_controlled_pressure_outlet",
     "convective_plane_flux_controlled_damped_outlet",
 )
-# the four the fused kernel implements (the driver exposes exactly these: fsi_config.py:32-37)
-KERNEL_OPEN_BOUNDARY_CODES = {
-    "equilibrium_all_population_reset": 0,
-    "regularized_velocity_pressure": 1,
-    "regularized_velocity_pressure_limited": 2,
-    "convective_pressure_outlet_experimental": 3,
-}
+# FsiLbmParams.ob_semantics code of each (FSI_OB_* in the C header); the FSI
+# driver config exposes the first four (fsi_config.py:32-37), LBMConfig all ten
+KERNEL_OPEN_BOUNDARY_CODES = {name: code for code, name in enumerate(OPEN_BOUNDARY_SEMANTICS)}
+OPEN_BOUNDARY_MASS_NEUTRAL_FLUX_CONTROL_MODES = (
+    "disabled",
+    "global_mass_error_density_offset",
+    "outlet_population_projection_report_only",
+)
+OPEN_BOUNDARY_MASS_NEUTRAL_REFERENCE_MASS_MODES = ("initial",)
 
 
 @dataclass
@@ -69,6 +71,23 @@ class LBMConfig:
     open_boundary_u_max: float = 0.1
     open_boundary_noneq_cap: float = 0.05
     open_boundary_population_floor: Optional[float] = None
+    open_boundary_flux_feedback_gain_u: float = 0.01
+    open_boundary_flux_feedback_gain_rho: float = 0.005
+    open_boundary_flux_filter_alpha: float = 0.05
+    open_boundary_flux_correction_cap_u: float = 0.005
+    open_boundary_flux_feedback_delta_cap_u: float = 0.0
+    open_boundary_flux_feedback_slew_alpha: float = 1.0
+    open_boundary_convective_blend_weight: float = 0.05
+    open_boundary_flux_control_measure_plane_offset: int = 0
+    open_boundary_flux_control_target_scale: float = 1.0
+    open_boundary_outlet_flux_drop_guard_enabled: bool = False
+    open_boundary_outlet_flux_drop_guard_min_ratio: float = 0.60
+    open_boundary_mass_neutral_flux_control_enabled: bool = False
+    open_boundary_mass_neutral_flux_control_mode: str = "disabled"
+    open_boundary_mass_neutral_mass_error_gain: float = 0.0
+    open_boundary_mass_neutral_mass_error_cap: float = 0.0
+    open_boundary_mass_neutral_correction_blend: float = 0.0
+    open_boundary_mass_neutral_reference_mass_mode: str = "initial"
     sparse_storage: bool = False
     force: Tuple[float, float, float] = (0.0, 0.0, 0.0)
     bc_x_left: int = 0
@@ -108,10 +127,58 @@ class LBMConfig:
             raise ValueError("open_boundary_u_max must be positive")
         if self.open_boundary_noneq_cap <= 0.0:
             raise ValueError("open_boundary_noneq_cap must be positive")
+        self._check_flux_control()
         if self.collision not in ("mrt", "bgk"):
             raise ValueError("collision must be 'mrt' or 'bgk'")
         if self.population_storage not in ("fp32", "fp16"):
             raise ValueError("population_storage must be 'fp32' or 'fp16'")
+
+    def _check_flux_control(self):
+        """The outlet repair and flux-controller rules of lbm/config.py:109-165,
+        in the reference's order."""
+        def nonneg(name):
+            if getattr(self, name) < 0.0:
+                raise ValueError(f"{name} must be non-negative")
+
+        nonneg("open_boundary_flux_feedback_gain_u")
+        nonneg("open_boundary_flux_feedback_gain_rho")
+        if not (0.0 < self.open_boundary_flux_filter_alpha <= 1.0):
+            raise ValueError("open_boundary_flux_filter_alpha must be in (0, 1]")
+        if self.open_boundary_flux_correction_cap_u <= 0.0:
+            raise ValueError("open_boundary_flux_correction_cap_u must be positive")
+        nonneg("open_boundary_flux_feedback_delta_cap_u")
+        if not (0.0 < self.open_boundary_flux_feedback_slew_alpha <= 1.0):
+            raise ValueError("open_boundary_flux_feedback_slew_alpha must be in (0, 1]")
+        if not (0.0 <= self.open_boundary_convective_blend_weight <= 1.0):
+            raise ValueError("open_boundary_convective_blend_weight must be in [0, 1]")
+        offset = self.open_boundary_flux_control_measure_plane_offset
+        if int(offset) != offset:
+            raise ValueError("open_boundary_flux_control_measure_plane_offset must be an integer")
+        if not (0 <= int(offset) <= 2):
+            raise ValueError("open_boundary_flux_control_measure_plane_offset must be 0, 1, or 2")
+        self.open_boundary_flux_control_measure_plane_offset = int(offset)
+        if self.open_boundary_flux_control_target_scale <= 0.0:
+            raise ValueError("open_boundary_flux_control_target_scale must be positive")
+        self.open_boundary_flux_control_target_scale = float(self.open_boundary_flux_control_target_scale)
+        if not (0.0 < self.open_boundary_outlet_flux_drop_guard_min_ratio <= 1.0):
+            raise ValueError("open_boundary_outlet_flux_drop_guard_min_ratio must be in (0, 1]")
+        self.open_boundary_mass_neutral_flux_control_enabled = bool(self.open_boundary_mass_neutral_flux_control_enabled)
+        if self.open_boundary_mass_neutral_flux_control_mode not in OPEN_BOUNDARY_MASS_NEUTRAL_FLUX_CONTROL_MODES:
+            raise ValueError("open_boundary_mass_neutral_flux_control_mode must be one of "
+                             f"{OPEN_BOUNDARY_MASS_NEUTRAL_FLUX_CONTROL_MODES}")
+        if self.open_boundary_mass_neutral_reference_mass_mode not in OPEN_BOUNDARY_MASS_NEUTRAL_REFERENCE_MASS_MODES:
+            raise ValueError("open_boundary_mass_neutral_reference_mass_mode must be one of "
+                             f"{OPEN_BOUNDARY_MASS_NEUTRAL_REFERENCE_MASS_MODES}")
+        if self.open_boundary_mass_neutral_flux_control_enabled and \
+                self.open_boundary_mass_neutral_flux_control_mode == "disabled":
+            raise ValueError("open_boundary_mass_neutral_flux_control_enabled cannot be true when mode is disabled")
+        nonneg("open_boundary_mass_neutral_mass_error_gain")
+        nonneg("open_boundary_mass_neutral_mass_error_cap")
+        if not (0.0 <= self.open_boundary_mass_neutral_correction_blend <= 1.0):
+            raise ValueError("open_boundary_mass_neutral_correction_blend must be in [0, 1]")
+        for name in ("open_boundary_mass_neutral_mass_error_gain", "open_boundary_mass_neutral_mass_error_cap",
+                     "open_boundary_mass_neutral_correction_blend"):
+            setattr(self, name, float(getattr(self, name)))
 
 
 @dataclass

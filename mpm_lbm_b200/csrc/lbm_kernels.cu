@@ -172,9 +172,133 @@ __device__ __forceinline__ float regularized_pop(const FsiLbmParams& p, bool lim
   return out;
 }
 
+// ---- pressure-outlet repair of semantics 4-9 (fluid.py:1106-1346) ----------
+__device__ __forceinline__ float ob_bounded(float v, float lim) { return v > lim ? lim : (v < -lim ? -lim : v); }
+
+// _limit_open_boundary_population (fluid.py:1043-1049)
+__device__ __forceinline__ float ob_floor_limit(const FsiLbmParams& p, float v) {
+  return (p.limiter && p.floor_enabled && v < p.ob_floor) ? p.ob_floor : v;
+}
+
+// The repair records of the populations a thread evaluates.  Each record of
+// the flow filter (flow_outlet_flux_error_filtered_run <- (1 - a) f + a e,
+// fluid.py:1127-1131) is an affine map of f; fd, fb hold the composite of the
+// thread's records in order as f -> (1 - fd) f + fb (zero: no record).
+struct ObRepair {
+  int count;
+  float corr, delta, fdelta;
+  bool gain;
+  float fd, fb;
+};
+
+__device__ __forceinline__ void ob_filter_add(ObRepair& r, float alpha, float err) {
+  r.fb = (1.0f - alpha) * r.fb + alpha * err;
+  r.fd = r.fd + alpha * (1.0f - r.fd);
+}
+
+// composite of map (d1, b1) followed by map (d2, b2)
+__device__ __forceinline__ void ob_filter_then(float& d1, float& b1, float d2, float b2) {
+  b1 = (1.0f - d2) * b1 + b2;
+  d1 = d1 + d2 - d1 * d2;
+}
+
+// Slot of outlet row (j, k) for its filter composite: plane 4 of the plane
+// array, in the reference's loop order over the face (j outer, k inner).
+__device__ __forceinline__ float* ob_filter_slot(const FsiLbmState& st, int j, int k) {
+  const int64_t n = (int64_t)st.ny * st.nz;
+  return st.plane + 16 * n + 2 * ((int64_t)j * st.nz + k);
+}
+
+// One unknown population s of a right-face pressure-outlet cell (bc_right == 1)
+// under semantics 4-9: trho = rho_bc_right, tu = v[ni] (mac_n: rho, v of ni
+// from the last macroscopic update), Fn / Fn2 = F[ni] / F[n2i]; dc holds the
+// controller feedback.  Records go to r.
+__device__ float repaired_outlet_pop(const FsiLbmParams& p, const FsiLbmDiag* dc, int s, float trho,
+                                     float tu0, float tu1, float tu2, float Fn, float Fn2, bool n2_fluid,
+                                     const float* mac_n, ObRepair& r) {
+  const int sem = p.ob_semantics;
+  const float vx_in = p.vel_bc_left[0];  // vx_bcxl
+  const float noneq = Fn - feq(s, mac_n[0], mac_n[1], mac_n[2], mac_n[3]);
+  const float before = feq(s, trho, tu0, tu1, tu2) + noneq;  // _regularized_population (fluid.py:1032-1035)
+  float inner;
+  if (sem == FSI_OB_REG_MASS_BALANCED || sem == FSI_OB_CONV_MASS_BALANCED) {  // fluid.py:1266-1276
+    const float rho_fb = ob_bounded(0.02f * (p.rho0 - mac_n[0]), 0.01f);
+    const float vel_fb = ob_bounded(0.05f * (vx_in - tu0), 0.02f);
+    const float after = feq(s, trho + rho_fb, tu0 + vel_fb, tu1, tu2) + noneq;
+    r.count += 1;
+    r.corr += fabsf(rho_fb) + fabsf(vel_fb);
+    r.delta += fabsf(after - before);
+    inner = ob_floor_limit(p, after);
+  } else if (sem == FSI_OB_REG_FLUX_MATCHED || sem == FSI_OB_CONV_FLUX_MATCHED) {  // fluid.py:1287-1306
+    const float rho_fb = ob_bounded(p.ob_gain_rho * (p.rho0 - mac_n[0]), 0.01f);
+    const float verr = vx_in - tu0;
+    const float vel_fb = ob_bounded(p.ob_gain_u * verr, p.ob_cap_u);
+    const float after = feq(s, trho + rho_fb, tu0 + vel_fb, tu1, tu2) + noneq;
+    r.count += 1;
+    r.corr += fabsf(rho_fb) + fabsf(vel_fb);
+    r.delta += fabsf(after - before);
+    r.fdelta += fabsf(vel_fb);
+    r.gain = true;
+    ob_filter_add(r, p.ob_filter_alpha, verr);
+    inner = ob_floor_limit(p, after);
+  } else {  // plane-flux controlled, fluid.py:1319-1337
+    const float rho_fb = dc->pc_rho_fb;
+    const float mn = (sem == FSI_OB_REG_PLANE_FLUX && p.ob_mass_neutral) ? dc->mn_rho_fb : 0.0f;
+    const float vel_fb = dc->pc_u_fb;
+    const float after = feq(s, trho + rho_fb + mn, tu0 + vel_fb, tu1, tu2) + noneq;
+    const float corr = fabsf(rho_fb) + fabsf(mn) + fabsf(vel_fb);
+    r.count += 1;
+    r.corr += corr;
+    r.delta += fabsf(after - before);
+    r.fdelta += corr;
+    r.gain = true;
+    inner = ob_floor_limit(p, after);
+  }
+  if (sem == FSI_OB_REG_MASS_BALANCED || sem == FSI_OB_REG_FLUX_MATCHED || sem == FSI_OB_REG_PLANE_FLUX) return inner;
+  // convective blend (fluid.py:1278-1285, 1308-1317, 1339-1346)
+  const float conv = ob_floor_limit(p, n2_fluid ? 2.0f * Fn - Fn2 : Fn);
+  const float blend = sem == FSI_OB_CONV_MASS_BALANCED ? 0.15f : p.ob_blend;
+  const float repaired = conv + blend * (inner - conv);
+  const float dd = fabsf(repaired - conv);
+  r.count += 1;
+  r.delta += dd;
+  if (sem == FSI_OB_CONV_FLUX_MATCHED) {
+    r.fdelta += dd;
+    ob_filter_add(r, p.ob_filter_alpha, vx_in - tu0);
+  } else if (sem == FSI_OB_CONV_PLANE_FLUX) {
+    r.corr += dd;
+    r.fdelta += dd;
+  }
+  return ob_floor_limit(p, repaired);
+}
+
+// one thread's repair records into the diagnostics (step and run)
+__device__ __forceinline__ void ob_repair_flush(const FsiLbmParams& p, FsiLbmDiag* d, const ObRepair& r) {
+  if (r.count) {
+    atomicAdd(&d->obr_count_step, r.count);
+    atomicAdd(&d->obr_count_run, r.count);
+  }
+  if (r.corr != 0.f) {
+    atomicAdd(&d->obr_corr_step, r.corr);
+    atomicAdd(&d->obr_corr_run, r.corr);
+  }
+  if (r.delta != 0.f) {
+    atomicAdd(&d->obr_delta_step, r.delta);
+    atomicAdd(&d->obr_delta_run, r.delta);
+  }
+  if (r.fdelta != 0.f) {
+    atomicAdd(&d->obf_delta_step, r.fdelta);
+    atomicAdd(&d->obf_delta_run, r.fdelta);
+  }
+  if (r.gain) d->obf_gain_step = p.ob_gain_u;
+}
+
 // Boundary_condition for one fluid face cell (fluid.py:926-1024, 1348-1493).
+// rec: diagnostics the repair records go to (null: none, a readout);
+// ctl: controller state; slot: the row's filter composite (with rec).
 __device__ void apply_face_bc(const FsiLbmParams& p, const float* vdyn, int side, const FaceIn& in, float* F,
-                              int* cnt) {
+                              int* cnt, FsiLbmDiag* rec = nullptr, const FsiLbmDiag* ctl = nullptr,
+                              float* slot = nullptr) {
   const int bc = side == 0 ? p.bc_left : p.bc_right;
   
   if (p.ob_semantics == FSI_OB_EQUILIBRIUM_RESET) {
@@ -196,6 +320,21 @@ __device__ void apply_face_bc(const FsiLbmParams& p, const float* vdyn, int side
       if (in.n2_fluid) ex = 2.0f * in.Fni[q] - in.Fn2[q];
       if (p.limiter && p.floor_enabled && ex < p.ob_floor) ex = p.ob_floor;
       F[(side == 0 ? kUnknownL(q) : kUnknownR(q))] = ex;
+    }
+    return;
+  }
+  if (p.ob_semantics >= FSI_OB_REG_MASS_BALANCED && side == 1 && bc == 1) {
+    ObRepair r{0, 0.f, 0.f, 0.f, false, 0.f, 0.f};
+#pragma unroll
+    for (int q = 0; q < 5; ++q)
+      F[kUnknownR(q)] = repaired_outlet_pop(p, ctl, kUnknownR(q), p.rho_bc_right, in.mac_n[1], in.mac_n[2],
+                                            in.mac_n[3], in.Fni[q], in.Fn2[q], in.n2_fluid, in.mac_n, r);
+    if (rec) {
+      ob_repair_flush(p, rec, r);
+      if (slot && r.fd != 0.f) {
+        slot[0] = r.fd;
+        slot[1] = r.fb;
+      }
     }
     return;
   }
@@ -248,12 +387,13 @@ __device__ __forceinline__ void flush_counts(const Case& c, const int* cnt) {
 struct FaceVal {
   float val;
   int packed;  // five 6-bit limiter counters
+  ObRepair rep;
 };
 
 __device__ __forceinline__ FaceVal face_population(const FsiLbmParams& p, const float* vdyn, int side, int lane,
                                                    float Fn, float Fn2, bool n2_fluid, const float* mac_n,
-                                                   const float* mac_l) {
-  FaceVal r{0.f, 0};
+                                                   const float* mac_l, FsiLbmDiag* d) {
+  FaceVal r{0.f, 0, ObRepair{0, 0.f, 0.f, 0.f, false, 0.f, 0.f}};
   const int bc = side == 0 ? p.bc_left : p.bc_right;
   const float* vb = side == 0 ? (vdyn ? vdyn : p.vel_bc_left) : p.vel_bc_right;
   if (p.ob_semantics == FSI_OB_EQUILIBRIUM_RESET) {  // fluid.py:926-1024
@@ -265,6 +405,11 @@ __device__ __forceinline__ FaceVal face_population(const FsiLbmParams& p, const 
   }
   if (lane >= 5) return r;
   const int s = side == 0 ? kUnknownL(lane) : kUnknownR(lane);
+  if (p.ob_semantics >= FSI_OB_REG_MASS_BALANCED && side == 1 && bc == 1) {
+    r.val = repaired_outlet_pop(p, d, s, p.rho_bc_right, mac_n[1], mac_n[2], mac_n[3], Fn, Fn2, n2_fluid, mac_n,
+                                r.rep);
+    return r;
+  }
   if (p.ob_semantics == FSI_OB_CONVECTIVE && side == 1 && bc == 1) {  // fluid.py:1098-1103
     float ex = n2_fluid ? 2.0f * Fn - Fn2 : Fn;
     if (p.limiter && p.floor_enabled && ex < p.ob_floor) ex = p.ob_floor;
@@ -288,6 +433,29 @@ __device__ __forceinline__ FaceVal face_population(const FsiLbmParams& p, const 
   r.val = regularized_pop(p, p.ob_semantics == FSI_OB_REGULARIZED_LIMITED, s, trho, t0, t1, t2, Fn, mac_n, cnt);
   r.packed = cnt[0] | (cnt[1] << 6) | (cnt[2] << 12) | (cnt[3] << 18) | (cnt[4] << 24);
   return r;
+}
+
+// the repair records of a face warp's lanes (lane q: unknown population q of
+// the face cell of face row `row`), one set of atomics per warp, and the
+// row's filter composite in population order
+__device__ __forceinline__ void ob_repair_warp(const Case& c, int lane, int row, const ObRepair& r) {
+  ObRepair w;
+  w.count = (int)__reduce_add_sync(kFull, (unsigned)r.count);
+  w.corr = warp_sum(r.corr);
+  w.delta = warp_sum(r.delta);
+  w.fdelta = warp_sum(r.fdelta);
+  w.gain = __any_sync(kFull, r.gain);
+  float fd = 0.f, fb = 0.f;
+#pragma unroll
+  for (int q = 0; q < 5; ++q) ob_filter_then(fd, fb, __shfl_sync(kFull, r.fd, q), __shfl_sync(kFull, r.fb, q));
+  if (lane == 0) {
+    ob_repair_flush(c.p, c.s.diag, w);
+    if (fd != 0.f) {
+      float* slot = ob_filter_slot(c.s, row % c.s.ny, row / c.s.ny);
+      slot[0] = fd;
+      slot[1] = fb;
+    }
+  }
 }
 
 // Open boundary of one x face for the warp holding that face cell: the five
@@ -318,7 +486,7 @@ __device__ __forceinline__ void bc_face_warp(const Case& c, int lane, int row, u
   float mac_n[4], mac_l[4];
   load_plane(c, SIDE == 0 ? (n1_solid ? 0 : 1) : (n1_solid ? 3 : 2), row, mac_n);
   load_plane(c, SIDE == 0 ? (n1_solid ? 1 : 0) : 2, row, mac_l);
-  const FaceVal r = face_population(c.p, c.s.vel_left_dyn, SIDE, lane, Fn, Fn2, n2_fluid, mac_n, mac_l);
+  const FaceVal r = face_population(c.p, c.s.vel_left_dyn, SIDE, lane, Fn, Fn2, n2_fluid, mac_n, mac_l, c.s.diag);
   if (c.p.ob_semantics == FSI_OB_EQUILIBRIUM_RESET) {
 #pragma unroll
     for (int s = 0; s < 19; ++s) {
@@ -336,6 +504,42 @@ __device__ __forceinline__ void bc_face_warp(const Case& c, int lane, int row, u
                           (r.packed >> 24) & 63};
       flush_counts(c, cnt);
     }
+    if (SIDE == 1 && c.p.ob_semantics >= FSI_OB_REG_MASS_BALANCED && c.p.bc_right == 1)
+      ob_repair_warp(c, lane, row, r.rep);
+  }
+}
+
+// ---- plane sums of the outlet flux controller (fluid.py:1152-1187, 1225-1229)
+// From the macroscopic state the collision uses, which is the rho, v the
+// reference's controller reads at the open boundary of the same step:
+// t[0] rho u_x over the fluid cells of x = 0, t[1] over the measure plane
+// (x = nx - 1 - offset, at least 0), t[2] the measure plane's fluid cell
+// count, t[3..6] rho u_x over x = nx-1, nx-2, nx-3, nx-4 (each at least 0),
+// t[7] the fluid mass (mass-neutral feedback only).
+__device__ __forceinline__ void plane_flux_add(const Case& c, int x, bool fluid, float rho, float ux, float* t) {
+  const int nx = c.s.nx;
+  const int mi = max(0, nx - 1 - c.p.ob_measure_offset);
+  const float q = fluid ? rho * ux : 0.f;
+  t[0] += x == 0 ? q : 0.f;
+  t[1] += x == mi ? q : 0.f;
+  t[2] += (fluid && x == mi) ? 1.f : 0.f;
+  t[3] += x == nx - 1 ? q : 0.f;
+  t[4] += x == max(0, nx - 2) ? q : 0.f;
+  t[5] += x == max(0, nx - 3) ? q : 0.f;
+  t[6] += x == max(0, nx - 4) ? q : 0.f;
+  t[7] += fluid ? rho : 0.f;
+}
+
+// one warp's sums into pc_acc; x0 .. x0 + w - 1 is the warp's x range
+__device__ __forceinline__ void plane_flux_flush(const Case& c, int lane, int x0, int w, const float* t) {
+  const int nx = c.s.nx;
+  const int mi = max(0, nx - 1 - c.p.ob_measure_offset);
+  const bool planes = x0 == 0 || (mi >= x0 && mi < x0 + w) || x0 + w > nx - 4;
+#pragma unroll
+  for (int a = 0; a < 8; ++a) {
+    if (a < 7 ? !planes : !c.p.ob_mass_neutral) continue;
+    const float v = warp_sum(t[a]);
+    if (lane == 0 && v != 0.f) atomicAdd(&c.s.diag->pc_acc[a], v);
   }
 }
 
@@ -544,6 +748,11 @@ __device__ __forceinline__ void lbm_step_tile(const Case& c, int bx, int by, int
       pp[m + row] = ux;
       pp[2 * m + row] = uy;
       pp[3 * m + row] = uz;
+    }
+    if (c.p.ob_semantics >= FSI_OB_REG_PLANE_FLUX) {
+      float t[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+      plane_flux_add(c, x, fluid, rho, ux, t);
+      plane_flux_flush(c, lane, bx * 32, 32, t);
     }
   }
 
@@ -767,7 +976,7 @@ __device__ __forceinline__ void bc_face_warp2(const Case& c, int lane, int row, 
   float mac_n[4], mac_l[4];
   load_plane(c, SIDE == 0 ? (n1_solid ? 0 : 1) : (n1_solid ? 3 : 2), row, mac_n);
   load_plane(c, SIDE == 0 ? (n1_solid ? 1 : 0) : 2, row, mac_l);
-  const FaceVal r = face_population(c.p, c.s.vel_left_dyn, SIDE, lane, Fn, Fn2, n2_fluid, mac_n, mac_l);
+  const FaceVal r = face_population(c.p, c.s.vel_left_dyn, SIDE, lane, Fn, Fn2, n2_fluid, mac_n, mac_l, c.s.diag);
   if (c.p.ob_semantics == FSI_OB_EQUILIBRIUM_RESET) {
 #pragma unroll
     for (int s = 0; s < 19; ++s) {
@@ -785,6 +994,8 @@ __device__ __forceinline__ void bc_face_warp2(const Case& c, int lane, int row, 
                           (r.packed >> 24) & 63};
       flush_counts(c, cnt);
     }
+    if (SIDE == 1 && c.p.ob_semantics >= FSI_OB_REG_MASS_BALANCED && c.p.bc_right == 1)
+      ob_repair_warp(c, lane, row, r.rep);
   }
 }
 
@@ -962,6 +1173,12 @@ __device__ __forceinline__ void lbm_step_tile2(const Case& c, int bx, int by, Di
         pp[2 * m + row] = uy.y;
         pp[3 * m + row] = uz.y;
       }
+    }
+    if (c.p.ob_semantics >= FSI_OB_REG_PLANE_FLUX) {
+      float t[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+      plane_flux_add(c, x0, fluid0, rho.x, ux.x, t);
+      plane_flux_add(c, x0 + 1, fluid1, rho.y, ux.y, t);
+      plane_flux_flush(c, lane, bx * 64, 64, t);
     }
   }
 
@@ -1415,7 +1632,7 @@ __global__ void k_flush_bc(const Case c) {
         pop_slot(c, q, cell, fl, nb, s, ss[s], sc[s]);
         F[s] = Pop<H>::ld_rw(c, ss[s], sc[s]);
       }
-      apply_face_bc(c.p, c.s.vel_left_dyn, side, in, F, cnt);
+      apply_face_bc(c.p, c.s.vel_left_dyn, side, in, F, cnt, c.s.diag, c.s.diag, ob_filter_slot(c.s, j, k));
 #pragma unroll
       for (int s = 0; s < 19; ++s) Pop<H>::st(c, ss[s], sc[s], F[s]);
     }
@@ -1449,7 +1666,7 @@ __device__ __forceinline__ uint8_t readout_cell(const Case& c, int64_t i, float 
       FaceIn in;
       int face_x;
       face_inputs<H>(c, side, q.j, q.k, in, face_x);
-      apply_face_bc(c.p, c.s.vel_left_dyn, side, in, F, cnt);
+      apply_face_bc(c.p, c.s.vel_left_dyn, side, in, F, cnt, nullptr, c.s.diag);  // a readout records nothing
     }
   }
   const int64_t P = c.s.pitch;
@@ -1599,6 +1816,9 @@ static int check_state(const FsiLbmState* s, const FsiLbmParams* p) {
     return invalid("pitch must cover nx*ny*nz and be a multiple of 32");
   if (19 * s->pitch > (int64_t)UINT32_MAX) return invalid("lattice too large: 19 * pitch must be below 2^32");
   if (p->tune < FSI_TUNE_LBM_OCC3 || p->tune > FSI_TUNE_LBM_OCC4_PF) return invalid("unknown FsiLbmParams.tune");
+  if (p->ob_semantics < FSI_OB_EQUILIBRIUM_RESET || p->ob_semantics > FSI_OB_CONV_PLANE_FLUX)
+    return invalid("unknown FsiLbmParams.ob_semantics");
+  if (p->ob_measure_offset < 0) return invalid("ob_measure_offset must be >= 0");
   if ((p->bc_left || p->bc_right) && (s->nx < 4 || (s->nx % 32 == 1) || (s->nx % 32 == 2)))
     return invalid("x open boundaries need nx >= 4 and nx % 32 not in {1, 2}");
   if (!s->pop || !s->flags || !s->nbr || !s->diag) return invalid("null device pointer in FsiLbmState");
@@ -1686,6 +1906,162 @@ extern "C" int fsi_lbm_to_natural(const FsiLbmState* s, void* stream) {
   return launch_check("k_to_natural");
 }
 
+// After each step, before its (pending) open boundary is applied: the clear
+// of the repair step counters (clear_open_boundary_limiter_step_counters,
+// fluid.py:571-586) and, under semantics 8 and 9, the outlet flux controller
+// update_open_boundary_plane_flux_controller (fluid.py:1141-1263) from the
+// plane sums the step accumulated in pc_acc, which it then zeroes.
+// step_clear = 0, run = 1: a controller update on its own (the reference's
+// kernel called directly), which clears no step counter of its own.
+// compose: first fold the flow-filter composites the last open-boundary
+// application left in the outlet row slots (semantics 6, 7) into
+// flow_outlet_flux_error_filtered_run, in row order, and clear the slots.
+// One block of kObThreads threads.
+constexpr int kObThreads = 1024;
+
+__global__ void __launch_bounds__(kObThreads) k_ob_controller(const FsiLbmState st, const FsiLbmParams p,
+                                                              int step_clear, int run, int compose) {
+  FsiLbmDiag* d = st.diag;
+  if (compose) {
+    __shared__ float sd[kObThreads], sb[kObThreads];
+    const int n = st.ny * st.nz;
+    const int per = (n + kObThreads - 1) / kObThreads;
+    const int t = threadIdx.x;
+    float* slots = ob_filter_slot(st, 0, 0);
+    float cd = 0.f, cb = 0.f;
+    for (int i = t * per; i < min(n, (t + 1) * per); ++i) {
+      ob_filter_then(cd, cb, slots[2 * i], slots[2 * i + 1]);
+      slots[2 * i] = 0.f;
+      slots[2 * i + 1] = 0.f;
+    }
+    sd[t] = cd;
+    sb[t] = cb;
+    __syncthreads();
+    for (int w = 1; w < kObThreads; w *= 2) {  // ordered tree: left part first
+      if ((t % (2 * w)) == 0) {
+        float ld = sd[t], lb = sb[t];
+        ob_filter_then(ld, lb, sd[t + w], sb[t + w]);
+        sd[t] = ld;
+        sb[t] = lb;
+      }
+      __syncthreads();
+    }
+    if (t == 0 && sd[0] != 0.f) d->obf_err_filtered_run = (1.0f - sd[0]) * d->obf_err_filtered_run + sb[0];
+  }
+  if (threadIdx.x != 0) return;
+  if (step_clear) {
+    d->obr_count_step = 0;
+    d->obr_corr_step = 0.f;
+    d->obr_delta_step = 0.f;
+    d->obf_delta_step = 0.f;
+    d->obf_gain_step = 0.f;
+    d->pc_update_step = d->pc_sat_step = 0;
+    d->mn_update_step = d->mn_sat_step = 0;
+  }
+  if (!run) return;
+  d->pc_guard_step = 0;
+  d->pc_guard_ref = 0.f;
+  const float target = p.ob_target_scale * d->pc_acc[0];
+  const float measured = d->pc_acc[1];
+  float area = d->pc_acc[2];
+  if (area <= 0.f) area = 1.f;
+  d->pc_target = target;
+  d->pc_measured = measured;
+  d->pc_area = area;
+  d->pc_true_outlet = d->pc_acc[3];
+  d->pc_near[0] = d->pc_acc[4];
+  d->pc_near[1] = d->pc_acc[5];
+  d->pc_near[2] = d->pc_acc[6];
+  const float filtered = (1.0f - p.ob_filter_alpha) * d->pc_err_filtered + p.ob_filter_alpha * (target - measured);
+  d->pc_err_filtered = filtered;
+  d->obf_err_filtered_run = filtered;
+  const float requested = p.ob_gain_u * filtered / area;
+  const float bounded = ob_bounded(requested, p.ob_cap_u);
+  const float previous = d->pc_u_fb;
+  float limited = bounded;
+  if (p.ob_delta_cap_u > 0.f) limited = previous + ob_bounded(bounded - previous, p.ob_delta_cap_u);
+  float next = previous + p.ob_slew_alpha * (limited - previous);
+  if (p.ob_guard) {  // outlet flux drop guard
+    const float reference = fmaxf(fabsf(target), fabsf(measured));
+    d->pc_guard_ref = reference;
+    if (reference > 1.0e-12f && fabsf(d->pc_true_outlet) < p.ob_guard_min_ratio * reference && next < previous) {
+      next = previous;
+      d->pc_guard_step = 1;
+      d->pc_guard_run += 1;
+    }
+  }
+  d->pc_u_fb = next;
+  d->pc_rho_fb = ob_bounded(p.ob_gain_rho * filtered / area, 0.01f);
+  if (p.ob_mass_neutral) {  // global_mass_error_density_offset
+    const float mass = d->pc_acc[7];
+    d->mn_mass = mass;
+    if (d->mn_initialized == 0) {
+      d->mn_reference = fabsf(mass) <= 1.0e-12f ? 1.0f : mass;
+      d->mn_initialized = 1;
+    }
+    float reference = d->mn_reference;
+    if (fabsf(reference) <= 1.0e-12f) {
+      reference = 1.0f;
+      d->mn_reference = reference;
+    }
+    const float err = (mass - reference) / reference;
+    const float raw = -p.ob_mn_gain * err;
+    const float bm = ob_bounded(raw, p.ob_mn_cap);
+    d->mn_error = err;
+    d->mn_rho_fb = p.ob_mn_blend * bm;
+    d->mn_update_step = 1;
+    d->mn_update_run += 1;
+    if (fabsf(raw - bm) > 1.0e-12f) {
+      d->mn_sat_step = 1;
+      d->mn_sat_run += 1;
+    }
+  }
+  d->obf_gain_step = p.ob_gain_u;
+  d->pc_update_step = 1;
+  d->pc_update_run += 1;
+  if (fabsf(requested - bounded) > 1.0e-12f) {
+    d->pc_sat_step = 1;
+    d->pc_sat_run += 1;
+  }
+#pragma unroll
+  for (int a = 0; a < 8; ++a) d->pc_acc[a] = 0.f;
+}
+
+// plane sums of the controller from given macroscopic fields (lattice order,
+// vel as three planes of pitch entries), for a controller update on its own
+__global__ void __launch_bounds__(256) k_plane_flux_sums(const Case c, const float* __restrict__ rho,
+                                                         const float* __restrict__ vel) {
+  const int nx = c.s.nx;
+  const int64_t n = (int64_t)nx * c.s.ny * c.s.nz;
+  float t[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const bool fluid = !(c.s.flags[i] & kSolid);
+    plane_flux_add(c, (int)(i % nx), fluid, rho[i], vel[i], t);
+  }
+#pragma unroll
+  for (int a = 0; a < 8; ++a) {
+    const float v = warp_sum(t[a]);
+    if ((threadIdx.x & 31) == 0 && v != 0.f) atomicAdd(&c.s.diag->pc_acc[a], v);
+  }
+}
+
+extern "C" int fsi_ob_controller_update(const FsiLbmState* s, const FsiLbmParams* p, const float* rho,
+                                        const float* vel, void* stream) {
+  int rc = check_state(s, p);
+  if (rc) return rc;
+  if (!rho || !vel) return invalid("null rho or vel");
+  cudaStream_t st = (cudaStream_t)stream;
+  const Case c = make_case(s, p, nullptr);
+  if ((rc = cuda_check(cudaMemsetAsync(s->diag->pc_acc, 0, sizeof(s->diag->pc_acc), st), "memset pc_acc")))
+    return rc;
+  const int64_t n = (int64_t)s->nx * s->ny * s->nz;
+  const int blocks = (int)std::min<int64_t>(blocks_for(n, 256), 4LL * lbm_sm_count());
+  k_plane_flux_sums<<<blocks, 256, 0, st>>>(c, rho, vel);
+  if ((rc = launch_check("k_plane_flux_sums"))) return rc;
+  k_ob_controller<<<1, 32, 0, st>>>(*s, *p, 0, 1, 0);
+  return launch_check("k_ob_controller");
+}
+
 extern "C" int fsi_lbm_substep(const FsiLbmState* s, const FsiLbmParams* p, const FsiStepCtl* ctl, void* stream) {
   int rc = check_state(s, p);
   if (rc) return rc;
@@ -1716,7 +2092,7 @@ extern "C" int fsi_lbm_substep(const FsiLbmState* s, const FsiLbmParams* p, cons
     c.pf_dist = lbm_sm_count() * (p->tune == FSI_TUNE_LBM_OCC4_PF ? 4 : 3);
   const bool odd = ctl->parity != 0, h = s->store_fp16 != 0;
   const bool moving = ctl->mode & FSI_MODE_MOVING_BB, pen = ctl->mode & FSI_MODE_PENALTY;
-  const bool bcw = p->bc_left != 0 || p->bc_right != 0;
+  const bool bcw = p->bc_left != 0 || p->bc_right != 0 || p->ob_semantics >= FSI_OB_REG_PLANE_FLUX;
   if (moving && pen) return invalid("penalty steps use static bounce-back (fluid.py:2099-2103)");
   const dim3 grid2((unsigned)((s->nx + 63) / 64), (unsigned)((s->ny * s->nz + 3) / 4));
   const dim3 block2(32, 4);
@@ -1758,7 +2134,14 @@ extern "C" int fsi_lbm_substep(const FsiLbmState* s, const FsiLbmParams* p, cons
 #undef FSI_LAUNCH
 #undef FSI_KLAUNCH
   if ((rc = cuda_check(lerr, "k_lbm_step (launch)"))) return rc;
-  return launch_check("k_lbm_step");
+  if ((rc = launch_check("k_lbm_step"))) return rc;
+  if (p->ob_semantics >= FSI_OB_REG_MASS_BALANCED) {
+    const int compose = p->ob_semantics == FSI_OB_REG_FLUX_MATCHED || p->ob_semantics == FSI_OB_CONV_FLUX_MATCHED;
+    k_ob_controller<<<1, compose ? kObThreads : 32, 0, st>>>(*s, *p, 1, p->ob_semantics >= FSI_OB_REG_PLANE_FLUX,
+                                                            compose);
+    return launch_check("k_ob_controller");
+  }
+  return FSI_OK;
 }
 
 extern "C" int fsi_lbm_flush_bc(const FsiLbmState* s, const FsiLbmParams* p, const FsiStepCtl* ctl, void* stream) {
@@ -1777,7 +2160,12 @@ extern "C" int fsi_lbm_flush_bc(const FsiLbmState* s, const FsiLbmParams* p, con
     k_flush_bc<true><<<blocks_for(n, 128), 128, 0, st>>>(c);
   else
     k_flush_bc<false><<<blocks_for(n, 128), 128, 0, st>>>(c);
-  return launch_check("k_flush_bc");
+  if ((rc = launch_check("k_flush_bc"))) return rc;
+  if (p->ob_semantics == FSI_OB_REG_FLUX_MATCHED || p->ob_semantics == FSI_OB_CONV_FLUX_MATCHED) {
+    k_ob_controller<<<1, kObThreads, 0, st>>>(*s, *p, 0, 0, 1);
+    return launch_check("k_ob_controller");
+  }
+  return FSI_OK;
 }
 
 extern "C" int fsi_mask_rebuild(const FsiLbmState* s, const FsiLbmParams* p, const FsiStepCtl* ctl, float threshold,

@@ -83,7 +83,7 @@ class LBMFluid3D:
         self.t_phi, self.t_smass, self.t_svel = z32(P), z32(P), z32(3, P)
         self.t_cf, self.t_hydro, self.t_accum = z32(3, P), z32(3, P), z32(3, P)
         self.t_hpp = z32(2, 3, P)
-        self.t_plane = z32(4, 4, self.ny * self.nz)
+        self.t_plane = z32(5, 4, self.ny * self.nz)
         self.t_change = torch.zeros(P, dtype=torch.int32, device=dev)
         self.t_diag = torch.zeros((ctypes.sizeof(FsiLbmDiag) + 255) // 256 * 256, dtype=torch.uint8, device=dev)
         self.t_out_pop = None
@@ -136,6 +136,19 @@ class LBMFluid3D:
         p.ob_rho_min, p.ob_rho_max = cfg.open_boundary_rho_min, cfg.open_boundary_rho_max
         p.ob_u_max, p.ob_noneq_cap = cfg.open_boundary_u_max, cfg.open_boundary_noneq_cap
         p.ob_floor = float(cfg.open_boundary_population_floor) if cfg.open_boundary_population_floor is not None else -1e30
+        p.ob_gain_u, p.ob_gain_rho = cfg.open_boundary_flux_feedback_gain_u, cfg.open_boundary_flux_feedback_gain_rho
+        p.ob_filter_alpha, p.ob_cap_u = cfg.open_boundary_flux_filter_alpha, cfg.open_boundary_flux_correction_cap_u
+        p.ob_delta_cap_u = cfg.open_boundary_flux_feedback_delta_cap_u
+        p.ob_slew_alpha = cfg.open_boundary_flux_feedback_slew_alpha
+        p.ob_blend = cfg.open_boundary_convective_blend_weight
+        p.ob_target_scale = cfg.open_boundary_flux_control_target_scale
+        p.ob_guard_min_ratio = cfg.open_boundary_outlet_flux_drop_guard_min_ratio
+        p.ob_mn_gain = cfg.open_boundary_mass_neutral_mass_error_gain
+        p.ob_mn_cap = cfg.open_boundary_mass_neutral_mass_error_cap
+        p.ob_mn_blend = cfg.open_boundary_mass_neutral_correction_blend
+        p.ob_measure_offset = int(cfg.open_boundary_flux_control_measure_plane_offset)
+        p.ob_guard = int(bool(cfg.open_boundary_outlet_flux_drop_guard_enabled))
+        p.ob_mass_neutral = int(self._mass_neutral_active())
         if self._penalty is not None:
             p.penalty_beta, p.penalty_phi_min, p.penalty_cap = self._penalty
         p.tune = int(self.tune)
@@ -496,10 +509,16 @@ class LBMFluid3D:
                 "mb_subcycle_force_accum_norm_max": float(d.accum_norm_max),
                 "mb_subcycle_force_mean_norm_max": float(d.mean_norm_max)}
 
+    def _mass_neutral_active(self) -> bool:
+        cfg = self.config
+        return bool(cfg.open_boundary_mass_neutral_flux_control_enabled
+                    and cfg.open_boundary_mass_neutral_flux_control_mode == "global_mass_error_density_offset")
+
     def get_open_boundary_limiter_stats(self):
-        """fluid.py:804-924 (counter part).  Applies a pending open-boundary step first."""
+        """fluid.py:804-924 with the same keys.  Applies a pending open-boundary step first."""
         self.flush_open_boundary()
         d = self._diag()
+        cfg = self.config
         st, run = list(d.ob_step), list(d.ob_run)
         names = ["rho_clip_count", "velocity_clip_count", "noneq_clip_count", "population_floor_count",
                  "reconstructed_population_count"]
@@ -511,7 +530,137 @@ class LBMFluid3D:
         out["limiter_activation_count"] = sum(run[:4])
         out["limiter_activation_denominator"] = int(run[4])
         out["limiter_activation_fraction"] = float(sum(run[:4]) / run[4]) if run[4] else 0.0
+        updates, saturations = int(d.pc_update_run), int(d.pc_sat_run)
+        mn_updates, mn_saturations = int(d.mn_update_run), int(d.mn_sat_run)
+        u_fb, rho_fb, mn_fb = float(d.pc_u_fb), float(d.pc_rho_fb), float(d.mn_rho_fb)
+        cap = abs(float(cfg.open_boundary_flux_correction_cap_u))
+        out.update({
+            "mass_balance_correction_count_step": int(d.obr_count_step),
+            "mass_balance_correction_count_run": int(d.obr_count_run),
+            "mass_balance_correction_abs_sum_step": float(d.obr_corr_step),
+            "mass_balance_correction_abs_sum_run": float(d.obr_corr_run),
+            "unknown_population_delta_abs_sum_step": float(d.obr_delta_step),
+            "unknown_population_delta_abs_sum_run": float(d.obr_delta_run),
+            "flow_correction_delta_abs_sum_step": float(d.obf_delta_step),
+            "flow_correction_delta_abs_sum_run": float(d.obf_delta_run),
+            "flow_outlet_flux_error_filtered_run": float(d.obf_err_filtered_run),
+            "flow_correction_gain_effective_step": float(d.obf_gain_step),
+            "flow_feedback_gain_u": float(cfg.open_boundary_flux_feedback_gain_u),
+            "flow_feedback_gain_rho": float(cfg.open_boundary_flux_feedback_gain_rho),
+            "flow_filter_alpha": float(cfg.open_boundary_flux_filter_alpha),
+            "flow_correction_cap_u": float(cfg.open_boundary_flux_correction_cap_u),
+            "flow_feedback_delta_cap_u": float(cfg.open_boundary_flux_feedback_delta_cap_u),
+            "flow_feedback_slew_alpha": float(cfg.open_boundary_flux_feedback_slew_alpha),
+            "flow_convective_blend_weight": float(cfg.open_boundary_convective_blend_weight),
+            "flow_control_measure_plane_offset": int(cfg.open_boundary_flux_control_measure_plane_offset),
+            "flow_control_target_scale": float(cfg.open_boundary_flux_control_target_scale),
+            "flow_outlet_flux_drop_guard_enabled": bool(cfg.open_boundary_outlet_flux_drop_guard_enabled),
+            "flow_outlet_flux_drop_guard_min_ratio": float(cfg.open_boundary_outlet_flux_drop_guard_min_ratio),
+            "mass_neutral_flux_control_enabled": bool(cfg.open_boundary_mass_neutral_flux_control_enabled),
+            "mass_neutral_flux_control_mode": cfg.open_boundary_mass_neutral_flux_control_mode,
+            "mass_neutral_mass_error_gain": float(cfg.open_boundary_mass_neutral_mass_error_gain),
+            "mass_neutral_mass_error_cap": float(cfg.open_boundary_mass_neutral_mass_error_cap),
+            "mass_neutral_correction_blend": float(cfg.open_boundary_mass_neutral_correction_blend),
+            "mass_neutral_reference_mass_mode": cfg.open_boundary_mass_neutral_reference_mass_mode,
+            "mass_neutral_projection_report_only": bool(
+                cfg.open_boundary_mass_neutral_flux_control_mode == "outlet_population_projection_report_only"),
+            "mass_neutral_runtime_behavior_active": self._mass_neutral_active(),
+            "mass_neutral_mass_current": float(d.mn_mass),
+            "mass_neutral_mass_initial_reference": float(d.mn_reference),
+            "mass_neutral_mass_error": float(d.mn_error),
+            "mass_neutral_rho_feedback": mn_fb,
+            "mass_neutral_rho_feedback_abs": abs(mn_fb),
+            "mass_neutral_feedback_saturation_count_step": int(d.mn_sat_step),
+            "mass_neutral_feedback_saturation_count_run": mn_saturations,
+            "mass_neutral_feedback_update_count_step": int(d.mn_update_step),
+            "mass_neutral_feedback_update_count_run": mn_updates,
+            "mass_neutral_feedback_saturation_fraction_run": float(mn_saturations / mn_updates if mn_updates else 0.0),
+            "near_outlet_flux_xminus1": float(d.pc_near[0]),
+            "near_outlet_flux_xminus2": float(d.pc_near[1]),
+            "near_outlet_flux_xminus3": float(d.pc_near[2]),
+            "controller_true_outlet_flux_for_guard": float(d.pc_true_outlet),
+            "controller_target_outlet_flux": float(d.pc_target),
+            "controller_measured_outlet_flux": float(d.pc_measured),
+            "controller_raw_flux_error": float(d.pc_target) - float(d.pc_measured),
+            "controller_filtered_flux_error": float(d.pc_err_filtered),
+            "controller_outlet_fluid_area": float(d.pc_area),
+            "controller_u_feedback": u_fb,
+            "controller_u_feedback_abs": abs(u_fb),
+            "controller_density_feedback": rho_fb,
+            "controller_density_feedback_abs": abs(rho_fb),
+            "controller_delta_cap_u": float(cfg.open_boundary_flux_feedback_delta_cap_u),
+            "controller_slew_alpha": float(cfg.open_boundary_flux_feedback_slew_alpha),
+            "controller_authority_ratio": float(abs(u_fb) / cap if cap else 0.0),
+            "controller_saturation_count_step": int(d.pc_sat_step),
+            "controller_saturation_count_run": saturations,
+            "controller_update_count_step": int(d.pc_update_step),
+            "controller_update_count_run": updates,
+            "controller_saturation_fraction_run": float(saturations / updates if updates else 0.0),
+            "controller_measure_plane_offset": int(cfg.open_boundary_flux_control_measure_plane_offset),
+            "controller_target_scale": float(cfg.open_boundary_flux_control_target_scale),
+            "controller_drop_guard_active_step": int(d.pc_guard_step),
+            "controller_drop_guard_activation_count_run": int(d.pc_guard_run),
+            "controller_drop_guard_reference_flux": float(d.pc_guard_ref),
+            "controller_drop_guard_min_ratio": float(cfg.open_boundary_outlet_flux_drop_guard_min_ratio),
+            "controller_drop_guard_activation_fraction_run": float(int(d.pc_guard_run) / updates if updates else 0.0),
+        })
         return out
+
+    # open-boundary counter and controller state of FsiLbmDiag (fluid.py:571-736)
+    _OB_REPAIR_FIELDS = ("obr_count_step", "obr_corr_step", "obr_delta_step", "obf_delta_step", "obf_gain_step",
+                         "obr_count_run", "obr_corr_run", "obr_delta_run", "obf_delta_run", "obf_err_filtered_run")
+    _OB_CONTROLLER_FIELDS = ("pc_acc", "pc_target", "pc_measured", "pc_area", "pc_true_outlet", "pc_near",
+                             "pc_err_filtered", "pc_u_fb", "pc_rho_fb", "pc_guard_ref", "pc_guard_step",
+                             "pc_guard_run", "pc_update_step", "pc_update_run", "pc_sat_step", "pc_sat_run",
+                             "mn_mass", "mn_reference", "mn_error", "mn_rho_fb", "mn_initialized", "mn_update_step",
+                             "mn_update_run", "mn_sat_step", "mn_sat_run")
+
+    def _diag_set(self, values: dict):
+        """Write FsiLbmDiag fields (stream-ordered with the kernels)."""
+        d = FsiLbmDiag()
+        for name, value in values.items():
+            setattr(d, name, value)
+        raw = bytes(d)
+        for name in values:
+            f = getattr(FsiLbmDiag, name)
+            src = torch.frombuffer(bytearray(raw[f.offset: f.offset + f.size]), dtype=torch.uint8)
+            self.t_diag[f.offset: f.offset + f.size].copy_(src)
+
+    def _diag_zero(self, names):
+        for name in names:
+            f = getattr(FsiLbmDiag, name)
+            self.t_diag[f.offset: f.offset + f.size].zero_()
+
+    def clear_open_boundary_limiter_run_counters(self):
+        """fluid.py:589-636: every limiter, repair and controller counter and state to zero."""
+        self.flush_open_boundary()
+        self._diag_zero(("ob_step", "ob_run") + self._OB_REPAIR_FIELDS + self._OB_CONTROLLER_FIELDS)
+
+    def set_open_boundary_limiter_run_counters(self, rho_clip_count, velocity_clip_count, noneq_clip_count,
+                                               population_floor_count, reconstructed_population_count):
+        """fluid.py:638-691 (restart of the limiter counters)."""
+        self.flush_open_boundary()
+        self._diag_zero(self._OB_REPAIR_FIELDS + self._OB_CONTROLLER_FIELDS)
+        counts = [int(rho_clip_count), int(velocity_clip_count), int(noneq_clip_count), int(population_floor_count),
+                  int(reconstructed_population_count)]
+        self._diag_set({"ob_step": (ctypes.c_int32 * 5)(), "ob_run": (ctypes.c_int32 * 5)(*counts)})
+
+    def set_open_boundary_repair_run_counters(self, mass_balance_correction_count, mass_balance_correction_abs_sum,
+                                              unknown_population_delta_abs_sum):
+        """fluid.py:693-736 (restart of the repair counters)."""
+        self.flush_open_boundary()
+        self._diag_zero(self._OB_REPAIR_FIELDS + self._OB_CONTROLLER_FIELDS)
+        self._diag_set({"obr_count_run": int(mass_balance_correction_count),
+                        "obr_corr_run": float(mass_balance_correction_abs_sum),
+                        "obr_delta_run": float(unknown_population_delta_abs_sum)})
+
+    def update_open_boundary_plane_flux_controller(self):
+        """fluid.py:1141-1263 called on its own, from the current rho, v and
+        solid fields (the step runs it by itself under semantics 8 and 9)."""
+        self.flush_open_boundary()
+        _, rho, vel = self._readout()
+        call("fsi_ob_controller_update", ctypes.byref(self.state), ctypes.byref(self.params), ptr(rho), ptr(vel),
+             self._stream())
 
     def get_lightweight_stability_stats(self):
         """fluid.py:738-802 on the device."""

@@ -35,10 +35,10 @@ RESTART_METADATA_KEY = "metadata_json"
 
 EXT_PREFIX = "ext_"
 EXT_STATE_KEY = "ext_state_json"
-EXT_VERSION = 1
+EXT_VERSION = 2
 # device tensors of LBMFluid3D / MPMSolid3D that a resume restores
 _LBM_TENSORS = ("t_pop", "t_flags", "t_nbr", "t_rho", "t_vel", "t_static", "t_old", "t_reinit", "t_phi", "t_smass",
-                "t_svel", "t_cf", "t_hydro", "t_accum", "t_hpp", "t_plane", "t_vin")
+                "t_svel", "t_cf", "t_hydro", "t_accum", "t_hpp", "t_plane", "t_vin", "t_diag")
 _LBM_ATTRS = ("parity", "bc_pending", "pp", "last_pp", "steps", "_accumulating", "_fused_accumulation",
               "_sample_count", "_hydro_src", "_old_equals_solid", "_penalty")
 _MPM_TENSORS = ("t_x", "t_v", "t_C", "t_F", "t_Jp", "t_mass", "t_vol0", "t_fixed", "t_fixed_x")

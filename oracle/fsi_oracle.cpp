@@ -71,6 +71,12 @@ enum {
   ORC_OB_REGULARIZED = 1,
   ORC_OB_REGULARIZED_LIMITED = 2,
   ORC_OB_CONVECTIVE = 3,
+  ORC_OB_REG_MASS_BALANCED = 4,
+  ORC_OB_CONV_MASS_BALANCED = 5,
+  ORC_OB_REG_FLUX_MATCHED = 6,
+  ORC_OB_CONV_FLUX_MATCHED = 7,
+  ORC_OB_REG_PLANE_FLUX = 8,
+  ORC_OB_CONV_PLANE_FLUX = 9,
 };
 
 // LBM parameters.  Mirrors LBMFluid3D.__init__/init_simulation
@@ -88,6 +94,14 @@ struct OrcLbmParams {
   int32_t limiter_enabled;
   int32_t floor_enabled;
   double ob_rho_min, ob_rho_max, ob_u_max, ob_noneq_cap, ob_floor;
+  // outlet repair and flux controller (LBMConfig.open_boundary_*, lbm/config.py:53-69)
+  double flux_gain_u, flux_gain_rho, flux_filter_alpha, flux_cap_u, flux_delta_cap_u, flux_slew_alpha;
+  double convective_blend, flux_target_scale, drop_guard_min_ratio;
+  double mn_gain, mn_cap, mn_blend;
+  int32_t measure_plane_offset;
+  int32_t drop_guard_enabled;
+  int32_t mass_neutral;  // enabled with mode global_mass_error_density_offset
+  int32_t pad_ob;
 };
 
 // Scalar LBM diagnostics (fluid.py:98-146, 212-223).
@@ -109,6 +123,16 @@ struct OrcLbmDiag {
   double mb_mean_norm_max;
   // open-boundary limiter counters: [0]=step, [1]=run
   int32_t ob_rho_clip[2], ob_velocity_clip[2], ob_noneq_clip[2], ob_floor_count[2], ob_reconstructed[2];
+  // outlet repair (fluid.py:98-118), [0] = step, [1] = run
+  int32_t mb_corr_count[2];
+  double mb_corr_abs_sum[2], pop_delta_abs_sum[2], flow_delta_abs_sum[2];
+  double flow_err_filtered_run, flow_gain_effective_step;
+  // plane-flux controller (fluid.py:119-146)
+  double target_flux, measured_flux, fluid_area, true_outlet_flux, near_flux[3];
+  double flux_err_filtered, u_feedback, rho_feedback, guard_reference;
+  int32_t guard_active_step, guard_count_run, ctl_update[2], ctl_saturation[2];
+  double mn_mass_current, mn_reference, mn_error, mn_rho_feedback;
+  int32_t mn_initialized, mn_update[2], mn_saturation[2], pad_mn;
 };
 
 struct OrcMpmParams {
@@ -504,16 +528,233 @@ inline R convective_outlet_population(const OrcLbmParams& p, int s, int64_t n1, 
   return ex;
 }
 
-// Boundary_condition dispatch (fluid.py:538-569) for the four semantics the
-// driver exposes (fsi_config.py:32-37): legacy 926-1024, regularized
-// 1348-1394, regularized-limited 1396-1442, convective 1444-1493.
+// fluid.py:1105-1112
+template <typename R>
+inline R bounded_scalar(R value, R limit) {
+  R out = value;
+  if (out > limit) out = limit;
+  if (out < -limit) out = -limit;
+  return out;
+}
+
+// _limit_open_boundary_population (fluid.py:1043-1049)
+template <typename R>
+inline R limit_population(const OrcLbmParams& p, R value) {
+  if (p.limiter_enabled && p.floor_enabled && value < (R)p.ob_floor) return (R)p.ob_floor;
+  return value;
+}
+
+// The repair and flow-correction fields one Boundary_condition call updates,
+// held in R (the reference's ti.f32 fields take each record in order).
+template <typename R>
+struct RepairRec {
+  int count[2];
+  R corr[2], delta[2], flow_delta[2], filtered, gain_step;
+};
+
+// fluid.py:1114-1120
+template <typename R>
+inline void record_repair(RepairRec<R>& r, R corr, R delta) {
+  for (int a = 0; a < 2; ++a) {
+    r.count[a] += 1;
+    r.corr[a] += corr;
+    r.delta[a] += delta;
+  }
+}
+
+// fluid.py:1122-1131
+template <typename R>
+inline void record_flow(const OrcLbmParams& p, RepairRec<R>& r, R corr, R err) {
+  r.flow_delta[0] += corr;
+  r.flow_delta[1] += corr;
+  r.filtered = ((R)1 - (R)p.flux_filter_alpha) * r.filtered + (R)p.flux_filter_alpha * err;
+  r.gain_step = (R)p.flux_gain_u;
+}
+
+// fluid.py:1133-1138
+template <typename R>
+inline void record_plane(const OrcLbmParams& p, RepairRec<R>& r, R corr, R delta) {
+  record_repair(r, corr, delta);
+  r.flow_delta[0] += corr;
+  r.flow_delta[1] += corr;
+  r.gain_step = (R)p.flux_gain_u;
+}
+
+// The regularized outlet population of semantics 4, 6, 8 (fluid.py:1265-1274,
+// 1286-1304, 1318-1335): target density rho_bcxr and velocity v[ni] repaired
+// by the semantics' feedback, the neighbour's non-equilibrium part kept.
+template <typename R>
+R repaired_regularized(const OrcLbmParams& p, int kind, RepairRec<R>& r, int s, const R* F, const R* rho,
+                       const R* v, int64_t n, const OrcLbmDiag* d) {
+  const R target_rho = (R)p.rho_bc[1];
+  const R tu[3] = {v[n * 3], v[n * 3 + 1], v[n * 3 + 2]};
+  const R vx_in = (R)p.vel_bc[0][0];
+  R rho_fb, vel_fb, extra = 0;
+  if (kind == ORC_OB_REG_MASS_BALANCED) {
+    rho_fb = bounded_scalar<R>((R)0.02 * ((R)p.rho0 - rho[n]), (R)0.01);
+    vel_fb = bounded_scalar<R>((R)0.05 * (vx_in - tu[0]), (R)0.02);
+  } else if (kind == ORC_OB_REG_FLUX_MATCHED) {
+    rho_fb = bounded_scalar<R>((R)p.flux_gain_rho * ((R)p.rho0 - rho[n]), (R)0.01);
+    vel_fb = bounded_scalar<R>((R)p.flux_gain_u * (vx_in - tu[0]), (R)p.flux_cap_u);
+  } else {
+    rho_fb = (R)d->rho_feedback;
+    if (p.ob_semantics == ORC_OB_REG_PLANE_FLUX && p.mass_neutral) extra = (R)d->mn_rho_feedback;
+    vel_fb = (R)d->u_feedback;
+  }
+  const R ru[3] = {tu[0] + vel_fb, tu[1], tu[2]};
+  const R before = regularized_population<R>(p, s, target_rho, tu, F, rho, v, n);
+  const R after = regularized_population<R>(p, s, target_rho + rho_fb + extra, ru, F, rho, v, n);
+  if (kind == ORC_OB_REG_MASS_BALANCED) {
+    record_repair<R>(r, std::fabs(rho_fb) + std::fabs(vel_fb), std::fabs(after - before));
+  } else if (kind == ORC_OB_REG_FLUX_MATCHED) {
+    record_repair<R>(r, std::fabs(rho_fb) + std::fabs(vel_fb), std::fabs(after - before));
+    record_flow<R>(p, r, std::fabs(vel_fb), vx_in - tu[0]);
+  } else {
+    record_plane<R>(p, r, std::fabs(rho_fb) + std::fabs(extra) + std::fabs(vel_fb), std::fabs(after - before));
+  }
+  return limit_population<R>(p, after);
+}
+
+// One unknown population of a pressure-outlet face cell under semantics 4-9
+// (fluid.py:1265-1346); the convective variants blend the extrapolation of
+// fluid.py:1098-1103 toward the regularized repair.
+template <typename R>
+R repaired_outlet_population(const OrcLbmParams& p, RepairRec<R>& r, int s, int64_t n, int64_t n2, const R* F,
+                             const R* rho, const R* v, const int8_t* solid, const OrcLbmDiag* d) {
+  const int sem = p.ob_semantics;
+  const int kind = sem == ORC_OB_CONV_MASS_BALANCED ? ORC_OB_REG_MASS_BALANCED
+                   : sem == ORC_OB_CONV_FLUX_MATCHED ? ORC_OB_REG_FLUX_MATCHED
+                   : sem == ORC_OB_CONV_PLANE_FLUX  ? ORC_OB_REG_PLANE_FLUX
+                                                    : sem;
+  if (kind == sem) return repaired_regularized<R>(p, kind, r, s, F, rho, v, n, d);
+  const R convective = convective_outlet_population<R>(p, s, n, n2, F, solid);
+  const R regularized = repaired_regularized<R>(p, kind, r, s, F, rho, v, n, d);
+  const R blend = sem == ORC_OB_CONV_MASS_BALANCED ? (R)0.15 : (R)p.convective_blend;
+  const R repaired = convective + blend * (regularized - convective);
+  const R dd = std::fabs(repaired - convective);
+  if (sem == ORC_OB_CONV_MASS_BALANCED) {
+    record_repair<R>(r, (R)0, dd);
+  } else if (sem == ORC_OB_CONV_FLUX_MATCHED) {
+    record_repair<R>(r, (R)0, dd);
+    record_flow<R>(p, r, dd, (R)p.vel_bc[0][0] - v[n * 3]);
+  } else {
+    record_plane<R>(p, r, dd, dd);
+  }
+  return limit_population<R>(p, repaired);
+}
+
+// update_open_boundary_plane_flux_controller (fluid.py:1141-1263), in the
+// reference's loop order with R accumulators.
+template <typename R>
+void plane_flux_controller(const OrcLbmParams& p, const R* rho, const R* v, const int8_t* solid, OrcLbmDiag* d) {
+  Grid<R> g{p.nx, p.ny, p.nz};
+  const int nx = p.nx, ny = p.ny, nz = p.nz;
+  R target = 0, measured = 0, area = 0, near1 = 0, near2 = 0, near3 = 0, true_out = 0;
+  d->guard_active_step = 0;
+  d->guard_reference = 0;
+  const int mi = std::max(0, nx - 1 - p.measure_plane_offset);
+  const int i1 = std::max(0, nx - 2), i2 = std::max(0, nx - 3), i3 = std::max(0, nx - 4);
+  auto flux = [&](int i, int j, int k) {
+    const int64_t c = g.id(i, j, k);
+    return rho[c] * v[c * 3];
+  };
+  for (int j = 0; j < ny; ++j)
+    for (int k = 0; k < nz; ++k) {
+      if (solid[g.id(0, j, k)] == 0) target += flux(0, j, k);
+      if (solid[g.id(mi, j, k)] == 0) {
+        measured += flux(mi, j, k);
+        area += (R)1;
+      }
+      if (solid[g.id(nx - 1, j, k)] == 0) true_out += flux(nx - 1, j, k);
+      if (solid[g.id(i1, j, k)] == 0) near1 += flux(i1, j, k);
+      if (solid[g.id(i2, j, k)] == 0) near2 += flux(i2, j, k);
+      if (solid[g.id(i3, j, k)] == 0) near3 += flux(i3, j, k);
+    }
+  target = (R)p.flux_target_scale * target;
+  if (area <= (R)0) area = (R)1;
+  d->target_flux = (double)target;
+  d->measured_flux = (double)measured;
+  d->fluid_area = (double)area;
+  d->true_outlet_flux = (double)true_out;
+  d->near_flux[0] = (double)near1;
+  d->near_flux[1] = (double)near2;
+  d->near_flux[2] = (double)near3;
+  const R raw = target - measured;
+  const R filtered = ((R)1 - (R)p.flux_filter_alpha) * (R)d->flux_err_filtered + (R)p.flux_filter_alpha * raw;
+  d->flux_err_filtered = (double)filtered;
+  d->flow_err_filtered_run = (double)filtered;
+  const R requested = (R)p.flux_gain_u * filtered / area;
+  const R bounded = bounded_scalar<R>(requested, (R)p.flux_cap_u);
+  const R previous = (R)d->u_feedback;
+  R limited = bounded;
+  if ((R)p.flux_delta_cap_u > (R)0) limited = previous + bounded_scalar<R>(bounded - previous, (R)p.flux_delta_cap_u);
+  R next = previous + (R)p.flux_slew_alpha * (limited - previous);
+  if (p.drop_guard_enabled) {
+    const R reference = std::max(std::fabs(target), std::fabs(measured));
+    d->guard_reference = (double)reference;
+    const R outlet = std::fabs(true_out);
+    if (reference > (R)1.0e-12 && outlet < (R)p.drop_guard_min_ratio * reference && next < previous) {
+      next = previous;
+      d->guard_active_step = 1;
+      d->guard_count_run += 1;
+    }
+  }
+  d->u_feedback = (double)next;
+  d->rho_feedback = (double)bounded_scalar<R>((R)p.flux_gain_rho * filtered / area, (R)0.01);
+  if (p.mass_neutral) {
+    R mass = 0;
+    for (int64_t c = 0; c < g.n(); ++c)
+      if (solid[c] == 0) mass += rho[c];
+    d->mn_mass_current = (double)mass;
+    if (d->mn_initialized == 0) {
+      R reference = mass;
+      if (std::fabs(reference) <= (R)1.0e-12) reference = (R)1;
+      d->mn_reference = (double)reference;
+      d->mn_initialized = 1;
+    }
+    R reference = (R)d->mn_reference;
+    if (std::fabs(reference) <= (R)1.0e-12) {
+      reference = (R)1;
+      d->mn_reference = 1.0;
+    }
+    const R err = (mass - reference) / reference;
+    const R raw_fb = -(R)p.mn_gain * err;
+    const R bounded_fb = bounded_scalar<R>(raw_fb, (R)p.mn_cap);
+    d->mn_error = (double)err;
+    d->mn_rho_feedback = (double)((R)p.mn_blend * bounded_fb);
+    d->mn_update[0] = 1;
+    d->mn_update[1] += 1;
+    if (std::fabs(raw_fb - bounded_fb) > (R)1.0e-12) {
+      d->mn_saturation[0] = 1;
+      d->mn_saturation[1] += 1;
+    }
+  }
+  d->flow_gain_effective_step = (double)(R)p.flux_gain_u;
+  d->ctl_update[0] = 1;
+  d->ctl_update[1] += 1;
+  if (std::fabs(requested - bounded) > (R)1.0e-12) {
+    d->ctl_saturation[0] = 1;
+    d->ctl_saturation[1] += 1;
+  }
+}
+
+// Boundary_condition dispatch (fluid.py:538-569): legacy 926-1024,
+// regularized 1348-1394, regularized-limited 1396-1442, convective 1444-1493,
+// and the outlet repairs of 1495-1792 (inlets and velocity outlets are the
+// plain regularized ones there).
 template <typename R>
 void lbm_boundary(const OrcLbmParams& p, R* F, const R* rho, const R* v, const int8_t* solid, OrcLbmDiag* d) {
   Grid<R> g{p.nx, p.ny, p.nz};
   // clear_open_boundary_limiter_step_counters (fluid.py:571-587)
   d->ob_rho_clip[0] = d->ob_velocity_clip[0] = d->ob_noneq_clip[0] = d->ob_floor_count[0] = 0;
   d->ob_reconstructed[0] = 0;
+  d->mb_corr_count[0] = 0;
+  d->mb_corr_abs_sum[0] = d->pop_delta_abs_sum[0] = d->flow_delta_abs_sum[0] = 0;
+  d->flow_gain_effective_step = 0;
+  d->ctl_saturation[0] = d->ctl_update[0] = d->mn_saturation[0] = d->mn_update[0] = 0;
+  d->guard_active_step = 0;
   const int nx = p.nx, ny = p.ny, nz = p.nz;
+  if (p.ob_semantics >= ORC_OB_REG_PLANE_FLUX) plane_flux_controller<R>(p, rho, v, solid, d);
   if (p.ob_semantics == ORC_OB_EQUILIBRIUM_RESET) {
     // x faces
     if (p.bc[0] == 1)
@@ -588,6 +829,16 @@ void lbm_boundary(const OrcLbmParams& p, R* F, const R* rho, const R* v, const i
   // x-axis open boundaries reconstructing only the unknown populations
   const bool limited = p.ob_semantics == ORC_OB_REGULARIZED_LIMITED;
   const bool convective = p.ob_semantics == ORC_OB_CONVECTIVE;
+  const bool repaired = p.ob_semantics >= ORC_OB_REG_MASS_BALANCED;
+  RepairRec<R> rec;
+  for (int a = 0; a < 2; ++a) {
+    rec.count[a] = d->mb_corr_count[a];
+    rec.corr[a] = (R)d->mb_corr_abs_sum[a];
+    rec.delta[a] = (R)d->pop_delta_abs_sum[a];
+    rec.flow_delta[a] = (R)d->flow_delta_abs_sum[a];
+  }
+  rec.filtered = (R)d->flow_err_filtered_run;
+  rec.gain_step = (R)d->flow_gain_effective_step;
   for (int side = 0; side < 2; ++side) {
     const int bc = p.bc[side];
     if (bc != 1 && bc != 2) continue;
@@ -604,6 +855,12 @@ void lbm_boundary(const OrcLbmParams& p, R* F, const R* rho, const R* v, const i
           n2i = bi;
         }
         const int64_t n = g.id(ni, j, k);
+        if (repaired && side == 1 && bc == 1) {
+          const int64_t n2 = g.id(n2i, j, k);
+          for (int q = 0; q < 5; ++q)
+            F[c * 19 + unknown[q]] = repaired_outlet_population<R>(p, rec, unknown[q], n, n2, F, rho, v, solid, d);
+          continue;
+        }
         if (convective && side == 1 && bc == 1) {
           const int64_t n2 = g.id(n2i, j, k);
           for (int q = 0; q < 5; ++q) F[c * 19 + unknown[q]] = convective_outlet_population<R>(p, unknown[q], n, n2, F, solid);
@@ -630,6 +887,14 @@ void lbm_boundary(const OrcLbmParams& p, R* F, const R* rho, const R* v, const i
         }
       }
   }
+  for (int a = 0; a < 2; ++a) {
+    d->mb_corr_count[a] = rec.count[a];
+    d->mb_corr_abs_sum[a] = (double)rec.corr[a];
+    d->pop_delta_abs_sum[a] = (double)rec.delta[a];
+    d->flow_delta_abs_sum[a] = (double)rec.flow_delta[a];
+  }
+  d->flow_err_filtered_run = (double)rec.filtered;
+  d->flow_gain_effective_step = (double)rec.gain_step;
 }
 
 // fluid.py:1794-1814
@@ -1269,6 +1534,10 @@ void couple_reaction(int kind, const OrcCouplingParams& cp, const OrcLbmParams& 
                                           const int8_t* solid, OrcLbmDiag* d) {                                   \
     lbm_boundary<R>(*p, F, rho, v, solid, d);                                                                      \
   }                                                                                                                \
+  extern "C" void orc##SUF##_lbm_plane_flux_controller(const OrcLbmParams* p, const R* rho, const R* v,            \
+                                                       const int8_t* solid, OrcLbmDiag* d) {                    \
+    plane_flux_controller<R>(*p, rho, v, solid, d);                                                                \
+  }                                                                                                                \
   extern "C" void orc##SUF##_lbm_macros(const OrcLbmParams* p, R* f, const R* F, R* rho, R* v,                     \
                                         const int8_t* solid, const R* cf, int threads) {                          \
     lbm_macros<R>(*p, f, F, rho, v, solid, cf, threads);                                                           \
@@ -1327,4 +1596,4 @@ extern "C" void orc_polar_rotation(const double* F, double* R) {
   for (int i = 0; i < 9; ++i) R[i] = Q.a[i / 3][i % 3];
 }
 
-extern "C" int orc_abi_version() { return 1; }
+extern "C" int orc_abi_version() { return 2; }

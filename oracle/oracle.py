@@ -39,6 +39,31 @@ OB_CODES = {
     "regularized_velocity_pressure": 1,
     "regularized_velocity_pressure_limited": 2,
     "convective_pressure_outlet_experimental": 3,
+    "regularized_mass_balanced_pressure_outlet": 4,
+    "convective_mass_balanced_pressure_outlet": 5,
+    "regularized_flux_matched_pressure_outlet": 6,
+    "convective_flux_matched_damped_outlet": 7,
+    "regularized_plane_flux_controlled_pressure_outlet": 8,
+    "convective_plane_flux_controlled_damped_outlet": 9,
+}
+# LBMConfig defaults of the outlet repair and flux controller (lbm/config.py:53-69)
+FLUX_CONTROL_DEFAULTS = {
+    "open_boundary_flux_feedback_gain_u": 0.01,
+    "open_boundary_flux_feedback_gain_rho": 0.005,
+    "open_boundary_flux_filter_alpha": 0.05,
+    "open_boundary_flux_correction_cap_u": 0.005,
+    "open_boundary_flux_feedback_delta_cap_u": 0.0,
+    "open_boundary_flux_feedback_slew_alpha": 1.0,
+    "open_boundary_convective_blend_weight": 0.05,
+    "open_boundary_flux_control_measure_plane_offset": 0,
+    "open_boundary_flux_control_target_scale": 1.0,
+    "open_boundary_outlet_flux_drop_guard_enabled": False,
+    "open_boundary_outlet_flux_drop_guard_min_ratio": 0.60,
+    "open_boundary_mass_neutral_flux_control_enabled": False,
+    "open_boundary_mass_neutral_flux_control_mode": "disabled",
+    "open_boundary_mass_neutral_mass_error_gain": 0.0,
+    "open_boundary_mass_neutral_mass_error_cap": 0.0,
+    "open_boundary_mass_neutral_correction_blend": 0.0,
 }
 
 # moment matrix of the reference (src/mpm_lbm/sim/lbm/fluid.py:231-249)
@@ -83,6 +108,12 @@ class LbmParams(ctypes.Structure):
         ("vel_bc", (ctypes.c_double * 3) * 6), ("limiter_enabled", ctypes.c_int32), ("floor_enabled", ctypes.c_int32),
         ("ob_rho_min", ctypes.c_double), ("ob_rho_max", ctypes.c_double), ("ob_u_max", ctypes.c_double),
         ("ob_noneq_cap", ctypes.c_double), ("ob_floor", ctypes.c_double),
+        ("flux_gain_u", ctypes.c_double), ("flux_gain_rho", ctypes.c_double), ("flux_filter_alpha", ctypes.c_double),
+        ("flux_cap_u", ctypes.c_double), ("flux_delta_cap_u", ctypes.c_double), ("flux_slew_alpha", ctypes.c_double),
+        ("convective_blend", ctypes.c_double), ("flux_target_scale", ctypes.c_double),
+        ("drop_guard_min_ratio", ctypes.c_double), ("mn_gain", ctypes.c_double), ("mn_cap", ctypes.c_double),
+        ("mn_blend", ctypes.c_double), ("measure_plane_offset", ctypes.c_int32),
+        ("drop_guard_enabled", ctypes.c_int32), ("mass_neutral", ctypes.c_int32), ("pad_ob", ctypes.c_int32),
     ]
 
 
@@ -97,6 +128,18 @@ class LbmDiag(ctypes.Structure):
         ("mb_mean_norm_max", ctypes.c_double), ("ob_rho_clip", ctypes.c_int32 * 2),
         ("ob_velocity_clip", ctypes.c_int32 * 2), ("ob_noneq_clip", ctypes.c_int32 * 2),
         ("ob_floor_count", ctypes.c_int32 * 2), ("ob_reconstructed", ctypes.c_int32 * 2),
+        ("mb_corr_count", ctypes.c_int32 * 2), ("mb_corr_abs_sum", ctypes.c_double * 2),
+        ("pop_delta_abs_sum", ctypes.c_double * 2), ("flow_delta_abs_sum", ctypes.c_double * 2),
+        ("flow_err_filtered_run", ctypes.c_double), ("flow_gain_effective_step", ctypes.c_double),
+        ("target_flux", ctypes.c_double), ("measured_flux", ctypes.c_double), ("fluid_area", ctypes.c_double),
+        ("true_outlet_flux", ctypes.c_double), ("near_flux", ctypes.c_double * 3),
+        ("flux_err_filtered", ctypes.c_double), ("u_feedback", ctypes.c_double), ("rho_feedback", ctypes.c_double),
+        ("guard_reference", ctypes.c_double), ("guard_active_step", ctypes.c_int32),
+        ("guard_count_run", ctypes.c_int32), ("ctl_update", ctypes.c_int32 * 2),
+        ("ctl_saturation", ctypes.c_int32 * 2), ("mn_mass_current", ctypes.c_double),
+        ("mn_reference", ctypes.c_double), ("mn_error", ctypes.c_double), ("mn_rho_feedback", ctypes.c_double),
+        ("mn_initialized", ctypes.c_int32), ("mn_update", ctypes.c_int32 * 2),
+        ("mn_saturation", ctypes.c_int32 * 2), ("pad_mn", ctypes.c_int32),
     ]
 
 
@@ -194,7 +237,7 @@ class OracleLBM:
                  open_boundary_semantics="equilibrium_all_population_reset", bc=(0, 0, 0, 0, 0, 0),
                  rho_bc=(1.0,) * 6, vel_bc=((0.0, 0.0, 0.0),) * 6, force=(0.0, 0.0, 0.0),
                  limiter_enabled=False, ob_rho_min=0.8, ob_rho_max=1.2, ob_u_max=0.1, ob_noneq_cap=0.05,
-                 ob_floor=None, collision="mrt", dtype=np.float32):
+                 ob_floor=None, collision="mrt", dtype=np.float32, flux_control=None):
         self.nx, self.ny, self.nz = int(nx), int(ny), int(nz)
         self.dtype = np.dtype(dtype)
         self.pfx = "32" if self.dtype == np.float32 else "64"
@@ -217,6 +260,26 @@ class OracleLBM:
         p.floor_enabled = int(ob_floor is not None)
         p.ob_rho_min, p.ob_rho_max, p.ob_u_max, p.ob_noneq_cap = ob_rho_min, ob_rho_max, ob_u_max, ob_noneq_cap
         p.ob_floor = float(ob_floor) if ob_floor is not None else -1.0e30
+        fc = dict(FLUX_CONTROL_DEFAULTS)
+        fc.update(flux_control or {})
+        self.flux_control = fc
+        p.flux_gain_u = fc["open_boundary_flux_feedback_gain_u"]
+        p.flux_gain_rho = fc["open_boundary_flux_feedback_gain_rho"]
+        p.flux_filter_alpha = fc["open_boundary_flux_filter_alpha"]
+        p.flux_cap_u = fc["open_boundary_flux_correction_cap_u"]
+        p.flux_delta_cap_u = fc["open_boundary_flux_feedback_delta_cap_u"]
+        p.flux_slew_alpha = fc["open_boundary_flux_feedback_slew_alpha"]
+        p.convective_blend = fc["open_boundary_convective_blend_weight"]
+        p.flux_target_scale = fc["open_boundary_flux_control_target_scale"]
+        p.drop_guard_min_ratio = fc["open_boundary_outlet_flux_drop_guard_min_ratio"]
+        p.mn_gain = fc["open_boundary_mass_neutral_mass_error_gain"]
+        p.mn_cap = fc["open_boundary_mass_neutral_mass_error_cap"]
+        p.mn_blend = fc["open_boundary_mass_neutral_correction_blend"]
+        p.measure_plane_offset = int(fc["open_boundary_flux_control_measure_plane_offset"])
+        p.drop_guard_enabled = int(bool(fc["open_boundary_outlet_flux_drop_guard_enabled"]))
+        p.mass_neutral = int(bool(fc["open_boundary_mass_neutral_flux_control_enabled"])
+                             and fc["open_boundary_mass_neutral_flux_control_mode"]
+                             == "global_mass_error_density_offset")
         self.p = p
         self.diag = LbmDiag()
         shp = (self.nx, self.ny, self.nz)
@@ -269,6 +332,10 @@ class OracleLBM:
     def Boundary_condition(self):
         _fn(self.pfx, "lbm_boundary")(ctypes.byref(self.p), _ptr(self.F), _ptr(self.rho), _ptr(self.v),
                                       _ptr(self.solid), ctypes.byref(self.diag))
+
+    def update_open_boundary_plane_flux_controller(self):
+        _fn(self.pfx, "lbm_plane_flux_controller")(ctypes.byref(self.p), _ptr(self.rho), _ptr(self.v),
+                                                   _ptr(self.solid), ctypes.byref(self.diag))
 
     def streaming3(self):
         _fn(self.pfx, "lbm_macros")(ctypes.byref(self.p), _ptr(self.f), _ptr(self.F), _ptr(self.rho),
@@ -349,7 +416,43 @@ class OracleLBM:
                 "noneq_clip_count_step": d.ob_noneq_clip[0], "noneq_clip_count_run": d.ob_noneq_clip[1],
                 "population_floor_count_step": d.ob_floor_count[0], "population_floor_count_run": d.ob_floor_count[1],
                 "reconstructed_population_count_step": d.ob_reconstructed[0],
-                "reconstructed_population_count_run": d.ob_reconstructed[1]}
+                "reconstructed_population_count_run": d.ob_reconstructed[1],
+                "mass_balance_correction_count_step": d.mb_corr_count[0],
+                "mass_balance_correction_count_run": d.mb_corr_count[1],
+                "mass_balance_correction_abs_sum_step": d.mb_corr_abs_sum[0],
+                "mass_balance_correction_abs_sum_run": d.mb_corr_abs_sum[1],
+                "unknown_population_delta_abs_sum_step": d.pop_delta_abs_sum[0],
+                "unknown_population_delta_abs_sum_run": d.pop_delta_abs_sum[1],
+                "flow_correction_delta_abs_sum_step": d.flow_delta_abs_sum[0],
+                "flow_correction_delta_abs_sum_run": d.flow_delta_abs_sum[1],
+                "flow_outlet_flux_error_filtered_run": d.flow_err_filtered_run,
+                "flow_correction_gain_effective_step": d.flow_gain_effective_step,
+                "mass_neutral_mass_current": d.mn_mass_current,
+                "mass_neutral_mass_initial_reference": d.mn_reference,
+                "mass_neutral_mass_error": d.mn_error,
+                "mass_neutral_rho_feedback": d.mn_rho_feedback,
+                "mass_neutral_feedback_saturation_count_step": d.mn_saturation[0],
+                "mass_neutral_feedback_saturation_count_run": d.mn_saturation[1],
+                "mass_neutral_feedback_update_count_step": d.mn_update[0],
+                "mass_neutral_feedback_update_count_run": d.mn_update[1],
+                "near_outlet_flux_xminus1": d.near_flux[0],
+                "near_outlet_flux_xminus2": d.near_flux[1],
+                "near_outlet_flux_xminus3": d.near_flux[2],
+                "controller_true_outlet_flux_for_guard": d.true_outlet_flux,
+                "controller_target_outlet_flux": d.target_flux,
+                "controller_measured_outlet_flux": d.measured_flux,
+                "controller_raw_flux_error": d.target_flux - d.measured_flux,
+                "controller_filtered_flux_error": d.flux_err_filtered,
+                "controller_outlet_fluid_area": d.fluid_area,
+                "controller_u_feedback": d.u_feedback,
+                "controller_density_feedback": d.rho_feedback,
+                "controller_saturation_count_step": d.ctl_saturation[0],
+                "controller_saturation_count_run": d.ctl_saturation[1],
+                "controller_update_count_step": d.ctl_update[0],
+                "controller_update_count_run": d.ctl_update[1],
+                "controller_drop_guard_active_step": d.guard_active_step,
+                "controller_drop_guard_activation_count_run": d.guard_count_run,
+                "controller_drop_guard_reference_flux": d.guard_reference}
 
 
 class OracleMPM:

@@ -152,6 +152,83 @@ def fixture_boundaries(out):
     np.savez_compressed(out, **data)
 
 
+# outlet repairs and the plane-flux controller (fluid.py:1105-1346, 1495-1792):
+# name, semantics, LBMConfig overrides
+REPAIR_CASES = [
+    ("rmb", "regularized_mass_balanced_pressure_outlet", {}),
+    ("cmb_floor", "convective_mass_balanced_pressure_outlet",
+     {"open_boundary_limiter_enabled": True, "open_boundary_population_floor": 0.0}),
+    ("rfm", "regularized_flux_matched_pressure_outlet",
+     {"open_boundary_flux_feedback_gain_u": 0.5, "open_boundary_flux_feedback_gain_rho": 0.3,
+      "open_boundary_flux_filter_alpha": 0.2}),
+    ("cfm", "convective_flux_matched_damped_outlet",
+     {"open_boundary_flux_feedback_gain_u": 0.5, "open_boundary_convective_blend_weight": 0.3}),
+    ("rpf_mn", "regularized_plane_flux_controlled_pressure_outlet",
+     {"open_boundary_flux_feedback_gain_u": 1.0, "open_boundary_flux_feedback_gain_rho": 0.1,
+      "open_boundary_flux_filter_alpha": 0.5, "open_boundary_flux_correction_cap_u": 0.004,
+      "open_boundary_flux_feedback_delta_cap_u": 0.001, "open_boundary_flux_feedback_slew_alpha": 0.5,
+      "open_boundary_flux_control_measure_plane_offset": 1, "open_boundary_outlet_flux_drop_guard_enabled": True,
+      "open_boundary_outlet_flux_drop_guard_min_ratio": 0.9,
+      "open_boundary_mass_neutral_flux_control_enabled": True,
+      "open_boundary_mass_neutral_flux_control_mode": "global_mass_error_density_offset",
+      "open_boundary_mass_neutral_mass_error_gain": 2.0, "open_boundary_mass_neutral_mass_error_cap": 0.001,
+      "open_boundary_mass_neutral_correction_blend": 0.5}),
+    ("cpf", "convective_plane_flux_controlled_damped_outlet",
+     {"open_boundary_flux_feedback_gain_u": 0.05, "open_boundary_flux_control_measure_plane_offset": 2,
+      "open_boundary_flux_control_target_scale": 1.1, "open_boundary_convective_blend_weight": 0.25,
+      "open_boundary_mass_neutral_flux_control_enabled": True,
+      "open_boundary_mass_neutral_flux_control_mode": "global_mass_error_density_offset",
+      "open_boundary_mass_neutral_mass_error_gain": 0.5, "open_boundary_mass_neutral_mass_error_cap": 0.01,
+      "open_boundary_mass_neutral_correction_blend": 1.0}),
+]
+# the numeric entries of get_open_boundary_limiter_stats the fixture keeps
+REPAIR_STAT_KEYS = [
+    "mass_balance_correction_count_step", "mass_balance_correction_count_run",
+    "mass_balance_correction_abs_sum_step", "mass_balance_correction_abs_sum_run",
+    "unknown_population_delta_abs_sum_step", "unknown_population_delta_abs_sum_run",
+    "flow_correction_delta_abs_sum_step", "flow_correction_delta_abs_sum_run",
+    "flow_outlet_flux_error_filtered_run", "flow_correction_gain_effective_step",
+    "population_floor_count_step", "mass_neutral_mass_current", "mass_neutral_mass_initial_reference",
+    "mass_neutral_mass_error", "mass_neutral_rho_feedback", "mass_neutral_feedback_saturation_count_run",
+    "mass_neutral_feedback_update_count_run", "near_outlet_flux_xminus1", "near_outlet_flux_xminus2",
+    "near_outlet_flux_xminus3", "controller_true_outlet_flux_for_guard", "controller_target_outlet_flux",
+    "controller_measured_outlet_flux", "controller_filtered_flux_error", "controller_outlet_fluid_area",
+    "controller_u_feedback", "controller_density_feedback", "controller_saturation_count_run",
+    "controller_update_count_run", "controller_drop_guard_active_step", "controller_drop_guard_activation_count_run",
+    "controller_drop_guard_reference_flux",
+]
+
+
+def fixture_outlet_repair(out):
+    """Boundary_condition, streaming3, Boundary_condition for each repair case
+    (the second call sees the first's controller and filter state)."""
+    rng = np.random.default_rng(2)
+    nx, ny, nz = 7, 5, 4
+    F, rho, v, cf, solid, svel = rand_state(rng, nx, ny, nz, solid_frac=0.2)
+    rho[nx - 2, 2, 2] = 0.0
+    data = dict(F=F, rho=rho, v=v, solid=solid)
+    for name, sem, over in REPAIR_CASES:
+        cfg = dict(nx=nx, ny=ny, nz=nz, open_boundary_semantics=sem, bc_x_left=2, bc_x_right=1,
+                   vel_bc_x_left=(0.04, 0.003, -0.002), vel_bc_x_right=(0.03, 0.0, 0.001),
+                   rho_bc_x_left=1.01, rho_bc_x_right=0.99)
+        cfg.update(over)
+        lbm = make_lbm(cfg)
+        for nm in ("F", "rho", "v", "solid"):
+            getattr(lbm, nm).from_numpy(data[nm])
+        for call in (1, 2):
+            lbm.Boundary_condition()
+            data[f"{name}_F{call}"] = lbm.F.to_numpy()
+            st = lbm.get_open_boundary_limiter_stats()
+            data[f"{name}_stats{call}"] = np.array([float(st[k]) for k in REPAIR_STAT_KEYS])
+            if call == 1:
+                lbm.streaming3()
+                data[f"{name}_rho1"] = lbm.rho.to_numpy()
+                data[f"{name}_v1"] = lbm.v.to_numpy()
+    data["cases"] = np.array(json.dumps(REPAIR_CASES))
+    data["stat_keys"] = np.array(json.dumps(REPAIR_STAT_KEYS))
+    np.savez_compressed(out, **data)
+
+
 def fixture_mpm(out):
     from src.mpm_lbm.sim.mpm.config import MPMConfig
     from src.mpm_lbm.sim.mpm.solid import MPMSolid3D
@@ -330,6 +407,7 @@ def fixture_driver(name, out, tmpdir):
 UNIT = {
     "lbm_kernels": fixture_lbm_kernels,
     "lbm_boundaries": fixture_boundaries,
+    "lbm_outlet_repair": fixture_outlet_repair,
     "mpm_kernels": fixture_mpm,
     "coupling_kernels": fixture_coupling,
 }

@@ -19,6 +19,11 @@ tests/test_step115_lbm_open_boundary_and_force_accumulation_contract.py:29):
 * reading a field element yields a value snapshot (taichi value semantics)
   that still remembers its storage slot, so ``ti.atomic_*`` and element
   assignment (``F[i][s] = v``, ``x[p].z = v``) write through;
+* assigning to a local variable (``u = v[i]``, ``w = u``) copies the value and
+  drops the storage link, as taichi's local variables do: the bodies of
+  ``@ti.kernel`` / ``@ti.func`` functions are recompiled with every plain
+  ``name = expr`` assignment wrapped in a copy, so that ``w[0] = ...`` later
+  changes neither ``u`` nor the field;
 * ``ti.svd`` returns rotations U, V with the sign of the smallest singular
   value flipped when det(F) < 0, so ``R = U @ V.T`` is the proper rotation
   (the value the reference uses, mpm/solid.py:233-234).
@@ -30,7 +35,10 @@ f32 rounding, not bit for bit.
 
 from __future__ import annotations
 
+import ast
+import inspect
 import itertools
+import textwrap
 
 import numpy as np
 
@@ -58,12 +66,61 @@ def data_oriented(cls):
     return cls
 
 
+def _ti_local(value):
+    """The value a taichi local variable holds: a copy without storage link."""
+    if isinstance(value, np.ndarray):
+        return np.array(value).view(TiArr)
+    return value
+
+
+class _LocalCopies(ast.NodeTransformer):
+    def visit_Assign(self, node):
+        self.generic_visit(node)
+        if all(isinstance(t, ast.Name) for t in node.targets):
+            node.value = ast.Call(func=ast.Name(id="_ti_local_copy", ctx=ast.Load()), args=[node.value], keywords=[])
+        return node
+
+    def visit_AnnAssign(self, node):
+        self.generic_visit(node)
+        if isinstance(node.target, ast.Name) and node.value is not None:
+            node.value = ast.Call(func=ast.Name(id="_ti_local_copy", ctx=ast.Load()), args=[node.value], keywords=[])
+        return node
+
+
+def _with_local_copies(fn):
+    """fn recompiled from its source with local assignments copying (see the
+    module docstring); fn itself if its source is not available."""
+    try:
+        src = textwrap.dedent(inspect.getsource(fn))
+        filename = inspect.getsourcefile(fn) or "<taichi_shim>"
+        first = inspect.getsourcelines(fn)[1]
+    except (OSError, TypeError):
+        return fn
+    tree = ast.parse(src)
+    fdef = tree.body[0]
+    if not isinstance(fdef, ast.FunctionDef) or fn.__code__.co_freevars:
+        return fn
+    fdef.decorator_list = []
+    _LocalCopies().visit(tree)
+    ast.fix_missing_locations(tree)
+    ast.increment_lineno(tree, first - 1)
+    glb = fn.__globals__
+    glb.setdefault("_ti_local_copy", _ti_local)
+    scope = {}
+    exec(compile(tree, filename, "exec"), glb, scope)
+    new = scope[fdef.name]
+    new.__defaults__ = fn.__defaults__
+    new.__kwdefaults__ = fn.__kwdefaults__
+    new.__qualname__ = fn.__qualname__
+    return new
+
+
 def kernel(fn):
-    return fn
+    return _with_local_copies(fn)
 
 
 def func(fn):
-    return fn
+    return _with_local_copies(fn)
 
 
 def template():

@@ -131,6 +131,71 @@ def test_boundaries_match_reference():
             np.testing.assert_array_equal(got, d[name + "_counts"], err_msg=name)
 
 
+def outlet_repair_oracle(d, sem, over, dtype=np.float32):
+    """An oracle lattice set up like a case of the lbm_outlet_repair fixture."""
+    nx, ny, nz = d["F"].shape[:3]
+    lim = bool(over.get("open_boundary_limiter_enabled", False))
+    floor = over.get("open_boundary_population_floor")
+    fc = {k: v for k, v in over.items() if k not in ("open_boundary_limiter_enabled", "open_boundary_population_floor")}
+    lbm = orc.OracleLBM(nx, ny, nz, open_boundary_semantics=sem, bc=(2, 1, 0, 0, 0, 0),
+                        rho_bc=(1.01, 0.99, 1, 1, 1, 1),
+                        vel_bc=((0.04, 0.003, -0.002), (0.03, 0.0, 0.001), (0, 0, 0), (0, 0, 0), (0, 0, 0),
+                                (0, 0, 0)),
+                        limiter_enabled=lim, ob_floor=floor, flux_control=fc, dtype=dtype)
+    lbm.init_simulation()
+    lbm.F[...] = d["F"]
+    lbm.rho[...] = d["rho"]
+    lbm.v[...] = d["v"]
+    lbm.solid[...] = d["solid"]
+    return lbm
+
+
+def test_outlet_repair_matches_reference():
+    """Semantics 4-9: populations and every repair / controller statistic of
+    two Boundary_condition calls with a macroscopic update between them.
+    Floating sums to rtol 1e-5 / atol 1e-7 (same f32 loop order), counts exact."""
+    d = load("lbm_outlet_repair")
+    keys = json.loads(str(d["stat_keys"]))
+    for name, sem, over in json.loads(str(d["cases"])):
+        lbm = outlet_repair_oracle(d, sem, over)
+        for call in (1, 2):
+            lbm.Boundary_condition()
+            np.testing.assert_allclose(lbm.F, d[f"{name}_F{call}"], rtol=2e-6, atol=1e-8, err_msg=f"{name} F{call}")
+            st = lbm.get_open_boundary_limiter_stats()
+            got = np.array([float(st[k]) if k in st else np.nan for k in keys])
+            want = d[f"{name}_stats{call}"]
+            for k, g, w in zip(keys, got, want):
+                if "count" in k or k.endswith("active_step"):
+                    assert g == w, (name, call, k, g, w)
+                else:
+                    assert abs(g - w) <= 1e-7 + 1e-5 * abs(w), (name, call, k, g, w)
+            if call == 1:
+                lbm.streaming3()
+                np.testing.assert_allclose(lbm.rho, d[f"{name}_rho1"], rtol=2e-6, atol=1e-8)
+                np.testing.assert_allclose(lbm.v, d[f"{name}_v1"], rtol=2e-5, atol=1e-8)
+
+
+def test_plane_flux_controller_contract():
+    """tests/test_step131_plane_flux_controller_contract.py:205-235 restated on
+    the oracle: with inlet flux above the outlet's the feedback saturates at
+    +cap, with the reverse at -cap, and a cleared run starts from zero."""
+    fc = {"open_boundary_flux_feedback_gain_u": 1.0, "open_boundary_flux_feedback_gain_rho": 0.0,
+          "open_boundary_flux_filter_alpha": 1.0, "open_boundary_flux_correction_cap_u": 0.002,
+          "open_boundary_convective_blend_weight": 0.02}
+    for inlet, outlet, sign in ((1.0, 0.0, 1.0), (0.0, 1.0, -1.0)):
+        lbm = orc.OracleLBM(8, 6, 6, open_boundary_semantics="regularized_plane_flux_controlled_pressure_outlet",
+                            bc=(2, 1, 0, 0, 0, 0), flux_control=fc)
+        lbm.rho[...] = 1.0
+        lbm.v[...] = 0.0
+        lbm.v[0, :, :, 0] = inlet
+        lbm.v[-1, :, :, 0] = outlet
+        lbm.update_open_boundary_plane_flux_controller()
+        st = lbm.get_open_boundary_limiter_stats()
+        assert st["controller_raw_flux_error"] * sign > 0.0
+        assert st["controller_u_feedback"] == pytest.approx(sign * 0.002)
+        assert st["controller_saturation_count_run"] == 1
+
+
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
 def test_mpm_kernels_match_reference(dtype):
     d = load("mpm_kernels")
