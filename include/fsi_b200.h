@@ -262,6 +262,55 @@ typedef struct FsiCampaignSums {
 int fsi_campaign_sums(const FsiLbmState* s, const FsiLbmParams* p, const FsiStepCtl* ctl, const uint8_t* regions,
                       FsiCampaignSums* out, void* stream);
 
+/* Per-x-plane statistics of the lattice fields, one device pass.  The
+ * reference's diagnostics (sim/diagnostics/lbm_boundary_diagnostics.py,
+ * lbm_stability_diagnostics.py) copy rho, v, solid, f and F to the host and
+ * reduce them with numpy in FP64; every quantity they report is a function
+ * of these per-plane records (host sums over planes give the totals).
+ * Keys: order-preserving uint32 codes of FP32 values (a min key of
+ * FSI_KEY_NONE_MIN or a max key of 0: no value); NaN is skipped by the
+ * min / max keys and counted separately. */
+#define FSI_KEY_NONE_MIN 0xffffffffu
+typedef struct FsiPlaneStats {
+  double flux;              /* fluid cells: sum of rho * v_x (FP64) */
+  double ux_sum, ux_sq;     /* fluid: sum of v_x, of v_x^2 */
+  double rho_sum, rho_sq;   /* fluid: sum of rho, of (rho - 1)^2 */
+  uint64_t speed_max;       /* fluid: max |v| (bits of the FP64 norm, NaN skipped; 0: none) */
+  int32_t fluid_cells;
+  int32_t ux_negative;      /* fluid cells with v_x < 0 */
+  uint32_t ux_min, ux_max, rho_min, rho_max;   /* fluid cells: keys */
+  int32_t rho_nan, rho_nonfinite, vel_nan, vel_nonfinite;  /* fluid cells (vel: any component) */
+  int32_t cell_nonfinite;   /* cells of any kind with a non-finite rho or v */
+  int32_t rho_low, rho_high, vel_high;                     /* fluid: rho < low, rho > high, |v| > vel_high */
+  int32_t rho_low_first, rho_high_first, vel_high_first;   /* smallest j * nz + k of those (INT32_MAX: none) */
+  uint32_t pop_min[2], pop_max[2];      /* populations f, F of all cells: keys */
+  int32_t pop_negative[2], pop_nonfinite[2];
+  float center_ux;          /* v_x at (x, cy, cz) */
+  int32_t center_fluid;     /* solid[x, cy, cz] == 0 */
+  int32_t ux_nan;           /* fluid cells with a NaN v_x */
+} FsiPlaneStats;
+
+typedef struct FsiFieldStatsArgs {
+  float rho_low, rho_high, vel_high;  /* density_outlier_stats low / high, velocity_outlier_stats threshold */
+  int32_t cy, cz;                     /* centerline cell of centerline_profile_x */
+  int32_t pad;
+  /* fsi_field_stats_arrays only: fields in lattice order (x fastest), n = nx*ny*nz */
+  const float* rho;       /* [n] */
+  const float* vel;       /* [3][n] */
+  const uint8_t* solid;   /* [n] non-zero: solid */
+  const float* pop_f;     /* [19][n] or NULL (zeros, as the reference's snapshot without f) */
+  const float* pop_F;     /* [19][n] or NULL */
+} FsiFieldStatsArgs;
+
+/* planes: [nx] device records, overwritten.  From the state's readout (as
+ * fsi_lbm_readout returns it; f and F are the same array there, so index 0
+ * and 1 of the population fields agree). */
+int fsi_lbm_field_stats(const FsiLbmState* s, const FsiLbmParams* p, const FsiStepCtl* ctl,
+                        const FsiFieldStatsArgs* a, FsiPlaneStats* planes, void* stream);
+/* The same from plain device fields (a snapshot the caller holds). */
+int fsi_field_stats_arrays(int32_t nx, int32_t ny, int32_t nz, const FsiFieldStatsArgs* a, FsiPlaneStats* planes,
+                           void* stream);
+
 /* ---- particles, projection, reaction transfer, MPM ---------------------- */
 
 typedef struct FsiParticles {

@@ -125,11 +125,29 @@ class FsiBatchDims(ctypes.Structure):
 
 FSI_BATCH_PENALTY, FSI_BATCH_MOVING = 0, 1
 
+
+class FsiPlaneStats(ctypes.Structure):
+    _fields_ = [("flux", c_f64), ("ux_sum", c_f64), ("ux_sq", c_f64), ("rho_sum", c_f64), ("rho_sq", c_f64),
+                ("speed_max", ctypes.c_uint64), ("fluid_cells", c_i32), ("ux_negative", c_i32),
+                ("ux_min", ctypes.c_uint32), ("ux_max", ctypes.c_uint32), ("rho_min", ctypes.c_uint32),
+                ("rho_max", ctypes.c_uint32), ("rho_nan", c_i32), ("rho_nonfinite", c_i32), ("vel_nan", c_i32),
+                ("vel_nonfinite", c_i32), ("cell_nonfinite", c_i32), ("rho_low", c_i32), ("rho_high", c_i32),
+                ("vel_high", c_i32), ("rho_low_first", c_i32), ("rho_high_first", c_i32),
+                ("vel_high_first", c_i32), ("pop_min", ctypes.c_uint32 * 2), ("pop_max", ctypes.c_uint32 * 2),
+                ("pop_negative", c_i32 * 2), ("pop_nonfinite", c_i32 * 2), ("center_ux", c_f32),
+                ("center_fluid", c_i32), ("ux_nan", c_i32)]
+
+
+class FsiFieldStatsArgs(ctypes.Structure):
+    _fields_ = [("rho_low", c_f32), ("rho_high", c_f32), ("vel_high", c_f32), ("cy", c_i32), ("cz", c_i32),
+                ("pad", c_i32), ("rho", c_p), ("vel", c_p), ("solid", c_p), ("pop_f", c_p), ("pop_F", c_p)]
+
 STRUCTS = {
     "FsiLbmDiag": FsiLbmDiag, "FsiLbmState": FsiLbmState, "FsiLbmParams": FsiLbmParams, "FsiStepCtl": FsiStepCtl,
     "FsiParticles": FsiParticles, "FsiGrid": FsiGrid, "FsiMpmParams": FsiMpmParams,
     "FsiCouplingParams": FsiCouplingParams, "FsiCouplingStats": FsiCouplingStats, "FsiMpmBins": FsiMpmBins,
     "FsiBatchCase": FsiBatchCase, "FsiBatchDims": FsiBatchDims, "FsiCampaignSums": FsiCampaignSums,
+    "FsiPlaneStats": FsiPlaneStats, "FsiFieldStatsArgs": FsiFieldStatsArgs,
 }
 
 # entry point -> argtypes (all return int)
@@ -146,6 +164,8 @@ SIGNATURES = {
     "fsi_force_accum_finalize": [_P(FsiLbmState), _P(FsiStepCtl), c_i32, c_p],
     "fsi_lbm_readout": [_P(FsiLbmState), _P(FsiLbmParams), _P(FsiStepCtl), c_p, c_p, c_p, c_p],
     "fsi_campaign_sums": [_P(FsiLbmState), _P(FsiLbmParams), _P(FsiStepCtl), c_p, c_p, c_p],
+    "fsi_lbm_field_stats": [_P(FsiLbmState), _P(FsiLbmParams), _P(FsiStepCtl), _P(FsiFieldStatsArgs), c_p, c_p],
+    "fsi_field_stats_arrays": [c_i32, c_i32, c_i32, _P(FsiFieldStatsArgs), c_p, c_p],
     "fsi_project": [_P(FsiLbmState), _P(FsiParticles), _P(FsiCouplingParams), c_p, c_p],
     "fsi_reaction_to_grid": [_P(FsiLbmState), c_p, _P(FsiParticles), _P(FsiGrid), _P(FsiCouplingParams), c_p, c_p],
     "fsi_mpm_p2g": [_P(FsiParticles), _P(FsiGrid), _P(FsiMpmParams), c_p],

@@ -1776,6 +1776,230 @@ __global__ void __launch_bounds__(256) k_campaign_sums(const Case c, const uint8
   }
 }
 
+// ---- per-x-plane field statistics (sim/diagnostics/lbm_*_diagnostics.py) --
+__device__ __forceinline__ uint32_t order_key(float v) {
+  const uint32_t b = __float_as_uint(v);
+  return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+
+// one thread's statistics of the cells of its x plane it visits
+struct PlaneAcc {
+  double flux, uxs, uxq, rs, rq, spd;
+  int fluid, neg, rnan, rnf, vnan, vnf, cnf, rlow, rhigh, vhigh, rlow_first, rhigh_first, vhigh_first, uxnan;
+  uint32_t uxmin, uxmax, rmin, rmax, pmin[2], pmax[2];
+  int pneg[2], pnf[2];
+  float cux;
+  int cfl;
+};
+
+__device__ __forceinline__ void plane_acc_init(PlaneAcc& a) {
+  a.flux = a.uxs = a.uxq = a.rs = a.rq = a.spd = 0.0;
+  a.fluid = a.neg = a.rnan = a.rnf = a.vnan = a.vnf = a.cnf = a.rlow = a.rhigh = a.vhigh = a.uxnan = 0;
+  a.rlow_first = a.rhigh_first = a.vhigh_first = INT32_MAX;
+  a.uxmin = a.rmin = a.pmin[0] = a.pmin[1] = 0xffffffffu;
+  a.uxmax = a.rmax = a.pmax[0] = a.pmax[1] = 0u;
+  a.pneg[0] = a.pneg[1] = a.pnf[0] = a.pnf[1] = 0;
+  a.cux = 0.f;
+  a.cfl = -1;
+}
+
+__device__ __forceinline__ void plane_acc_pops(PlaneAcc& a, int w, const float* F) {
+#pragma unroll
+  for (int s = 0; s < 19; ++s) {
+    const float v = F[s];
+    if (!isnan(v)) {
+      a.pmin[w] = min(a.pmin[w], order_key(v));
+      a.pmax[w] = max(a.pmax[w], order_key(v));
+    }
+    a.pneg[w] += v < 0.f ? 1 : 0;
+    a.pnf[w] += isfinite(v) ? 0 : 1;
+  }
+}
+
+// cell (in-plane index jk = j * nz + k) with its rho, v and solid state
+__device__ __forceinline__ void plane_acc_cell(PlaneAcc& a, const FsiFieldStatsArgs& g, int jk, bool fluid, float rho,
+                                               const float* u) {
+  const bool rho_ok = isfinite(rho), vel_ok = isfinite(u[0]) && isfinite(u[1]) && isfinite(u[2]);
+  a.cnf += (rho_ok && vel_ok) ? 0 : 1;
+  if (!fluid) return;
+  ++a.fluid;
+  const double r = rho, ux = u[0];
+  a.flux += r * ux;
+  a.uxs += ux;
+  a.uxq += ux * ux;
+  a.rs += r;
+  a.rq += (r - 1.0) * (r - 1.0);
+  a.neg += u[0] < 0.f ? 1 : 0;
+  if (!isnan(u[0])) {
+    a.uxmin = min(a.uxmin, order_key(u[0]));
+    a.uxmax = max(a.uxmax, order_key(u[0]));
+  } else {
+    ++a.uxnan;
+  }
+  if (!isnan(rho)) {
+    a.rmin = min(a.rmin, order_key(rho));
+    a.rmax = max(a.rmax, order_key(rho));
+  }
+  a.rnan += isnan(rho) ? 1 : 0;
+  a.rnf += rho_ok ? 0 : 1;
+  const bool vnan = isnan(u[0]) || isnan(u[1]) || isnan(u[2]);
+  a.vnan += vnan ? 1 : 0;
+  a.vnf += vel_ok ? 0 : 1;
+  const double sp = sqrt((double)u[0] * u[0] + (double)u[1] * u[1] + (double)u[2] * u[2]);
+  if (!vnan) a.spd = fmax(a.spd, sp);
+  if (rho < g.rho_low) {
+    ++a.rlow;
+    a.rlow_first = min(a.rlow_first, jk);
+  }
+  if (rho > g.rho_high) {
+    ++a.rhigh;
+    a.rhigh_first = min(a.rhigh_first, jk);
+  }
+  if (sp > (double)g.vel_high) {
+    ++a.vhigh;
+    a.vhigh_first = min(a.vhigh_first, jk);
+  }
+}
+
+// SRC 0: the state's readout; 1: plain fields in g.  Block (32, 8): lane
+// -> x = blockIdx.x * 32 + lane, warps and blockIdx.y stride over the rows
+// (j, k); one set of atomics per plane and block.
+template <int SRC, bool H>
+__global__ void __launch_bounds__(256) k_plane_stats(const Case c, const FsiFieldStatsArgs g, FsiPlaneStats* out) {
+  __shared__ PlaneAcc sacc[8][32];
+  const int lane = threadIdx.x, wy = threadIdx.y;
+  const int nx = c.s.nx, ny = c.s.ny, nz = c.s.nz;
+  const int x = blockIdx.x * 32 + lane;
+  const int64_t n = (int64_t)nx * ny * nz;
+  PlaneAcc a;
+  plane_acc_init(a);
+  if (x < nx) {
+    for (int r = blockIdx.y * 8 + wy; r < ny * nz; r += gridDim.y * 8) {
+      const int j = r % ny, k = r / ny;
+      const int64_t i = (int64_t)r * nx + x;
+      float F[19], rho, u[3];
+      bool fluid;
+      if (SRC == 0) {
+        fluid = !(readout_cell<H>(c, i, F, rho, u) & kSolid);
+        plane_acc_pops(a, 0, F);
+      } else {
+        fluid = g.solid[i] == 0;
+        rho = g.rho[i];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) u[d] = g.vel[d * n + i];
+#pragma unroll
+        for (int w = 0; w < 2; ++w) {
+          const float* src = w ? g.pop_F : g.pop_f;
+#pragma unroll
+          for (int s = 0; s < 19; ++s) F[s] = src ? src[s * n + i] : 0.f;
+          plane_acc_pops(a, w, F);
+        }
+      }
+      plane_acc_cell(a, g, j * nz + k, fluid, rho, u);
+      if (j == g.cy && k == g.cz) {
+        a.cux = u[0];
+        a.cfl = fluid ? 1 : 0;
+      }
+    }
+  }
+  sacc[wy][lane] = a;
+  __syncthreads();
+  if (wy != 0 || x >= nx) return;
+  for (int w = 1; w < 8; ++w) {
+    const PlaneAcc& b = sacc[w][lane];
+    a.flux += b.flux;
+    a.uxs += b.uxs;
+    a.uxq += b.uxq;
+    a.rs += b.rs;
+    a.rq += b.rq;
+    a.spd = fmax(a.spd, b.spd);
+    a.fluid += b.fluid;
+    a.neg += b.neg;
+    a.rnan += b.rnan;
+    a.rnf += b.rnf;
+    a.vnan += b.vnan;
+    a.vnf += b.vnf;
+    a.cnf += b.cnf;
+    a.rlow += b.rlow;
+    a.rhigh += b.rhigh;
+    a.vhigh += b.vhigh;
+    a.uxnan += b.uxnan;
+    a.rlow_first = min(a.rlow_first, b.rlow_first);
+    a.rhigh_first = min(a.rhigh_first, b.rhigh_first);
+    a.vhigh_first = min(a.vhigh_first, b.vhigh_first);
+    a.uxmin = min(a.uxmin, b.uxmin);
+    a.uxmax = max(a.uxmax, b.uxmax);
+    a.rmin = min(a.rmin, b.rmin);
+    a.rmax = max(a.rmax, b.rmax);
+    for (int q = 0; q < 2; ++q) {
+      a.pmin[q] = min(a.pmin[q], b.pmin[q]);
+      a.pmax[q] = max(a.pmax[q], b.pmax[q]);
+      a.pneg[q] += b.pneg[q];
+      a.pnf[q] += b.pnf[q];
+    }
+    if (b.cfl >= 0) {
+      a.cux = b.cux;
+      a.cfl = b.cfl;
+    }
+  }
+  if (SRC == 0) {  // f and F are one array in the readout
+    a.pmin[1] = a.pmin[0];
+    a.pmax[1] = a.pmax[0];
+    a.pneg[1] = a.pneg[0];
+    a.pnf[1] = a.pnf[0];
+  }
+  FsiPlaneStats* o = out + x;
+  auto addd = [](double* p, double v) {
+    if (v != 0.0) atomicAdd(p, v);
+  };
+  auto addi = [](int32_t* p, int v) {
+    if (v) atomicAdd(p, v);
+  };
+  addd(&o->flux, a.flux);
+  addd(&o->ux_sum, a.uxs);
+  addd(&o->ux_sq, a.uxq);
+  addd(&o->rho_sum, a.rs);
+  addd(&o->rho_sq, a.rq);
+  if (a.spd > 0.0) atomicMax(reinterpret_cast<unsigned long long*>(&o->speed_max), (unsigned long long)__double_as_longlong(a.spd));
+  addi(&o->fluid_cells, a.fluid);
+  addi(&o->ux_negative, a.neg);
+  addi(&o->rho_nan, a.rnan);
+  addi(&o->rho_nonfinite, a.rnf);
+  addi(&o->vel_nan, a.vnan);
+  addi(&o->vel_nonfinite, a.vnf);
+  addi(&o->cell_nonfinite, a.cnf);
+  addi(&o->rho_low, a.rlow);
+  addi(&o->rho_high, a.rhigh);
+  addi(&o->vel_high, a.vhigh);
+  addi(&o->ux_nan, a.uxnan);
+  if (a.rlow_first != INT32_MAX) atomicMin(&o->rho_low_first, a.rlow_first);
+  if (a.rhigh_first != INT32_MAX) atomicMin(&o->rho_high_first, a.rhigh_first);
+  if (a.vhigh_first != INT32_MAX) atomicMin(&o->vel_high_first, a.vhigh_first);
+  if (a.uxmin != 0xffffffffu) atomicMin(&o->ux_min, a.uxmin);
+  if (a.uxmax) atomicMax(&o->ux_max, a.uxmax);
+  if (a.rmin != 0xffffffffu) atomicMin(&o->rho_min, a.rmin);
+  if (a.rmax) atomicMax(&o->rho_max, a.rmax);
+  for (int q = 0; q < 2; ++q) {
+    if (a.pmin[q] != 0xffffffffu) atomicMin(&o->pop_min[q], a.pmin[q]);
+    if (a.pmax[q]) atomicMax(&o->pop_max[q], a.pmax[q]);
+    addi(&o->pop_negative[q], a.pneg[q]);
+    addi(&o->pop_nonfinite[q], a.pnf[q]);
+  }
+  if (a.cfl >= 0) {  // the one block holding (cy, cz) of this plane
+    o->center_ux = a.cux;
+    o->center_fluid = a.cfl;
+  }
+}
+
+__global__ void k_plane_stats_init(FsiPlaneStats* out, int nx) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= nx) return;
+  FsiPlaneStats z{};
+  z.ux_min = z.rho_min = z.pop_min[0] = z.pop_min[1] = 0xffffffffu;
+  z.rho_low_first = z.rho_high_first = z.vel_high_first = INT32_MAX;
+  out[x] = z;
+}
+
 // finalize_moving_boundary_force_accumulator (fluid.py:475-486)
 __global__ void k_accum_finalize(const Case c, int32_t sample_count) {
   const int64_t n = (int64_t)c.s.nx * c.s.ny * c.s.nz;
@@ -2236,6 +2460,45 @@ extern "C" int fsi_campaign_sums(const FsiLbmState* s, const FsiLbmParams* p, co
   else
     k_campaign_sums<false><<<blocks, 256, 0, st>>>(c, regions, out);
   return launch_check("k_campaign_sums");
+}
+
+static int plane_stats_launch(const Case& c, const FsiFieldStatsArgs* a, FsiPlaneStats* planes, bool arrays,
+                              cudaStream_t st) {
+  const int nx = c.s.nx, rows = c.s.ny * c.s.nz;
+  if (a->cy < 0 || a->cy >= c.s.ny || a->cz < 0 || a->cz >= c.s.nz) return invalid("centerline cell out of range");
+  k_plane_stats_init<<<(nx + 127) / 128, 128, 0, st>>>(planes, nx);
+  int rc = launch_check("k_plane_stats_init");
+  if (rc) return rc;
+  const int xt = (nx + 31) / 32;
+  const int gy = std::max(1, std::min((rows + 7) / 8, 2 * lbm_sm_count() / xt));
+  const dim3 grid((unsigned)xt, (unsigned)gy), block(32, 8);
+  if (arrays)
+    k_plane_stats<1, false><<<grid, block, 0, st>>>(c, *a, planes);
+  else if (c.s.store_fp16)
+    k_plane_stats<0, true><<<grid, block, 0, st>>>(c, *a, planes);
+  else
+    k_plane_stats<0, false><<<grid, block, 0, st>>>(c, *a, planes);
+  return launch_check("k_plane_stats");
+}
+
+extern "C" int fsi_lbm_field_stats(const FsiLbmState* s, const FsiLbmParams* p, const FsiStepCtl* ctl,
+                                   const FsiFieldStatsArgs* a, FsiPlaneStats* planes, void* stream) {
+  int rc = check_state(s, p);
+  if (rc) return rc;
+  if (!ctl || !a || !planes) return invalid("null step control, arguments or output");
+  return plane_stats_launch(make_case(s, p, ctl), a, planes, false, (cudaStream_t)stream);
+}
+
+extern "C" int fsi_field_stats_arrays(int32_t nx, int32_t ny, int32_t nz, const FsiFieldStatsArgs* a,
+                                      FsiPlaneStats* planes, void* stream) {
+  if (nx < 1 || ny < 1 || nz < 1) return invalid("lattice extents must be positive");
+  if ((int64_t)ny * nz > INT32_MAX / 2 || 19 * (int64_t)nx * ny * nz > INT64_MAX / 4) return invalid("lattice too large");
+  if (!a || !planes || !a->rho || !a->vel || !a->solid) return invalid("null rho, vel, solid or output");
+  Case c{};
+  c.s.nx = nx;
+  c.s.ny = ny;
+  c.s.nz = nz;
+  return plane_stats_launch(c, a, planes, true, (cudaStream_t)stream);
 }
 
 // ---- mask rebuild with a built-in change list ----------------------------
