@@ -311,6 +311,23 @@ int fsi_lbm_field_stats(const FsiLbmState* s, const FsiLbmParams* p, const FsiSt
 int fsi_field_stats_arrays(int32_t nx, int32_t ny, int32_t nz, const FsiFieldStatsArgs* a, FsiPlaneStats* planes,
                            void* stream);
 
+/* apply_wall_velocity_to_lbm_solid_vel (wall_velocity/application.py:118-158):
+ * cells whose grid velocity g has |g| > 0 get solid_vel = g (replace) or
+ * solid_vel + g (additive), capped to |.| <= cap, all in FP64 from the FP32
+ * solid_vel, written back as FP32.  grid: [3][pitch] FP64 in lattice order.
+ * out (device) receives the statistics of the reference's result dict. */
+#define FSI_WALL_REPLACE 0
+#define FSI_WALL_ADDITIVE 1
+typedef struct FsiWallVelocityStats {
+  double delta_norm_max, delta_norm_sum;   /* |after - before| over applied cells */
+  double before_norm_max, after_norm_max;  /* over all cells */
+  double after_norm_max_active, after_norm_sum_active;
+  int32_t applied_cells;
+  int32_t pad;
+} FsiWallVelocityStats;
+int fsi_apply_wall_velocity(const FsiLbmState* s, const double* grid, int32_t policy, double cap,
+                            FsiWallVelocityStats* out, void* stream);
+
 /* ---- particles, projection, reaction transfer, MPM ---------------------- */
 
 typedef struct FsiParticles {

@@ -138,6 +138,15 @@ class FsiPlaneStats(ctypes.Structure):
                 ("center_fluid", c_i32), ("ux_nan", c_i32)]
 
 
+class FsiWallVelocityStats(ctypes.Structure):
+    _fields_ = [("delta_norm_max", c_f64), ("delta_norm_sum", c_f64), ("before_norm_max", c_f64),
+                ("after_norm_max", c_f64), ("after_norm_max_active", c_f64), ("after_norm_sum_active", c_f64),
+                ("applied_cells", c_i32), ("pad", c_i32)]
+
+
+FSI_WALL_REPLACE, FSI_WALL_ADDITIVE = 0, 1
+
+
 class FsiFieldStatsArgs(ctypes.Structure):
     _fields_ = [("rho_low", c_f32), ("rho_high", c_f32), ("vel_high", c_f32), ("cy", c_i32), ("cz", c_i32),
                 ("pad", c_i32), ("rho", c_p), ("vel", c_p), ("solid", c_p), ("pop_f", c_p), ("pop_F", c_p)]
@@ -148,6 +157,7 @@ STRUCTS = {
     "FsiCouplingParams": FsiCouplingParams, "FsiCouplingStats": FsiCouplingStats, "FsiMpmBins": FsiMpmBins,
     "FsiBatchCase": FsiBatchCase, "FsiBatchDims": FsiBatchDims, "FsiCampaignSums": FsiCampaignSums,
     "FsiPlaneStats": FsiPlaneStats, "FsiFieldStatsArgs": FsiFieldStatsArgs,
+    "FsiWallVelocityStats": FsiWallVelocityStats,
 }
 
 # entry point -> argtypes (all return int)
@@ -166,6 +176,7 @@ SIGNATURES = {
     "fsi_campaign_sums": [_P(FsiLbmState), _P(FsiLbmParams), _P(FsiStepCtl), c_p, c_p, c_p],
     "fsi_lbm_field_stats": [_P(FsiLbmState), _P(FsiLbmParams), _P(FsiStepCtl), _P(FsiFieldStatsArgs), c_p, c_p],
     "fsi_field_stats_arrays": [c_i32, c_i32, c_i32, _P(FsiFieldStatsArgs), c_p, c_p],
+    "fsi_apply_wall_velocity": [_P(FsiLbmState), c_p, c_i32, c_f64, c_p, c_p],
     "fsi_project": [_P(FsiLbmState), _P(FsiParticles), _P(FsiCouplingParams), c_p, c_p],
     "fsi_reaction_to_grid": [_P(FsiLbmState), c_p, _P(FsiParticles), _P(FsiGrid), _P(FsiCouplingParams), c_p, c_p],
     "fsi_mpm_p2g": [_P(FsiParticles), _P(FsiGrid), _P(FsiMpmParams), c_p],

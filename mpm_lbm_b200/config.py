@@ -475,9 +475,27 @@ class FSIDriverConfig:
             raise ValueError("link_area_scale_min must be <= link_area_scale_max")
         if self.dynamic_solid_threshold < 0.0:
             raise ValueError("dynamic_solid_threshold must be non-negative")
-        # optional prescribed-motion features are out of this package's scope
-        if self.wall_velocity_application_mode != "disabled" or self.geometry_motion_application_mode != "disabled":
-            raise ValueError("wall-velocity and geometry-motion application are not supported by this backend")
+        # fsi_config.py:184-200: prescribed boundary motion and the wall velocity application
+        if self.boundary_motion_mode == "static" and self.boundary_motion_config_path is not None:
+            raise ValueError("boundary_motion_config_path must be None when boundary_motion_mode='static'")
+        if self.boundary_motion_mode == "prescribed_kinematic" and not self.boundary_motion_config_path:
+            raise ValueError("boundary_motion_config_path is required when boundary_motion_mode='prescribed_kinematic'")
+        if self.wall_velocity_application_mode == "disabled" and self.wall_velocity_application_config_path is not None:
+            raise ValueError("wall_velocity_application_config_path must be None when "
+                             "wall_velocity_application_mode='disabled'")
+        if self.wall_velocity_application_mode == "solid_vel_experimental":
+            if self.boundary_motion_mode != "prescribed_kinematic":
+                raise ValueError("wall_velocity_application_mode='solid_vel_experimental' requires "
+                                 "boundary_motion_mode='prescribed_kinematic'")
+            if not self.wall_velocity_application_config_path:
+                raise ValueError("wall_velocity_application_config_path is required when "
+                                 "wall_velocity_application_mode='solid_vel_experimental'")
+            if not Path(self.wall_velocity_application_config_path).is_file():
+                raise ValueError("wall_velocity_application_config_path must exist when "
+                                 "wall_velocity_application_mode='solid_vel_experimental'")
+        # the geometry-motion application (a host-side mask schedule) is out of this package's scope
+        if self.geometry_motion_application_mode != "disabled":
+            raise ValueError("geometry-motion application is not supported by this backend")
         self._validate_fsi_exchange_mapping()
         mapping = self.lbm_viscosity_mapping_report()
         if not math.isfinite(float(mapping["tau"])) or float(mapping["tau"]) <= 0.5:

@@ -2000,6 +2000,79 @@ __global__ void k_plane_stats_init(FsiPlaneStats* out, int nx) {
   out[x] = z;
 }
 
+// ---- wall velocity application to solid_vel (wall_velocity/application.py:118-158)
+__device__ __forceinline__ void atomic_max_dnonneg(double* addr, double v) {
+  atomicMax(reinterpret_cast<unsigned long long*>(addr), (unsigned long long)__double_as_longlong(v));
+}
+
+// |a| as numpy's norm computes it: products and sums rounded one by one (no
+// fused multiply-add), so caps and norms match the reference bit for bit
+__device__ __forceinline__ double norm3_rn(const double* a) {
+  return sqrt(__dadd_rn(__dadd_rn(__dmul_rn(a[0], a[0]), __dmul_rn(a[1], a[1])), __dmul_rn(a[2], a[2])));
+}
+
+__global__ void __launch_bounds__(256) k_wall_velocity(const Case c, const double* __restrict__ grid, int additive,
+                                                       double cap, FsiWallVelocityStats* out) {
+  const int64_t n = (int64_t)c.s.nx * c.s.ny * c.s.nz, P = c.s.pitch;
+  double dmax = 0.0, dsum = 0.0, bmax = 0.0, amax = 0.0, aamax = 0.0, aasum = 0.0;
+  int applied = 0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    double b[3], g[3], a[3], e[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      b[d] = (double)c.s.svel[d * P + i];
+      g[d] = grid[d * P + i];
+      a[d] = b[d];
+    }
+    const double bn = norm3_rn(b);
+    bmax = fmax(bmax, bn);
+    if (norm3_rn(g) > 0.0) {
+#pragma unroll
+      for (int d = 0; d < 3; ++d) a[d] = additive ? __dadd_rn(b[d], g[d]) : g[d];
+      const double an = norm3_rn(a);
+      if (an > cap) {
+        const double sc = __ddiv_rn(cap, an);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) a[d] = __dmul_rn(a[d], sc);
+      }
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        c.s.svel[d * P + i] = (float)a[d];
+        e[d] = __dsub_rn(a[d], b[d]);
+      }
+      const double dn = norm3_rn(e), an2 = norm3_rn(a);
+      ++applied;
+      dmax = fmax(dmax, dn);
+      dsum += dn;
+      aamax = fmax(aamax, an2);
+      aasum += an2;
+      amax = fmax(amax, an2);
+    } else {
+      amax = fmax(amax, bn);
+    }
+  }
+  dsum = warp_sum_d(dsum);
+  aasum = warp_sum_d(aasum);
+  applied = (int)__reduce_add_sync(0xffffffffu, (unsigned)applied);
+  for (int o = 16; o > 0; o >>= 1) {
+    dmax = fmax(dmax, __shfl_xor_sync(0xffffffffu, dmax, o));
+    bmax = fmax(bmax, __shfl_xor_sync(0xffffffffu, bmax, o));
+    amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, o));
+    aamax = fmax(aamax, __shfl_xor_sync(0xffffffffu, aamax, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (applied) {
+      atomicAdd(&out->applied_cells, applied);
+      atomicAdd(&out->delta_norm_sum, dsum);
+      atomicAdd(&out->after_norm_sum_active, aasum);
+      atomic_max_dnonneg(&out->delta_norm_max, dmax);
+      atomic_max_dnonneg(&out->after_norm_max_active, aamax);
+    }
+    atomic_max_dnonneg(&out->before_norm_max, bmax);
+    atomic_max_dnonneg(&out->after_norm_max, amax);
+  }
+}
+
 // finalize_moving_boundary_force_accumulator (fluid.py:475-486)
 __global__ void k_accum_finalize(const Case c, int32_t sample_count) {
   const int64_t n = (int64_t)c.s.nx * c.s.ny * c.s.nz;
@@ -2499,6 +2572,22 @@ extern "C" int fsi_field_stats_arrays(int32_t nx, int32_t ny, int32_t nz, const 
   c.s.ny = ny;
   c.s.nz = nz;
   return plane_stats_launch(c, a, planes, true, (cudaStream_t)stream);
+}
+
+extern "C" int fsi_apply_wall_velocity(const FsiLbmState* s, const double* grid, int32_t policy, double cap,
+                                       FsiWallVelocityStats* out, void* stream) {
+  if (!s || !grid || !out || !s->svel) return invalid("null state, grid, solid_vel or output");
+  if (policy != FSI_WALL_REPLACE && policy != FSI_WALL_ADDITIVE) return invalid("unknown wall velocity policy");
+  if (!(cap > 0.0)) return invalid("wall velocity cap must be positive");
+  cudaStream_t st = (cudaStream_t)stream;
+  int rc = cuda_check(cudaMemsetAsync(out, 0, sizeof(FsiWallVelocityStats), st), "memset wall velocity stats");
+  if (rc) return rc;
+  Case c{};
+  c.s = *s;
+  const int64_t n = (int64_t)s->nx * s->ny * s->nz;
+  const unsigned blocks = (unsigned)std::min<int64_t>(blocks_for(n, 256), (int64_t)lbm_sm_count() * 8);
+  k_wall_velocity<<<blocks, 256, 0, st>>>(c, grid, policy == FSI_WALL_ADDITIVE, cap, out);
+  return launch_check("k_wall_velocity");
 }
 
 // ---- mask rebuild with a built-in change list ----------------------------

@@ -84,6 +84,14 @@ class FSIDriver3D:
         self._graph_warm = False
         self.graph_kernels_per_step = None
         self.tuning = None
+        # wall velocity application (fsi_driver.py:458-482): the host builds the
+        # phase grid (callables taking (application config, n_grid, phase) and
+        # (application config, lbm_step), e.g. the reference's
+        # build_wall_velocity_grid and phase_for_lbm_step); the device applies it
+        self.wall_velocity_grid_builder = None
+        self.wall_velocity_phase_for_step = None
+        self.wall_velocity_application_report = None
+        self.wall_velocity_application_reports = []
 
     # ------------------------------------------------------------ init
     def _geometry_config(self):
@@ -231,7 +239,7 @@ class FSIDriver3D:
     def step_once(self):
         if not self.initialized:
             self.initialize()
-        if self.use_cuda_graph:
+        if self.use_cuda_graph and self.config.wall_velocity_application_mode == "disabled":
             self._step_graph()
             return
         self._step_eager()
@@ -302,6 +310,33 @@ class FSIDriver3D:
         t0 = time.perf_counter()
         self.projector.project(self.solid, self.lbm)
         self._t("projection_time", t0)
+        self._apply_wall_velocity_application_if_enabled()
+
+    def _apply_wall_velocity_application_if_enabled(self):
+        """fsi_driver.py:458-482: the opt-in solid_vel overwrite after each
+        projection (one device kernel; the phase grid is uploaded once)."""
+        mode = self.config.wall_velocity_application_mode
+        if mode == "disabled":
+            return None
+        if mode != "solid_vel_experimental":
+            raise ValueError(f"unsupported wall_velocity_application_mode: {mode}")
+        if self.config.boundary_motion_mode != "prescribed_kinematic":
+            raise ValueError("solid_vel_experimental wall velocity application requires prescribed_kinematic "
+                             "boundary motion")
+        from .wall_velocity import apply_wall_velocity_application_to_lbm
+
+        t0 = time.perf_counter()
+        report_path = None
+        if self.config.wall_velocity_application_report_enabled:
+            report_path = os.path.join(self.out_dir, "wall_velocity_application_report.json")
+        report = apply_wall_velocity_application_to_lbm(
+            self.lbm, self.config.wall_velocity_application_config_path, self.config.n_grid, self.current_lbm_step,
+            report_path=report_path, grid_builder=self.wall_velocity_grid_builder,
+            phase_for_step=self.wall_velocity_phase_for_step)
+        self.wall_velocity_application_report = report
+        self.wall_velocity_application_reports.append(report)
+        self._t("wall_velocity_application_time", t0)
+        return report
 
     def _mpm_loop(self, coupler=None, one_phase_reaction=None):
         """The FSI step's MPM substeps, each with the coupler's reaction
