@@ -102,7 +102,8 @@ typedef struct FsiLbmDiag {
   /* plane-flux controller (fluid.py:1141-1263): sums the step kernel accumulates
    * from its macroscopic state (rho * u_x of the fluid cells of x = 0, the
    * measure plane, x = nx-1, nx-2, nx-3, nx-4; fluid cells of the measure plane;
-   * total fluid mass), consumed and cleared by the controller update */
+   * [7] unused: the fluid mass goes to mn_mass_acc), consumed and cleared by the
+   * controller update */
   float pc_acc[8];
   float pc_target, pc_measured, pc_area, pc_true_outlet;
   float pc_near[3];
@@ -113,13 +114,15 @@ typedef struct FsiLbmDiag {
   int32_t mn_initialized;
   int32_t mn_update_step, mn_update_run, mn_sat_step, mn_sat_run;
   int32_t pad2;
+  double mn_mass_acc;  /* the fluid mass for the mass-neutral feedback, summed in FP64 (pc_acc[7] unused) */
 } FsiLbmDiag;
 
 typedef struct FsiLbmState {
   int32_t nx, ny, nz;
   int32_t store_fp16;       /* 0: float populations; 1: half (f/w - rho0) */
   int64_t pitch;            /* >= nx*ny*nz, multiple of 32 */
-  void* pop;                /* [19][pitch] float or __half */
+  void* pop;                /* 19 * pitch float or __half, in blocks of 32 cells: population s of cell i
+                               at (i / 32) * 608 + s * 32 + i % 32 */
   uint8_t* flags;           /* [pitch] FSI_CELL_* */
   uint32_t* nbr;            /* [pitch] bit s: cell + e_s is solid (valid with FSI_CELL_NEAR) */
   float* rho;               /* [pitch] stored density (override cells, readout) */

@@ -43,7 +43,7 @@ class FsiLbmDiag(ctypes.Structure):
         ("pc_update_run", c_i32), ("pc_sat_step", c_i32), ("pc_sat_run", c_i32), ("mn_mass", c_f32),
         ("mn_reference", c_f32), ("mn_error", c_f32), ("mn_rho_fb", c_f32), ("mn_initialized", c_i32),
         ("mn_update_step", c_i32), ("mn_update_run", c_i32), ("mn_sat_step", c_i32), ("mn_sat_run", c_i32),
-        ("pad2", c_i32),
+        ("pad2", c_i32), ("mn_mass_acc", c_f64),
     ]
 
 

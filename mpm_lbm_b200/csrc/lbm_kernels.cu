@@ -43,11 +43,17 @@ struct Case {
 template <bool H>
 struct Pop;
 
-// Element index of population s of a cell: 32-bit arithmetic (the host
-// checks 19 * pitch < 2^32), so that each access is one integer multiply-add
-// plus the address computation.
-__device__ __forceinline__ uint32_t pop_index(const Case& c, int s, int64_t cell) {
-  return (uint32_t)s * (uint32_t)c.s.pitch + (uint32_t)cell;
+// Element index of population s of a cell.  Populations are stored in
+// blocks of 32 cells: block b = cell / 32 holds the 19 populations of its
+// cells as 19 runs of 32 values, element (s, cell) at b * 608 + s * 32 +
+// cell % 32.  A warp of 32 aligned cells still reads 128 contiguous bytes
+// per population, and the 19 accesses of one cell differ by the constant
+// s * 128 bytes, which the compiler folds into the load / store immediate
+// (one address computation per cell instead of one per population).  The
+// block base is computed in 32 bits (the host checks 19 * pitch < 2^32).
+__device__ __forceinline__ int64_t pop_index(const Case&, int s, int64_t cell) {
+  const uint32_t i = (uint32_t)cell;
+  return (int64_t)(i + (i >> 5) * 576u) + 32 * s;
 }
 
 template <>
@@ -530,16 +536,23 @@ __device__ __forceinline__ void plane_flux_add(const Case& c, int x, bool fluid,
   t[7] += fluid ? rho : 0.f;
 }
 
-// one warp's sums into pc_acc; x0 .. x0 + w - 1 is the warp's x range
+// one warp's sums into pc_acc (the fluid mass in FP64 into mn_mass_acc, so
+// that its value does not depend on the order of the atomics); x0 .. x0 + w - 1
+// is the warp's x range
 __device__ __forceinline__ void plane_flux_flush(const Case& c, int lane, int x0, int w, const float* t) {
   const int nx = c.s.nx;
   const int mi = max(0, nx - 1 - c.p.ob_measure_offset);
   const bool planes = x0 == 0 || (mi >= x0 && mi < x0 + w) || x0 + w > nx - 4;
+  if (planes) {
 #pragma unroll
-  for (int a = 0; a < 8; ++a) {
-    if (a < 7 ? !planes : !c.p.ob_mass_neutral) continue;
-    const float v = warp_sum(t[a]);
-    if (lane == 0 && v != 0.f) atomicAdd(&c.s.diag->pc_acc[a], v);
+    for (int a = 0; a < 7; ++a) {
+      const float v = warp_sum(t[a]);
+      if (lane == 0 && v != 0.f) atomicAdd(&c.s.diag->pc_acc[a], v);
+    }
+  }
+  if (c.p.ob_mass_neutral) {
+    const double m = warp_sum_d((double)t[7]);
+    if (lane == 0 && m != 0.0) atomicAdd(&c.s.diag->mn_mass_acc, m);
   }
 }
 
@@ -872,7 +885,7 @@ __device__ __forceinline__ void prefetch_tile_l2(const Case& c, int bx, int by, 
   if (tid >= 19 * 8) return;
   const int s = tid >> 3, j = by * 8 + (tid & 7);
   if (j >= c.s.ny) return;
-  const uint32_t idx = pop_index(c, s, (int64_t)(bz * c.s.ny + j) * c.s.nx + bx * 32);
+  const int64_t idx = pop_index(c, s, (int64_t)(bz * c.s.ny + j) * c.s.nx + bx * 32);
   const void* ptr = H ? static_cast<const void*>(static_cast<const __half*>(c.s.pop) + idx)
                       : static_cast<const void*>(static_cast<const float*>(c.s.pop) + idx);
   asm volatile("prefetch.global.L2 [%0];" ::"l"(ptr));
@@ -2119,6 +2132,8 @@ static int check_state(const FsiLbmState* s, const FsiLbmParams* p) {
   if ((p->bc_left || p->bc_right) && (s->nx < 4 || (s->nx % 32 == 1) || (s->nx % 32 == 2)))
     return invalid("x open boundaries need nx >= 4 and nx % 32 not in {1, 2}");
   if (!s->pop || !s->flags || !s->nbr || !s->diag) return invalid("null device pointer in FsiLbmState");
+  if ((p->bc_left || p->bc_right || p->ob_semantics >= FSI_OB_REG_PLANE_FLUX) && !s->plane)
+    return invalid("open boundaries and the outlet flux controller need FsiLbmState.plane");
   return FSI_OK;
 }
 
@@ -2290,7 +2305,8 @@ __global__ void __launch_bounds__(kObThreads) k_ob_controller(const FsiLbmState 
   d->pc_u_fb = next;
   d->pc_rho_fb = ob_bounded(p.ob_gain_rho * filtered / area, 0.01f);
   if (p.ob_mass_neutral) {  // global_mass_error_density_offset
-    const float mass = d->pc_acc[7];
+    const float mass = (float)d->mn_mass_acc;
+    d->mn_mass_acc = 0.0;
     d->mn_mass = mass;
     if (d->mn_initialized == 0) {
       d->mn_reference = fabsf(mass) <= 1.0e-12f ? 1.0f : mass;
@@ -2331,15 +2347,20 @@ __global__ void __launch_bounds__(256) k_plane_flux_sums(const Case c, const flo
   const int nx = c.s.nx;
   const int64_t n = (int64_t)nx * c.s.ny * c.s.nz;
   float t[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  double mass = 0.0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const bool fluid = !(c.s.flags[i] & kSolid);
+    t[7] = 0.f;
     plane_flux_add(c, (int)(i % nx), fluid, rho[i], vel[i], t);
+    mass += (double)t[7];
   }
 #pragma unroll
-  for (int a = 0; a < 8; ++a) {
+  for (int a = 0; a < 7; ++a) {
     const float v = warp_sum(t[a]);
     if ((threadIdx.x & 31) == 0 && v != 0.f) atomicAdd(&c.s.diag->pc_acc[a], v);
   }
+  mass = warp_sum_d(mass);
+  if ((threadIdx.x & 31) == 0 && mass != 0.0) atomicAdd(&c.s.diag->mn_mass_acc, mass);
 }
 
 extern "C" int fsi_ob_controller_update(const FsiLbmState* s, const FsiLbmParams* p, const float* rho,
@@ -2350,6 +2371,8 @@ extern "C" int fsi_ob_controller_update(const FsiLbmState* s, const FsiLbmParams
   cudaStream_t st = (cudaStream_t)stream;
   const Case c = make_case(s, p, nullptr);
   if ((rc = cuda_check(cudaMemsetAsync(s->diag->pc_acc, 0, sizeof(s->diag->pc_acc), st), "memset pc_acc")))
+    return rc;
+  if ((rc = cuda_check(cudaMemsetAsync(&s->diag->mn_mass_acc, 0, sizeof(double), st), "memset mn_mass_acc")))
     return rc;
   const int64_t n = (int64_t)s->nx * s->ny * s->nz;
   const int blocks = (int)std::min<int64_t>(blocks_for(n, 256), 4LL * lbm_sm_count());

@@ -34,6 +34,13 @@ W = np.array([1 / 3] + [1 / 18] * 6 + [1 / 36] * 12, dtype=np.float32)
 LR = [0, 2, 1, 4, 3, 6, 5, 8, 7, 10, 9, 12, 11, 14, 13, 16, 15, 18, 17]
 
 
+def pop_blocks(t: torch.Tensor) -> torch.Tensor:
+    """[19][pitch] populations in the device storage order (blocks of 32
+    cells, each holding 19 runs of 32 values; FsiLbmState.pop)."""
+    n = t.shape[1]
+    return t.reshape(19, n // 32, 32).permute(1, 0, 2).reshape(19, n)
+
+
 def relaxation_rates(tau: float, collision: str = "mrt"):
     """S_dig of fluid.py:301-304 as (s_v, s_o); BGK relaxes all non-conserved moments at 1/tau."""
     s_v = 1.0 / tau
@@ -272,9 +279,8 @@ class LBMFluid3D:
         ref_to_lattice(arr, self.dims, 19, t)
         if self.fp16:
             w = torch.as_tensor(W, device=self.device)[:, None]
-            self.t_pop.copy_((t / w - self.rho0).to(torch.float16))
-        else:
-            self.t_pop.copy_(t)
+            t = t / w - self.rho0
+        self.t_pop.copy_(pop_blocks(t).to(self.t_pop.dtype))
         self._version += 1
 
     def _put_rho(self, arr):

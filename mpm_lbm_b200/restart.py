@@ -35,7 +35,7 @@ RESTART_METADATA_KEY = "metadata_json"
 
 EXT_PREFIX = "ext_"
 EXT_STATE_KEY = "ext_state_json"
-EXT_VERSION = 2
+EXT_VERSION = 3
 # device tensors of LBMFluid3D / MPMSolid3D that a resume restores
 _LBM_TENSORS = ("t_pop", "t_flags", "t_nbr", "t_rho", "t_vel", "t_static", "t_old", "t_reinit", "t_phi", "t_smass",
                 "t_svel", "t_cf", "t_hydro", "t_accum", "t_hpp", "t_plane", "t_vin", "t_diag")

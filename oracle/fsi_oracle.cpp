@@ -702,9 +702,13 @@ void plane_flux_controller(const OrcLbmParams& p, const R* rho, const R* v, cons
   d->u_feedback = (double)next;
   d->rho_feedback = (double)bounded_scalar<R>((R)p.flux_gain_rho * filtered / area, (R)0.01);
   if (p.mass_neutral) {
-    R mass = 0;
+    // the fluid mass in FP64 (the reference's f32 atomic sum depends on the
+    // order of its parallel loop; FP64 makes the sum order-independent), then
+    // rounded to R like the reference's field
+    double mass_d = 0.0;
     for (int64_t c = 0; c < g.n(); ++c)
-      if (solid[c] == 0) mass += rho[c];
+      if (solid[c] == 0) mass_d += (double)rho[c];
+    const R mass = (R)mass_d;
     d->mn_mass_current = (double)mass;
     if (d->mn_initialized == 0) {
       R reference = mass;

@@ -153,7 +153,10 @@ def outlet_repair_oracle(d, sem, over, dtype=np.float32):
 def test_outlet_repair_matches_reference():
     """Semantics 4-9: populations and every repair / controller statistic of
     two Boundary_condition calls with a macroscopic update between them.
-    Floating sums to rtol 1e-5 / atol 1e-7 (same f32 loop order), counts exact."""
+    Floating sums to rtol 1e-5 / atol 1e-7 (same f32 loop order), counts exact.
+    The oracle sums the mass-neutral fluid mass in FP64 where the reference
+    adds f32 values into an f32 total (rounding up to ~N * 2^-24 relative for
+    N fluid cells), so the mass error and its density feedback get atol 1e-5."""
     d = load("lbm_outlet_repair")
     keys = json.loads(str(d["stat_keys"]))
     for name, sem, over in json.loads(str(d["cases"])):
@@ -167,6 +170,8 @@ def test_outlet_repair_matches_reference():
             for k, g, w in zip(keys, got, want):
                 if "count" in k or k.endswith("active_step"):
                     assert g == w, (name, call, k, g, w)
+                elif k in ("mass_neutral_mass_error", "mass_neutral_rho_feedback"):
+                    assert abs(g - w) <= 1e-5, (name, call, k, g, w)
                 else:
                     assert abs(g - w) <= 1e-7 + 1e-5 * abs(w), (name, call, k, g, w)
             if call == 1:
