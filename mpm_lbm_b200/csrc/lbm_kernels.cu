@@ -37,6 +37,7 @@ struct Case {
   FsiStepCtl c;
   MrtK K;
   int pf_dist;  // tiles between a CTA's tile and the one it prefetches into L2 (0: none)
+  int aligned;  // nx % 32 == 0: every row starts a 32-cell block of the population storage
 };
 
 // ------------------------------------------------------------ storage ----
@@ -67,6 +68,13 @@ struct Pop<false> {
   static __device__ __forceinline__ void st(const Case& c, int s, int64_t cell, float v) {
     static_cast<float*>(c.s.pop)[pop_index(c, s, cell)] = v;
   }
+  // by block-layout index b (pop_index without the 32 s term)
+  static __device__ __forceinline__ float ldb(const Case& c, int s, int64_t b) {
+    return __ldg(static_cast<const float*>(c.s.pop) + b + 32 * s);
+  }
+  static __device__ __forceinline__ void stb(const Case& c, int s, int64_t b, float v) {
+    static_cast<float*>(c.s.pop)[b + 32 * s] = v;
+  }
 };
 
 // half storage of the scaled deviation from rest equilibrium: h = f / w - rho0
@@ -80,6 +88,14 @@ struct Pop<true> {
   static __device__ __forceinline__ void st(const Case& c, int s, int64_t cell, float v) {
     const float inv_w = s == 0 ? 3.0f : (s <= 6 ? 18.0f : 36.0f);
     static_cast<__half*>(c.s.pop)[pop_index(c, s, cell)] = __float2half_rn(v * inv_w - c.p.rho0);
+  }
+  static __device__ __forceinline__ float ldb(const Case& c, int s, int64_t b) {
+    const __half h = static_cast<const __half*>(c.s.pop)[b + 32 * s];
+    return lattice_w(s) * (c.p.rho0 + __half2float(h));
+  }
+  static __device__ __forceinline__ void stb(const Case& c, int s, int64_t b, float v) {
+    const float inv_w = s == 0 ? 3.0f : (s <= 6 ? 18.0f : 36.0f);
+    static_cast<__half*>(c.s.pop)[b + 32 * s] = __float2half_rn(v * inv_w - c.p.rho0);
   }
 };
 
@@ -569,10 +585,18 @@ struct DirAcc {
 struct Nbh {
   int rb[3][3];
   int xm, xp, x;
+  int bxm, bxp, bx;  // block-layout indices of xm, xp, x (row 0)
   __device__ __forceinline__ int at(int dx, int dy, int dz) const {
     return rb[dz + 1][dy + 1] + (dx < 0 ? xm : (dx > 0 ? xp : x));
   }
+  // block-layout index of a neighbour when every row starts a 32-cell block
+  // (Case::aligned): row part 19 * rb plus x part, one multiply-add
+  __device__ __forceinline__ int64_t blk(int dx, int dy, int dz) const {
+    return (int64_t)(uint32_t)(rb[dz + 1][dy + 1] * 19 + (dx < 0 ? bxm : (dx > 0 ? bxp : bx)));
+  }
 };
+
+__device__ __forceinline__ int block_index(int i) { return i + (int)((uint32_t)i >> 5) * 576; }
 
 __device__ __forceinline__ void make_nbh(const Case& c, int x, int j, int k, Nbh& n) {
   const int nx = c.s.nx, ny = c.s.ny, nz = c.s.nz;
@@ -585,6 +609,9 @@ __device__ __forceinline__ void make_nbh(const Case& c, int x, int j, int k, Nbh
   n.xm = x == 0 ? nx - 1 : x - 1;
   n.xp = x == nx - 1 ? 0 : x + 1;
   n.x = x;
+  n.bxm = block_index(n.xm);
+  n.bxp = block_index(n.xp);
+  n.bx = block_index(x);
 }
 
 template <bool H>
@@ -708,8 +735,13 @@ __device__ __forceinline__ void lbm_step_tile(const Case& c, int bx, int by, int
       for (int s = 0; s < 19; ++s) F[s] = ldp<H>(c, s, cell);
     } else if (nb == 0) {
       F[0] = ldp<H>(c, 0, cell);
+      if (c.aligned) {
 #pragma unroll
-      for (int s = 1; s < 19; ++s) F[s] = ldp<H>(c, kOpp(s), n.at(-kEx(s), -kEy(s), -kEz(s)));
+        for (int s = 1; s < 19; ++s) F[s] = Pop<H>::ldb(c, kOpp(s), n.blk(-kEx(s), -kEy(s), -kEz(s)));
+      } else {
+#pragma unroll
+        for (int s = 1; s < 19; ++s) F[s] = ldp<H>(c, kOpp(s), n.at(-kEx(s), -kEy(s), -kEz(s)));
+      }
     } else {
       F[0] = ldp<H>(c, 0, cell);
 #pragma unroll
@@ -834,8 +866,13 @@ __device__ __forceinline__ void lbm_step_tile(const Case& c, int bx, int by, int
         for (int s = 0; s < 19; ++s) stp<H>(c, kOpp(s), cell, F[s]);
       } else {
         stp<H>(c, 0, cell, F[0]);
+        if (c.aligned) {
 #pragma unroll
-        for (int s = 1; s < 19; ++s) stp<H>(c, s, n.at(kEx(s), kEy(s), kEz(s)), F[s]);
+          for (int s = 1; s < 19; ++s) Pop<H>::stb(c, s, n.blk(kEx(s), kEy(s), kEz(s)), F[s]);
+        } else {
+#pragma unroll
+          for (int s = 1; s < 19; ++s) stp<H>(c, s, n.at(kEx(s), kEy(s), kEz(s)), F[s]);
+        }
       }
     } else {
       store_near_solid<ODD, H, MOVING>(c, n, cell, nb, rho, F);
@@ -2155,6 +2192,7 @@ static Case make_case(const FsiLbmState* s, const FsiLbmParams* p, const FsiStep
     c.c = FsiStepCtl{0, 0, 0, 0};
   c.K = make_mrt_k(p->s_v, p->s_o);
   c.pf_dist = 0;
+  c.aligned = (s->nx % 32) == 0;
   return c;
 }
 
@@ -2686,6 +2724,7 @@ __device__ __forceinline__ bool stage_case(const FsiBatchCase& bc, Case& sc, boo
     sc.K = make_mrt_k(bc.lp.s_v, bc.lp.s_o);
     sc.pf_dist = 0;
   }
+  if (tid == 0) sc.aligned = (bc.lbm.nx % 32) == 0;
   __syncthreads();
   return true;
 }
