@@ -320,6 +320,11 @@ enum { kSx = 0, kSv = 3, kSC = 6, kSF = 15, kSn = 24 };  // staged particle stat
 enum { kMetaChunks = 0, kMetaRec = 1, kMetaOverflow = 4, kMetaDirty = 5 };
 constexpr int kSeqT = 256;
 constexpr int kTileFloats = (7 * kTileCap + 3) & ~3;  // keeps the payload 16-byte aligned
+// G2P: the staged node velocities use 3 * nv <= 3 * kTileCap floats of the
+// tile; the two stencil halves of a particle meet behind them (12 sums per
+// particle)
+constexpr int kXchOffset = (3 * kTileCap + 3) & ~3;
+static_assert(kXchOffset + 12 * kChunk <= kTileFloats, "G2P exchange does not fit the tile");
 constexpr size_t kSeqSmem = sizeof(float) * (kTileFloats + (kQn + kSn) * kChunk);
 
 struct SeqArgs {
@@ -446,11 +451,49 @@ __device__ __forceinline__ void box_reduce(bool live, const int nb[3], int* s_lo
 
 constexpr int kRun = kChunk / (kSeqT / 32);  // particles per warp in the scatter
 
+// G2P gather of one particle over the stencil offsets o = SUB, SUB + 2, ...
+// (the two halves of the 27 nodes, one per warp of a pair) from the node
+// velocities staged in tile (box bx, nv nodes): the arithmetic of the
+// one-phase g2p_node, with the offsets, weights and offset distances known
+// per offset at compile time and the grid-range test skipped for particles
+// whose whole stencil lies inside the grid.
+template <int SUB>
+__device__ __forceinline__ void g2p_gather_half(const float* tile, int nv, const Box& bx, int G, const BSpline& b,
+                                                float dx, float s4, float* nvl, float* nC) {
+  float dp[3][3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int o = 0; o < 3; ++o) dp[a][o] = ((float)o - b.fx[a]) * dx;
+  const int e0 = bx.ext[0], e01 = bx.ext[0] * bx.ext[1];
+  const int li0 = ((b.base[2] - bx.lo[2]) * bx.ext[1] + (b.base[1] - bx.lo[1])) * bx.ext[0] + (b.base[0] - bx.lo[0]);
+  const bool inside = b.base[0] >= 0 && b.base[0] + 2 < G && b.base[1] >= 0 && b.base[1] + 2 < G &&
+                      b.base[2] >= 0 && b.base[2] + 2 < G;
+#pragma unroll
+  for (int o = SUB; o < 27; o += 2) {
+    const int ox = o / 9, oy = (o / 3) % 3, oz = o % 3;
+    const int I = b.base[0] + ox, Jj = b.base[1] + oy, K = b.base[2] + oz;
+    if (inside || (I >= 0 && I < G && Jj >= 0 && Jj < G && K >= 0 && K < G)) {
+      const int li = li0 + oz * e01 + oy * e0 + ox;
+      const float gv[3] = {tile[li], tile[nv + li], tile[2 * nv + li]};
+      const float dpos[3] = {dp[0][ox], dp[1][oy], dp[2][oz]};
+      const float w = b.w[0][ox] * b.w[1][oy] * b.w[2][oz];
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        nvl[q] += w * gv[q];
+#pragma unroll
+        for (int cc = 0; cc < 3; ++cc) nC[q * 3 + cc] += (w * gv[q]) * dpos[cc] * s4;
+      }
+    }
+  }
+}
+
 // launch A.s of the sequence for the chunks vb, vb + vg, ... (kSeqT threads,
 // kSeqSmem bytes of dynamic shared memory)
 template <bool REACT>
 __device__ __forceinline__ void mpm_seq_body(const SeqArgs& A, int vb, int vg) {
-  constexpr int T = kSeqT, GP = T / kChunk, NW = T / 32;  // G2P: two lanes per particle
+  constexpr int T = kSeqT, NW = T / 32;
+  static_assert(kSeqT == 2 * kChunk, "G2P: two warps per 32 particles, one per stencil half");
   extern __shared__ float4 seq_smem4[];
   // G2P: [3][nv] node velocities; payload: [4][nv] lattice box; scatter: [7][nv] tile
   float* const tile = reinterpret_cast<float*>(seq_smem4);
@@ -522,8 +565,9 @@ __device__ __forceinline__ void mpm_seq_body(const SeqArgs& A, int vb, int vg) {
       const Box bx = load_box(A.box + bg * A.box_stride + 6 * c);
       const bool staged = bx.vol <= kTileCap;
       const int nv = staged ? bx.vol : 0;
-      // this lane's particle, read ahead of the staging barrier
-      const int lp = tid / GP, sub = tid % GP;
+      // this lane's particle, read ahead of the staging barrier: warps 2 i and
+      // 2 i + 1 take particles 32 i .. 32 i + 31, each one half of the stencil
+      const int lp = (wid >> 1) * 32 + lane, sub = wid & 1;
       int p = 0;
       float X[3] = {0.f, 0.f, 0.f}, Fo[9];
 #pragma unroll
@@ -553,49 +597,37 @@ __device__ __forceinline__ void mpm_seq_body(const SeqArgs& A, int vb, int vg) {
         tile[2 * nv + li] = v[2];
       }
       __syncthreads();  // also publishes the s_lo / s_hi reset
-      if (lp < ch.y) {  // uniform over a particle's GP lanes
-        BSpline b;
+      float nvl[3] = {0.f, 0.f, 0.f}, nC[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+      BSpline b;
+      if (lp < ch.y) {
         bspline(X, mp.inv_dx, b);
-        float nvl[3] = {0.f, 0.f, 0.f}, nC[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         if (!staged) {
           if (sub == 0) g2p_gather_global(g, mp, b, nvl, nC);
+        } else if (sub == 0) {
+          g2p_gather_half<0>(tile, nv, bx, G, b, mp.dx, s4, nvl, nC);
         } else {
-#pragma unroll
-          for (int o0 = 0; o0 < 27; o0 += GP) {
-            const int o = o0 + sub;
-            if (o < 27) {
-              const int ox = o / 9, oy = (o / 3) % 3, oz = o % 3;
-              const int I = b.base[0] + ox, Jj = b.base[1] + oy, K = b.base[2] + oz;
-              if (I >= 0 && I < G && Jj >= 0 && Jj < G && K >= 0 && K < G) {
-                const int li = ((K - bx.lo[2]) * bx.ext[1] + (Jj - bx.lo[1])) * bx.ext[0] + (I - bx.lo[0]);
-                const float gv[3] = {tile[li], tile[nv + li], tile[2 * nv + li]};
-                const float dpos[3] = {((float)ox - b.fx[0]) * mp.dx, ((float)oy - b.fx[1]) * mp.dx,
-                                       ((float)oz - b.fx[2]) * mp.dx};
-                const float w = bspline_w(b.fx[0], ox) * bspline_w(b.fx[1], oy) * bspline_w(b.fx[2], oz);
-#pragma unroll
-                for (int q = 0; q < 3; ++q) {
-                  nvl[q] += w * gv[q];
-#pragma unroll
-                  for (int cc = 0; cc < 3; ++cc) nC[q * 3 + cc] += (w * gv[q]) * dpos[cc] * s4;
-                }
-              }
-            }
-          }
+          g2p_gather_half<1>(tile, nv, bx, G, b, mp.dx, s4, nvl, nC);
         }
-        const unsigned grp = ((1u << GP) - 1u) << (lane & ~(GP - 1));
+      }
+      // the odd half's sums to the even half's lanes, through the part of
+      // the tile the staged velocities leave free
+      float* const xch = tile + kXchOffset;
+      if (sub == 1 && lp < ch.y) {
 #pragma unroll
-        for (int w = 1; w < GP; w <<= 1) {
+        for (int q = 0; q < 3; ++q) xch[q * kChunk + lp] = nvl[q];
 #pragma unroll
-          for (int q = 0; q < 3; ++q) nvl[q] += __shfl_xor_sync(grp, nvl[q], w, GP);
+        for (int q = 0; q < 9; ++q) xch[(3 + q) * kChunk + lp] = nC[q];
+      }
+      __syncthreads();
+      if (sub == 0 && lp < ch.y) {
 #pragma unroll
-          for (int q = 0; q < 9; ++q) nC[q] += __shfl_xor_sync(grp, nC[q], w, GP);
-        }
-        if (sub == 0) {
-          g2p_finish_f(pt, p, mp, X, nvl, nC, Fo, do_p2g ? ss : nullptr, kChunk, lp);
+        for (int q = 0; q < 3; ++q) nvl[q] += xch[q * kChunk + lp];
 #pragma unroll
-          for (int r = 0; r < 3; ++r) nb[r] = base_of(X[r], mp.inv_dx);
-          nb_live = true;
-        }
+        for (int q = 0; q < 9; ++q) nC[q] += xch[(3 + q) * kChunk + lp];
+        g2p_finish_f(pt, p, mp, X, nvl, nC, Fo, do_p2g ? ss : nullptr, kChunk, lp);
+#pragma unroll
+        for (int r = 0; r < 3; ++r) nb[r] = base_of(X[r], mp.inv_dx);
+        nb_live = true;
       }
     } else {
       __syncthreads();  // publishes the s_lo / s_hi reset
