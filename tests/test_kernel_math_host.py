@@ -146,3 +146,22 @@ def test_unforced_collision_equals_forced_with_zero_force(hostlib):
         hostlib.host_collide_unforced(P(F), ctypes.c_float(rho), P(u), ctypes.c_float(1 / 0.6),
                                       ctypes.c_float(1.4), P(b))
         np.testing.assert_array_equal(a, b)
+
+
+def test_population_block_order_matches_the_device_index():
+    """pop_blocks (the host writer's conversion) puts population s of cell i
+    at (i / 32) * 608 + s * 32 + i % 32, the element index the kernels use,
+    and i + (i >> 5) * 576 + 32 s is that index in the form the kernels
+    compute it."""
+    import torch
+
+    from mpm_lbm_b200.lbm import pop_blocks
+
+    pitch = 256
+    planes = torch.arange(19 * pitch, dtype=torch.float32).reshape(19, pitch)  # value = s * pitch + i
+    flat = pop_blocks(planes).reshape(-1)
+    for s in (0, 1, 7, 18):
+        for i in (0, 1, 31, 32, 33, 100, 255):
+            idx = (i // 32) * 608 + s * 32 + i % 32
+            assert idx == i + (i >> 5) * 576 + 32 * s
+            assert int(flat[idx]) == s * pitch + i
