@@ -30,7 +30,9 @@
 extern "C" {
 #endif
 
-#define FSI_ABI_VERSION 1
+/* 2: populations in blocks of 32 cells (FsiLbmState.pop), FsiLbmDiag.mn_mass_acc,
+ *    fsi_project_ordered.  1: populations in [19][pitch] planes. */
+#define FSI_ABI_VERSION 2
 
 enum {
   FSI_OK = 0,
@@ -232,7 +234,9 @@ int fsi_mask_rebuild(const FsiLbmState* s, const FsiLbmParams* p, const FsiStepC
  * device allocator).  Limits: nx*ny*nz <= 1048576 cells, else FSI_E_INVALID;
  * all calls on one device share the array, so calls must not overlap in
  * time (order them on one stream); the first call on each device looks the
- * array up (cudaGetSymbolAddress) and should be made outside stream capture. */
+ * array up (cudaGetSymbolAddress) and should be made outside stream capture.
+ * The address is kept for the life of the process: do not call this entry
+ * point after a cudaDeviceReset of that device. */
 int fsi_mask_rebuild_static_scratch(const FsiLbmState* s, const FsiLbmParams* p, const FsiStepCtl* ctl,
                                     float threshold, void* stream);
 
@@ -391,6 +395,30 @@ typedef struct FsiCouplingStats {
  * phi/mass/momentum onto the lattice, normalise + clamp.  stats: device. */
 int fsi_project(const FsiLbmState* s, const FsiParticles* pt, const FsiCouplingParams* cp, FsiCouplingStats* stats,
                 void* stream);
+
+/* The same projection with every cell's sums taken in the reference's order:
+ * particle index ascending, each term added in FP32 with IEEE rounding and no
+ * fused multiply-add (projection.py:39-65 run by one thread, the order a
+ * serial ti.cpu run sums its atomic adds in).  solid_phi, solid_mass and
+ * solid_vel are then bit-identical to that serial sum for the same particle
+ * state and the same on every run, so the solid mask it feeds
+ * (update_dynamic_solid, fluid.py:1847-1861) does not depend on the order of
+ * float atomics even for cells whose phi sits within a few ulps of the
+ * threshold.  fsi_project's float atomics sum in an unspecified order.
+ * Particles are sorted by B-spline base cell over the bounding box of the
+ * base cells; each cell then gathers its contributors (at most 27 base-cell
+ * lists), ranks them by particle index and sums them in rank order. */
+typedef struct FsiProjectScratch {
+  int32_t key_capacity;       /* >= (nx + 2) * (ny + 2) * (nz + 2) */
+  int32_t particle_capacity;  /* >= the particle count */
+  int32_t* count;             /* [key_capacity + 1], zero before the first call; kept zero after each call */
+  int32_t* start;             /* [key_capacity + 1] */
+  int32_t* list;              /* [particle_capacity] particle ids by base cell, ascending within a cell */
+  int32_t* key;               /* [particle_capacity] */
+  int32_t* box;               /* [8] base-cell bounding box of the last call */
+} FsiProjectScratch;
+int fsi_project_ordered(const FsiLbmState* s, const FsiParticles* pt, const FsiCouplingParams* cp,
+                        const FsiProjectScratch* scratch, FsiCouplingStats* stats, void* stream);
 
 /* Reaction transfer LBM -> MPM grid: penalty (coupling/penalty.py:90-129),
  * engineering (moving_boundary.py:58-110) or link-area (link_area.py:84-193,

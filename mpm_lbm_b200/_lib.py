@@ -12,6 +12,9 @@ import threading
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "libfsi_b200.so")
+# FSI_ABI_VERSION of include/fsi_b200.h.  2: populations stored in blocks of 32
+# cells, FsiLbmDiag with the FP64 mass-neutral sum, fsi_project_ordered.
+ABI_VERSION = 2
 
 c_i32, c_i64, c_f32, c_f64, c_p = ctypes.c_int32, ctypes.c_int64, ctypes.c_float, ctypes.c_double, ctypes.c_void_p
 
@@ -90,6 +93,11 @@ class FsiMpmBins(ctypes.Structure):
                 ("perm", c_p), ("chunk", c_p), ("box", c_p), ("meta", c_p)]
 
 
+class FsiProjectScratch(ctypes.Structure):
+    _fields_ = [("key_capacity", c_i32), ("particle_capacity", c_i32), ("count", c_p), ("start", c_p),
+                ("list", c_p), ("key", c_p), ("box", c_p)]
+
+
 class FsiMpmParams(ctypes.Structure):
     _fields_ = [("dx", c_f32), ("inv_dx", c_f32), ("dt", c_f32), ("mu", c_f32), ("la", c_f32),
                 ("gravity", c_f32 * 3), ("damping", c_f32), ("bound", c_i32), ("lock_z", c_i32), ("pad", c_i32)]
@@ -158,6 +166,7 @@ STRUCTS = {
     "FsiBatchCase": FsiBatchCase, "FsiBatchDims": FsiBatchDims, "FsiCampaignSums": FsiCampaignSums,
     "FsiPlaneStats": FsiPlaneStats, "FsiFieldStatsArgs": FsiFieldStatsArgs,
     "FsiWallVelocityStats": FsiWallVelocityStats,
+    "FsiProjectScratch": FsiProjectScratch,
 }
 
 # entry point -> argtypes (all return int)
@@ -178,6 +187,8 @@ SIGNATURES = {
     "fsi_field_stats_arrays": [c_i32, c_i32, c_i32, _P(FsiFieldStatsArgs), c_p, c_p],
     "fsi_apply_wall_velocity": [_P(FsiLbmState), c_p, c_i32, c_f64, c_p, c_p],
     "fsi_project": [_P(FsiLbmState), _P(FsiParticles), _P(FsiCouplingParams), c_p, c_p],
+    "fsi_project_ordered": [_P(FsiLbmState), _P(FsiParticles), _P(FsiCouplingParams), _P(FsiProjectScratch), c_p,
+                            c_p],
     "fsi_reaction_to_grid": [_P(FsiLbmState), c_p, _P(FsiParticles), _P(FsiGrid), _P(FsiCouplingParams), c_p, c_p],
     "fsi_mpm_p2g": [_P(FsiParticles), _P(FsiGrid), _P(FsiMpmParams), c_p],
     "fsi_mpm_grid_update": [_P(FsiGrid), _P(FsiMpmParams), c_p],
@@ -220,7 +231,7 @@ def load():
             fn = getattr(lib, name)
             fn.argtypes = args
             fn.restype = RESTYPES.get(name, ctypes.c_int)
-        if lib.fsi_abi_version() != 1:
+        if lib.fsi_abi_version() != ABI_VERSION:
             raise FsiError("libfsi_b200.so ABI version mismatch")
         _lib = lib
         return lib

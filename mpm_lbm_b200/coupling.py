@@ -9,7 +9,7 @@ import ctypes
 import numpy as np
 import torch
 
-from ._lib import FsiCouplingParams, FsiCouplingStats, call, ptr, stream_handle
+from ._lib import FsiCouplingParams, FsiCouplingStats, FsiProjectScratch, call, ptr, stream_handle
 
 AREA_POLICIES = ("uniform", "inverse_length", "length")
 
@@ -71,10 +71,43 @@ class MPMToLBMProjector3D:
         self.eps_mass = 1.0e-12
         self.params = _base_params(sim_config)
         self.stats = _StatsBuffer(device if device is not None else "cuda")
+        self._scratch = None
+        self._scratch_t = None
+
+    def _ordered_scratch(self, lbm, solid):
+        """Device scratch of fsi_project_ordered, allocated on first use (the
+        driver's first FSI step runs eagerly, before any graph capture)."""
+        keys = (lbm.nx + 2) * (lbm.ny + 2) * (lbm.nz + 2)
+        n = int(solid.n_particles)
+        sc = self._scratch
+        if sc is None or sc.key_capacity < keys or sc.particle_capacity < n:
+            dev = lbm.device
+            t = {"count": torch.zeros(keys + 1, dtype=torch.int32, device=dev),
+                 "start": torch.empty(keys + 1, dtype=torch.int32, device=dev),
+                 "list": torch.empty(max(n, 1), dtype=torch.int32, device=dev),
+                 "key": torch.empty(max(n, 1), dtype=torch.int32, device=dev),
+                 "box": torch.empty(8, dtype=torch.int32, device=dev)}
+            sc = FsiProjectScratch()
+            sc.key_capacity, sc.particle_capacity = keys, n
+            for k, v in t.items():
+                setattr(sc, k, v.data_ptr())
+            self._scratch, self._scratch_t = sc, t
+        return sc
 
     def project(self, solid, lbm, clear=True):
+        """projection.py:21-97 with every cell's sums in particle order
+        (fsi_project_ordered): the same bits as a serial run of the
+        reference's loop, on every run."""
         if not clear:
             raise NotImplementedError("projection without clearing is not supported")
+        sc = self._ordered_scratch(lbm, solid)
+        call("fsi_project_ordered", ctypes.byref(lbm.state), ctypes.byref(solid.particles),
+             ctypes.byref(self.params), ctypes.byref(sc), self.stats.ptr(), stream_handle())
+        lbm._version += 1
+
+    def project_unordered(self, solid, lbm):
+        """The same projection with float atomics (fsi_project): the sums'
+        order, and so their last bits, vary from run to run."""
         call("fsi_project", ctypes.byref(lbm.state), ctypes.byref(solid.particles), ctypes.byref(self.params),
              self.stats.ptr(), stream_handle())
         lbm._version += 1

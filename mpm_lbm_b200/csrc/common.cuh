@@ -14,6 +14,8 @@ namespace fsi {
 void set_error(const std::string& msg);
 // counts kernel launches issued through this library (see fsi_launch_count)
 void count_launch();
+// SMs of the current device (148 on B200; queried once per device)
+int device_sm_count();
 
 inline int cuda_check(cudaError_t e, const char* what) {
   if (e == cudaSuccess) return FSI_OK;

@@ -592,7 +592,8 @@ struct Nbh {
   // block-layout index of a neighbour when every row starts a 32-cell block
   // (Case::aligned): row part 19 * rb plus x part, one multiply-add
   __device__ __forceinline__ int64_t blk(int dx, int dy, int dz) const {
-    return (int64_t)(uint32_t)(rb[dz + 1][dy + 1] * 19 + (dx < 0 ? bxm : (dx > 0 ? bxp : bx)));
+    // unsigned arithmetic: 19 * row base reaches 2^32 (the host bounds 19 * pitch by 2^32)
+    return (int64_t)((uint32_t)rb[dz + 1][dy + 1] * 19u + (uint32_t)(dx < 0 ? bxm : (dx > 0 ? bxp : bx)));
   }
 };
 
@@ -2196,17 +2197,7 @@ static Case make_case(const FsiLbmState* s, const FsiLbmParams* p, const FsiStep
   return c;
 }
 
-static int lbm_sm_count() {
-  static int cached[64] = {0};
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
-  if (!cached[dev]) {
-    int n = 0;
-    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
-    cached[dev] = n;
-  }
-  return cached[dev];
-}
+static int lbm_sm_count() { return device_sm_count(); }
 
 static inline unsigned blocks_for(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
@@ -2540,7 +2531,7 @@ extern "C" int fsi_mask_rebuild(const FsiLbmState* s, const FsiLbmParams* p, con
   const int64_t n = (int64_t)s->nx * s->ny * s->nz;
   k_mask_update<<<blocks_for(n, 256), 256, 0, st>>>(c, threshold);
   if ((rc = launch_check("k_mask_update"))) return rc;
-  const unsigned g = 148 * 4;
+  const unsigned g = (unsigned)lbm_sm_count() * 4;
   if (s->store_fp16)
     k_relink<true><<<g, 128, 0, st>>>(c);
   else
@@ -2883,7 +2874,7 @@ extern "C" int fsi_batch_mask_rebuild(FsiBatchCase* cases, const FsiBatchDims* d
   if ((rc = launch_check("k_batch_ctl"))) return rc;
   k_batch_mask_update<<<dim3(batch_x(d->max_cells, 256, 1 << 20), d->n_cases), 256, 0, st>>>(cases);
   if ((rc = launch_check("k_batch_mask_update"))) return rc;
-  const dim3 g2(std::max(1, 148 * 4 / std::max(1, d->n_cases)), d->n_cases);
+  const dim3 g2(std::max(1, lbm_sm_count() * 4 / std::max(1, d->n_cases)), d->n_cases);
   if (d->store_fp16)
     k_batch_relink<true><<<g2, 128, 0, st>>>(cases);
   else

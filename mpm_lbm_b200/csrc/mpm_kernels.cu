@@ -14,6 +14,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 
 #include "common.cuh"
@@ -101,6 +102,317 @@ __global__ void k_project_normalize(LatView L, FsiCouplingParams cp, float* phi,
                                     FsiCouplingStats* st) {
   project_normalize_warp(L, cp, phi, smass, svel, st,
                          (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31));
+}
+
+// ------------------------------------- projection in particle order ----
+// projection.py:39-65 adds, for particle p = 0, 1, ... and its 27 stencil
+// offsets, w * vol / cell_volume, w * m and w * m * v to the cells; a serial
+// run sums every cell's terms in ascending p.  Here particles are sorted by
+// B-spline base cell (a counting sort over the bounding box of the base cells,
+// each base cell's list then ordered by p), and one warp per cell collects the
+// contributors of its <= 27 base cells, ranks them by p and sums the terms in
+// that order with IEEE FP32 adds.  The term arithmetic is written with
+// explicit round-to-nearest operations, so no multiply-add is contracted and
+// every term is the one a serial FP32 run computes.
+//
+// scratch->box: [0..2] max(-base), [3..5] max(base) over the particles whose
+// base cell touches the lattice (base in [-2, dim - 1] on each axis); a memset
+// of 0x80 bytes (INT_MIN-like) is the empty box.
+
+struct OrdBase {
+  int b[3];
+  float fx[3];
+};
+
+__device__ __forceinline__ OrdBase ordered_base(const FsiParticles& pt, int p, float inv_dx) {
+  OrdBase o;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const float Xp = __fmul_rn(pt.x[a * pt.n + p], inv_dx);
+    o.b[a] = (int)__fsub_rn(Xp, 0.5f);
+    o.fx[a] = __fsub_rn(Xp, (float)o.b[a]);
+  }
+  return o;
+}
+
+__device__ __forceinline__ bool ordered_base_touches(const LatView& L, const OrdBase& o) {
+  return o.b[0] >= -2 && o.b[0] < L.nx && o.b[1] >= -2 && o.b[1] < L.ny && o.b[2] >= -2 && o.b[2] < L.nz;
+}
+
+// quadratic B-spline weight of offset d for fractional position f, in the
+// reference's evaluation order (solid.py:222-230 / projection.py:45-47)
+__device__ __forceinline__ float ordered_w(float f, int d) {
+  if (d == 0) {
+    const float t = __fsub_rn(1.5f, f);
+    return __fmul_rn(__fmul_rn(0.5f, t), t);
+  }
+  if (d == 1) {
+    const float t = __fsub_rn(f, 1.0f);
+    return __fsub_rn(0.75f, __fmul_rn(t, t));
+  }
+  const float t = __fsub_rn(f, 0.5f);
+  return __fmul_rn(__fmul_rn(0.5f, t), t);
+}
+
+struct OrdBox {
+  int lo[3], hi[3], ext[3];
+  int64_t keys;
+};
+
+__device__ __forceinline__ OrdBox ordered_box(const int32_t* box) {
+  OrdBox B;
+  int64_t k = 1;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    B.lo[a] = -box[a];
+    B.hi[a] = box[3 + a];
+    B.ext[a] = B.hi[a] >= B.lo[a] ? B.hi[a] - B.lo[a] + 1 : 0;
+    k *= B.ext[a];
+  }
+  B.keys = k;
+  return B;
+}
+
+__global__ void k_po_box(LatView L, FsiParticles pt, float inv_dx, int32_t* __restrict__ box) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  int v[6];
+#pragma unroll
+  for (int a = 0; a < 6; ++a) v[a] = INT_MIN;
+  if (p < pt.n) {
+    const OrdBase o = ordered_base(pt, p, inv_dx);
+    if (ordered_base_touches(L, o)) {
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        v[a] = -o.b[a];
+        v[3 + a] = o.b[a];
+      }
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < 6; ++a) {
+#pragma unroll
+    for (int s = 16; s > 0; s >>= 1) v[a] = max(v[a], __shfl_xor_sync(0xffffffffu, v[a], s));
+  }
+  if ((threadIdx.x & 31) == 0 && v[3] != INT_MIN) {
+#pragma unroll
+    for (int a = 0; a < 6; ++a) atomicMax(box + a, v[a]);
+  }
+}
+
+__device__ __forceinline__ int ordered_key(const OrdBox& B, const int b[3]) {
+  return ((b[2] - B.lo[2]) * B.ext[1] + (b[1] - B.lo[1])) * B.ext[0] + (b[0] - B.lo[0]);
+}
+
+__global__ void k_po_count(LatView L, FsiParticles pt, float inv_dx, const int32_t* __restrict__ box,
+                           int32_t* __restrict__ key, int32_t* __restrict__ count) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= pt.n) return;
+  const OrdBox B = ordered_box(box);
+  const OrdBase o = ordered_base(pt, p, inv_dx);
+  int k = -1;
+  if (ordered_base_touches(L, o)) {
+    k = ordered_key(B, o.b);
+    atomicAdd(count + k, 1);
+  }
+  key[p] = k;
+}
+
+// one CTA: exclusive scan of count[0, keys) into start[0, keys], count zeroed
+constexpr int kPoScanT = 1024;
+__global__ __launch_bounds__(kPoScanT) void k_po_scan(const int32_t* __restrict__ box, int32_t* __restrict__ count,
+                                                      int32_t* __restrict__ start) {
+  __shared__ int s_w[kPoScanT / 32];
+  const OrdBox B = ordered_box(box);
+  const int nk = (int)B.keys;
+  const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
+  const int per = (nk + kPoScanT - 1) / kPoScanT;
+  const int k0 = min(t * per, nk), k1 = min(k0 + per, nk);
+  int sum = 0;
+  for (int k = k0; k < k1; ++k) sum += count[k];
+  int inc = sum;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += y;
+  }
+  if (lane == 31) s_w[wid] = inc;
+  __syncthreads();
+  if (wid == 0) {
+    const int a0 = s_w[lane];
+    int a = a0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, a, o);
+      if (lane >= o) a += y;
+    }
+    s_w[lane] = a - a0;
+  }
+  __syncthreads();
+  int off = s_w[wid] + inc - sum;
+  for (int k = k0; k < k1; ++k) {
+    const int c = count[k];
+    start[k] = off;
+    count[k] = 0;
+    off += c;
+  }
+  if (t == kPoScanT - 1) start[nk] = off;
+}
+
+__global__ void k_po_fill(int n, const int32_t* __restrict__ key, const int32_t* __restrict__ start,
+                          int32_t* __restrict__ cursor, int32_t* __restrict__ list) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const int k = key[p];
+  if (k >= 0) list[start[k] + atomicAdd(cursor + k, 1)] = p;
+}
+
+// orders each base cell's list by particle id and leaves count zero
+__global__ void k_po_sort(const int32_t* __restrict__ box, const int32_t* __restrict__ start,
+                          int32_t* __restrict__ count, int32_t* __restrict__ list) {
+  const int64_t nk = ordered_box(box).keys;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nk; k += (int64_t)gridDim.x * blockDim.x) {
+    const int s = start[k], e = start[k + 1];
+    if (e - s > 1) {
+      for (int i = s + 1; i < e; ++i) {
+        const int v = list[i];
+        int j = i - 1;
+        while (j >= s && list[j] > v) {
+          list[j + 1] = list[j];
+          --j;
+        }
+        list[j + 1] = v;
+      }
+    }
+    if (e > s) count[k] = 0;
+  }
+}
+
+// the five terms particle p adds to the cell at offset d from its base cell
+__device__ __forceinline__ void ordered_terms(const FsiParticles& pt, const FsiCouplingParams& cp, int p,
+                                              const OrdBase& o, const int d[3], float t[5]) {
+  const int n = pt.n;
+  const float w = __fmul_rn(__fmul_rn(ordered_w(o.fx[0], d[0]), ordered_w(o.fx[1], d[1])), ordered_w(o.fx[2], d[2]));
+  const float J = fmaxf(pt.Jp[p], 0.0f);
+  const float cur_vol = __fmul_rn(pt.vol0[p], J);
+  const float mc = __fmul_rn(w, pt.mass[p]);
+  t[0] = __fdiv_rn(__fmul_rn(w, cur_vol), cp.cell_volume_norm);
+  t[1] = mc;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) t[2 + a] = __fmul_rn(mc, __fmul_rn(pt.v[a * n + p], cp.vel_scale));
+}
+
+constexpr int kPoWarps = 4;
+constexpr int kPoCap = 504;             // contributors per cell ranked in shared memory
+constexpr int kPoStride = kPoCap + 1;   // term rows on distinct banks
+
+__global__ __launch_bounds__(32 * kPoWarps) void k_po_gather(LatView L, FsiParticles pt, FsiCouplingParams cp,
+                                                             const int32_t* __restrict__ box,
+                                                             const int32_t* __restrict__ start,
+                                                             const int32_t* __restrict__ list, float* __restrict__ phi,
+                                                             float* __restrict__ smass, float* __restrict__ svel) {
+  __shared__ int s_cand[kPoWarps][kPoCap];
+  __shared__ float s_term[kPoWarps][5 * kPoStride];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int* cand = s_cand[wid];
+  float* term = s_term[wid];
+  const OrdBox B = ordered_box(box);
+  if (B.keys == 0) return;
+  // cells reached from the box: [lo, hi + 2] clipped to the lattice
+  int clo[3], cext[3];
+  const int dims[3] = {L.nx, L.ny, L.nz};
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    clo[a] = max(B.lo[a], 0);
+    cext[a] = max(min(B.hi[a] + 2, dims[a] - 1) - clo[a] + 1, 0);
+  }
+  const int64_t ncell = (int64_t)cext[0] * cext[1] * cext[2];
+  // lane l < 27 owns stencil offset d = (l / 9, l / 3 % 3, l % 3): base cell = cell - d
+  const int d[3] = {lane / 9, (lane / 3) % 3, lane % 3};
+  for (int64_t q = (int64_t)blockIdx.x * kPoWarps + wid; q < ncell; q += (int64_t)gridDim.x * kPoWarps) {
+    const int ci = clo[0] + (int)(q % cext[0]);
+    const int cj = clo[1] + (int)((q / cext[0]) % cext[1]);
+    const int ck = clo[2] + (int)(q / ((int64_t)cext[0] * cext[1]));
+    const int b[3] = {ci - d[0], cj - d[1], ck - d[2]};
+    int s = 0, len = 0;
+    if (lane < 27 && b[0] >= B.lo[0] && b[0] <= B.hi[0] && b[1] >= B.lo[1] && b[1] <= B.hi[1] && b[2] >= B.lo[2] &&
+        b[2] <= B.hi[2]) {
+      const int k = ordered_key(B, b);
+      s = start[k];
+      len = start[k + 1] - s;
+    }
+    int off = len;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, off, o);
+      if (lane >= o) off += y;
+    }
+    const int K = __shfl_sync(0xffffffffu, off, 31);
+    off -= len;
+    if (K == 0) continue;
+    const int64_t c = lat_cell(L, ci, cj, ck);
+    float acc = 0.f;  // lane v < 5: running sum of term v
+    if (K <= kPoCap) {
+      for (int i = 0; i < len; ++i) cand[off + i] = list[s + i];
+      __syncwarp();
+      for (int i = lane; i < K; i += 32) {
+        const int p = cand[i];
+        int rank = 0;
+        for (int j = 0; j < K; ++j) rank += cand[j] < p;
+        const OrdBase o = ordered_base(pt, p, cp.inv_dx_norm);
+        const int dd[3] = {ci - o.b[0], cj - o.b[1], ck - o.b[2]};
+        float t[5];
+        ordered_terms(pt, cp, p, o, dd, t);
+#pragma unroll
+        for (int v = 0; v < 5; ++v) term[v * kPoStride + rank] = t[v];
+      }
+      __syncwarp();
+      if (lane < 5)
+        for (int r = 0; r < K; ++r) acc = __fadd_rn(acc, term[lane * kPoStride + r]);
+      __syncwarp();
+    } else {
+      // more contributors than the shared ranking holds: lane 0 merges the 27
+      // sorted base-cell lists (heads and ends staged in cand), kPoCap terms at
+      // a time, and lanes 0-4 continue their sums over each batch
+      if (lane < 27) {
+        cand[lane] = s;
+        cand[27 + lane] = s + len;
+      }
+      __syncwarp();
+      for (int done = 0; done < K; done += kPoCap) {
+        const int m = min(kPoCap, K - done);
+        if (lane == 0) {
+          for (int r = 0; r < m; ++r) {
+            int best = INT_MAX, bl = 0;
+            for (int l = 0; l < 27; ++l) {
+              const int h = cand[l];
+              if (h < cand[27 + l]) {
+                const int v = list[h];
+                if (v < best) {
+                  best = v;
+                  bl = l;
+                }
+              }
+            }
+            cand[bl] += 1;
+            const OrdBase o = ordered_base(pt, best, cp.inv_dx_norm);
+            const int dd[3] = {ci - o.b[0], cj - o.b[1], ck - o.b[2]};
+            float t[5];
+            ordered_terms(pt, cp, best, o, dd, t);
+#pragma unroll
+            for (int v = 0; v < 5; ++v) term[v * kPoStride + r] = t[v];
+          }
+        }
+        __syncwarp();
+        if (lane < 5)
+          for (int r = 0; r < m; ++r) acc = __fadd_rn(acc, term[lane * kPoStride + r]);
+        __syncwarp();
+      }
+    }
+    if (lane < 5) {
+      float* dst = lane == 0 ? phi + c : (lane == 1 ? smass + c : svel + (int64_t)(lane - 2) * L.pitch + c);
+      *dst = acc;
+    }
+  }
 }
 
 // ------------------------------------------------------------ reaction ----
@@ -275,6 +587,47 @@ extern "C" int fsi_project(const FsiLbmState* s, const FsiParticles* pt, const F
   const LatView L{s->nx, s->ny, s->nz, P};
   k_project_scatter<<<nblk(pt->n, 128), 128, 0, st>>>(L, *pt, *cp, s->phi, s->smass, s->svel);
   if ((rc = launch_check("k_project_scatter"))) return rc;
+  const int64_t n = (int64_t)s->nx * s->ny * s->nz;
+  k_project_normalize<<<nblk(n, 256), 256, 0, st>>>(L, *cp, s->phi, s->smass, s->svel, stats);
+  return launch_check("k_project_normalize");
+}
+
+extern "C" int fsi_project_ordered(const FsiLbmState* s, const FsiParticles* pt, const FsiCouplingParams* cp,
+                                   const FsiProjectScratch* sc, FsiCouplingStats* stats, void* stream) {
+  if (!s || !cp || !sc || !stats) return invalid("null argument");
+  int rc = check_particles(pt);
+  if (rc) return rc;
+  if (!s->phi || !s->smass || !s->svel) return invalid("projection needs phi, smass, svel");
+  if (!sc->count || !sc->start || !sc->list || !sc->key || !sc->box) return invalid("null projection scratch array");
+  const int64_t keys = (int64_t)(s->nx + 2) * (s->ny + 2) * (s->nz + 2);
+  if (keys > INT_MAX - 1) return invalid("lattice too large for the ordered projection");
+  if (sc->key_capacity < keys) return invalid("scratch key_capacity below (nx + 2) * (ny + 2) * (nz + 2)");
+  if (sc->particle_capacity < pt->n) return invalid("scratch particle_capacity below the particle count");
+  cudaStream_t st = (cudaStream_t)stream;
+  const int64_t P = s->pitch;
+  if ((rc = cuda_check(cudaMemsetAsync(s->phi, 0, sizeof(float) * P, st), "clear phi"))) return rc;
+  if ((rc = cuda_check(cudaMemsetAsync(s->smass, 0, sizeof(float) * P, st), "clear smass"))) return rc;
+  if ((rc = cuda_check(cudaMemsetAsync(s->svel, 0, sizeof(float) * 3 * P, st), "clear svel"))) return rc;
+  if ((rc = cuda_check(cudaMemsetAsync(stats, 0, offsetof(FsiCouplingStats, active_reaction_particle_count), st),
+                       "clear projection stats")))
+    return rc;
+  if ((rc = cuda_check(cudaMemsetAsync(sc->box, 0x80, 6 * sizeof(int32_t), st), "clear projection box"))) return rc;
+  const LatView L{s->nx, s->ny, s->nz, P};
+  const float inv_dx = cp->inv_dx_norm;
+  const int sms = device_sm_count();
+  k_po_box<<<nblk(pt->n, 256), 256, 0, st>>>(L, *pt, inv_dx, sc->box);
+  if ((rc = launch_check("k_po_box"))) return rc;
+  k_po_count<<<nblk(pt->n, 256), 256, 0, st>>>(L, *pt, inv_dx, sc->box, sc->key, sc->count);
+  if ((rc = launch_check("k_po_count"))) return rc;
+  k_po_scan<<<1, kPoScanT, 0, st>>>(sc->box, sc->count, sc->start);
+  if ((rc = launch_check("k_po_scan"))) return rc;
+  k_po_fill<<<nblk(pt->n, 256), 256, 0, st>>>(pt->n, sc->key, sc->start, sc->count, sc->list);
+  if ((rc = launch_check("k_po_fill"))) return rc;
+  k_po_sort<<<sms * 2, 256, 0, st>>>(sc->box, sc->start, sc->count, sc->list);
+  if ((rc = launch_check("k_po_sort"))) return rc;
+  k_po_gather<<<sms * 8, 32 * kPoWarps, 0, st>>>(L, *pt, *cp, sc->box, sc->start, sc->list, s->phi, s->smass,
+                                                 s->svel);
+  if ((rc = launch_check("k_po_gather"))) return rc;
   const int64_t n = (int64_t)s->nx * s->ny * s->nz;
   k_project_normalize<<<nblk(n, 256), 256, 0, st>>>(L, *cp, s->phi, s->smass, s->svel, stats);
   return launch_check("k_project_normalize");

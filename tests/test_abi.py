@@ -32,7 +32,7 @@ def test_every_declared_symbol_is_exported_and_bound(lib):
     for name in names:
         assert hasattr(lib, name), name
         assert name in _lib.SIGNATURES, name
-    assert lib.fsi_abi_version() == 1
+    assert lib.fsi_abi_version() == _lib.ABI_VERSION == 2
     # no kernel has run in this process without a GPU
     assert _lib.launch_count() == 0
 

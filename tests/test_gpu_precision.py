@@ -70,3 +70,47 @@ def test_storage_form_against_fp64_oracle(storage, tune, fp64_reference):
     assert tip_err <= tip_tol
     # the FP16 deviation storage keeps the mass exactly representable at rest
     assert rho_err < 1e-3
+
+
+# ---- the same targets at the benchmark's size ------------------------------
+# 128 x 64 x 64 duct, plate 2 x 32 x 48 cells (24,576 particles), tau 0.55,
+# u_x = 0.05, S = 120 and M = 40 substeps per FSI step, 3 FSI steps (360 LBM
+# steps), replayed as a CUDA graph as the benchmark runs it.
+BENCH_FSI_STEPS = 3
+
+
+@pytest.fixture(scope="module")
+def fp64_reference_bench():
+    import os
+
+    from mpm_lbm_b200.cases import DuctPlateCase
+
+    case = DuctPlateCase(lattice=(128, 64, 64), tau=0.55, u_in=0.05, plate=(2, 32, 48))
+    drv = orc.fsi_driver_for_case(case, dtype=np.float64, threads=os.cpu_count() or 1)
+    for _ in range(BENCH_FSI_STEPS):
+        drv.step_once()
+    _, parts = case.geometry()
+    tip = parts["free_tip"].astype(bool)
+    disp = (drv.solid.x[tip] - parts["x"][tip].astype(np.float64)).mean(axis=0)
+    return case, {"v": drv.lbm.v.astype(np.float64), "fluid": drv.lbm.solid == 0, "tip": disp}
+
+
+@pytest.mark.parametrize("storage", ["fp32", "fp16"])
+def test_storage_form_at_benchmark_size(storage, fp64_reference_bench):
+    import torch
+
+    case, ref = fp64_reference_bench
+    drv = case.make_driver(storage=storage, graph=True)
+    drv.lbm.tune = 1
+    for _ in range(BENCH_FSI_STEPS):
+        drv.step_once()
+    torch.cuda.synchronize()
+    v = drv.lbm.v.to_numpy().astype(np.float64)
+    fluid = (drv.lbm.solid.to_numpy() == 0) & ref["fluid"]
+    v_err = np.linalg.norm(v[fluid] - ref["v"][fluid]) / np.linalg.norm(ref["v"][fluid])
+    tip = drv.flap_tip_displacement().cpu().numpy()
+    tip_err = np.linalg.norm(tip - ref["tip"]) / np.linalg.norm(ref["tip"])
+    print(f"{storage} 128x64x64: velocity rel L2 {v_err:.3e}, flap-tip displacement rel {tip_err:.3e}")
+    v_tol, tip_tol = TARGETS[storage]
+    assert v_err <= v_tol
+    assert tip_err <= tip_tol

@@ -1,7 +1,10 @@
 """fsi_mask_rebuild_static_scratch (the mask rebuild whose changed-cell list
 lives in the library's own device array) against fsi_mask_rebuild with a
 caller-provided change_list: two twin lattices, two consecutive rebuilds with
-a moving solid-fraction blob, both called through the C ABI."""
+a moving solid-fraction blob, both called through the C ABI.  The twin that
+uses the built-in list is handed a state whose change_list is NULL, so the
+caller's buffer cannot be what makes it work, and the device's free memory is
+the same before and after its second call."""
 
 import ctypes
 
@@ -41,11 +44,15 @@ def _blob(center, radius):
     return np.clip(radius + 0.5 - d, 0.0, 1.0).astype(np.float32)
 
 
-def _rebuild(lbm, name, threshold=0.5):
-    from mpm_lbm_b200._lib import call
+def _rebuild(lbm, name, threshold=0.5, no_scratch=False):
+    from mpm_lbm_b200._lib import FsiLbmState, call
 
     lbm.flush_open_boundary()
-    call(name, ctypes.byref(lbm.state), ctypes.byref(lbm.params), ctypes.byref(lbm._ctl()), ctypes.c_float(threshold),
+    state = lbm.state
+    if no_scratch:
+        state = FsiLbmState.from_buffer_copy(lbm.state)
+        state.change_list = None
+    call(name, ctypes.byref(state), ctypes.byref(lbm.params), ctypes.byref(lbm._ctl()), ctypes.c_float(threshold),
          lbm._stream())
     lbm._old_equals_solid = False
     lbm._version += 1
@@ -61,15 +68,22 @@ def _compare(a, b):
 
 
 def test_static_scratch_rebuild_matches_caller_scratch():
+    import torch
+
     a, b = _lattice(), _lattice()
     _compare(a, b)
     changes = []
-    for center, radius in (((14, 12, 10), 5.0), ((17, 12, 10), 6.0)):
+    for call_no, (center, radius) in enumerate((((14, 12, 10), 5.0), ((17, 12, 10), 6.0))):
         phi = _blob(center, radius)
         for lbm in (a, b):
             lbm.solid_phi.from_numpy(phi)
         _rebuild(a, "fsi_mask_rebuild")
-        _rebuild(b, "fsi_mask_rebuild_static_scratch")
+        torch.cuda.synchronize()
+        free_before = torch.cuda.mem_get_info()[0]
+        _rebuild(b, "fsi_mask_rebuild_static_scratch", no_scratch=True)
+        torch.cuda.synchronize()
+        if call_no == 1:  # the first call looked the array up; the second must not allocate at all
+            assert torch.cuda.mem_get_info()[0] == free_before
         _compare(a, b)
         changes.append(a._diag().change_count)
         for lbm in (a, b):
