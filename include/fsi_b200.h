@@ -268,6 +268,12 @@ typedef struct FsiCampaignSums {
 } FsiCampaignSums;
 int fsi_campaign_sums(const FsiLbmState* s, const FsiLbmParams* p, const FsiStepCtl* ctl, const uint8_t* regions,
                       FsiCampaignSums* out, void* stream);
+/* The same sums from plain device fields in lattice order (x fastest,
+ * n = nx * ny * nz): rho [n], vel [3][n], pop [19][n] (NULL: no population
+ * check), solid [n] (non-zero: solid) -- the host copies _copy_lbm_fields
+ * makes (official_subcycled_flow_solver.py:352-365), held on the device. */
+int fsi_campaign_sums_arrays(int32_t nx, int32_t ny, int32_t nz, const float* rho, const float* vel, const float* pop,
+                             const uint8_t* solid, const uint8_t* regions, FsiCampaignSums* out, void* stream);
 
 /* Per-x-plane statistics of the lattice fields, one device pass.  The
  * reference's diagnostics (sim/diagnostics/lbm_boundary_diagnostics.py,
@@ -446,14 +452,14 @@ int fsi_mpm_g2p(const FsiParticles* pt, const FsiGrid* g, const FsiMpmParams* mp
  *     B-spline base cell, and within a block by base cell, and cuts every bin
  *     into chunks of at most FSI_BIN_CHUNK particles (bins may go stale
  *     between calls: that costs speed only);
- *   - fsi_mpm_substeps_binned runs substeps chunk by chunk: each chunk is
- *     scattered into a shared-memory tile covering its stencil box and the
+ *   - fsi_mpm_substeps_binned runs substeps chunk by chunk, one warp per
+ *     chunk: each chunk is scattered into a shared-memory tile covering its stencil box and the
  *     tile is flushed with one atomic per touched node value; the gather
  *     evaluates the grid update per node while staging the chunk's box.  A
  *     substep leaves momentum (not velocity), mass and f_ext in its grid
  *     buffer; three buffers rotate, and only the boxes recorded for a buffer
  *     are zeroed before it is reused, so no dense pass over the grid is made. */
-#define FSI_BIN_CHUNK 128
+#define FSI_BIN_CHUNK 32
 #define FSI_BIN_EDGE 8
 
 /* count, start and chunk must be 16-byte aligned */

@@ -24,6 +24,7 @@ FSI_TUNE_LBM_OCC3, FSI_TUNE_LBM_OCC4, FSI_TUNE_LBM_PAIR, FSI_TUNE_LBM_OCC3_PF, F
 
 
 FSI_CAMPAIGN_REGIONS = 8
+FSI_BIN_CHUNK, FSI_BIN_EDGE = 32, 8  # particles per chunk of a bin, bin edge in cells
 
 
 class FsiCampaignSums(ctypes.Structure):
@@ -183,6 +184,7 @@ SIGNATURES = {
     "fsi_force_accum_finalize": [_P(FsiLbmState), _P(FsiStepCtl), c_i32, c_p],
     "fsi_lbm_readout": [_P(FsiLbmState), _P(FsiLbmParams), _P(FsiStepCtl), c_p, c_p, c_p, c_p],
     "fsi_campaign_sums": [_P(FsiLbmState), _P(FsiLbmParams), _P(FsiStepCtl), c_p, c_p, c_p],
+    "fsi_campaign_sums_arrays": [c_i32, c_i32, c_i32, c_p, c_p, c_p, c_p, c_p, c_p, c_p],
     "fsi_lbm_field_stats": [_P(FsiLbmState), _P(FsiLbmParams), _P(FsiStepCtl), _P(FsiFieldStatsArgs), c_p, c_p],
     "fsi_field_stats_arrays": [c_i32, c_i32, c_i32, _P(FsiFieldStatsArgs), c_p, c_p],
     "fsi_apply_wall_velocity": [_P(FsiLbmState), c_p, c_i32, c_f64, c_p, c_p],

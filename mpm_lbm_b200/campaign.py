@@ -77,6 +77,43 @@ class CampaignReductions:
         }
 
 
+def campaign_sums_from_fields(fields: dict[str, np.ndarray], regions: dict[str, np.ndarray], device="cuda"
+                              ) -> dict[str, Any]:
+    """The sums of CampaignReductions from host copies in the reference's
+    layouts (_copy_lbm_fields, solver.py:352-365: rho (nx, ny, nz), velocity
+    (nx, ny, nz, 3), population (nx, ny, nz, 19), solid (nx, ny, nz)), held
+    on the device in lattice order (fsi_campaign_sums_arrays)."""
+    rho = np.asarray(fields["rho"], np.float32)
+    nx, ny, nz = rho.shape
+    if len(regions) > FSI_CAMPAIGN_REGIONS:
+        raise ValueError(f"at most {FSI_CAMPAIGN_REGIONS} flux regions")
+    names = list(regions)
+    code = np.zeros((nx, ny, nz), np.uint8)
+    for bit, name in enumerate(names):
+        code |= (np.asarray(regions[name]).astype(bool).astype(np.uint8) << bit).astype(np.uint8)
+
+    def dev(a, comps=False):
+        a = np.asarray(a)
+        a = a.transpose(3, 2, 1, 0) if comps else a.transpose(2, 1, 0)
+        return torch.from_numpy(np.ascontiguousarray(a)).to(device)
+
+    t_rho = dev(rho)
+    t_vel = dev(np.asarray(fields["velocity"], np.float32), True)
+    pop = fields.get("population")
+    t_pop = dev(np.asarray(pop, np.float32), True) if pop is not None else None
+    t_solid = dev((np.asarray(fields["solid"]) != 0).astype(np.uint8))
+    t_reg = dev(code)
+    size = ctypes.sizeof(FsiCampaignSums)
+    t_out = torch.zeros((size + 255) // 256 * 256, dtype=torch.uint8, device=device)
+    call("fsi_campaign_sums_arrays", nx, ny, nz, ptr(t_rho), ptr(t_vel), ptr(t_pop), ptr(t_solid), ptr(t_reg),
+         ptr(t_out), stream_handle())
+    st = FsiCampaignSums.from_buffer_copy(t_out[:size].cpu().numpy().tobytes())
+    return {"fluid_mass": float(st.fluid_mass),
+            "flux": {name: float(st.region_flux[bit]) for bit, name in enumerate(names)},
+            "fluid_cells": int(st.fluid_cells), "rho_finite": st.nonfinite_rho == 0,
+            "velocity_finite": st.nonfinite_vel == 0, "population_finite": st.nonfinite_pop == 0}
+
+
 def _assert_finite_row(row: dict[str, Any]) -> None:
     """solver.py:830-835."""
     for key, value in row.items():

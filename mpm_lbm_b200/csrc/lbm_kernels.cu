@@ -1763,9 +1763,18 @@ __global__ void k_readout(const Case c, float* out_pop, float* out_rho, float* o
 // cell count and the counts of cells with a non-finite rho, v or population;
 // over the cells of region r (bit r of regions[i], any solid state) the flux
 // sum(rho * u_x).  Products and sums in FP64; one atomic per CTA and value.
-template <bool H>
-__global__ void __launch_bounds__(256) k_campaign_sums(const Case c, const uint8_t* __restrict__ regions,
-                                                       FsiCampaignSums* out) {
+// The cells come from the lattice state (ARR false: readout of the AA
+// layout) or from plain fields in lattice order (ARR true: a snapshot).
+struct CampaignArrays {
+  const float* rho;       // [n]
+  const float* vel;       // [3][n]
+  const float* pop;       // [19][n] or null (no population check)
+  const uint8_t* solid;   // [n] non-zero: solid
+};
+
+template <bool H, bool ARR>
+__global__ void __launch_bounds__(256) k_campaign_sums(const Case c, const CampaignArrays a,
+                                                       const uint8_t* __restrict__ regions, FsiCampaignSums* out) {
   __shared__ double s_d[8][1 + FSI_CAMPAIGN_REGIONS];
   __shared__ int s_i[8][4];
   const int64_t n = (int64_t)c.s.nx * c.s.ny * c.s.nz;
@@ -1774,16 +1783,30 @@ __global__ void __launch_bounds__(256) k_campaign_sums(const Case c, const uint8
   for (int r = 0; r < FSI_CAMPAIGN_REGIONS; ++r) flux[r] = 0.0;
   int cells = 0, bad_rho = 0, bad_vel = 0, bad_pop = 0;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    float F[19], rho, u[3];
-    const uint8_t fl = readout_cell<H>(c, i, F, rho, u);
-    if (!(fl & kSolid)) {
+    float rho, u[3];
+    bool solid, pf = true;
+    if (ARR) {
+      rho = a.rho[i];
+      u[0] = a.vel[i];
+      u[1] = a.vel[n + i];
+      u[2] = a.vel[2 * n + i];
+      solid = a.solid[i] != 0;
+      if (!solid && a.pop) {
+#pragma unroll
+        for (int s = 0; s < 19; ++s) pf = pf && isfinite(a.pop[(int64_t)s * n + i]);
+      }
+    } else {
+      float F[19];
+      const uint8_t fl = readout_cell<H>(c, i, F, rho, u);
+      solid = (fl & kSolid) != 0;
+#pragma unroll
+      for (int s = 0; s < 19; ++s) pf = pf && isfinite(F[s]);
+    }
+    if (!solid) {
       ++cells;
       mass += (double)rho;
       bad_rho += isfinite(rho) ? 0 : 1;
       bad_vel += (isfinite(u[0]) && isfinite(u[1]) && isfinite(u[2])) ? 0 : 1;
-      bool pf = true;
-#pragma unroll
-      for (int s = 0; s < 19; ++s) pf = pf && isfinite(F[s]);
       bad_pop += pf ? 0 : 1;
     }
     const unsigned rg = regions ? regions[i] : 0u;
@@ -2581,9 +2604,27 @@ extern "C" int fsi_campaign_sums(const FsiLbmState* s, const FsiLbmParams* p, co
   const int64_t n = (int64_t)s->nx * s->ny * s->nz;
   const unsigned blocks = (unsigned)std::min<int64_t>(blocks_for(n, 256), (int64_t)lbm_sm_count() * 8);
   if (s->store_fp16)
-    k_campaign_sums<true><<<blocks, 256, 0, st>>>(c, regions, out);
+    k_campaign_sums<true, false><<<blocks, 256, 0, st>>>(c, CampaignArrays{}, regions, out);
   else
-    k_campaign_sums<false><<<blocks, 256, 0, st>>>(c, regions, out);
+    k_campaign_sums<false, false><<<blocks, 256, 0, st>>>(c, CampaignArrays{}, regions, out);
+  return launch_check("k_campaign_sums");
+}
+
+extern "C" int fsi_campaign_sums_arrays(int32_t nx, int32_t ny, int32_t nz, const float* rho, const float* vel,
+                                        const float* pop, const uint8_t* solid, const uint8_t* regions,
+                                        FsiCampaignSums* out, void* stream) {
+  if (nx <= 0 || ny <= 0 || nz <= 0) return invalid("lattice dimensions must be positive");
+  if (!rho || !vel || !solid || !out) return invalid("null field or output");
+  cudaStream_t st = (cudaStream_t)stream;
+  int rc;
+  if ((rc = cuda_check(cudaMemsetAsync(out, 0, sizeof(FsiCampaignSums), st), "memset campaign sums"))) return rc;
+  Case c{};
+  c.s.nx = nx;
+  c.s.ny = ny;
+  c.s.nz = nz;
+  const int64_t n = (int64_t)nx * ny * nz;
+  const unsigned blocks = (unsigned)std::min<int64_t>(blocks_for(n, 256), (int64_t)lbm_sm_count() * 8);
+  k_campaign_sums<false, true><<<blocks, 256, 0, st>>>(c, CampaignArrays{rho, vel, pop, solid}, regions, out);
   return launch_check("k_campaign_sums");
 }
 

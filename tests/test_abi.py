@@ -64,3 +64,15 @@ def test_invalid_arguments_fail_loudly(lib):
     rc = lib.fsi_lbm_substep(None, None, None, None)
     assert rc == -1
     assert "null" in _lib.last_error()
+
+
+def test_header_constants_match_binding():
+    text = open(HEADER, encoding="utf-8").read()
+
+    def define(name):
+        return int(re.search(rf"#define {name} (\d+)", text).group(1))
+
+    assert define("FSI_ABI_VERSION") == _lib.ABI_VERSION
+    assert define("FSI_BIN_CHUNK") == _lib.FSI_BIN_CHUNK
+    assert define("FSI_BIN_EDGE") == _lib.FSI_BIN_EDGE
+    assert define("FSI_CAMPAIGN_REGIONS") == _lib.FSI_CAMPAIGN_REGIONS

@@ -1,14 +1,19 @@
 """Device reductions of the subcycled-flow campaign (fsi_campaign_sums,
-mpm_lbm_b200.campaign) against the reference's host computation
-(solvers/official_subcycled_flow_solver.py:465-540), restated here in numpy
-on the host copies of rho, v, f and solid exactly as the reference makes them
-(_copy_lbm_fields, 352-365).
+fsi_campaign_sums_arrays, mpm_lbm_b200.campaign).
 
-Duct/plate case with open x faces after FSI steps (the open boundary of the
-last substep pending, so the readout applies it).  FP64 sums of FP32 fields
-in another order: rtol 1e-12; gates, flags and counts exact.  A non-finite
-population written into one fluid cell clears population_finite and the
-finite gate.
+1. Against the reference's own rows: the reference's _stability_row and
+   _mass_flux_row (solvers/official_subcycled_flow_solver.py:443-515) ran on
+   seeded host snapshots (tests/golden/make_campaign_fixture.py); the same
+   snapshots go to the device, fsi_campaign_sums_arrays sums them and
+   campaign builds the rows.  FP64 sums of FP32 fields in another order: rtol
+   1e-12 (mass_delta_rel, a difference of two near-equal sums: atol 1e-12);
+   gates, flags and counts exact.
+2. On the drop-in's own state: fsi_campaign_sums over the lattice state of a
+   duct/plate case with open x faces after FSI steps (the open boundary of
+   the last substep pending, so the readout applies it) against the same
+   sums of the host copies _copy_lbm_fields makes (352-365).  A non-finite
+   population written into one fluid cell clears population_finite and the
+   finite gate.
 """
 
 import numpy as np
@@ -34,6 +39,23 @@ def _host_rows(fields, masks, diagnostics):
     return {"mass": float(np.sum(rho[fluid])), "inlet": float(np.sum(rho[inlet] * ux[inlet])),
             "outlet": float(np.sum(rho[outlet] * ux[outlet])), "midplane": float(np.sum(rho[mid] * ux[mid])),
             "cells": int(fluid.sum()), **finite}
+
+
+def test_device_rows_equal_the_reference_rows():
+    from mpm_lbm_b200 import campaign
+    from tests.test_campaign_rows import compare_rows, load_fixture
+
+    snaps, masks, ref = load_fixture()
+    regions = campaign.campaign_regions(masks)
+    initial = None
+    for k, snap in enumerate(snaps):
+        sums = campaign.campaign_sums_from_fields(snap, regions)
+        assert sums["fluid_cells"] == int((snap["solid"] == 0).sum())
+        compare_rows(campaign.stability_row(ref["base"][k], ref["diagnostics"][k], sums), ref["rows"]["stability"][k],
+                     rtol=1e-12)
+        if k < len(ref["rows"]["mass_flux"]):
+            row, initial = campaign.mass_flux_row(ref["base"][k], sums, initial)
+            compare_rows(row, ref["rows"]["mass_flux"][k], rtol=1e-12, atol=1e-12)
 
 
 def _masks(drv):

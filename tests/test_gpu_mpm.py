@@ -85,8 +85,11 @@ def compare_grid(gpu, ora, rel=2e-5):
     _close(gpu.grid_f_ext.to_numpy(), ora.grid_f_ext, rel, "grid_f_ext")
 
 
-def expected_bins(x, n_grid, edge=8, chunk=128):
+def expected_bins(x, n_grid, edge=8, chunk=None):
     """Bin keys, counts and chunk table restated on the CPU in FP32."""
+    from mpm_lbm_b200._lib import FSI_BIN_CHUNK
+
+    chunk = FSI_BIN_CHUNK if chunk is None else chunk
     inv_dx = np.float32(n_grid)
     xp = (x.astype(np.float32) * inv_dx).astype(np.float32)
     base = (xp - np.float32(0.5)).astype(np.int32)  # truncation toward zero
