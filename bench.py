@@ -81,37 +81,76 @@ def measured_peak():
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled during the timed region.
+    """SM clocks and clock-event (throttle) reasons sampled during the timed
+    region: read-only NVML queries every 5 ms from a thread (nvidia-smi's
+    100 ms polling as the fallback).  The sampler is started and its first
+    sample awaited before the timed region opens."""
 
-    The sampler is started and its first sample awaited before the timed
-    region opens, so that the samples cover the region itself."""
+    REASONS = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20, "sw_power_cap": 0x4}
 
-    def __init__(self, gpu_index=0):
-        self.proc = None
-        self.lines = []
+    def __init__(self, gpu_index=0, interval_s=0.005):
         self.gpu = gpu_index
+        self.interval = interval_s
+        self.samples = []  # (time, sm_mhz, max_mhz, reason bits)
         self.marks = []
+        self._stop = threading.Event()
+        self.proc = None
+        self.source = None
 
     def __enter__(self):
-        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
-             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-             "clocks_event_reasons.sw_power_cap")
+        try:
+            import pynvml
+
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.gpu)
+            mx = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+
+            def read():
+                return (time.time(), float(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)), float(mx),
+                        int(pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)))
+
+            read()
+            self.source = "nvml"
+        except Exception:
+            read = None
+        if read is not None:
+            def loop():
+                while not self._stop.is_set():
+                    try:
+                        self.samples.append(read())
+                    except Exception:
+                        break
+                    time.sleep(self.interval)
+
+            self.t = threading.Thread(target=loop, daemon=True)
+            self.t.start()
+        else:
+            self._start_smi()
+        t0 = time.time()
+        while not self.samples and time.time() - t0 < 5.0:
+            time.sleep(0.005)
+        return self
+
+    def _start_smi(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active")
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={q}",
                                           "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
+            self.source = "nvidia-smi"
+
+            def read():
+                for line in self.proc.stdout:
+                    p = [x.strip() for x in line.split(",")]
+                    try:
+                        self.samples.append((time.time(), float(p[1]), float(p[2]), int(p[4], 16)))
+                    except (ValueError, IndexError):
+                        continue
+
+            self.t = threading.Thread(target=read, daemon=True)
             self.t.start()
-            t0 = time.time()
-            while not self.lines and time.time() - t0 < 5.0:
-                time.sleep(0.01)
         except Exception:
             self.proc = None
-        return self
-
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append((time.time(), line.strip()))
 
     def open_region(self):
         self.marks = [time.time()]
@@ -120,6 +159,7 @@ class ClockSampler:
         self.marks.append(time.time())
 
     def __exit__(self, *a):
+        self._stop.set()
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -128,34 +168,43 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         lo, hi = (self.marks + [None, None])[:2] if self.marks else (None, None)
-        for ts, ln in self.lines:
-            if lo is not None and hi is not None and not (lo - 0.1 <= ts <= hi + 0.1):
+        sm, mx, reasons = [], None, set()
+        for ts, mhz, mmax, bits in list(self.samples):
+            if lo is not None and hi is not None and not (lo <= ts <= hi):
                 continue
-            p = [x.strip() for x in ln.split(",")]
-            if len(p) < 9:
-                continue
-            try:
-                sm.append(float(p[1]))
-                mx = float(p[2])
-            except ValueError:
-                continue
-            for nm, val in zip(names, p[5:9]):
-                if val.lower() == "active":
-                    reasons.add(nm)
-        if not sm:
-            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": 0}
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+            sm.append(mhz)
+            mx = mmax
+            for name, bit in self.REASONS.items():
+                if bits & bit:
+                    reasons.add(name)
+        out = {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+               "samples": len(sm), "source": self.source}
+        if not sm and self.samples:  # region shorter than one sample: the nearest one
+            ts, mhz, mmax, bits = min(self.samples, key=lambda r: abs(r[0] - (lo or r[0])))
+            out.update(sm_mhz=mhz, sm_max_mhz=mmax, samples=0,
+                       reasons=sorted(n for n, b in self.REASONS.items() if bits & b))
+        return out
 
 
-def oracle_driver(wl, substeps, mpm_substeps):
-    """The CPU oracle (C++ restatement, OpenMP over cells on all host threads)
-    on the same case: FSI steps of `substeps` LBM and `mpm_substeps` MPM substeps."""
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
+def oracle_driver(wl, substeps, mpm_substeps, threads=None):
+    """The CPU oracle (C++ restatement, OpenMP over cells; all host threads by
+    default) on the same case: FSI steps of `substeps` LBM and `mpm_substeps`
+    MPM substeps."""
     from oracle import oracle as orc
 
-    threads = os.cpu_count() or 1
+    threads = threads or os.cpu_count() or 1
     return orc.fsi_driver_for_case(wl.case, substeps=substeps, mpm_substeps=mpm_substeps, threads=threads), threads
 
 
@@ -165,15 +214,25 @@ def cpu_sample_text(wl, steps, substeps, mpm_substeps):
 
 
 def cpu_baseline(wl, steps=1):
-    """MLUPS of the CPU oracle on a bounded sample of the workload: one FSI step."""
+    """MLUPS of the CPU oracle on a bounded sample of the workload: one FSI
+    step on all host threads, and a shorter FSI step (12 LBM + 4 MPM
+    substeps, the same 3:1 ratio per LBM substep) on one thread."""
     substeps, mpm_substeps = wl.S, wl.M
     drv, threads = oracle_driver(wl, substeps, mpm_substeps)
     t0 = time.perf_counter()
     for _ in range(steps):
         drv.step_once()
     dt = time.perf_counter() - t0
+    one_sub, one_msub = 12, 4
+    drv1, _ = oracle_driver(wl, one_sub, one_msub, threads=1)
+    t0 = time.perf_counter()
+    drv1.step_once()
+    dt1 = time.perf_counter() - t0
     return {"value": steps * substeps * wl.cells / dt / 1e6, "unit": "MLUPS", "cores": threads, "kind": "port",
-            "sample": cpu_sample_text(wl, steps, substeps, mpm_substeps)}
+            "cpu_model": cpu_model(), "nproc": os.cpu_count(),
+            "sample": cpu_sample_text(wl, steps, substeps, mpm_substeps),
+            "one_thread": {"value": one_sub * wl.cells / dt1 / 1e6, "unit": "MLUPS", "cores": 1,
+                           "sample": cpu_sample_text(wl, 1, one_sub, one_msub)}}
 
 
 def dist_setup():
@@ -208,7 +267,7 @@ def run_reference(args, wl, ws, rank):
         drv.step_once()
     secs = time.perf_counter() - t0
     value = args.steps * sub * wl.cells / secs / 1e6
-    cb = {"value": value, "unit": "MLUPS", "cores": threads, "kind": "port",
+    cb = {"value": value, "unit": "MLUPS", "cores": threads, "kind": "port", "cpu_model": cpu_model(),
           "sample": cpu_sample_text(wl, args.steps, sub, msub)}
     print(json.dumps({"impl": "reference", "metric": "coupled-FSI MLUPS", "value": value, "unit": "MLUPS",
                       "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -233,9 +292,15 @@ def run_batched(args):
 
     from mpm_lbm_b200.batch import FSIBatch, sample_box_cases
 
+    from mpm_lbm_b200.autotune import tune_batch
+
     cases = sample_box_cases(args.cases, seed=0)
     cells = sum(c.cells for c in cases)
-    batch = FSIBatch(capacity=len(cases), storage=args.storage, mpm_substeps=10)
+    tuning = tune_batch(lambda: [c.make_driver(storage=args.storage) for c in cases], storage=args.storage,
+                        mpm_substeps=10)
+    torch.cuda.empty_cache()
+    batch = FSIBatch(capacity=len(cases), storage=args.storage, mpm_substeps=10, lbm_tune=tuning["lbm_tune"],
+                     mpm_ctas=tuning["mpm_ctas"])
     for c in cases:
         batch.add(c.make_driver(storage=args.storage))
     for _ in range(max(args.warmup, 3)):
@@ -253,7 +318,8 @@ def run_batched(args):
            "higher_is_better": True, "dtype": "f32" if args.storage == "fp32" else "f16-storage/f32-compute",
            "data": "synthetic", "config": {"workload": f"batch_{len(cases)}_box_cases", "cases": len(cases),
                                            "cells": cells, "kernels_per_step": batch.graph_kernels,
-                                           "lbm_tune": batch.dims.lbm_tune}}
+                                           "lbm_tune": batch.dims.lbm_tune, "mpm_ctas": batch.dims.mpm_ctas,
+                                           "tuning_ms_per_step": tuning["ms_per_step"]}}
     del batch
     if not args.no_one_by_one:
         tot = 0.0
@@ -466,6 +532,17 @@ def main():
     mpm_ms = time_mpm_phase(drv)
     mpm = {"kernel": "k_mpm_seq", "ms_per_substep": mpm_ms, "launches_per_substep": (wl.M + 2) / wl.M,
            "share_of_step": wl.M * mpm_ms / ms_step}
+
+    # ---- the whole coupled FSI step against the same roofline: per step
+    # S LBM substeps (alg_bytes each), M MPM substeps of 204 B per particle and
+    # 48 B per active grid node, and 25 B per cell for projection and mask
+    n_p = drv.solid.n_particles
+    active_nodes = int((drv.solid._last_grid()[1] > 0).sum().item())
+    step_bytes = wl.S * alg_bytes + wl.M * (n_p * 204 + active_nodes * 48) + wl.cells * 25
+    coupled = step_bytes / (ms_step * 1e-3) / 1e9
+    roofline["coupled_frac"] = coupled / peak
+    roofline["coupled"] = {"achieved": coupled, "bytes_per_step": step_bytes, "active_grid_nodes": active_nodes,
+                           "bytes": "S*(2*19*s*fluid_cells + cells) + M*(204*particles + 48*active_nodes) + 25*cells"}
 
     # ---- end to end through the public API with host buffers
     pinned_in = torch.tensor([wl.case.u_in, 0.0, 0.0], dtype=torch.float32).pin_memory()

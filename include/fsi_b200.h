@@ -452,14 +452,14 @@ int fsi_mpm_g2p(const FsiParticles* pt, const FsiGrid* g, const FsiMpmParams* mp
  *     B-spline base cell, and within a block by base cell, and cuts every bin
  *     into chunks of at most FSI_BIN_CHUNK particles (bins may go stale
  *     between calls: that costs speed only);
- *   - fsi_mpm_substeps_binned runs substeps chunk by chunk, one warp per
- *     chunk: each chunk is scattered into a shared-memory tile covering its stencil box and the
+ *   - fsi_mpm_substeps_binned runs substeps chunk by chunk: each chunk is
+ *     scattered into a shared-memory tile covering its stencil box and the
  *     tile is flushed with one atomic per touched node value; the gather
  *     evaluates the grid update per node while staging the chunk's box.  A
  *     substep leaves momentum (not velocity), mass and f_ext in its grid
  *     buffer; three buffers rotate, and only the boxes recorded for a buffer
  *     are zeroed before it is reused, so no dense pass over the grid is made. */
-#define FSI_BIN_CHUNK 32
+#define FSI_BIN_CHUNK 128
 #define FSI_BIN_EDGE 8
 
 /* count, start and chunk must be 16-byte aligned */
@@ -552,6 +552,8 @@ typedef struct FsiBatchDims {
   int32_t max_chunks;             /* max FsiMpmBins.max_chunks */
   int32_t max_bins;               /* max FsiMpmBins.n_bins */
   int32_t lbm_tune;               /* FSI_TUNE_LBM_OCC3, or FSI_TUNE_LBM_PAIR when every case has an even nx */
+  int32_t mpm_ctas;               /* CTAs per case of the batched MPM substeps (0: about one per chunk of the
+                                     largest case); a launch variant picked by the batch autotuner */
 } FsiBatchDims;
 
 /* MPMToLBMProjector3D.project per case (coupling/projection.py:21-97). */

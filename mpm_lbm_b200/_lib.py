@@ -24,7 +24,7 @@ FSI_TUNE_LBM_OCC3, FSI_TUNE_LBM_OCC4, FSI_TUNE_LBM_PAIR, FSI_TUNE_LBM_OCC3_PF, F
 
 
 FSI_CAMPAIGN_REGIONS = 8
-FSI_BIN_CHUNK, FSI_BIN_EDGE = 32, 8  # particles per chunk of a bin, bin edge in cells
+FSI_BIN_CHUNK, FSI_BIN_EDGE = 128, 8  # particles per chunk of a bin, bin edge in cells
 
 
 class FsiCampaignSums(ctypes.Structure):
@@ -129,7 +129,7 @@ class FsiBatchCase(ctypes.Structure):
 class FsiBatchDims(ctypes.Structure):
     _fields_ = [("n_cases", c_i32), ("store_fp16", c_i32), ("max_lbm_tiles", c_i32), ("max_particles", c_i32),
                 ("max_cells", c_i64), ("max_chunks", c_i32), ("max_bins", c_i32),
-                ("lbm_tune", c_i32)]
+                ("lbm_tune", c_i32), ("mpm_ctas", c_i32)]
 
 
 FSI_BATCH_PENALTY, FSI_BATCH_MOVING = 0, 1

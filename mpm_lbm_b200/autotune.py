@@ -75,3 +75,52 @@ def tune_lbm(lbm, step_fn, candidates=None, steps=10, reps=3):
     lbm.tune = best
     lbm._sync_params()
     return {"choice": best, "ms_per_substep": times}
+
+
+def tune_batch(make_drivers, capacity=None, storage="fp32", mpm_substeps=10, device="cuda", steps=4, reps=2):
+    """Launch variants of the batched form (FSIBatch): the LBM step kernel
+    (one cell per thread, or two on the paired FP32 pipe when every case has
+    an even nx) and the CTA count per case of the batched MPM substeps (the
+    default of about one per chunk of the largest case, half and twice that).
+    make_drivers() builds the cases' initialised drivers; they run in a
+    throwaway batch (their state advances and is discarded), each variant as
+    a CUDA graph of one batched FSI step replayed `steps` times between
+    events, the best of `reps`.  Returns {"lbm_tune", "mpm_ctas",
+    "ms_per_step": {(lbm_tune, mpm_ctas): ms}}."""
+    from .batch import FSIBatch
+
+    drivers = make_drivers()
+    cap = capacity or len(drivers)
+    batch = FSIBatch(capacity=cap, storage=storage, mpm_substeps=mpm_substeps, device=device)
+    for drv in drivers:
+        batch.add(drv)
+    lbm_opts = [FSI_TUNE_LBM_OCC3]
+    if all(d.lbm.nx % 2 == 0 for d in drivers):
+        lbm_opts.append(FSI_TUNE_LBM_PAIR)
+    chunks = max(1, int(batch.dims.max_chunks))
+    default = min(chunks, 2 * ((int(batch.dims.max_particles) + 127) // 128) + 8)
+    mpm_opts = [0] + sorted({max(1, default // 2), min(65535, default * 2)} - {default})
+    times = {}
+    stream = torch.cuda.current_stream()
+    for lt in lbm_opts:
+        for mc in mpm_opts:
+            batch.lbm_tune, batch.mpm_ctas = lt, mc
+            batch._update_dims()
+            batch.invalidate_graph()
+            batch.step(use_graph=True)  # capture and warm
+            torch.cuda.synchronize()
+            best = float("inf")
+            for _ in range(reps):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                for _ in range(steps):
+                    batch.step(use_graph=True)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                best = min(best, e0.elapsed_time(e1) / steps)
+            times[(lt, mc)] = best
+    batch.invalidate_graph()
+    choice = min(times, key=times.get)
+    del batch, drivers
+    return {"lbm_tune": int(choice[0]), "mpm_ctas": int(choice[1]),
+            "ms_per_step": {f"{k[0]}/{k[1]}": v for k, v in times.items()}}

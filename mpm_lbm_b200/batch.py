@@ -160,14 +160,17 @@ def sample_box_cases(n, seed=0, edges=(32, 48, 64, 96), lbm_steps=200, mpm_subst
 class FSIBatch:
     """Up to `capacity` independent FSI cases, advanced together."""
 
-    def __init__(self, capacity, storage="fp32", mpm_substeps=10, device="cuda", lbm_tune=None):
+    def __init__(self, capacity, storage="fp32", mpm_substeps=10, device="cuda", lbm_tune=None, mpm_ctas=0):
         """lbm_tune: FSI_TUNE_LBM_OCC3 (0, default) or FSI_TUNE_LBM_PAIR (2, every
-        case's nx even)."""
+        case's nx even); mpm_ctas: CTAs per case of the batched MPM substeps (0:
+        about one per chunk of the largest case).  autotune.tune_batch picks
+        both by timing."""
         self.capacity = int(capacity)
         self.storage = storage
         self.M = int(mpm_substeps)
         self.device = torch.device(device)
         self.lbm_tune = lbm_tune
+        self.mpm_ctas = int(mpm_ctas)
         self.slots = [None] * self.capacity          # FSIDriver3D per slot
         self.records = (FsiBatchCase * self.capacity)()
         self.t_cases = torch.zeros(ctypes.sizeof(self.records), dtype=torch.uint8, device=self.device)
@@ -278,6 +281,7 @@ class FSIBatch:
         act = [drv for drv in self.slots if drv is not None]
         d.n_cases = self.capacity
         d.store_fp16 = int(self.storage == "fp16")
+        d.mpm_ctas = int(self.mpm_ctas)
         all_even = all(x.lbm.nx % 2 == 0 for x in act)
         if self.lbm_tune is None:
             d.lbm_tune = FSI_TUNE_LBM_OCC3  # the faster of the two on B200 (see profiles/)

@@ -1,9 +1,9 @@
-// Binned MPM substeps: particles sorted by 8x8x8-cell block and cut into
-// chunks of <= 32; one launch per substep, in which each warp takes whole
-// chunks through the G2P gather of the previous substep (grid update evaluated
-// while the chunk's node box is staged), the P2G stress / reaction payload and
-// the P2G scatter staged in a shared-memory tile, flushed with one global
-// atomic per touched node value.  Three grid buffers rotate so that only the boxes
+// Binned MPM substeps: particles sorted by 4x4x4-cell block and cut into
+// chunks; one launch per substep, in which each CTA takes whole chunks
+// through the G2P gather of the previous substep (grid update evaluated while
+// the chunk's node box is staged), the P2G stress / reaction payload and the
+// P2G scatter staged in a shared-memory tile, flushed with one global atomic
+// per touched node value.  Three grid buffers rotate so that only the boxes
 // touched two substeps earlier are zeroed, by the launch after their last
 // reader.
 //
@@ -26,6 +26,10 @@ namespace {
 
 constexpr int kChunk = FSI_BIN_CHUNK;  // particles per chunk
 constexpr int kEdge = FSI_BIN_EDGE;
+// nodes staged per CTA: the stencils of a chunk of one bin span at most
+// (8 + 2)^3 = 1000 nodes; the rest absorbs drift since the last binning (a
+// 13^3 box).  7 floats per node in P2G = 61.5 KB.
+constexpr int kTileCap = 2197;
 
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
@@ -295,41 +299,33 @@ __device__ __forceinline__ void g2p_gather_global(const FsiGrid& g, const FsiMpm
 enum { kQmv = 0, kQaff = 4, kQbase = 16, kQfx1 = 20, kQwx = 24, kQwy = 28, kQwz = 32, kQn = 36 };
 
 // ---- fused substep sequence --------------------------------------------------
-// M substeps in M + 1 launches (after a prologue).  The unit of work is one
-// chunk (<= 32 particles of one bin, sorted by base cell) taken by one warp;
-// the warps of a CTA are independent (no CTA barrier), so an SM keeps many
-// chunks' latency chains in flight.  Launch s, for each chunk of a warp: the
-// gather of substep s - 1 (G2P from grid buffer (s - 1) % 3, lane = particle,
-// the chunk's node box staged in the warp's shared memory with the grid
-// update evaluated per node), the new particle state written to the particle
-// fields and kept in registers, then the P2G payload of substep s from that
-// state (lane = particle: stress with the FP64 polar rotation, B-spline data,
-// reaction force) and its scatter (lane = stencil node, the chunk's particles
-// in order, runs of equal base cell summed in registers) into the warp's node
-// tile, flushed into buffer s % 3 with one global atomic per touched node
-// value.  The launch boundary is the one grid-wide step (every scatter of
-// substep s is complete before any gather of it).  The launch also zeroes the
-// boxes substep s - 2 recorded in buffer (s + 1) % 3, whose last reader (the
-// gather of substep s - 2) ran in the launch before: three buffers, so that no
-// launch zeroes a buffer that another warp of the same launch still reads or
-// writes.  The arithmetic is the one of the three-kernel substep above
-// (p2g_particle, reaction_particle, g2p_node and g2p_finish on the same values).
+// M substeps in M + 1 launches (after a prologue).  Launch s, for each chunk of
+// its CTA: the gather of substep s - 1 (G2P from grid buffer (s - 1) % 3, the
+// new particle state written to the particle fields and kept in shared
+// memory), then the P2G payload of substep s from that state and its scatter
+// into buffer s % 3.  A chunk's particles belong to one CTA for the launch, so
+// gather, payload and scatter of a chunk follow each other without any
+// grid-wide synchronisation; the launch boundary is the one grid-wide step
+// (every scatter of substep s is complete before any gather of it).  The
+// launch also zeroes the boxes substep s - 2 recorded in buffer (s + 1) % 3,
+// whose last reader (the gather of substep s - 2) ran in the launch before:
+// three buffers, so that no launch zeroes a buffer that another CTA of the
+// same launch still reads or writes.  The arithmetic is the one of the
+// three-kernel substep above (p2g_particle, reaction_particle, g2p_node and
+// g2p_finish on the same values).
 
+enum { kSx = 0, kSv = 3, kSC = 6, kSF = 15, kSn = 24 };  // staged particle state rows
 // bins->meta: [0] chunks, [1 + b] records in box[b], [4] chunks scattered
 // without the tile, [5 + b] buffer b holds recorded boxes not yet zeroed
 enum { kMetaChunks = 0, kMetaRec = 1, kMetaOverflow = 4, kMetaDirty = 5 };
-static_assert(kChunk == 32, "one warp per chunk: a lane per particle");
-constexpr int kSeqT = 128;            // threads per CTA: 4 independent warps
-constexpr int kSeqW = kSeqT / 32;
-// nodes staged per warp: the stencils of 32 particles sorted by base cell
-// span a few cells (a 4 x 4 x 3 box at 8 per cell); 6^3 absorbs a cell of
-// drift since the binning and sparser chunks.  Larger boxes go through global
-// memory (same arithmetic).
-constexpr int kWarpTileCap = 216;
-constexpr int kWarpTileFloats = 7 * kWarpTileCap;            // [7][nv] scatter / [4][nv] lattice / [3][nv] G2P
-constexpr int kWarpFloats = kWarpTileFloats + kQn * kChunk;  // + [kChunk][kQn] P2G payload records
-static_assert(kWarpTileFloats % 4 == 0 && kWarpFloats % 4 == 0, "payload records must stay 16-byte aligned");
-constexpr size_t kSeqSmem = sizeof(float) * kWarpFloats * kSeqW;
+constexpr int kSeqT = 256;
+constexpr int kTileFloats = (7 * kTileCap + 3) & ~3;  // keeps the payload 16-byte aligned
+// G2P: the staged node velocities use 3 * nv <= 3 * kTileCap floats of the
+// tile; the two stencil halves of a particle meet behind them (12 sums per
+// particle)
+constexpr int kXchOffset = (3 * kTileCap + 3) & ~3;
+static_assert(kXchOffset + 12 * kChunk <= kTileFloats, "G2P exchange does not fit the tile");
+constexpr size_t kSeqSmem = sizeof(float) * (kTileFloats + (kQn + kSn) * kChunk);
 
 struct SeqArgs {
   FsiParticles pt;
@@ -439,35 +435,31 @@ __device__ __forceinline__ void reaction_particle_staged(const float* __restrict
 
 __device__ __forceinline__ int base_of(float x, float inv_dx) { return (int)(__fmul_rn(x, inv_dx) - 0.5f); }
 
-// zeroes the node boxes recorded for a buffer: warp wg of ws takes records
-// wg, wg + ws, ...
-__device__ __forceinline__ void zero_boxes_warp(const FsiGrid& go, const int32_t* __restrict__ rec, int nrec, int wg,
-                                                int ws, int lane) {
-  const int G = go.n;
-  const int64_t N = (int64_t)G * G * G;
-  for (int r = wg; r < nrec; r += ws) {
-    const Box bx = load_box(rec + 6 * r);
-    for (int li = lane; li < bx.vol; li += 32) {
-      int i, j, k;
-      box_ijk(bx, li, i, j, k);
-      const int64_t node = ((int64_t)k * G + j) * G + i;
-      go.v[node] = 0.f;
-      go.v[N + node] = 0.f;
-      go.v[2 * N + node] = 0.f;
-      go.m[node] = 0.f;
-      go.f_ext[node] = 0.f;
-      go.f_ext[N + node] = 0.f;
-      go.f_ext[2 * N + node] = 0.f;
+// the chunk's node box: min / max base node over the live threads (every
+// thread of the CTA calls this, live or not)
+__device__ __forceinline__ void box_reduce(bool live, const int nb[3], int* s_lo, int* s_hi) {
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+    const int lo = __reduce_min_sync(0xffffffffu, live ? nb[r] : INT_MAX);
+    const int hi = __reduce_max_sync(0xffffffffu, live ? nb[r] : INT_MIN);
+    if ((threadIdx.x & 31) == 0) {
+      if (lo != INT_MAX) atomicMin(&s_lo[r], lo);
+      if (hi != INT_MIN) atomicMax(&s_hi[r], hi);
     }
   }
 }
 
-// G2P gather of one particle from the node velocities staged in tile (box
-// bx, nv nodes): the arithmetic of the one-phase g2p_node, with the offsets,
-// weights and offset distances known per node at compile time and the
-// grid-range test skipped for stencils inside the grid.
-__device__ __forceinline__ void g2p_gather_staged(const float* tile, int nv, const Box& bx, int G, const BSpline& b,
-                                                  float dx, float s4, float* nvl, float* nC) {
+constexpr int kRun = kChunk / (kSeqT / 32);  // particles per warp in the scatter
+
+// G2P gather of one particle over the stencil offsets o = SUB, SUB + 2, ...
+// (the two halves of the 27 nodes, one per warp of a pair) from the node
+// velocities staged in tile (box bx, nv nodes): the arithmetic of the
+// one-phase g2p_node, with the offsets, weights and offset distances known
+// per offset at compile time and the grid-range test skipped for particles
+// whose whole stencil lies inside the grid.
+template <int SUB>
+__device__ __forceinline__ void g2p_gather_half(const float* tile, int nv, const Box& bx, int G, const BSpline& b,
+                                                float dx, float s4, float* nvl, float* nC) {
   float dp[3][3];
 #pragma unroll
   for (int a = 0; a < 3; ++a)
@@ -478,7 +470,7 @@ __device__ __forceinline__ void g2p_gather_staged(const float* tile, int nv, con
   const bool inside = b.base[0] >= 0 && b.base[0] + 2 < G && b.base[1] >= 0 && b.base[1] + 2 < G &&
                       b.base[2] >= 0 && b.base[2] + 2 < G;
 #pragma unroll
-  for (int o = 0; o < 27; ++o) {
+  for (int o = SUB; o < 27; o += 2) {
     const int ox = o / 9, oy = (o / 3) % 3, oz = o % 3;
     const int I = b.base[0] + ox, Jj = b.base[1] + oy, K = b.base[2] + oz;
     if (inside || (I >= 0 && I < G && Jj >= 0 && Jj < G && K >= 0 && K < G)) {
@@ -496,27 +488,33 @@ __device__ __forceinline__ void g2p_gather_staged(const float* tile, int nv, con
   }
 }
 
-// launch A.s of the sequence: warp wg = vb * kSeqW + w of ws = vg * kSeqW
-// takes chunks wg, wg + ws, ... (kSeqT threads, kSeqSmem bytes of dynamic
-// shared memory)
+// launch A.s of the sequence for the chunks vb, vb + vg, ... (kSeqT threads,
+// kSeqSmem bytes of dynamic shared memory)
 template <bool REACT>
 __device__ __forceinline__ void mpm_seq_body(const SeqArgs& A, int vb, int vg) {
+  constexpr int T = kSeqT, NW = T / 32;
+  static_assert(kSeqT == 2 * kChunk, "G2P: two warps per 32 particles, one per stencil half");
   extern __shared__ float4 seq_smem4[];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  // the warp's shared memory: node tile, then the P2G payload records
-  float* const tile = reinterpret_cast<float*>(seq_smem4) + wid * kWarpFloats;
-  float* const sp = tile + kWarpTileFloats;
+  // G2P: [3][nv] node velocities; payload: [4][nv] lattice box; scatter: [7][nv] tile
+  float* const tile = reinterpret_cast<float*>(seq_smem4);
+  float* const sp = tile + kTileFloats;  // [kChunk][kQn] P2G payload
+  float* const ss = sp + kQn * kChunk;   // [kSn][kChunk] particle state
+  __shared__ int s_lo[3], s_hi[3];
+  __shared__ float s_scale;
+  __shared__ int s_cnt[NW];
+  __shared__ float s_fmax[NW][2];
+  __shared__ double s_dsum[NW][6];
   const FsiParticles& pt = A.pt;
   const FsiMpmParams& mp = A.mp;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const int s = A.s;
   const bool do_g2p = s > 0, do_p2g = s < A.M;
   const int bg = (s + 2) % 3, bs = s % 3, bz = (s + 1) % 3;
   const int G = A.grid[0].n;
   const int64_t N = (int64_t)G * G * G;
   const int nch = A.meta[kMetaChunks];
-  const int wg = vb * kSeqW + wid, ws = vg * kSeqW;
   FsiCouplingStats* const st = REACT ? A.stats + bs : nullptr;
-  if (vb == 0 && threadIdx.x == 0) {
+  if (vb == 0 && tid == 0) {
     if (s == 0) {  // the prologue zeroed every buffer
       A.meta[kMetaDirty + 1] = 0;
       A.meta[kMetaDirty + 2] = 0;
@@ -528,168 +526,235 @@ __device__ __forceinline__ void mpm_seq_body(const SeqArgs& A, int vb, int vg) {
     }
     if (REACT) zero_reaction_stats(A.stats + bz);  // the record of substep s + 1
   }
-  float scale = 1.0f;  // link-area scale of the reaction (kind 2), per warp
-  if (REACT && do_p2g && A.cp.kind == 2) {
+  if (REACT && do_p2g && tid == 0) {
     float raw = 1.f;
-    if (lane == 0) scale = link_area_scale(A.diag, A.cp, &raw);
-    scale = __shfl_sync(0xffffffffu, scale, 0);
-    if (vb == 0 && threadIdx.x == 0) {
-      st->area_scale = scale;
+    s_scale = A.cp.kind == 2 ? link_area_scale(A.diag, A.cp, &raw) : 1.0f;
+    if (vb == 0 && A.cp.kind == 2) {
+      st->area_scale = s_scale;
       st->raw_area_scale = raw;
     }
   }
-  if (s >= 2) zero_boxes_warp(grid_of(A, bz), A.box + bz * A.box_stride, A.meta[kMetaRec + bz], wg, ws, lane);
+  if (s >= 2) {
+    // the boxes of substep s - 2: CTAs left without a chunk (fewer chunks than
+    // CTAs) zero them, off the path of the CTAs that have one; with no idle
+    // CTA every CTA takes a share
+    const int nrec = A.meta[kMetaRec + bz], idle = vg - nch;
+    if (idle <= 0)
+      zero_boxes(grid_of(A, bz), A.box + bz * A.box_stride, nrec, vb, vg);
+    else if (vb >= nch)
+      zero_boxes(grid_of(A, bz), A.box + bz * A.box_stride, nrec, vb - nch, idle);
+  }
 
   const float s4 = 4.0f * mp.inv_dx * mp.inv_dx;
   const int n = pt.n;
   int n_act = 0;
   float pmax = 0.f, gmax = 0.f;
   double pn[3] = {0.0, 0.0, 0.0}, gn[3] = {0.0, 0.0, 0.0};
-  for (int c = wg; c < nch; c += ws) {
-    const int2 ch = A.chunks[c];
-    const bool live = lane < ch.y;
-    const int p = live ? A.perm[ch.x + lane] : 0;
-    // the particle's state: x and F (the F the gather updates), mass, vol0
-    float X[3] = {0.f, 0.f, 0.f}, Fo[9], V[3] = {0.f, 0.f, 0.f}, Cn[9];
-#pragma unroll
-    for (int a = 0; a < 9; ++a) Fo[a] = Cn[a] = 0.f;
-    float pmass = 0.f, pvol0 = 0.f;
-    if (live) {
-#pragma unroll
-      for (int a = 0; a < 3; ++a) X[a] = pt.x[a * n + p];
-#pragma unroll
-      for (int a = 0; a < 9; ++a) Fo[a] = pt.F[(int64_t)a * n + p];
-      if (do_p2g) {
-        pmass = pt.mass[p];
-        pvol0 = pt.vol0[p];
-      }
+  for (int c = vb; c < nch; c += vg) {
+    __syncthreads();  // the previous chunk is done with the tile, the stages and the box
+    if (tid < 3) {
+      s_lo[tid] = INT_MAX;
+      s_hi[tid] = INT_MIN;
     }
-    float Fn[9];
-#pragma unroll
-    for (int a = 0; a < 9; ++a) Fn[a] = Fo[a];
+    const int2 ch = A.chunks[c];
+    int nb[3] = {0, 0, 0};  // base node of this thread's particle after the gather
+    bool nb_live = false;
+    // particle reads of the payload, issued ahead of the gather
+    const int pslot = (wid >> 1) * 32 + lane;
+    int pq = 0;
+    float pmass = 0.f, pvol0 = 0.f;
+    if (do_p2g && pslot < ch.y) {
+      pq = A.perm[ch.x + pslot];
+      pmass = pt.mass[pq];
+      pvol0 = pt.vol0[pq];
+    }
     if (do_g2p) {
       // ---- G2P of substep s - 1 from buffer bg
       const FsiGrid g = grid_of(A, bg);
       const Box bx = load_box(A.box + bg * A.box_stride + 6 * c);
-      const bool staged = bx.vol <= kWarpTileCap;
+      const bool staged = bx.vol <= kTileCap;
       const int nv = staged ? bx.vol : 0;
-      for (int li = lane; li < nv; li += 32) {
+      // this lane's particle, read ahead of the staging barrier: warps 2 i and
+      // 2 i + 1 take particles 32 i .. 32 i + 31, each one half of the stencil
+      const int lp = (wid >> 1) * 32 + lane, sub = wid & 1;
+      int p = 0;
+      float X[3] = {0.f, 0.f, 0.f}, Fo[9];
+#pragma unroll
+      for (int a = 0; a < 9; ++a) Fo[a] = 0.f;
+      if (lp < ch.y) {
+        p = A.perm[ch.x + lp];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) X[a] = pt.x[a * n + p];
+        if (sub == 0) {
+#pragma unroll
+          for (int a = 0; a < 9; ++a) Fo[a] = pt.F[(int64_t)a * n + p];
+        }
+      }
+      for (int li = tid; li < nv; li += T) {
         int i, j, k;
         box_ijk(bx, li, i, j, k);
         const int64_t node = ((int64_t)k * G + j) * G + i;
         const float m = g.m[node];
         const float P[3] = {g.v[node], g.v[N + node], g.v[2 * N + node]};
-        const float f[3] = {g.f_ext[node], g.f_ext[N + node], g.f_ext[2 * N + node]};
         float v[3] = {P[0], P[1], P[2]};
-        if (m > 0.0f) grid_node_velocity(P, m, f, i, j, k, G, mp, v);
+        if (m > 0.0f) {
+          const float f[3] = {g.f_ext[node], g.f_ext[N + node], g.f_ext[2 * N + node]};
+          grid_node_velocity(P, m, f, i, j, k, G, mp, v);
+        }
         tile[li] = v[0];
         tile[nv + li] = v[1];
         tile[2 * nv + li] = v[2];
       }
-      __syncwarp();
-      if (live) {
-        float nvl[3] = {0.f, 0.f, 0.f};
-        BSpline b;
+      __syncthreads();  // also publishes the s_lo / s_hi reset
+      float nvl[3] = {0.f, 0.f, 0.f}, nC[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+      BSpline b;
+      if (lp < ch.y) {
         bspline(X, mp.inv_dx, b);
-        if (staged)
-          g2p_gather_staged(tile, nv, bx, G, b, mp.dx, s4, nvl, Cn);
-        else
-          g2p_gather_global(g, mp, b, nvl, Cn);
-        g2p_finish_f(pt, p, mp, X, nvl, Cn, Fo, nullptr, 0, 0, V, Fn);
+        if (!staged) {
+          if (sub == 0) g2p_gather_global(g, mp, b, nvl, nC);
+        } else if (sub == 0) {
+          g2p_gather_half<0>(tile, nv, bx, G, b, mp.dx, s4, nvl, nC);
+        } else {
+          g2p_gather_half<1>(tile, nv, bx, G, b, mp.dx, s4, nvl, nC);
+        }
       }
-      __syncwarp();  // the tile is free again
-    } else if (live) {
-      // ---- first launch: the state from the particle fields
+      // the odd half's sums to the even half's lanes, through the part of
+      // the tile the staged velocities leave free
+      float* const xch = tile + kXchOffset;
+      if (sub == 1 && lp < ch.y) {
 #pragma unroll
-      for (int a = 0; a < 3; ++a) V[a] = pt.v[a * n + p];
+        for (int q = 0; q < 3; ++q) xch[q * kChunk + lp] = nvl[q];
 #pragma unroll
-      for (int a = 0; a < 9; ++a) Cn[a] = pt.C[(int64_t)a * n + p];
+        for (int q = 0; q < 9; ++q) xch[(3 + q) * kChunk + lp] = nC[q];
+      }
+      __syncthreads();
+      if (sub == 0 && lp < ch.y) {
+#pragma unroll
+        for (int q = 0; q < 3; ++q) nvl[q] += xch[q * kChunk + lp];
+#pragma unroll
+        for (int q = 0; q < 9; ++q) nC[q] += xch[(3 + q) * kChunk + lp];
+        g2p_finish_f(pt, p, mp, X, nvl, nC, Fo, do_p2g ? ss : nullptr, kChunk, lp);
+#pragma unroll
+        for (int r = 0; r < 3; ++r) nb[r] = base_of(X[r], mp.inv_dx);
+        nb_live = true;
+      }
+    } else {
+      __syncthreads();  // publishes the s_lo / s_hi reset
+      if (tid < ch.y) {
+        // ---- first launch: stage the state from the particle fields
+        const int p = A.perm[ch.x + tid];
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+          const float x = pt.x[q * n + p];
+          ss[(kSx + q) * kChunk + tid] = x;
+          ss[(kSv + q) * kChunk + tid] = pt.v[q * n + p];
+          nb[q] = base_of(x, mp.inv_dx);
+        }
+#pragma unroll
+        for (int q = 0; q < 9; ++q) {
+          ss[(kSC + q) * kChunk + tid] = pt.C[(int64_t)q * n + p];
+          ss[(kSF + q) * kChunk + tid] = pt.F[(int64_t)q * n + p];
+        }
+        nb_live = true;
+      }
     }
     if (!do_p2g) continue;
-    // ---- node box of substep s: base nodes of the chunk's particles + 2
+    box_reduce(nb_live, nb, s_lo, s_hi);
+    __syncthreads();  // the state stage and the box of substep s are complete
     int32_t rec[6];
 #pragma unroll
     for (int r = 0; r < 3; ++r) {
-      const int b = base_of(X[r], mp.inv_dx);
-      const int lo = __reduce_min_sync(0xffffffffu, live ? b : INT_MAX);
-      const int hi = __reduce_max_sync(0xffffffffu, live ? b : INT_MIN);
-      rec[r] = max(lo, 0);
-      rec[3 + r] = hi == INT_MIN ? -1 : min(min(hi, G) + 2, G - 1);
+      rec[r] = max(s_lo[r], 0);
+      rec[3 + r] = s_hi[r] == INT_MIN ? -1 : min(min(s_hi[r], G) + 2, G - 1);
     }
     const Box bx = load_box(rec);
-    const bool staged = bx.vol <= kWarpTileCap;
+    const bool staged = bx.vol <= kTileCap;
     const int nv = staged ? bx.vol : 0;
-    if (lane < 6) {
-      int32_t rv = rec[0];
+    if (tid == 0) {
+      int32_t* const out = A.box + bs * A.box_stride + 6 * c;
 #pragma unroll
-      for (int r = 1; r < 6; ++r) rv = lane == r ? rec[r] : rv;  // a select chain keeps rec in registers
-      A.box[bs * A.box_stride + 6 * c + lane] = rv;
+      for (int r = 0; r < 6; ++r) out[r] = rec[r];
+      if (!staged) atomicAdd(A.meta + kMetaOverflow, 1);
     }
-    if (lane == 0 && !staged) atomicAdd(A.meta + kMetaOverflow, 1);
-    // ---- P2G payload of substep s (lane = particle)
-    BSpline b;
-    float pf[3] = {0.f, 0.f, 0.f};
-    if (live) {
-      bspline(X, mp.inv_dx, b);
-      P2GParticle q;
-      p2g_particle_rows(Fn, Cn, V, 1, 0, pmass, pvol0, mp, q);
-      pt.Jp[p] = q.J;
-      float* const rq = sp + lane * kQn;
-      *reinterpret_cast<float4*>(rq + kQmv) = make_float4(q.mv[0], q.mv[1], q.mv[2], q.mass);
-      *reinterpret_cast<float4*>(rq + kQaff) = make_float4(q.aff[0], q.aff[1], q.aff[2], q.aff[3]);
-      *reinterpret_cast<float4*>(rq + kQaff + 4) = make_float4(q.aff[4], q.aff[5], q.aff[6], q.aff[7]);
-      rq[kQaff + 8] = q.aff[8];
-    }
-    if (REACT) {
-      // the chunk's lattice box (force field, phi) in the tile
-      for (int li = lane; li < nv; li += 32) {
-        int i, j, k;
-        box_ijk(bx, li, i, j, k);
-        float h0 = 0.f, h1 = 0.f, h2 = 0.f, ph = 0.f;
-        if (i < A.L.nx && j < A.L.ny && k < A.L.nz) {
-          const int64_t cl = lat_cell(A.L, i, j, k);
-          h0 = A.hydro[cl];
-          h1 = A.hydro[A.L.pitch + cl];
-          h2 = A.hydro[2 * A.L.pitch + cl];
-          if (A.cp.kind != 0) ph = A.phi[cl];
+    // ---- P2G payload of substep s: warps of role 0 the stress and affine
+    // momentum, warps of role 1 the B-spline data and the reaction force
+    {
+      const int role = wid & 1, slot = pslot;
+      if (role == 0) {
+        if (slot < ch.y) {
+          const int p = pq;
+          P2GParticle q;
+          p2g_particle_rows(ss + kSF * kChunk, ss + kSC * kChunk, ss + kSv * kChunk, kChunk, slot, pmass, pvol0, mp,
+                            q);
+          pt.Jp[p] = q.J;
+          float* const rq = sp + slot * kQn;
+          *reinterpret_cast<float4*>(rq + kQmv) = make_float4(q.mv[0], q.mv[1], q.mv[2], q.mass);
+          *reinterpret_cast<float4*>(rq + kQaff) = make_float4(q.aff[0], q.aff[1], q.aff[2], q.aff[3]);
+          *reinterpret_cast<float4*>(rq + kQaff + 4) = make_float4(q.aff[4], q.aff[5], q.aff[6], q.aff[7]);
+          rq[kQaff + 8] = q.aff[8];
         }
-        tile[li] = h0;
-        tile[nv + li] = h1;
-        tile[2 * nv + li] = h2;
-        tile[3 * nv + li] = ph;
-      }
-      __syncwarp();
-      if (live) {
-        const float J = det3(Fn);
-        ReactParticle rp;
-        if (staged)
-          reaction_particle_staged(tile, bx, nv, A.L, A.cp, b, J, pvol0, scale, rp);
-        else
-          reaction_particle(A.L, A.hydro, A.phi, A.cp, b, J, pvol0, scale, rp);
-        if (rp.act) ++n_act;
-        pmax = fmaxf(pmax, rp.pnorm);
-        if (rp.gated)
-          for (int r = 0; r < 3; ++r) pn[r] += (double)rp.pf[r];
-        if (rp.scatter)
-          for (int r = 0; r < 3; ++r) pf[r] = rp.pf[r];
+      } else {
+        if (REACT && staged) {
+          // the chunk's lattice box (force field, phi) into shared memory, by
+          // the role-1 warps only (named barrier 1)
+          for (int li = slot; li < nv; li += T / 2) {
+            int i, j, k;
+            box_ijk(bx, li, i, j, k);
+            float h0 = 0.f, h1 = 0.f, h2 = 0.f, ph = 0.f;
+            if (i < A.L.nx && j < A.L.ny && k < A.L.nz) {
+              const int64_t cl = lat_cell(A.L, i, j, k);
+              h0 = A.hydro[cl];
+              h1 = A.hydro[A.L.pitch + cl];
+              h2 = A.hydro[2 * A.L.pitch + cl];
+              if (A.cp.kind != 0) ph = A.phi[cl];
+            }
+            tile[li] = h0;
+            tile[nv + li] = h1;
+            tile[2 * nv + li] = h2;
+            tile[3 * nv + li] = ph;
+          }
+          asm volatile("bar.sync 1, %0;" ::"n"(kSeqT / 2) : "memory");
+        }
+        if (slot < ch.y) {
+          const float X[3] = {ss[kSx * kChunk + slot], ss[(kSx + 1) * kChunk + slot], ss[(kSx + 2) * kChunk + slot]};
+          BSpline b;
+          bspline(X, mp.inv_dx, b);
+          float pf[3] = {0.f, 0.f, 0.f};
+          if (REACT) {
+            float Fp[9];
+#pragma unroll
+            for (int r = 0; r < 9; ++r) Fp[r] = ss[(kSF + r) * kChunk + slot];
+            const float J = det3(Fp);
+            ReactParticle rp;
+            if (staged)
+              reaction_particle_staged(tile, bx, nv, A.L, A.cp, b, J, pvol0, s_scale, rp);
+            else
+              reaction_particle(A.L, A.hydro, A.phi, A.cp, b, J, pvol0, s_scale, rp);
+            if (rp.act) ++n_act;
+            pmax = fmaxf(pmax, rp.pnorm);
+            if (rp.gated)
+              for (int r = 0; r < 3; ++r) pn[r] += (double)rp.pf[r];
+            if (rp.scatter)
+              for (int r = 0; r < 3; ++r) pf[r] = rp.pf[r];
+          }
+          float* const rq = sp + slot * kQn;
+          *reinterpret_cast<float4*>(rq + kQbase) =
+              make_float4(__int_as_float(b.base[0]), __int_as_float(b.base[1]), __int_as_float(b.base[2]), b.fx[0]);
+          *reinterpret_cast<float4*>(rq + kQfx1) = make_float4(b.fx[1], b.fx[2], pf[0], pf[1]);
+          *reinterpret_cast<float4*>(rq + kQwx) = make_float4(b.w[0][0], b.w[0][1], b.w[0][2], pf[2]);
+          *reinterpret_cast<float4*>(rq + kQwy) = make_float4(b.w[1][0], b.w[1][1], b.w[1][2], 0.f);
+          *reinterpret_cast<float4*>(rq + kQwz) = make_float4(b.w[2][0], b.w[2][1], b.w[2][2], 0.f);
+        }
       }
     }
-    if (live) {
-      float* const rq = sp + lane * kQn;
-      *reinterpret_cast<float4*>(rq + kQbase) =
-          make_float4(__int_as_float(b.base[0]), __int_as_float(b.base[1]), __int_as_float(b.base[2]), b.fx[0]);
-      *reinterpret_cast<float4*>(rq + kQfx1) = make_float4(b.fx[1], b.fx[2], pf[0], pf[1]);
-      *reinterpret_cast<float4*>(rq + kQwx) = make_float4(b.w[0][0], b.w[0][1], b.w[0][2], pf[2]);
-      *reinterpret_cast<float4*>(rq + kQwy) = make_float4(b.w[1][0], b.w[1][1], b.w[1][2], 0.f);
-      *reinterpret_cast<float4*>(rq + kQwz) = make_float4(b.w[2][0], b.w[2][1], b.w[2][2], 0.f);
-    }
-    __syncwarp();  // payload complete; the lattice box is no longer needed
-    for (int i = lane; i < 7 * nv; i += 32) tile[i] = 0.f;
-    __syncwarp();
-    // ---- P2G scatter of substep s into buffer bs: lane o on stencil node o,
-    // the chunk's particles one at a time; they are sorted by base node
-    // (fsi_mpm_bin), so a run of particles with the same base is summed in
-    // registers and added to the tile once per node value
+    __syncthreads();  // payload complete; the lattice box is no longer needed
+    for (int i = tid; i < 7 * nv; i += T) tile[i] = 0.f;
+    __syncthreads();
+    // ---- P2G scatter of substep s into buffer bs.  Warp w takes kRun
+    // consecutive particles of the chunk, one at a time, lane o on stencil node
+    // o; particles are sorted by base node within the chunk (fsi_mpm_bin), so
+    // a run of particles with the same base is summed in registers and added
+    // to the tile with one shared-memory atomic per node value.
     const FsiGrid g = grid_of(A, bs);
     float* const dst[7] = {g.v, g.v + N, g.v + 2 * N, g.m, g.f_ext, g.f_ext + N, g.f_ext + 2 * N};
     {
@@ -701,18 +766,15 @@ __device__ __forceinline__ void mpm_seq_body(const SeqArgs& A, int vb, int vg) {
 #pragma unroll
       for (int q = 0; q < NQ; ++q) acc[q] = 0.f;
       int cb0 = INT_MIN, cb1 = 0, cb2 = 0;  // base of the run (warp-uniform)
-      // adds the run's sums of this lane's node to the tile (or the grid);
-      // called by the whole warp
+      // adds the run's sums of this lane's node to the tile (or the grid)
       auto flush_run = [&]() {
         const int I = cb0 + ox, Jj = cb1 + oy, K = cb2 + oz;
-        if (staged) __syncwarp();  // the previous run's tile updates are done
         if (lane < 27 && I >= 0 && I < G && Jj >= 0 && Jj < G && K >= 0 && K < G) {
           if (staged) {
-            // the lanes of a run hold distinct nodes: plain read-modify-write
             const int li = ((K - bx.lo[2]) * bx.ext[1] + (Jj - bx.lo[1])) * bx.ext[0] + (I - bx.lo[0]);
 #pragma unroll
             for (int q = 0; q < NQ; ++q)
-              if (acc[q] != 0.f) tile[q * nv + li] += acc[q];
+              if (acc[q] != 0.f) atomicAdd(&tile[q * nv + li], acc[q]);
           } else {
             const int64_t node = ((int64_t)K * G + Jj) * G + I;
 #pragma unroll
@@ -723,7 +785,8 @@ __device__ __forceinline__ void mpm_seq_body(const SeqArgs& A, int vb, int vg) {
 #pragma unroll
         for (int q = 0; q < NQ; ++q) acc[q] = 0.f;
       };
-      for (int lp = 0; lp < ch.y; ++lp) {
+      const int p1 = min(wid * kRun + kRun, ch.y);
+      for (int lp = wid * kRun; lp < p1; ++lp) {
         const float* const rq = sp + lp * kQn;
         const float4 q4 = *reinterpret_cast<const float4*>(rq + kQbase);
         const int b0 = __float_as_int(q4.x), b1 = __float_as_int(q4.y), b2 = __float_as_int(q4.z);
@@ -770,8 +833,8 @@ __device__ __forceinline__ void mpm_seq_body(const SeqArgs& A, int vb, int vg) {
         gmax = fmaxf(gmax, sqrtf(gm2));
       }
     }
-    __syncwarp();
-    for (int li = lane; li < nv; li += 32) {
+    __syncthreads();
+    for (int li = tid; li < nv; li += T) {
       int i, j, k;
       box_ijk(bx, li, i, j, k);
       const int64_t node = ((int64_t)k * G + j) * G + i;
@@ -781,11 +844,10 @@ __device__ __forceinline__ void mpm_seq_body(const SeqArgs& A, int vb, int vg) {
         if (v != 0.f) atomicAdd(dst[q] + node, v);
       }
     }
-    __syncwarp();  // the tile and the records are free for the next chunk
   }
   if (REACT && do_p2g) {
     // diagnostics reductions (penalty.py:202-240, moving_boundary.py:312-374):
-    // warp, then one global atomic per warp and quantity
+    // warp, then CTA, then one global atomic per CTA and quantity
     const int na = __reduce_add_sync(0xffffffffu, (unsigned)n_act);
     const float pm = warp_max(pmax), gm = warp_max(gmax);
     double r6[6];
@@ -795,12 +857,29 @@ __device__ __forceinline__ void mpm_seq_body(const SeqArgs& A, int vb, int vg) {
       r6[3 + r] = warp_sum_d(gn[r]);
     }
     if (lane == 0) {
-      if (na) atomicAdd(&st->active_reaction_particle_count, na);
-      if (pm > 0.f) atomic_max_nonneg(&st->max_particle_reaction_norm, pm);
-      if (gm > 0.f) atomic_max_nonneg(&st->max_grid_reaction_norm, gm);
+      s_cnt[wid] = na;
+      s_fmax[wid][0] = pm;
+      s_fmax[wid][1] = gm;
+#pragma unroll
+      for (int r = 0; r < 6; ++r) s_dsum[wid][r] = r6[r];
+    }
+    __syncthreads();
+    if (tid == 0) {
+      int ca = 0;
+      float m0 = 0.f, m1 = 0.f;
+      double d[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+      for (int w = 0; w < NW; ++w) {
+        ca += s_cnt[w];
+        m0 = fmaxf(m0, s_fmax[w][0]);
+        m1 = fmaxf(m1, s_fmax[w][1]);
+        for (int r = 0; r < 6; ++r) d[r] += s_dsum[w][r];
+      }
+      if (ca) atomicAdd(&st->active_reaction_particle_count, ca);
+      if (m0 > 0.f) atomic_max_nonneg(&st->max_particle_reaction_norm, m0);
+      if (m1 > 0.f) atomic_max_nonneg(&st->max_grid_reaction_norm, m1);
       for (int r = 0; r < 3; ++r) {
-        if (r6[r] != 0.0) atomicAdd(&st->net_particle_reaction[r], r6[r]);
-        if (r6[3 + r] != 0.0) atomicAdd(&st->net_grid_reaction[r], r6[3 + r]);
+        if (d[r] != 0.0) atomicAdd(&st->net_particle_reaction[r], d[r]);
+        if (d[3 + r] != 0.0) atomicAdd(&st->net_grid_reaction[r], d[3 + r]);
       }
     }
   }
@@ -813,7 +892,7 @@ __global__ __launch_bounds__(kSeqT) void k_mpm_seq_prologue(const __grid_constan
 }
 
 template <bool REACT>
-__global__ __launch_bounds__(kSeqT, 4) void k_mpm_seq(const __grid_constant__ SeqArgs A) {
+__global__ __launch_bounds__(kSeqT, 2) void k_mpm_seq(const __grid_constant__ SeqArgs A) {
   griddep_wait();
   griddep_launch();
   mpm_seq_body<REACT>(A, blockIdx.x, gridDim.x);
@@ -879,7 +958,7 @@ int sm_count() { return device_sm_count(); }
 
 inline unsigned nblk(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
-// CTAs of a fused-sequence launch: one resident wave (at most one warp per chunk)
+// CTAs of a fused-sequence launch: one resident wave (at most one CTA per chunk)
 int seq_ctas(bool react, int max_chunks, int* ctas) {
   static int occ[64][2] = {};
   int dev = 0;
@@ -897,8 +976,7 @@ int seq_ctas(bool react, int max_chunks, int* ctas) {
       return rc;
     o = b > 0 ? b : 1;
   }
-  // one resident wave of CTAs of kSeqW warps, at most one warp per chunk
-  *ctas = std::max(1, std::min((max_chunks + kSeqW - 1) / kSeqW, sm_count() * o));
+  *ctas = std::max(1, std::min(max_chunks, sm_count() * o));
   return FSI_OK;
 }
 
@@ -1060,7 +1138,7 @@ __global__ __launch_bounds__(kSeqT) void k_batch_mpm_seq_prologue(const FsiBatch
   seq_prologue_body(A, blockIdx.x, gridDim.x);
 }
 
-__global__ __launch_bounds__(kSeqT, 4) void k_batch_mpm_seq(const FsiBatchCase* __restrict__ cases, int s, int M) {
+__global__ __launch_bounds__(kSeqT, 2) void k_batch_mpm_seq(const FsiBatchCase* __restrict__ cases, int s, int M) {
   __shared__ SeqArgs A;
   const FsiBatchCase& bc = cases[blockIdx.y];
   if (!bc.active) return;
@@ -1122,10 +1200,11 @@ extern "C" int fsi_batch_mpm_substeps(FsiBatchCase* cases, const FsiBatchDims* d
       attr_set[dev] = true;
     }
   }
-  // about one warp per chunk of the largest case (a bin's chunks hold <= kChunk particles each; bins
-  // partly filled add chunks): warps stride over the case's chunk table
-  const unsigned gx = (unsigned)std::min<int64_t>(nblk(d->max_chunks, kSeqW),
-                                                  nblk(2 * nblk(d->max_particles, kChunk) + 8, kSeqW));
+  // about one CTA per chunk of the largest case (a bin's chunks hold <= 128 particles each; bins
+  // partly filled add chunks): CTAs stride over the case's chunk table
+  if (d->mpm_ctas < 0 || d->mpm_ctas > 65535) return invalid("FsiBatchDims.mpm_ctas must be in 0..65535");
+  const unsigned gx = d->mpm_ctas > 0 ? (unsigned)d->mpm_ctas
+                                      : (unsigned)std::min<int64_t>(d->max_chunks, 2 * nblk(d->max_particles, kChunk) + 8);
   const dim3 gc(gx, d->n_cases);
   k_batch_mpm_seq_prologue<<<gc, kSeqT, 0, st>>>(cases);
   if ((rc = launch_check("k_batch_mpm_seq_prologue"))) return rc;

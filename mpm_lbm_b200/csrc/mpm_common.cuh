@@ -233,12 +233,11 @@ __device__ __forceinline__ float det3(const float (&M)[9]) {
 // advect, clamp, update F and apply the step-112 controls, then store
 // (solid.py:261-315); nv and nC are the gathered velocity and affine matrix.
 // With a stage (rows x 3, v 3, C 9, F 9 of stride ld, column col) the new
-// state is also written there; vo / Fno receive the new velocity and F.
+// state is also written there.
 // Fo: the particle's deformation gradient before the substep
 __device__ __forceinline__ void g2p_finish_f(const FsiParticles& pt, int p, const FsiMpmParams& mp, float X[3],
                                              const float nv[3], float nC[9], const float Fo[9],
-                                             float* stage = nullptr, int ld = 0, int col = 0, float* vo = nullptr,
-                                             float* Fno = nullptr) {
+                                             float* stage = nullptr, int ld = 0, int col = 0) {
   const int n = pt.n;
   float v[3];
 #pragma unroll
@@ -323,14 +322,6 @@ __device__ __forceinline__ void g2p_finish_f(const FsiParticles& pt, int p, cons
       stage[(6 + a) * ld + col] = nC[a];
       stage[(15 + a) * ld + col] = Fn[a];
     }
-  }
-  if (vo) {
-#pragma unroll
-    for (int a = 0; a < 3; ++a) vo[a] = v[a];
-  }
-  if (Fno) {
-#pragma unroll
-    for (int a = 0; a < 9; ++a) Fno[a] = Fn[a];
   }
 }
 

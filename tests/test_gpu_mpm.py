@@ -291,7 +291,8 @@ def test_binned_layout_and_argument_checks():
 
     nb, mc = ctypes.c_int32(), ctypes.c_int32()
     call("fsi_mpm_bins_layout", 1000, 50, ctypes.byref(nb), ctypes.byref(mc))
-    assert nb.value == 7 ** 3 and mc.value == 8 + 7 ** 3  # ceil(50 / 8)^3 bins; ceil(1000 / 128) + min(1000, bins)
+    # ceil(50 / 8)^3 bins; ceil(1000 / FSI_BIN_CHUNK) + min(1000, bins) chunks
+    assert nb.value == 7 ** 3 and mc.value == 8 + 7 ** 3
     with pytest.raises(FsiError):
         call("fsi_mpm_bins_layout", 0, 50, ctypes.byref(nb), ctypes.byref(mc))
     gpu, _ = make_solids()
