@@ -11,7 +11,7 @@ mpm_lbm_b200.lbm_boundary_diagnostics and mpm_lbm_b200.lbm_stability_diagnostics
 (tests/test_diagnostics.py on the CPU, tests/test_gpu_diagnostics.py on the
 device).  Usage::
 
-    python tests/golden/make_diagnostics_fixture.py [--ref /root/reference]
+    python tests/golden/make_diagnostics_fixture.py --ref PATH
 """
 
 from __future__ import annotations
@@ -105,8 +105,10 @@ def _jsonable(value):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("REF_ROOT"), help="reference checkout (or set REF_ROOT)")
     args = ap.parse_args()
+    if not args.ref:
+        ap.error("give the reference checkout with --ref or REF_ROOT")
     bd = _load(args.ref, "lbm_boundary_diagnostics")
     sd = _load(args.ref, "lbm_stability_diagnostics")
     out = {"snapshots": {}, "records": {}}

@@ -6,7 +6,7 @@ in for it (sequential, f32 storage).  Outputs ``tests/golden/*.npz``, which
 the CPU tests use to pin the oracle and the GPU tests use to pin the CUDA
 path.  Usage::
 
-    python tests/golden/make_fixtures.py [--ref /root/reference] [--only NAME]
+    python tests/golden/make_fixtures.py --ref PATH [--only NAME]
 
 Each fixture stores its inputs and the reference's outputs in the reference's
 own layouts (cell fields (nx, ny, nz[, c]), particle fields (n[, c])).
@@ -415,9 +415,11 @@ UNIT = {
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default=os.environ.get("REF_ROOT", "/root/reference"))
+    ap.add_argument("--ref", default=os.environ.get("REF_ROOT"), help="reference checkout (or set REF_ROOT)")
     ap.add_argument("--only", default=None)
     args = ap.parse_args()
+    if not args.ref:
+        ap.error("give the reference checkout with --ref or REF_ROOT")
     install_shim(args.ref)
     names = list(UNIT) + list(DRIVER_CASES) + ["drv_duct_lim"]
     if args.only:

@@ -8,7 +8,7 @@ write_lbm_restart_npz; the file it wrote (tests/golden/lbm_restart_ref.npz) and
 the statistics dictionary it returned (tests/golden/lbm_restart_ref_stats.json)
 pin mpm_lbm_b200.restart in tests/test_restart.py.  Usage::
 
-    python tests/golden/make_restart_fixture.py [--ref /root/reference]
+    python tests/golden/make_restart_fixture.py --ref PATH
 """
 
 from __future__ import annotations
@@ -45,8 +45,10 @@ def fixture_metadata(n=N):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("REF_ROOT"), help="reference checkout (or set REF_ROOT)")
     args = ap.parse_args()
+    if not args.ref:
+        ap.error("give the reference checkout with --ref or REF_ROOT")
     path = os.path.join(args.ref, "src", "mpm_lbm", "sim", "lbm", "restart.py")
     spec = importlib.util.spec_from_file_location("reference_lbm_restart", path)
     mod = importlib.util.module_from_spec(spec)

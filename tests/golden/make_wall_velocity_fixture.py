@@ -10,7 +10,7 @@ mpm_lbm_b200.wall_velocity (tests/test_wall_velocity.py on the CPU,
 tests/test_gpu_wall_velocity.py on the device).  ``inputs()`` rebuilds the
 seeded arrays.  Usage::
 
-    python tests/golden/make_wall_velocity_fixture.py [--ref /root/reference]
+    python tests/golden/make_wall_velocity_fixture.py --ref PATH
 """
 
 from __future__ import annotations
@@ -74,8 +74,10 @@ class _Lattice:
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("REF_ROOT"), help="reference checkout (or set REF_ROOT)")
     args = ap.parse_args()
+    if not args.ref:
+        ap.error("give the reference checkout with --ref or REF_ROOT")
     sys.path.insert(0, HERE)
     import taichi_shim  # noqa: E402
 
