@@ -296,9 +296,12 @@ def run_batched(args):
 
     cases = sample_box_cases(args.cases, seed=0)
     cells = sum(c.cells for c in cases)
-    tuning = tune_batch(lambda: [c.make_driver(storage=args.storage) for c in cases], storage=args.storage,
-                        mpm_substeps=10)
-    torch.cuda.empty_cache()
+    if args.no_autotune:
+        tuning = {"lbm_tune": 0 if args.lbm_tune is None else args.lbm_tune, "mpm_ctas": 0, "ms_per_step": None}
+    else:
+        tuning = tune_batch(lambda: [c.make_driver(storage=args.storage) for c in cases], storage=args.storage,
+                            mpm_substeps=10)
+        torch.cuda.empty_cache()
     batch = FSIBatch(capacity=len(cases), storage=args.storage, mpm_substeps=10, lbm_tune=tuning["lbm_tune"],
                      mpm_ctas=tuning["mpm_ctas"])
     for c in cases:

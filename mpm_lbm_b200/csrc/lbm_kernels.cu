@@ -625,6 +625,16 @@ __device__ __forceinline__ void stp(const Case& c, int s, int idx, float v) {
   Pop<H>::st(c, s, (int64_t)idx, v);
 }
 
+// mb_subcycle_force_accum_norm_max over the lanes of a warp that reach this
+// point (the LINK cells of the warp): one redux and one atomic per warp
+// instead of one contended atomic per cell (norms are non-negative, so their
+// bit patterns order as unsigned integers)
+__device__ __forceinline__ void accum_max_warp(const Case& c, float nrm) {
+  const unsigned am = __activemask();
+  const unsigned mx = __reduce_max_sync(am, __float_as_uint(nrm));
+  if ((int)(threadIdx.x & 31) == __ffs(am) - 1) atomic_max_nonneg(&c.s.diag->accum_norm_max, __uint_as_float(mx));
+}
+
 // Streaming of a cell next to a solid: half-way bounce-back, with the
 // moving-wall correction and momentum-exchange link force when MOVING
 // (fluid.py:431-440, 488-519).
@@ -889,7 +899,7 @@ __device__ __forceinline__ void lbm_step_tile(const Case& c, int bx, int by, int
         c.s.accum[d * P + cell] = a[d];
         prev[d * P + cell] = 0.f;
       }
-      atomic_max_nonneg(&c.s.diag->accum_norm_max, sqrtf(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]));
+      accum_max_warp(c, sqrtf(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]));
     } else {
 #pragma unroll
       for (int d = 0; d < 3; ++d) prev[d * P + cell] = 0.f;
@@ -1357,7 +1367,7 @@ __device__ __forceinline__ void lbm_step_tile2(const Case& c, int bx, int by, Di
           c.s.accum[d * P + cell] = a[d];
           prev[d * P + cell] = 0.f;
         }
-        atomic_max_nonneg(&c.s.diag->accum_norm_max, sqrtf(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]));
+        accum_max_warp(c, sqrtf(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]));
       } else {
 #pragma unroll
         for (int d = 0; d < 3; ++d) prev[d * P + cell] = 0.f;
@@ -1530,15 +1540,23 @@ __device__ __forceinline__ bool is_changed(const Case& c, int64_t i) {
 }
 
 // reinitialize_new_fluid_cells (fluid.py:1863-1877) and AA re-pairing of the
-// changed cells idx0, idx0 + stride, ... of the change list.
+// changed cells widx0, widx0 + wstride, ... of the change list, one warp per
+// changed cell: lane t < 19 rebuilds the neighbour data of the cell's
+// neighbour t (t = 0: the cell), lane s in 1..18 re-pairs the cell's link s
+// (the links of one cell hold distinct population slots; a link shared by two
+// changed cells is handled by the lower index), lane 0 resets the cell itself.
+// The neighbour rebuild only touches NEAR / LINK bits and nbr, which the link
+// step does not read, so the lanes need no ordering between the two.
 template <bool H>
-__device__ __forceinline__ void relink_cells(const Case& c, int idx0, int stride) {
+__device__ __forceinline__ void relink_cells(const Case& c, int widx0, int wstride) {
   const int count = c.s.diag->change_count;
-  for (int idx = idx0; idx < count; idx += stride) {
+  const int lane = threadIdx.x & 31;
+  for (int idx = widx0; idx < count; idx += wstride) {
     const int64_t ci = c.s.change_list[idx];
     const Coord q = coord_of(c, ci);
-    // neighbour-derived data of ci and its 18 neighbours
-    for (int t = 0; t < 19; ++t) {
+    if (lane < 19) {
+      // neighbour-derived data of ci (lane 0) and its 18 neighbours
+      const int t = lane;
       const int64_t m = t == 0 ? ci : nb_cell(c, q, kEx(t), kEy(t), kEz(t));
       const Coord qm = coord_of(c, m);
       uint32_t mask;
@@ -1556,53 +1574,55 @@ __device__ __forceinline__ void relink_cells(const Case& c, int idx0, int stride
       flag_bits(c.s.flags, m, want, (uint8_t)((kNear | kLink) & ~want));
     }
     const bool reinit_c = c.s.reinit_flag[ci] != 0;
-    if (c.c.parity == 0 && !reinit_c) continue;
-    for (int s = 1; s < 19; ++s) {
+    const int s = lane;
+    if ((c.c.parity != 0 || reinit_c) && s >= 1 && s < 19) {
       const int64_t z = nb_cell(c, q, kEx(s), kEy(s), kEz(s));
-      if (z != ci && is_changed(c, z) && z < ci) continue;  // handled by the other endpoint
-      // canonical orientation: link (y, zz = y + e_sd) with sd odd
-      int64_t y, zz;
-      int sd;
-      if (s & 1) {
-        y = ci;
-        zz = z;
-        sd = s;
-      } else {
-        y = z;
-        zz = ci;
-        sd = kOpp(s);
-      }
-      const bool yf = !(c.s.flags[y] & kSolid), zf = !(c.s.flags[zz] & kSolid);
-      if (c.c.parity == 1) {
-        const bool old_ff = !c.s.old_solid[y] && !c.s.old_solid[zz];
-        const bool new_ff = yf && zf;
-        if (old_ff != new_ff) {
-          const float a = Pop<H>::ld_rw(c, sd, zz);
-          const float b = Pop<H>::ld_rw(c, kOpp(sd), y);
-          Pop<H>::st(c, sd, zz, b);
-          Pop<H>::st(c, kOpp(sd), y, a);
+      // a link to another changed cell with a lower index belongs to that cell
+      if (!(z != ci && is_changed(c, z) && z < ci)) {
+        // canonical orientation: link (y, zz = y + e_sd) with sd odd
+        int64_t y, zz;
+        int sd;
+        if (s & 1) {
+          y = ci;
+          zz = z;
+          sd = s;
+        } else {
+          y = z;
+          zz = ci;
+          sd = kOpp(s);
+        }
+        const bool yf = !(c.s.flags[y] & kSolid), zf = !(c.s.flags[zz] & kSolid);
+        if (c.c.parity == 1) {
+          const bool old_ff = !c.s.old_solid[y] && !c.s.old_solid[zz];
+          const bool new_ff = yf && zf;
+          if (old_ff != new_ff) {
+            const float a = Pop<H>::ld_rw(c, sd, zz);
+            const float b = Pop<H>::ld_rw(c, kOpp(sd), y);
+            Pop<H>::st(c, sd, zz, b);
+            Pop<H>::st(c, kOpp(sd), y, a);
+          }
+        }
+        if (c.s.reinit_flag[zz]) {
+          float u[3];
+          reset_velocity(c, zz, u);
+          const float v = feq(sd, c.p.rho0, u[0], u[1], u[2]);
+          if (c.c.parity == 1 && yf)
+            Pop<H>::st(c, kOpp(sd), y, v);
+          else
+            Pop<H>::st(c, sd, zz, v);
+        }
+        if (c.s.reinit_flag[y]) {
+          float u[3];
+          reset_velocity(c, y, u);
+          const float v = feq(kOpp(sd), c.p.rho0, u[0], u[1], u[2]);
+          if (c.c.parity == 1 && zf)
+            Pop<H>::st(c, sd, zz, v);
+          else
+            Pop<H>::st(c, kOpp(sd), y, v);
         }
       }
-      if (c.s.reinit_flag[zz]) {
-        float u[3];
-        reset_velocity(c, zz, u);
-        const float v = feq(sd, c.p.rho0, u[0], u[1], u[2]);
-        if (c.c.parity == 1 && yf)
-          Pop<H>::st(c, kOpp(sd), y, v);
-        else
-          Pop<H>::st(c, sd, zz, v);
-      }
-      if (c.s.reinit_flag[y]) {
-        float u[3];
-        reset_velocity(c, y, u);
-        const float v = feq(kOpp(sd), c.p.rho0, u[0], u[1], u[2]);
-        if (c.c.parity == 1 && zf)
-          Pop<H>::st(c, sd, zz, v);
-        else
-          Pop<H>::st(c, kOpp(sd), y, v);
-      }
     }
-    if (reinit_c) {
+    if (reinit_c && lane == 0) {
       float u[3];
       reset_velocity(c, ci, u);
       Pop<H>::st(c, 0, ci, feq(0, c.p.rho0, u[0], u[1], u[2]));
@@ -1617,7 +1637,7 @@ __device__ __forceinline__ void relink_cells(const Case& c, int idx0, int stride
 
 template <bool H>
 __global__ void k_relink(const Case c) {
-  relink_cells<H>(c, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+  relink_cells<H>(c, (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), (int)((gridDim.x * blockDim.x) >> 5));
 }
 
 // reinit flags are consumed only after every link of every changed cell is done
@@ -2147,13 +2167,15 @@ __global__ void __launch_bounds__(256) k_wall_velocity(const Case c, const doubl
   }
 }
 
-// finalize_moving_boundary_force_accumulator (fluid.py:475-486)
+// finalize_moving_boundary_force_accumulator (fluid.py:475-486), grid-stride
+// over the cells; the two norm maxima are reduced over the CTA and added with
+// one atomic each per CTA (one per warp contended on the two addresses)
 __global__ void k_accum_finalize(const Case c, int32_t sample_count) {
+  __shared__ float s_max[2][32];
   const int64_t n = (int64_t)c.s.nx * c.s.ny * c.s.nz;
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  float mean_n = 0.f;
-  if (i < n) {
-    const int64_t P = c.s.pitch;
+  const int64_t P = c.s.pitch;
+  float mean_max = 0.f, acc_max = 0.f;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     float a[3];
     for (int d = 0; d < 3; ++d) a[d] = c.s.accum[d * P + i];
     if ((c.c.mode & FSI_MODE_SUBCYCLED) && (c.s.flags[i] & kLink)) {
@@ -2163,7 +2185,7 @@ __global__ void k_accum_finalize(const Case c, int32_t sample_count) {
         last[d * P + i] = 0.f;
         c.s.accum[d * P + i] = a[d];
       }
-      atomic_max_nonneg(&c.s.diag->accum_norm_max, sqrtf(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]));
+      acc_max = fmaxf(acc_max, sqrtf(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]));
     }
     if (sample_count > 0) {
       const float inv = 1.0f / (float)sample_count;
@@ -2172,11 +2194,26 @@ __global__ void k_accum_finalize(const Case c, int32_t sample_count) {
         m[d] = a[d] * inv;
         c.s.hydro[d * P + i] = m[d];
       }
-      mean_n = sqrtf(m[0] * m[0] + m[1] * m[1] + m[2] * m[2]);
+      mean_max = fmaxf(mean_max, sqrtf(m[0] * m[0] + m[1] * m[1] + m[2] * m[2]));
     }
   }
-  const float mx = warp_max(mean_n);
-  if ((threadIdx.x & 31) == 0 && mx > 0.f) atomic_max_nonneg(&c.s.diag->mean_norm_max, mx);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  mean_max = warp_max(mean_max);
+  acc_max = warp_max(acc_max);
+  if (lane == 0) {
+    s_max[0][wid] = mean_max;
+    s_max[1][wid] = acc_max;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float m0 = 0.f, m1 = 0.f;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+      m0 = fmaxf(m0, s_max[0][w]);
+      m1 = fmaxf(m1, s_max[1][w]);
+    }
+    if (m0 > 0.f) atomic_max_nonneg(&c.s.diag->mean_norm_max, m0);
+    if (m1 > 0.f) atomic_max_nonneg(&c.s.diag->accum_norm_max, m1);
+  }
 }
 
 // ------------------------------------------------------------- host ABI ----
@@ -2575,7 +2612,8 @@ extern "C" int fsi_force_accum_finalize(const FsiLbmState* s, const FsiStepCtl* 
   p.s_v = p.s_o = 1.f;
   const Case c = make_case(s, &p, ctl);
   const int64_t n = (int64_t)s->nx * s->ny * s->nz;
-  k_accum_finalize<<<blocks_for(n, 256), 256, 0, st>>>(c, sample_count);
+  k_accum_finalize<<<(unsigned)std::min<int64_t>(blocks_for(n, 256), (int64_t)lbm_sm_count() * 8), 256, 0, st>>>(
+      c, sample_count);
   return launch_check("k_accum_finalize");
 }
 
@@ -2830,7 +2868,7 @@ __global__ void k_batch_relink(const FsiBatchCase* __restrict__ cases) {
   __shared__ Case sc;
   const FsiBatchCase& bc = cases[blockIdx.y];
   if (bc.mode != FSI_BATCH_MOVING || !stage_case(bc, sc, false)) return;
-  relink_cells<H>(sc, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+  relink_cells<H>(sc, (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), (int)((gridDim.x * blockDim.x) >> 5));
 }
 
 __global__ void k_batch_clear_reinit(const FsiBatchCase* __restrict__ cases) {

@@ -58,50 +58,78 @@ __global__ void k_project_scatter(LatView L, FsiParticles pt, FsiCouplingParams 
   if (p < pt.n) project_particle(L, pt, cp, phi, smass, svel, p);
 }
 
-// cells base + lane of one warp (base warp-uniform: the reductions need the
-// whole warp)
-__device__ __forceinline__ void project_normalize_warp(const LatView& L, const FsiCouplingParams& cp, float* phi,
-                                                       float* smass, float* svel, FsiCouplingStats* st,
-                                                       int64_t base) {
-  const int64_t n = (int64_t)L.nx * L.ny * L.nz;
-  const int64_t c = base + (threadIdx.x & 31);
+// normalize_projection (projection.py:67-91) of one cell, with the cell's
+// share of the projection statistics accumulated in a
+struct ProjAcc {
   double pm = 0.0, pvr = 0.0, pvc = 0.0;
   float mx = 0.f;
-  int active = 0;
-  if (c < n) {
-    const float raw = phi[c];
-    const float m = smass[c];
-    mx = raw;
-    if (m > cp.eps_mass) {
-      for (int a = 0; a < 3; ++a) svel[a * L.pitch + c] = svel[a * L.pitch + c] / m;
-    } else {
-      for (int a = 0; a < 3; ++a) svel[a * L.pitch + c] = 0.f;
-    }
-    const float cl = fminf(1.0f, fmaxf(0.0f, raw));
-    phi[c] = cl;
-    active = cl > 1.0e-8f;
-    pm = m;
-    pvr = (double)raw * cp.cell_volume_norm;
-    pvc = (double)cl * cp.cell_volume_norm;
+  int na = 0;
+};
+
+__device__ __forceinline__ void project_normalize_cell(const LatView& L, const FsiCouplingParams& cp, float* phi,
+                                                       float* smass, float* svel, int64_t c, ProjAcc& a) {
+  const float raw = phi[c];
+  const float m = smass[c];
+  a.mx = fmaxf(a.mx, raw);
+  if (m > cp.eps_mass) {
+    for (int q = 0; q < 3; ++q) svel[q * L.pitch + c] = svel[q * L.pitch + c] / m;
+  } else {
+    for (int q = 0; q < 3; ++q) svel[q * L.pitch + c] = 0.f;
   }
-  pm = warp_sum_d(pm);
-  pvr = warp_sum_d(pvr);
-  pvc = warp_sum_d(pvc);
-  mx = warp_max(fmaxf(mx, 0.f));
-  const int na = __popc(__ballot_sync(0xffffffffu, active));
-  if ((threadIdx.x & 31) == 0) {
-    if (pm != 0.0) atomicAdd(&st->projected_mass, pm);
-    if (pvr != 0.0) atomicAdd(&st->projected_volume_raw, pvr);
-    if (pvc != 0.0) atomicAdd(&st->projected_volume_clamped, pvc);
-    if (mx > 0.f) atomic_max_nonneg(&st->max_phi_raw, mx);
-    if (na) atomicAdd(&st->active_cell_count, na);
+  const float cl = fminf(1.0f, fmaxf(0.0f, raw));
+  phi[c] = cl;
+  a.na += cl > 1.0e-8f;
+  a.pm += m;
+  a.pvr += (double)raw * cp.cell_volume_norm;
+  a.pvc += (double)cl * cp.cell_volume_norm;
+}
+
+// the CTA's statistics into st: warp sums, then the CTA's warps in shared
+// memory, then one atomic per CTA and value (an atomic per warp serialised
+// tens of thousands of FP64 adds on five addresses)
+__device__ __forceinline__ void project_stats_flush(ProjAcc a, FsiCouplingStats* st) {
+  __shared__ double s_d[32][3];
+  __shared__ float s_m[32];
+  __shared__ int s_n[32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  a.pm = warp_sum_d(a.pm);
+  a.pvr = warp_sum_d(a.pvr);
+  a.pvc = warp_sum_d(a.pvc);
+  a.mx = warp_max(fmaxf(a.mx, 0.f));
+  a.na = __reduce_add_sync(0xffffffffu, (unsigned)a.na);
+  if (lane == 0) {
+    s_d[wid][0] = a.pm;
+    s_d[wid][1] = a.pvr;
+    s_d[wid][2] = a.pvc;
+    s_m[wid] = a.mx;
+    s_n[wid] = a.na;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    ProjAcc t;
+    for (int w = 0; w < nw; ++w) {
+      t.pm += s_d[w][0];
+      t.pvr += s_d[w][1];
+      t.pvc += s_d[w][2];
+      t.mx = fmaxf(t.mx, s_m[w]);
+      t.na += s_n[w];
+    }
+    if (t.pm != 0.0) atomicAdd(&st->projected_mass, t.pm);
+    if (t.pvr != 0.0) atomicAdd(&st->projected_volume_raw, t.pvr);
+    if (t.pvc != 0.0) atomicAdd(&st->projected_volume_clamped, t.pvc);
+    if (t.mx > 0.f) atomic_max_nonneg(&st->max_phi_raw, t.mx);
+    if (t.na) atomicAdd(&st->active_cell_count, t.na);
   }
 }
 
+// grid-stride over the cells (every thread of the CTA reaches the flush)
 __global__ void k_project_normalize(LatView L, FsiCouplingParams cp, float* phi, float* smass, float* svel,
                                     FsiCouplingStats* st) {
-  project_normalize_warp(L, cp, phi, smass, svel, st,
-                         (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31));
+  const int64_t n = (int64_t)L.nx * L.ny * L.nz;
+  ProjAcc a;
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (int64_t)gridDim.x * blockDim.x)
+    project_normalize_cell(L, cp, phi, smass, svel, c, a);
+  project_stats_flush(a, st);
 }
 
 // ------------------------------------- projection in particle order ----
@@ -588,7 +616,8 @@ extern "C" int fsi_project(const FsiLbmState* s, const FsiParticles* pt, const F
   k_project_scatter<<<nblk(pt->n, 128), 128, 0, st>>>(L, *pt, *cp, s->phi, s->smass, s->svel);
   if ((rc = launch_check("k_project_scatter"))) return rc;
   const int64_t n = (int64_t)s->nx * s->ny * s->nz;
-  k_project_normalize<<<nblk(n, 256), 256, 0, st>>>(L, *cp, s->phi, s->smass, s->svel, stats);
+  k_project_normalize<<<(unsigned)std::min<int64_t>(nblk(n, 256), 8LL * device_sm_count()), 256, 0, st>>>(
+      L, *cp, s->phi, s->smass, s->svel, stats);
   return launch_check("k_project_normalize");
 }
 
@@ -629,7 +658,8 @@ extern "C" int fsi_project_ordered(const FsiLbmState* s, const FsiParticles* pt,
                                                  s->svel);
   if ((rc = launch_check("k_po_gather"))) return rc;
   const int64_t n = (int64_t)s->nx * s->ny * s->nz;
-  k_project_normalize<<<nblk(n, 256), 256, 0, st>>>(L, *cp, s->phi, s->smass, s->svel, stats);
+  k_project_normalize<<<(unsigned)std::min<int64_t>(nblk(n, 256), 8LL * device_sm_count()), 256, 0, st>>>(
+      L, *cp, s->phi, s->smass, s->svel, stats);
   return launch_check("k_project_normalize");
 }
 
@@ -719,9 +749,10 @@ __global__ void k_batch_project_normalize(const FsiBatchCase* __restrict__ cases
   const LatView L = lat_of(bc);
   const FsiCouplingParams cp = bc.cp;
   const int64_t n = (int64_t)L.nx * L.ny * L.nz;
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t base = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += stride)
-    project_normalize_warp(L, cp, bc.lbm.phi, bc.lbm.smass, bc.lbm.svel, bc.proj_stats, base);
+  ProjAcc a;
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (int64_t)gridDim.x * blockDim.x)
+    project_normalize_cell(L, cp, bc.lbm.phi, bc.lbm.smass, bc.lbm.svel, c, a);
+  project_stats_flush(a, bc.proj_stats);
 }
 
 }  // namespace
