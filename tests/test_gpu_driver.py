@@ -52,6 +52,20 @@ def test_driver_matches_reference(name, mpm_path, tmp_path):
     rows = drv.run()
     ref_rows = json.loads(str(d["rows"]))
     assert len(rows) == len(ref_rows)
+    # the measured differences, relative to each field's largest magnitude
+    got_f = {"rho": drv.lbm.rho.to_numpy(), "v": drv.lbm.v.to_numpy(), "F": drv.lbm.F.to_numpy(),
+             "phi": drv.lbm.solid_phi.to_numpy(), "hydro": drv.lbm.hydro_force.to_numpy(),
+             "x": drv.solid.x.to_numpy(), "mpm_v": drv.solid.v.to_numpy(), "mpm_F": drv.solid.F.to_numpy()}
+    ref_f = {"rho": d["lbm_rho"], "v": d["lbm_v"], "F": d["lbm_F"], "phi": d["lbm_solid_phi"],
+             "hydro": d["lbm_hydro_force"], "x": d["mpm_x"], "mpm_v": d["mpm_v"], "mpm_F": d["mpm_F"]}
+    errs = {k: float(np.abs(got_f[k].astype(np.float64) - ref_f[k]).max() / max(np.abs(ref_f[k]).max(), 1e-30))
+            for k in got_f}
+    row_err = 0.0
+    for got, ref in zip(rows, ref_rows):
+        for k, v in ref.items():
+            if isinstance(v, (int, float)) and not isinstance(v, bool) and k != "elapsed_seconds":
+                row_err = max(row_err, abs(got[k] - v) / max(abs(v), 1e-6))
+    print(name, mpm_path, {k: f"{e:.1e}" for k, e in errs.items()}, f"rows {row_err:.1e}")
     np.testing.assert_array_equal(drv.lbm.solid.to_numpy(), d["lbm_solid"])
     np.testing.assert_allclose(drv.lbm.rho.to_numpy(), d["lbm_rho"], rtol=1e-5, atol=1e-6)
     np.testing.assert_allclose(drv.lbm.v.to_numpy(), d["lbm_v"], rtol=1e-3, atol=2e-7)
