@@ -27,9 +27,12 @@ namespace {
 constexpr int kChunk = FSI_BIN_CHUNK;  // particles per chunk
 constexpr int kEdge = FSI_BIN_EDGE;
 // nodes staged per CTA: the stencils of a chunk of one bin span at most
-// (8 + 2)^3 = 1000 nodes; the rest absorbs drift since the last binning (a
-// 13^3 box).  7 floats per node in P2G = 61.5 KB.
-constexpr int kTileCap = 2197;
+// (8 + 2)^3 = 1000 nodes; the rest absorbs a node of drift since the last
+// binning (an 11^3 box).  Two regions of shared memory: the scatter tile (7
+// floats per node, 37 KB) and the stage of the gather's node velocities and of
+// the reaction's lattice box (4 floats per node), so that the tile can be
+// zeroed while the payload is built.
+constexpr int kTileCap = 1331;
 
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
@@ -319,13 +322,13 @@ enum { kSx = 0, kSv = 3, kSC = 6, kSF = 15, kSn = 24 };  // staged particle stat
 // without the tile, [5 + b] buffer b holds recorded boxes not yet zeroed
 enum { kMetaChunks = 0, kMetaRec = 1, kMetaOverflow = 4, kMetaDirty = 5 };
 constexpr int kSeqT = 256;
-constexpr int kTileFloats = (7 * kTileCap + 3) & ~3;  // keeps the payload 16-byte aligned
+constexpr int kTileFloats = (7 * kTileCap + 3) & ~3;  // keeps the next region 16-byte aligned
 // G2P: the staged node velocities use 3 * nv <= 3 * kTileCap floats of the
-// tile; the two stencil halves of a particle meet behind them (12 sums per
-// particle)
+// stage; the two stencil halves of a particle meet behind them (12 sums per
+// particle).  The reaction's lattice box uses 4 * nv.
 constexpr int kXchOffset = (3 * kTileCap + 3) & ~3;
-static_assert(kXchOffset + 12 * kChunk <= kTileFloats, "G2P exchange does not fit the tile");
-constexpr size_t kSeqSmem = sizeof(float) * (kTileFloats + (kQn + kSn) * kChunk);
+constexpr int kStageFloats = ((kXchOffset + 12 * kChunk > 4 * kTileCap ? kXchOffset + 12 * kChunk : 4 * kTileCap) + 3) & ~3;
+constexpr size_t kSeqSmem = sizeof(float) * (kTileFloats + kStageFloats + (kQn + kSn) * kChunk);
 
 struct SeqArgs {
   FsiParticles pt;
@@ -496,8 +499,9 @@ __device__ __forceinline__ void mpm_seq_body(const SeqArgs& A, int vb, int vg) {
   static_assert(kSeqT == 2 * kChunk, "G2P: two warps per 32 particles, one per stencil half");
   extern __shared__ float4 seq_smem4[];
   // G2P: [3][nv] node velocities; payload: [4][nv] lattice box; scatter: [7][nv] tile
-  float* const tile = reinterpret_cast<float*>(seq_smem4);
-  float* const sp = tile + kTileFloats;  // [kChunk][kQn] P2G payload
+  float* const tile = reinterpret_cast<float*>(seq_smem4);  // [7][nv] scatter tile
+  float* const stg = tile + kTileFloats;                      // [3][nv] node velocities / [4][nv] lattice box
+  float* const sp = stg + kStageFloats;  // [kChunk][kQn] P2G payload
   float* const ss = sp + kQn * kChunk;   // [kSn][kChunk] particle state
   __shared__ int s_lo[3], s_hi[3];
   __shared__ float s_scale;
@@ -581,6 +585,10 @@ __device__ __forceinline__ void mpm_seq_body(const SeqArgs& A, int vb, int vg) {
       float X[3] = {0.f, 0.f, 0.f}, Fo[9];
 #pragma unroll
       for (int a = 0; a < 9; ++a) Fo[a] = 0.f;
+      // the fixed flag and position, loaded with the state so that the
+      // finish does not wait on them
+      int pfixed = 0;
+      float pfx[3] = {0.f, 0.f, 0.f};
       if (lp < ch.y) {
         p = A.perm[ch.x + lp];
 #pragma unroll
@@ -588,6 +596,9 @@ __device__ __forceinline__ void mpm_seq_body(const SeqArgs& A, int vb, int vg) {
         if (sub == 0) {
 #pragma unroll
           for (int a = 0; a < 9; ++a) Fo[a] = pt.F[(int64_t)a * n + p];
+          pfixed = pt.fixed[p];
+#pragma unroll
+          for (int a = 0; a < 3; ++a) pfx[a] = pt.fixed_x[a * n + p];
         }
       }
       for (int li = tid; li < nv; li += T) {
@@ -601,9 +612,9 @@ __device__ __forceinline__ void mpm_seq_body(const SeqArgs& A, int vb, int vg) {
           const float f[3] = {g.f_ext[node], g.f_ext[N + node], g.f_ext[2 * N + node]};
           grid_node_velocity(P, m, f, i, j, k, G, mp, v);
         }
-        tile[li] = v[0];
-        tile[nv + li] = v[1];
-        tile[2 * nv + li] = v[2];
+        stg[li] = v[0];
+        stg[nv + li] = v[1];
+        stg[2 * nv + li] = v[2];
       }
       __syncthreads();  // also publishes the s_lo / s_hi reset
       float nvl[3] = {0.f, 0.f, 0.f}, nC[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
@@ -613,14 +624,14 @@ __device__ __forceinline__ void mpm_seq_body(const SeqArgs& A, int vb, int vg) {
         if (!staged) {
           if (sub == 0) g2p_gather_global(g, mp, b, nvl, nC);
         } else if (sub == 0) {
-          g2p_gather_half<0>(tile, nv, bx, G, b, mp.dx, s4, nvl, nC);
+          g2p_gather_half<0>(stg, nv, bx, G, b, mp.dx, s4, nvl, nC);
         } else {
-          g2p_gather_half<1>(tile, nv, bx, G, b, mp.dx, s4, nvl, nC);
+          g2p_gather_half<1>(stg, nv, bx, G, b, mp.dx, s4, nvl, nC);
         }
       }
       // the odd half's sums to the even half's lanes, through the part of
       // the tile the staged velocities leave free
-      float* const xch = tile + kXchOffset;
+      float* const xch = stg + kXchOffset;
       if (sub == 1 && lp < ch.y) {
 #pragma unroll
         for (int q = 0; q < 3; ++q) xch[q * kChunk + lp] = nvl[q];
@@ -633,7 +644,7 @@ __device__ __forceinline__ void mpm_seq_body(const SeqArgs& A, int vb, int vg) {
         for (int q = 0; q < 3; ++q) nvl[q] += xch[q * kChunk + lp];
 #pragma unroll
         for (int q = 0; q < 9; ++q) nC[q] += xch[(3 + q) * kChunk + lp];
-        g2p_finish_f(pt, p, mp, X, nvl, nC, Fo, do_p2g ? ss : nullptr, kChunk, lp);
+        g2p_finish_f(pt, p, mp, X, nvl, nC, Fo, do_p2g ? ss : nullptr, kChunk, lp, pfixed, pfx);
 #pragma unroll
         for (int r = 0; r < 3; ++r) nb[r] = base_of(X[r], mp.inv_dx);
         nb_live = true;
@@ -708,10 +719,10 @@ __device__ __forceinline__ void mpm_seq_body(const SeqArgs& A, int vb, int vg) {
               h2 = A.hydro[2 * A.L.pitch + cl];
               if (A.cp.kind != 0) ph = A.phi[cl];
             }
-            tile[li] = h0;
-            tile[nv + li] = h1;
-            tile[2 * nv + li] = h2;
-            tile[3 * nv + li] = ph;
+            stg[li] = h0;
+            stg[nv + li] = h1;
+            stg[2 * nv + li] = h2;
+            stg[3 * nv + li] = ph;
           }
           asm volatile("bar.sync 1, %0;" ::"n"(kSeqT / 2) : "memory");
         }
@@ -727,7 +738,7 @@ __device__ __forceinline__ void mpm_seq_body(const SeqArgs& A, int vb, int vg) {
             const float J = det3(Fp);
             ReactParticle rp;
             if (staged)
-              reaction_particle_staged(tile, bx, nv, A.L, A.cp, b, J, pvol0, s_scale, rp);
+              reaction_particle_staged(stg, bx, nv, A.L, A.cp, b, J, pvol0, s_scale, rp);
             else
               reaction_particle(A.L, A.hydro, A.phi, A.cp, b, J, pvol0, s_scale, rp);
             if (rp.act) ++n_act;
@@ -745,11 +756,12 @@ __device__ __forceinline__ void mpm_seq_body(const SeqArgs& A, int vb, int vg) {
           *reinterpret_cast<float4*>(rq + kQwy) = make_float4(b.w[1][0], b.w[1][1], b.w[1][2], 0.f);
           *reinterpret_cast<float4*>(rq + kQwz) = make_float4(b.w[2][0], b.w[2][1], b.w[2][2], 0.f);
         }
+        // the scatter tile, free since the last flush, zeroed by the role-1
+        // warps while the role-0 warps finish the polar rotation
+        for (int i = slot; i < 7 * nv; i += T / 2) tile[i] = 0.f;
       }
     }
-    __syncthreads();  // payload complete; the lattice box is no longer needed
-    for (int i = tid; i < 7 * nv; i += T) tile[i] = 0.f;
-    __syncthreads();
+    __syncthreads();  // payload complete, tile zeroed
     // ---- P2G scatter of substep s into buffer bs.  Warp w takes kRun
     // consecutive particles of the chunk, one at a time, lane o on stencil node
     // o; particles are sorted by base node within the chunk (fsi_mpm_bin), so

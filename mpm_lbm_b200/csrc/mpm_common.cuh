@@ -233,11 +233,14 @@ __device__ __forceinline__ float det3(const float (&M)[9]) {
 // advect, clamp, update F and apply the step-112 controls, then store
 // (solid.py:261-315); nv and nC are the gathered velocity and affine matrix.
 // With a stage (rows x 3, v 3, C 9, F 9 of stride ld, column col) the new
-// state is also written there.
+// state is also written there.  fixed_pre / fx_pre: the particle's fixed flag
+// and fixed position when the caller loaded them ahead (-1 / null: loaded
+// here).
 // Fo: the particle's deformation gradient before the substep
 __device__ __forceinline__ void g2p_finish_f(const FsiParticles& pt, int p, const FsiMpmParams& mp, float X[3],
                                              const float nv[3], float nC[9], const float Fo[9],
-                                             float* stage = nullptr, int ld = 0, int col = 0) {
+                                             float* stage = nullptr, int ld = 0, int col = 0, int fixed_pre = -1,
+                                             const float* fx_pre = nullptr) {
   const int n = pt.n;
   float v[3];
 #pragma unroll
@@ -275,7 +278,7 @@ __device__ __forceinline__ void g2p_finish_f(const FsiParticles& pt, int p, cons
     for (int a = 0; a < 3; ++a) v[a] *= d;
   }
   if (mp.lock_z) {
-    X[2] = pt.fixed_x[2 * n + p];
+    X[2] = fx_pre ? fx_pre[2] : pt.fixed_x[2 * n + p];
     v[2] = 0.f;
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
@@ -287,10 +290,10 @@ __device__ __forceinline__ void g2p_finish_f(const FsiParticles& pt, int p, cons
     Fn[8] = 1.0f;
     J = det3(Fn);
   }
-  if (pt.fixed[p]) {
+  if (fixed_pre >= 0 ? fixed_pre != 0 : pt.fixed[p] != 0) {
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-      X[a] = pt.fixed_x[a * n + p];
+      X[a] = fx_pre ? fx_pre[a] : pt.fixed_x[a * n + p];
       v[a] = 0.f;
     }
 #pragma unroll

@@ -4,10 +4,20 @@ The fixtures tests/golden/drv_*.npz hold FSIDriver3D.run() of the reference
 (its own Taichi kernel code executed by tests/golden/taichi_shim.py) for the
 modes none / penalty / moving_boundary (engineering and link-area) /
 subcycled / duct with the limited regularized open boundary.  The CUDA driver
-runs the same config; tolerances (FP32 after a few coupled steps): fields
-rtol 1e-3 on rho/v-scale quantities, particle positions atol 1e-6 (normalised
-units), diagnostics rows rtol 2e-3 / atol 2e-7 (the reference's f32 rest state
-carries ~4e-9 round-off velocities); masks and link counts exact.
+runs the same config; masks and link counts must be exact.
+
+Field tolerances are relative to each field's largest magnitude (measured
+maxima over the six cases and both MPM paths in brackets):
+  rho, populations 2e-6 [5.4e-7]; solid_phi 1e-6 [1.8e-7]; hydro_force 2e-5
+  [5.6e-6]; particle positions 1e-6 absolute (normalised units) [0];
+  particle velocities 1e-5 [1.6e-6]; deformation gradients 1e-6 [1.2e-7];
+  fluid velocity 1e-4 [1.9e-5], except in penalty mode 2e-3 [6.6e-4]: there
+  the penalty force beta phi rho (u_s - u) feeds back on the velocity every
+  step, and the fixture's sequential f32 sums (no fused multiply-add) differ
+  from the kernel's in the last bits.
+Diagnostics rows: rtol 2e-3 / atol 2e-7 (the rows hold maxima and sums of
+those fields; the reference's f32 rest state carries ~4e-9 round-off
+velocities, so near-zero entries need the absolute part).
 """
 
 import json
@@ -66,6 +76,11 @@ def test_driver_matches_reference(name, mpm_path, tmp_path):
             if isinstance(v, (int, float)) and not isinstance(v, bool) and k != "elapsed_seconds":
                 row_err = max(row_err, abs(got[k] - v) / max(abs(v), 1e-6))
     print(name, mpm_path, {k: f"{e:.1e}" for k, e in errs.items()}, f"rows {row_err:.1e}")
+    bounds = {"rho": 2e-6, "F": 2e-6, "phi": 1e-6, "hydro": 2e-5, "mpm_v": 1e-5, "mpm_F": 1e-6,
+              "v": 2e-3 if cfg.get("coupling_mode") == "penalty" else 1e-4}
+    for k, b in bounds.items():
+        assert errs[k] <= b, (k, errs[k], b)
+    assert float(np.abs(got_f["x"].astype(np.float64) - ref_f["x"]).max()) <= 1e-6
     np.testing.assert_array_equal(drv.lbm.solid.to_numpy(), d["lbm_solid"])
     np.testing.assert_allclose(drv.lbm.rho.to_numpy(), d["lbm_rho"], rtol=1e-5, atol=1e-6)
     np.testing.assert_allclose(drv.lbm.v.to_numpy(), d["lbm_v"], rtol=1e-3, atol=2e-7)
