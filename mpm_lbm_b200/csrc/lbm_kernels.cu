@@ -87,7 +87,7 @@ struct Pop<true> {
   static __device__ __forceinline__ float ld_rw(const Case& c, int s, int64_t cell) { return ld(c, s, cell); }
   static __device__ __forceinline__ void st(const Case& c, int s, int64_t cell, float v) {
     const float inv_w = s == 0 ? 3.0f : (s <= 6 ? 18.0f : 36.0f);
-    static_cast<__half*>(c.s.pop)[pop_index(c, s, cell)] = __float2half_rn(v * inv_w - c.p.rho0);
+    static_cast<__half*>(c.s.pop)[pop_index(c, s, cell)] = __float2half_rn(__fmaf_rn(v, inv_w, -c.p.rho0));
   }
   static __device__ __forceinline__ float ldb(const Case& c, int s, int64_t b) {
     const __half h = static_cast<const __half*>(c.s.pop)[b + 32 * s];
@@ -95,7 +95,7 @@ struct Pop<true> {
   }
   static __device__ __forceinline__ void stb(const Case& c, int s, int64_t b, float v) {
     const float inv_w = s == 0 ? 3.0f : (s <= 6 ? 18.0f : 36.0f);
-    static_cast<__half*>(c.s.pop)[b + 32 * s] = __float2half_rn(v * inv_w - c.p.rho0);
+    static_cast<__half*>(c.s.pop)[b + 32 * s] = __float2half_rn(__fmaf_rn(v, inv_w, -c.p.rho0));
   }
 };
 
@@ -679,6 +679,8 @@ __device__ __forceinline__ void store_near_solid(const Case& c, const Nbh& n, in
 // post-collision populations; rho: its density.
 __device__ __forceinline__ void dirstats_warp(const Case& c, const Nbh& n, uint32_t nb, float rho, const float* out,
                                               DirAcc& acc) {
+  // warps without a link cell (most of the lattice) skip the 18 ballots
+  if (!__any_sync(kFull, nb != 0u)) return;
   const int64_t P = c.s.pitch;
   const int lane = threadIdx.x & 31;
 #pragma unroll
@@ -981,20 +983,33 @@ struct Pop2<false> {
   static __device__ __forceinline__ void st(const Case& c, int s, int64_t cell, float2 v) {
     *reinterpret_cast<float2*>(static_cast<float*>(c.s.pop) + pop_index(c, s, cell)) = v;
   }
+  // by block-layout index b of the pair's first cell (b even)
+  static __device__ __forceinline__ float2 ldb(const Case& c, int s, int64_t b) {
+    return __ldg(reinterpret_cast<const float2*>(static_cast<const float*>(c.s.pop) + b + 32 * s));
+  }
+  static __device__ __forceinline__ void stb(const Case& c, int s, int64_t b, float2 v) {
+    *reinterpret_cast<float2*>(static_cast<float*>(c.s.pop) + b + 32 * s) = v;
+  }
 };
 
 template <>
 struct Pop2<true> {
   static __device__ __forceinline__ float2 ld(const Case& c, int s, int64_t cell) {
-    const __half2 h = *reinterpret_cast<const __half2*>(static_cast<const __half*>(c.s.pop) + pop_index(c, s, cell));
-    const float2 f = __half22float2(h);
-    const float w = lattice_w(s);
-    return make_float2(w * (c.p.rho0 + f.x), w * (c.p.rho0 + f.y));
+    return ldb(c, s, pop_index(c, 0, cell));
   }
   static __device__ __forceinline__ void st(const Case& c, int s, int64_t cell, float2 v) {
+    stb(c, s, pop_index(c, 0, cell), v);
+  }
+  // the decode and encode of Pop<true> on both cells at once (paired FP32
+  // instructions, the same roundings)
+  static __device__ __forceinline__ float2 ldb(const Case& c, int s, int64_t b) {
+    const __half2 h = *reinterpret_cast<const __half2*>(static_cast<const __half*>(c.s.pop) + b + 32 * s);
+    return __fmul2_rn(make_float2(lattice_w(s), lattice_w(s)), __fadd2_rn(make_float2(c.p.rho0, c.p.rho0), __half22float2(h)));
+  }
+  static __device__ __forceinline__ void stb(const Case& c, int s, int64_t b, float2 v) {
     const float inv_w = s == 0 ? 3.0f : (s <= 6 ? 18.0f : 36.0f);
-    *reinterpret_cast<__half2*>(static_cast<__half*>(c.s.pop) + pop_index(c, s, cell)) =
-        __floats2half2_rn(v.x * inv_w - c.p.rho0, v.y * inv_w - c.p.rho0);
+    const float2 e = __ffma2_rn(v, make_float2(inv_w, inv_w), make_float2(-c.p.rho0, -c.p.rho0));
+    *reinterpret_cast<__half2*>(static_cast<__half*>(c.s.pop) + b + 32 * s) = __floats2half2_rn(e.x, e.y);
   }
 };
 
@@ -1060,18 +1075,134 @@ __device__ __forceinline__ void bc_face_warp2(const Case& c, int lane, int row, 
   }
 }
 
-// post-streaming populations of one fluid cell next to a solid (per-cell path)
-template <bool ODD, bool H>
-__device__ __forceinline__ void set_near_solid_loads(const Case& c, const Nbh& n, int cell, uint32_t nb, float* F) {
-  F[0] = ldp<H>(c, 0, cell);
+// Neighbourhood of the cell pair (x0, x0 + 1) of a thread (x0 even): the
+// nine wrapped row bases (rows j + dy, k + dz) and the x coordinates x0 - 1,
+// x0, x0 + 1, x0 + 2 (wrapped), with their block-layout indices for lattices
+// whose rows start 32-cell blocks (Case::aligned).  One structure serves both
+// members, so that a thread holds one set of row bases.
+struct PairNbh {
+  int rb[3][3];
+  int xs[4];
+  uint32_t bxs[4];
+  // cell index of the neighbour (dx, dy, dz) of member m (0: x0, 1: x0 + 1)
+  __device__ __forceinline__ int cell(int m, int dx, int dy, int dz) const {
+    return rb[dz + 1][dy + 1] + xs[m + dx + 1];
+  }
+  // block-layout index of population 0 of that neighbour (pop_index without
+  // the 32 s term); aligned: 19 * row base + block index of x, one multiply-add
+  __device__ __forceinline__ int64_t blk(bool aligned, int m, int dx, int dy, int dz) const {
+    if (aligned) return (int64_t)((uint32_t)rb[dz + 1][dy + 1] * 19u + bxs[m + dx + 1]);
+    const uint32_t i = (uint32_t)cell(m, dx, dy, dz);
+    return (int64_t)(i + (i >> 5) * 576u);
+  }
+};
+
+__device__ __forceinline__ void make_pair_nbh(const Case& c, int x0, int j, int k, PairNbh& q) {
+  const int nx = c.s.nx, ny = c.s.ny, nz = c.s.nz;
+  const int jj[3] = {j == 0 ? ny - 1 : j - 1, j, j == ny - 1 ? 0 : j + 1};
+  const int kk[3] = {k == 0 ? nz - 1 : k - 1, k, k == nz - 1 ? 0 : k + 1};
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = 0; b < 3; ++b) q.rb[a][b] = (kk[a] * ny + jj[b]) * nx;
+  q.xs[0] = x0 == 0 ? nx - 1 : x0 - 1;
+  q.xs[1] = x0;
+  q.xs[2] = x0 + 1;  // x0 even and nx even: x0 + 1 < nx
+  q.xs[3] = x0 + 2 >= nx ? x0 + 2 - nx : x0 + 2;
+  q.bxs[0] = (uint32_t)block_index(q.xs[0]);
+  q.bxs[1] = (uint32_t)block_index(x0);
+  q.bxs[2] = q.bxs[1] + 1u;  // x0 even: x0 + 1 lies in the same 32-cell block
+  q.bxs[3] = (uint32_t)block_index(q.xs[3]);
+}
+
+template <int M>
+__device__ __forceinline__ float cm(const float2& v) {
+  return M ? v.y : v.x;
+}
+template <int M>
+__device__ __forceinline__ void set_cm(float2& v, float a) {
+  if (M)
+    v.y = a;
+  else
+    v.x = a;
+}
+
+// post-streaming populations of member M of a pair when it is a fluid cell
+// next to a solid (per-cell path, written into component M of F)
+template <bool ODD, bool H, int M>
+__device__ __forceinline__ void near_solid_loads2(const Case& c, const PairNbh& q, int cell, uint32_t nb, float2* F) {
+  set_cm<M>(F[0], ldp<H>(c, 0, cell));
 #pragma unroll
   for (int s = 1; s < 19; ++s) {
-    if (!ODD)
-      F[s] = ldp<H>(c, s, cell);
-    else if ((nb >> kOpp(s)) & 1u)
-      F[s] = ldp<H>(c, s, cell);
+    float v;
+    if (!ODD || ((nb >> kOpp(s)) & 1u))
+      v = ldp<H>(c, s, cell);
     else
-      F[s] = ldp<H>(c, kOpp(s), n.at(-kEx(s), -kEy(s), -kEz(s)));
+      v = Pop<H>::ldb(c, kOpp(s), q.blk(c.aligned, M, -kEx(s), -kEy(s), -kEz(s)));
+    set_cm<M>(F[s], v);
+  }
+}
+
+// streaming of member M next to a solid: store_near_solid for component M of
+// the pair's post-collision populations
+template <bool ODD, bool H, bool MOVING, int M>
+__device__ __forceinline__ void near_solid_stores2(const Case& c, const PairNbh& q, int cell, uint32_t nb, float rho,
+                                                   const float2* F) {
+  float* hpp = c.s.hpp + (int64_t)c.c.pp * 3 * c.s.pitch;
+  const int64_t P = c.s.pitch;
+#pragma unroll
+  for (int s = 0; s < 19; ++s) {
+    float val = cm<M>(F[s]);
+    const bool bb = (nb >> s) & 1u;
+    if (MOVING && bb) {
+      const int ip = q.cell(M, kEx(s), kEy(s), kEz(s));
+      const float ew = (float)kEx(s) * c.s.svel[ip] + (float)kEy(s) * c.s.svel[P + ip] + (float)kEz(s) * c.s.svel[2 * P + ip];
+      const float corr = -6.0f * lattice_w(s) * rho * ew;
+      const float f0 = val;
+      val = f0 + corr;
+      const float tot = val + f0;  // solid force = e_s (bounced + f)
+      if (kEx(s)) atomicAdd(hpp + ip, (float)kEx(s) * tot);
+      if (kEy(s)) atomicAdd(hpp + P + ip, (float)kEy(s) * tot);
+      if (kEz(s)) atomicAdd(hpp + 2 * P + ip, (float)kEz(s) * tot);
+    }
+    if (!ODD || s == 0 || bb)
+      stp<H>(c, kOpp(s), cell, val);
+    else
+      Pop<H>::stb(c, s, q.blk(c.aligned, M, kEx(s), kEy(s), kEz(s)), val);
+  }
+}
+
+// dirstats_warp for member M of every lane's pair
+template <int M>
+__device__ __forceinline__ void dirstats_warp2(const Case& c, const PairNbh& q, uint32_t nb, float rho, const float2* F,
+                                               DirAcc& acc) {
+  if (!__any_sync(kFull, nb != 0u)) return;
+  const int64_t P = c.s.pitch;
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int s = 1; s < 19; ++s) {
+    const bool link = (nb >> s) & 1u;
+    const unsigned m = __ballot_sync(kFull, link);
+    if (m == 0u) continue;
+    float ac = 0.f, tot = 0.f;
+    if (link) {
+      const int ip = q.cell(M, kEx(s), kEy(s), kEz(s));
+      const float ew = (float)kEx(s) * c.s.svel[ip] + (float)kEy(s) * c.s.svel[P + ip] + (float)kEz(s) * c.s.svel[2 * P + ip];
+      const float corr = -6.0f * lattice_w(s) * rho * ew;
+      const float f0 = cm<M>(F[s]);
+      tot = (f0 + corr) + f0;
+      ac = fabsf(corr);
+    }
+    const float sum = warp_sum(ac), mx = warp_max(ac), ts = warp_sum(tot);
+    if (lane == 0) {
+      atomicAdd(&acc.cnt[s], __popc(m));
+      atomicAdd(&acc.csum[s], sum);
+      atomic_max_nonneg(&acc.cmax[s], mx);
+      if (kEx(s)) atomicAdd(&acc.imp[s][0], -(float)kEx(s) * ts);
+      if (kEy(s)) atomicAdd(&acc.imp[s][1], -(float)kEy(s) * ts);
+      if (kEz(s)) atomicAdd(&acc.imp[s][2], -(float)kEz(s) * ts);
+      acc.any = 1;
+    }
   }
 }
 
@@ -1106,7 +1237,7 @@ __device__ __forceinline__ void lbm_step_tile2(const Case& c, int bx, int by, Di
   const bool inrow = row < ny * nz;
   const bool valid = inrow && x0 < nx;  // nx even: x0 + 1 < nx as well
   const int j = inrow ? row % ny : 0, k = inrow ? row / ny : 0;
-  const int cell0 = row * nx + x0;
+  const int cell0 = valid ? row * nx + x0 : 0;
   const int64_t P = c.s.pitch;
   const bool dirstats = MOVING && (c.c.mode & FSI_MODE_DIRSTATS);
   if (dirstats) {
@@ -1132,16 +1263,12 @@ __device__ __forceinline__ void lbm_step_tile2(const Case& c, int bx, int by, Di
   const uint32_t nb0 = (fluid0 && (fl[0] & kNear)) ? c.s.nbr[cell0] : 0u;
   const uint32_t nb1 = (fluid1 && (fl[1] & kNear)) ? c.s.nbr[cell0 + 1] : 0u;
   const bool plain = (nb0 | nb1) == 0u;
-  Nbh n0, n1;
-  if (ODD || !plain) {
-    make_nbh(c, valid ? x0 : 0, j, k, n0);
-    n1 = n0;
-    n1.x = valid ? x0 + 1 : 0;
-    n1.xm = valid ? x0 : 0;
-    n1.xp = (valid && x0 + 2 < nx) ? x0 + 2 : 0;
-  }
+  PairNbh q;
+  if (ODD || !plain) make_pair_nbh(c, valid ? x0 : 0, j, k, q);
 
-  // ---- post-streaming populations (AA layout, fluid.py:431-440)
+  // ---- post-streaming populations (AA layout, fluid.py:431-440): a pair
+  // moves as one float2 / half2 where the layout keeps it adjacent (every
+  // direction on even steps, directions without an x component on odd steps)
   float2 F[19];
   if (fluid0 || fluid1) {
     if (plain) {
@@ -1150,24 +1277,22 @@ __device__ __forceinline__ void lbm_step_tile2(const Case& c, int bx, int by, Di
         for (int s = 0; s < 19; ++s) F[s] = Pop2<H>::ld(c, s, cell0);
       } else {
         F[0] = Pop2<H>::ld(c, 0, cell0);
+        const bool al = c.aligned;
 #pragma unroll
         for (int s = 1; s < 19; ++s) {
           if (kEx(s) == 0) {
-            F[s] = Pop2<H>::ld(c, kOpp(s), n0.at(0, -kEy(s), -kEz(s)));
+            F[s] = Pop2<H>::ldb(c, kOpp(s), q.blk(al, 0, 0, -kEy(s), -kEz(s)));
           } else {
-            F[s].x = ldp<H>(c, kOpp(s), n0.at(-kEx(s), -kEy(s), -kEz(s)));
-            F[s].y = ldp<H>(c, kOpp(s), n1.at(-kEx(s), -kEy(s), -kEz(s)));
+            F[s].x = Pop<H>::ldb(c, kOpp(s), q.blk(al, 0, -kEx(s), -kEy(s), -kEz(s)));
+            F[s].y = Pop<H>::ldb(c, kOpp(s), q.blk(al, 1, -kEx(s), -kEy(s), -kEz(s)));
           }
         }
       }
     } else {
-      float a[19], b[19];
 #pragma unroll
-      for (int s = 0; s < 19; ++s) a[s] = b[s] = 0.f;
-      if (fluid0) set_near_solid_loads<ODD, H>(c, n0, cell0, nb0, a);
-      if (fluid1) set_near_solid_loads<ODD, H>(c, n1, cell0 + 1, nb1, b);
-#pragma unroll
-      for (int s = 0; s < 19; ++s) F[s] = make_float2(a[s], b[s]);
+      for (int s = 0; s < 19; ++s) F[s] = make_float2(0.f, 0.f);
+      if (fluid0) near_solid_loads2<ODD, H, 0>(c, q, cell0, nb0, F);
+      if (fluid1) near_solid_loads2<ODD, H, 1>(c, q, cell0 + 1, nb1, F);
     }
   } else {
 #pragma unroll
@@ -1182,13 +1307,15 @@ __device__ __forceinline__ void lbm_step_tile2(const Case& c, int bx, int by, Di
 
   // ---- macroscopic state the collision uses (streaming3, fluid.py:1794-1814)
   float2 cf0 = p2(0.f), cf1 = p2(0.f), cf2 = p2(0.f);
-#pragma unroll
-  for (int i = 0; i < 2; ++i) {
-    if ((i ? fluid1 : fluid0) && (fl[i] & kCF)) {
-      set_comp(cf0, i, c.s.cell_force[cell0 + i]);
-      set_comp(cf1, i, c.s.cell_force[P + cell0 + i]);
-      set_comp(cf2, i, c.s.cell_force[2 * P + cell0 + i]);
-    }
+  if (fluid0 && (fl[0] & kCF)) {
+    cf0.x = c.s.cell_force[cell0];
+    cf1.x = c.s.cell_force[P + cell0];
+    cf2.x = c.s.cell_force[2 * P + cell0];
+  }
+  if (fluid1 && (fl[1] & kCF)) {
+    cf0.y = c.s.cell_force[cell0 + 1];
+    cf1.y = c.s.cell_force[P + cell0 + 1];
+    cf2.y = c.s.cell_force[2 * P + cell0 + 1];
   }
   float2 rho, ux, uy, uz;
   {
@@ -1199,20 +1326,24 @@ __device__ __forceinline__ void lbm_step_tile2(const Case& c, int bx, int by, Di
     uy = mul2(fma2(p2(0.5f), add2(p2(c.p.force[1]), cf1), jy), inv);
     uz = mul2(fma2(p2(0.5f), add2(p2(c.p.force[2]), cf2), jz), inv);
   }
+  if (valid && ((fl[0] | fl[1]) & kOverride)) {
 #pragma unroll
-  for (int i = 0; i < 2; ++i) {
-    const bool fi = i ? fluid1 : fluid0;
-    if (valid && (fl[i] & kOverride)) {
-      set_comp(rho, i, c.s.rho[cell0 + i]);
-      set_comp(ux, i, c.s.vel[cell0 + i]);
-      set_comp(uy, i, c.s.vel[P + cell0 + i]);
-      set_comp(uz, i, c.s.vel[2 * P + cell0 + i]);
-    } else if (!fi) {
-      set_comp(rho, i, c.p.rho0);
-      set_comp(ux, i, 0.f);
-      set_comp(uy, i, 0.f);
-      set_comp(uz, i, 0.f);
+    for (int i = 0; i < 2; ++i) {
+      if (fl[i] & kOverride) {
+        set_comp(rho, i, c.s.rho[cell0 + i]);
+        set_comp(ux, i, c.s.vel[cell0 + i]);
+        set_comp(uy, i, c.s.vel[P + cell0 + i]);
+        set_comp(uz, i, c.s.vel[2 * P + cell0 + i]);
+      }
     }
+  }
+  if (!fluid0 && !(valid && (fl[0] & kOverride))) {
+    rho.x = c.p.rho0;
+    ux.x = uy.x = uz.x = 0.f;
+  }
+  if (!fluid1 && !(valid && (fl[1] & kOverride))) {
+    rho.y = c.p.rho0;
+    ux.y = uy.y = uz.y = 0.f;
   }
   if (BCW) {
     __syncwarp();
@@ -1313,6 +1444,7 @@ __device__ __forceinline__ void lbm_step_tile2(const Case& c, int bx, int by, Di
           }
         }
       } else {
+        const bool al = c.aligned;
         if (both) {
           Pop2<H>::st(c, 0, cell0, F[0]);
         } else {
@@ -1322,32 +1454,36 @@ __device__ __forceinline__ void lbm_step_tile2(const Case& c, int bx, int by, Di
 #pragma unroll
         for (int s = 1; s < 19; ++s) {
           if (both && kEx(s) == 0) {
-            Pop2<H>::st(c, s, n0.at(0, kEy(s), kEz(s)), F[s]);
+            Pop2<H>::stb(c, s, q.blk(al, 0, 0, kEy(s), kEz(s)), F[s]);
           } else {
-            if (fluid0) stp<H>(c, s, n0.at(kEx(s), kEy(s), kEz(s)), F[s].x);
-            if (fluid1) stp<H>(c, s, n1.at(kEx(s), kEy(s), kEz(s)), F[s].y);
+            if (fluid0) Pop<H>::stb(c, s, q.blk(al, 0, kEx(s), kEy(s), kEz(s)), F[s].x);
+            if (fluid1) Pop<H>::stb(c, s, q.blk(al, 1, kEx(s), kEy(s), kEz(s)), F[s].y);
           }
         }
       }
     } else {
+      if (fluid0) {
+        if (nb0)
+          near_solid_stores2<ODD, H, MOVING, 0>(c, q, cell0, nb0, rho.x, F);
+        else if (!ODD) {
 #pragma unroll
-      for (int i = 0; i < 2; ++i) {
-        if (!(i ? fluid1 : fluid0)) continue;
-        float out[19];
-#pragma unroll
-        for (int s = 0; s < 19; ++s) out[s] = comp(F[s], i);
-        const uint32_t nb = i ? nb1 : nb0;
-        const Nbh& n = i ? n1 : n0;
-        const int cell = cell0 + i;
-        if (nb) {
-          store_near_solid<ODD, H, MOVING>(c, n, cell, nb, comp(rho, i), out);
-        } else if (!ODD) {
-#pragma unroll
-          for (int s = 0; s < 19; ++s) stp<H>(c, kOpp(s), cell, out[s]);
+          for (int s = 0; s < 19; ++s) stp<H>(c, kOpp(s), cell0, F[s].x);
         } else {
-          stp<H>(c, 0, cell, out[0]);
+          stp<H>(c, 0, cell0, F[0].x);
 #pragma unroll
-          for (int s = 1; s < 19; ++s) stp<H>(c, s, n.at(kEx(s), kEy(s), kEz(s)), out[s]);
+          for (int s = 1; s < 19; ++s) Pop<H>::stb(c, s, q.blk(c.aligned, 0, kEx(s), kEy(s), kEz(s)), F[s].x);
+        }
+      }
+      if (fluid1) {
+        if (nb1)
+          near_solid_stores2<ODD, H, MOVING, 1>(c, q, cell0 + 1, nb1, rho.y, F);
+        else if (!ODD) {
+#pragma unroll
+          for (int s = 0; s < 19; ++s) stp<H>(c, kOpp(s), cell0 + 1, F[s].y);
+        } else {
+          stp<H>(c, 0, cell0 + 1, F[0].y);
+#pragma unroll
+          for (int s = 1; s < 19; ++s) Pop<H>::stb(c, s, q.blk(c.aligned, 1, kEx(s), kEy(s), kEz(s)), F[s].y);
         }
       }
     }
@@ -1376,14 +1512,8 @@ __device__ __forceinline__ void lbm_step_tile2(const Case& c, int bx, int by, Di
   }
 
   if (dirstats) {
-    float o0[19], o1[19];
-#pragma unroll
-    for (int s = 0; s < 19; ++s) {
-      o0[s] = F[s].x;
-      o1[s] = F[s].y;
-    }
-    dirstats_warp(c, n0, fluid0 ? nb0 : 0u, rho.x, o0, acc);
-    dirstats_warp(c, n1, fluid1 ? nb1 : 0u, rho.y, o1, acc);
+    dirstats_warp2<0>(c, q, fluid0 ? nb0 : 0u, rho.x, F, acc);
+    dirstats_warp2<1>(c, q, fluid1 ? nb1 : 0u, rho.y, F, acc);
     __syncthreads();
     if (acc.any) {
       const int tid = threadIdx.y * 32 + lane;
@@ -1402,7 +1532,7 @@ __device__ __forceinline__ void lbm_step_tile2(const Case& c, int bx, int by, Di
 }
 
 template <bool ODD, bool H, bool MOVING, bool BCW, bool PEN>
-__global__ void __launch_bounds__(128, 3) k_lbm_step2(const __grid_constant__ Case c) {
+__global__ void __launch_bounds__(128, 4) k_lbm_step2(const __grid_constant__ Case c) {
   __shared__ DirAcc acc;
   griddep_wait();
   griddep_launch();
