@@ -450,8 +450,8 @@ int fsi_mpm_g2p(const FsiParticles* pt, const FsiGrid* g, const FsiMpmParams* mp
  * driven by fsi_driver.py's MPM loops), organised around particle bins:
  *   - fsi_mpm_bin sorts particle ids by FSI_BIN_EDGE^3-cell block of their
  *     B-spline base cell, and within a block by base cell, and cuts every bin
- *     into chunks of at most FSI_BIN_CHUNK particles (bins may go stale
- *     between calls: that costs speed only);
+ *     into ceil(count / FSI_BIN_CHUNK) chunks of equal size (sizes differ by
+ *     at most one; bins may go stale between calls: that costs speed only);
  *   - fsi_mpm_substeps_binned runs substeps chunk by chunk: each chunk is
  *     scattered into a shared-memory tile covering its stencil box and the
  *     tile is flushed with one atomic per touched node value; the gather

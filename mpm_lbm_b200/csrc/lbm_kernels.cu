@@ -665,10 +665,6 @@ __device__ __forceinline__ void store_near_solid(const Case& c, const Nbh& n, in
   }
 }
 
-// One tile of the fused step: the 32 x 8 cells (x, row = k * ny + j) of tile
-// (bx, by).  Called by the single-case kernel (c in the parameter bank) and by
-// the batched kernel (c staged in shared memory); acc: the CTA's shared
-// per-direction accumulator.
 // Per-direction bounce-back reductions of one step (fluid.py:488-536: link
 // counts, |correction| sum and max, fluid impulse), called by every lane of
 // the warp together after the streaming stores: per direction the warp's link
@@ -710,38 +706,38 @@ __device__ __forceinline__ void dirstats_warp(const Case& c, const Nbh& n, uint3
   }
 }
 
-template <bool ODD, bool H, bool MOVING, bool BCW, bool PEN>
-__device__ __forceinline__ void lbm_step_tile(const Case& c, int bx, int by, int bz, DirAcc& acc) {
-  const int lane = threadIdx.x;
-  const int nx = c.s.nx, ny = c.s.ny, nz = c.s.nz;
-  const int x = bx * 32 + lane;
-  const int jr = by * 8 + threadIdx.y;
+// One cell of the fused step, read before its collision: position, flags,
+// solid-neighbour mask and post-streaming populations.  The step of a cell is
+// step_cell_load followed by step_cell_finish, so that a thread can issue the
+// loads of several cells before it collides the first.
+struct StepCell {
+  int x, jr, k;
+  uint8_t fl;
+  uint32_t nb;
+  float F[19];
+};
+
+template <bool ODD, bool H>
+__device__ __forceinline__ void step_cell_load(const Case& c, int x, int jr, int bz, StepCell& q) {
+  const int nx = c.s.nx, ny = c.s.ny;
   const bool inrow = jr < ny;
   const bool valid = inrow && x < nx;
   const int j = inrow ? jr : 0, k = bz;
   const int row = k * ny + j;
   const int cell = row * nx + x;
-  const bool dirstats = MOVING && (c.c.mode & FSI_MODE_DIRSTATS);
-  if (dirstats) {
-    const int tid = threadIdx.y * 32 + lane;
-    for (int i = tid; i < 19; i += 256) {
-      acc.cnt[i] = 0;
-      acc.csum[i] = 0.f;
-      acc.cmax[i] = 0.f;
-      acc.imp[i][0] = acc.imp[i][1] = acc.imp[i][2] = 0.f;
-    }
-    if (tid == 0) acc.any = 0;
-    __syncthreads();
-  }
-
+  q.x = x;
+  q.jr = jr;
+  q.k = bz;
   const uint8_t fl = valid ? c.s.flags[cell] : kSolid;
   const bool fluid = !(fl & kSolid);
   const uint32_t nb = (fluid && (fl & kNear)) ? c.s.nbr[cell] : 0u;
+  q.fl = fl;
+  q.nb = nb;
   Nbh n;
   if (ODD || nb) make_nbh(c, x < nx ? x : 0, j, k, n);
+  float* const F = q.F;
 
   // ---- post-streaming populations of this cell (AA layout, fluid.py:431-440)
-  float F[19];
   if (fluid) {
     if (!ODD) {
 #pragma unroll
@@ -767,6 +763,30 @@ __device__ __forceinline__ void lbm_step_tile(const Case& c, int bx, int by, int
 #pragma unroll
     for (int s = 0; s < 19; ++s) F[s] = 0.f;
   }
+
+}
+
+// The rest of the step of one cell (everything after its loads) for the warp's
+// 32 cells x = 32 bx + lane of one row; ends with the cell's part of the
+// per-direction link statistics (the caller synchronises the CTA and flushes
+// them).
+template <bool ODD, bool H, bool MOVING, bool BCW, bool PEN>
+__device__ __forceinline__ void step_cell_finish(const Case& c, int bx, StepCell& q, DirAcc& acc) {
+  const int lane = threadIdx.x;
+  const int nx = c.s.nx, ny = c.s.ny, nz = c.s.nz;
+  const int x = q.x;
+  const bool inrow = q.jr < ny;
+  const bool valid = inrow && x < nx;
+  const int j = inrow ? q.jr : 0, k = q.k;
+  const int row = k * ny + j;
+  const int cell = row * nx + x;
+  const bool dirstats = MOVING && (c.c.mode & FSI_MODE_DIRSTATS);
+  const uint8_t fl = q.fl;
+  const bool fluid = !(fl & kSolid);
+  const uint32_t nb = q.nb;
+  Nbh n;
+  if (ODD || nb) make_nbh(c, x < nx ? x : 0, j, k, n);
+  float* const F = q.F;
 
   // ---- pending open boundary of the previous step (fluid.py:538-569)
   if (BCW && c.c.bc_pending && inrow) {
@@ -908,23 +928,52 @@ __device__ __forceinline__ void lbm_step_tile(const Case& c, int bx, int by, int
     }
   }
 
-  if (dirstats) {
-    dirstats_warp(c, n, fluid ? nb : 0u, rho, F, acc);
-    __syncthreads();
-    if (acc.any) {
-      const int tid = threadIdx.y * 32 + lane;
-      for (int i = tid; i < 19; i += 256) {
-        if (acc.cnt[i]) {
-          atomicAdd(&c.s.diag->link_count[i], acc.cnt[i]);
-          atomicAdd(&c.s.diag->corr_abs_sum[i], acc.csum[i]);
-          atomic_max_nonneg(&c.s.diag->corr_abs_max[i], acc.cmax[i]);
-          atomicAdd(&c.s.diag->fluid_impulse[i][0], acc.imp[i][0]);
-          atomicAdd(&c.s.diag->fluid_impulse[i][1], acc.imp[i][1]);
-          atomicAdd(&c.s.diag->fluid_impulse[i][2], acc.imp[i][2]);
-        }
+  if (dirstats) dirstats_warp(c, n, fluid ? nb : 0u, rho, F, acc);
+}
+
+// the CTA's per-direction link statistics of one step: zeroed before the
+// tile's cells, flushed to FsiLbmDiag after them (one atomic per direction)
+__device__ __forceinline__ void dirstats_begin(DirAcc& acc, int nthreads) {
+  const int tid = threadIdx.y * 32 + threadIdx.x;
+  for (int i = tid; i < 19; i += nthreads) {
+    acc.cnt[i] = 0;
+    acc.csum[i] = 0.f;
+    acc.cmax[i] = 0.f;
+    acc.imp[i][0] = acc.imp[i][1] = acc.imp[i][2] = 0.f;
+  }
+  if (tid == 0) acc.any = 0;
+  __syncthreads();
+}
+
+__device__ __forceinline__ void dirstats_end(const Case& c, DirAcc& acc, int nthreads) {
+  __syncthreads();
+  if (acc.any) {
+    const int tid = threadIdx.y * 32 + threadIdx.x;
+    for (int i = tid; i < 19; i += nthreads) {
+      if (acc.cnt[i]) {
+        atomicAdd(&c.s.diag->link_count[i], acc.cnt[i]);
+        atomicAdd(&c.s.diag->corr_abs_sum[i], acc.csum[i]);
+        atomic_max_nonneg(&c.s.diag->corr_abs_max[i], acc.cmax[i]);
+        atomicAdd(&c.s.diag->fluid_impulse[i][0], acc.imp[i][0]);
+        atomicAdd(&c.s.diag->fluid_impulse[i][1], acc.imp[i][1]);
+        atomicAdd(&c.s.diag->fluid_impulse[i][2], acc.imp[i][2]);
       }
     }
   }
+}
+
+// One tile of the fused step: the 32 x 8 cells (x, row = k * ny + j) of tile
+// (bx, by).  Called by the single-case kernel (c in the parameter bank) and by
+// the batched kernel (c staged in shared memory); acc: the CTA's shared
+// per-direction accumulator.
+template <bool ODD, bool H, bool MOVING, bool BCW, bool PEN>
+__device__ __forceinline__ void lbm_step_tile(const Case& c, int bx, int by, int bz, DirAcc& acc) {
+  const bool dirstats = MOVING && (c.c.mode & FSI_MODE_DIRSTATS);
+  if (dirstats) dirstats_begin(acc, 256);
+  StepCell q;
+  step_cell_load<ODD, H>(c, bx * 32 + (int)threadIdx.x, by * 8 + (int)threadIdx.y, bz, q);
+  step_cell_finish<ODD, H, MOVING, BCW, PEN>(c, bx, q, acc);
+  if (dirstats) dirstats_end(c, acc, 256);
 }
 
 // L2 prefetch of the populations of tile (bx, by, bz) of a 32 x 8 x 1 tiling:

@@ -67,6 +67,10 @@ __global__ void k_bin_count(FsiParticles pt, float inv_dx, int G, int nb, int32_
 // chunk table, and the counts reset to zero for the next binning.  Each
 // thread owns a contiguous, 4-aligned range of bins and reads it with 16-byte
 // loads, so the pass costs a few memory latencies rather than one per bin.
+//
+// Chunks: a bin of c particles is cut into ceil(c / kChunk) chunks of equal
+// size (sizes differ by at most one), so that no chunk of a few particles
+// follows a full one.
 __device__ __forceinline__ int4 ld_bins4(const int32_t* p, int b, int b1) {
   if (b + 4 <= b1) return *reinterpret_cast<const int4*>(p + b);
   int4 v = make_int4(0, 0, 0, 0);
@@ -75,6 +79,8 @@ __device__ __forceinline__ int4 ld_bins4(const int32_t* p, int b, int b1) {
   if (b + 2 < b1) v.z = p[b + 2];
   return v;
 }
+
+__device__ __forceinline__ int chunks_of(int c) { return (c + kChunk - 1) / kChunk; }
 
 __device__ __forceinline__ void bin_scan_body(int nbins, int32_t* __restrict__ count, int32_t* __restrict__ start,
                                               int2* __restrict__ chunk, int32_t* __restrict__ meta) {
@@ -86,8 +92,7 @@ __device__ __forceinline__ void bin_scan_body(int nbins, int32_t* __restrict__ c
   for (int b = b0; b < b1; b += 4) {
     const int4 c = ld_bins4(count, b, b1);
     ps += c.x + c.y + c.z + c.w;
-    cs += (c.x + kChunk - 1) / kChunk + (c.y + kChunk - 1) / kChunk + (c.z + kChunk - 1) / kChunk +
-          (c.w + kChunk - 1) / kChunk;
+    cs += chunks_of(c.x) + chunks_of(c.y) + chunks_of(c.z) + chunks_of(c.w);
   }
   int pi = ps, ci = cs;
 #pragma unroll
@@ -129,7 +134,16 @@ __device__ __forceinline__ void bin_scan_body(int nbins, int32_t* __restrict__ c
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       st[q] = po;
-      for (int j = 0; j < cv[q]; j += kChunk) chunk[co++] = make_int2(po + j, min(kChunk, cv[q] - j));
+      const int nc = chunks_of(cv[q]);
+      if (nc > 0) {
+        const int sz = cv[q] / nc, rem = cv[q] - sz * nc;  // rem chunks of sz + 1, then sz
+        int off = po;
+        for (int i = 0; i < nc; ++i) {
+          const int n = sz + (i < rem ? 1 : 0);
+          chunk[co++] = make_int2(off, n);
+          off += n;
+        }
+      }
       po += cv[q];
     }
     if (b + 4 <= b1) {

@@ -85,11 +85,30 @@ def compare_grid(gpu, ora, rel=2e-5):
     _close(gpu.grid_f_ext.to_numpy(), ora.grid_f_ext, rel, "grid_f_ext")
 
 
-def expected_bins(x, n_grid, edge=8, chunk=None):
-    """Bin keys, counts and chunk table restated on the CPU in FP32."""
+def expected_chunks(counts, start):
+    """Chunk table of fsi_mpm_bin: each bin of c particles cut into
+    ceil(c / FSI_BIN_CHUNK) chunks of equal size (the first c % n one
+    larger)."""
     from mpm_lbm_b200._lib import FSI_BIN_CHUNK
 
-    chunk = FSI_BIN_CHUNK if chunk is None else chunk
+    cap = FSI_BIN_CHUNK
+    chunks = []
+    for s, k in zip(start, counts):
+        k = int(k)
+        if k == 0:
+            continue
+        n = (k + cap - 1) // cap
+        sz, rem = divmod(k, n)
+        off = int(s)
+        for i in range(n):
+            m = sz + (1 if i < rem else 0)
+            chunks.append((off, m))
+            off += m
+    return np.array(chunks, np.int32).reshape(-1, 2)
+
+
+def expected_bins(x, n_grid, edge=8):
+    """Bin keys, counts and chunk table restated on the CPU in FP32."""
     inv_dx = np.float32(n_grid)
     xp = (x.astype(np.float32) * inv_dx).astype(np.float32)
     base = (xp - np.float32(0.5)).astype(np.int32)  # truncation toward zero
@@ -98,8 +117,7 @@ def expected_bins(x, n_grid, edge=8, chunk=None):
     key = (c[:, 2] * nb + c[:, 1]) * nb + c[:, 0]
     counts = np.bincount(key, minlength=nb ** 3)
     start = np.concatenate([[0], np.cumsum(counts)[:-1]])
-    chunks = [(s + j, min(chunk, k - j)) for s, k in zip(start, counts) for j in range(0, k, chunk)]
-    return key.astype(np.int32), counts, start, np.array(chunks, np.int32).reshape(-1, 2)
+    return key.astype(np.int32), counts, start, expected_chunks(counts, start)
 
 
 @pytest.mark.parametrize("case", ["block", "edges"])
