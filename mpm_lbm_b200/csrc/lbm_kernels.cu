@@ -493,29 +493,34 @@ __device__ __forceinline__ void bc_face_warp(const Case& c, int lane, int row, u
   if ((solid_bits >> lf) & 1u) return;
   const bool n1_solid = (solid_bits >> l1) & 1u;
   const bool n2_fluid = n1_solid ? true : !((solid_bits >> l2) & 1u);
-  const int src1 = n1_solid ? lf : l1, src2 = n1_solid ? lf : l2;
-  float Fn = 0.f, Fn2 = 0.f;
-#pragma unroll
-  for (int q = 0; q < 5; ++q) {
-    const int s = SIDE == 0 ? kUnknownL(q) : kUnknownR(q);
-    const float a = __shfl_sync(kFull, F[s], src1);
-    const float b = __shfl_sync(kFull, F[s], src2);
-    if (lane == q) {
-      Fn = a;
-      Fn2 = b;
-    }
-  }
-  float mac_n[4], mac_l[4];
-  load_plane(c, SIDE == 0 ? (n1_solid ? 0 : 1) : (n1_solid ? 3 : 2), row, mac_n);
-  load_plane(c, SIDE == 0 ? (n1_solid ? 1 : 0) : 2, row, mac_l);
-  const FaceVal r = face_population(c.p, c.s.vel_left_dyn, SIDE, lane, Fn, Fn2, n2_fluid, mac_n, mac_l, c.s.diag);
+  float mac_n[4], mac_l[4] = {0.f, 0.f, 0.f, 0.f};
+  // an equilibrium-reset velocity face (bc 2) reads no plane either
+  if (!(c.p.ob_semantics == FSI_OB_EQUILIBRIUM_RESET && (SIDE == 0 ? c.p.bc_left : c.p.bc_right) == 2))
+    load_plane(c, SIDE == 0 ? (n1_solid ? 1 : 0) : 2, row, mac_l);
   if (c.p.ob_semantics == FSI_OB_EQUILIBRIUM_RESET) {
+    // the equilibrium reset reads neither the neighbours' unknown
+    // populations nor the neighbour plane (face_population)
+    const FaceVal r = face_population(c.p, c.s.vel_left_dyn, SIDE, lane, 0.f, 0.f, n2_fluid, mac_l, mac_l, c.s.diag);
 #pragma unroll
     for (int s = 0; s < 19; ++s) {
       const float v = __shfl_sync(kFull, r.val, s);
       if (lane == lf) F[s] = v;
     }
   } else {
+    const int src1 = n1_solid ? lf : l1, src2 = n1_solid ? lf : l2;
+    float Fn = 0.f, Fn2 = 0.f;
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+      const int s = SIDE == 0 ? kUnknownL(q) : kUnknownR(q);
+      const float a = __shfl_sync(kFull, F[s], src1);
+      const float b = __shfl_sync(kFull, F[s], src2);
+      if (lane == q) {
+        Fn = a;
+        Fn2 = b;
+      }
+    }
+    load_plane(c, SIDE == 0 ? (n1_solid ? 0 : 1) : (n1_solid ? 3 : 2), row, mac_n);
+    const FaceVal r = face_population(c.p, c.s.vel_left_dyn, SIDE, lane, Fn, Fn2, n2_fluid, mac_n, mac_l, c.s.diag);
 #pragma unroll
     for (int q = 0; q < 5; ++q) {
       const float v = __shfl_sync(kFull, r.val, q);
@@ -818,7 +823,10 @@ __device__ __forceinline__ void step_cell_finish(const Case& c, int bx, StepCell
   }
   if (BCW) {
     __syncwarp();
-    const int plane = x == 0 ? 0 : (x == 1 ? 1 : (x == nx - 2 ? 2 : (x == nx - 1 ? 3 : -1)));
+    // planes x = 0, 1, nx - 2, nx - 1 lie in the first and last 32-cell tiles
+    // of a row (nx >= 4 with open faces), so other warps skip the test
+    const bool edge_tile = bx == 0 || bx >= ((nx - 2) >> 5);
+    const int plane = !edge_tile ? -1 : (x == 0 ? 0 : (x == 1 ? 1 : (x == nx - 2 ? 2 : (x == nx - 1 ? 3 : -1))));
     if (valid && plane >= 0) {
       float* pp = c.s.plane + (int64_t)plane * 4 * ny * nz;
       const int64_t m = (int64_t)ny * nz;
