@@ -236,6 +236,8 @@ def cpu_baseline(wl, steps=1):
 
 
 def dist_setup():
+    """One process per GPU under torchrun: NCCL over the node's GPUs, or gloo
+    for a host-only run (the reference arm on a machine without a GPU)."""
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -245,9 +247,26 @@ def dist_setup():
         import torch
         import torch.distributed as dist
 
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+            backend = "nccl"
+        else:
+            backend = "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
     return ws, rank, local
+
+
+def max_over_ranks(x, device=None):
+    """x maximised over the ranks of the default process group (x itself when
+    there is none): independent replicas are done when the slowest is."""
+    import torch
+    import torch.distributed as dist
+
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(x)
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
 
 
 def run_reference(args, wl, ws, rank):
@@ -457,6 +476,10 @@ def main():
     ws, rank, local = dist_setup()
     if args.impl == "reference":
         run_reference(args, wl, ws, rank)
+        if ws > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
         return
     import torch
 
@@ -499,11 +522,7 @@ def main():
         clk.close_region()
     step_ms = [a.elapsed_time(b) for a, b in evs]
     total_ms = float(sum(step_ms))
-    if ws > 1:
-        t = torch.tensor([total_ms], device=device)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
-        torch.distributed.barrier()
+    total_ms = max_over_ranks(total_ms, device)
     fluid_cells = int(lbm.fluid_mask().sum().item())
     value = ws * args.steps * wl.S * wl.cells / (total_ms * 1e-3) / 1e6
     ms_step = total_ms / args.steps
@@ -553,6 +572,8 @@ def main():
     pinned_out = torch.empty(3, n, dtype=torch.float32).pin_memory()
     torch.cuda.synchronize()
     e_steps = max(3, args.steps // 2)
+    if ws > 1:
+        torch.distributed.barrier()
     t0 = time.perf_counter()
     for k in range(e_steps):
         pinned_in[0] = wl.case.u_in
@@ -560,7 +581,7 @@ def main():
         drv.step_once()
         pinned_out.copy_(drv.solid.t_x, non_blocking=True)
         torch.cuda.current_stream().synchronize()
-    e2e_s = time.perf_counter() - t0
+    e2e_s = max_over_ranks(time.perf_counter() - t0, device)
     e2e_value = ws * e_steps * wl.S * wl.cells / e2e_s / 1e6
 
     result = {
